@@ -1,0 +1,265 @@
+/*
+ * gxy_seed.h -- C ABI of the B200 seed->HSP stage for lastz-gxy.
+ *
+ * The stage replaces, bit for bit, what the reference computes in
+ *   PosTable::build            src/pos_table.rs:35-83
+ *   PosTable::prune_hot_words  src/pos_table.rs:113-136
+ *   seed_search::search        src/seed_search.rs:271-351
+ *     (DiagHash src/diag_hash.rs:34-53, extend_hit src/hsp.rs:66-211,
+ *      extend_hit_avx2 src/hsp_simd.rs:27-243, entropy gate src/entropy.rs:27-67)
+ * and is called where the reference's driver calls them (src/driver.rs:212-240,
+ * src/tweener.rs:111-126).  Paths are relative to the nekrut/lastz-gxy root.
+ *
+ * Conventions: every entry point returns a gxy_status; on failure
+ * gxy_last_error() returns a message for the calling thread.  No torch or CUDA
+ * types appear in the signatures.  Sequences cross the boundary in the
+ * reference's PackedSeq layout (src/sequences.rs:53-66):
+ *   codes: 2-bit A=0 C=1 G=2 T=3, 4 per byte, position i at bits 2*(i&3) of byte i>>2
+ *   valid: bit i&7 of byte i>>3 set when position i is unambiguous ACGT
+ *   mask : bit i&7 of byte i>>3 set when position i was soft-masked (lowercase)
+ * Coordinates in returned HSPs are those of the sequences passed in (chunk-local
+ * target, strand-local query), exactly like the reference's Vec<Hsp>.
+ */
+#ifndef GXY_SEED_H
+#define GXY_SEED_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef enum {
+    GXY_OK = 0,
+    GXY_EINVAL = 1,         /* bad argument (reference: a panic or a parse error) */
+    GXY_ENOMEM = 2,         /* device or host allocation failed */
+    GXY_EUNSUPPORTED = 3,   /* outside the exact envelope (seed weight > 15, i32 overflow risk) */
+    GXY_ETIMEDOUT = 4,      /* a bounded device or host wait ran out */
+    GXY_ECUDA = 5,          /* CUDA runtime error */
+    GXY_ENOTREADY = 6,      /* serving: request not finished yet */
+    GXY_EOVERFLOW = 7       /* a caller-provided buffer is too small; *needed is set */
+} gxy_status;
+
+typedef struct gxy_ctx gxy_ctx;       /* one device, its streams and memory pool */
+typedef struct gxy_table gxy_table;   /* device-resident PosTable */
+typedef struct gxy_dseq gxy_dseq;     /* device-resident PackedSeq */
+typedef struct gxy_server gxy_server; /* serving loop */
+
+/* Host view of a PackedSeq (src/sequences.rs:61-66). */
+typedef struct {
+    const uint8_t* codes;
+    const uint8_t* valid;
+    const uint8_t* mask;
+    uint64_t len;
+} gxy_packed_seq;
+
+/* SearchParams{step, hsp: HspParams{x_drop, hsp_threshold}, transitions,
+ * entropy_threshold} (src/seed_search.rs:19-30, src/hsp.rs:46-49) plus the
+ * ScoringMatrix fields the path reads (src/scoring.rs:32-40):
+ * sub[r*4+q] = score of target code r against query code q; ambig = score of
+ * a column where either base is not ACGT. */
+typedef struct {
+    int32_t sub[16];
+    int32_t ambig;
+    int32_t xdrop;
+    int32_t hspthresh;
+    uint32_t step;
+    uint8_t transitions;   /* 0, 1, >=2 (treated as 2), src/seed_search.rs:295-316 */
+    uint8_t has_entropy;   /* entropy_threshold.is_some() */
+    uint8_t pad_[2];
+    int32_t entropy_thr;
+} gxy_search_params;
+
+/* Hsp (src/hsp.rs:19-24), #[repr(C)]-compatible, 16 bytes. */
+typedef struct {
+    uint32_t t_start;
+    uint32_t q_start;
+    uint32_t length;
+    int32_t score;
+} gxy_hsp;
+
+/* Output of a search.  If hsps == NULL on entry the library allocates it
+ * (free with gxy_hsp_buf_free).  Otherwise it is a caller buffer of cap
+ * entries; when too small the call returns GXY_EOVERFLOW and len holds the
+ * number needed.  HSPs come back in canonical order: by diagonal
+ * (t_start - q_start), then t_start, length, score -- the reference sorts by
+ * (diagonal, t_start) and dedups (src/seed_search.rs:348-349). */
+typedef struct {
+    gxy_hsp* hsps;
+    uint64_t len;
+    uint64_t cap;
+} gxy_hsp_buf;
+
+/* Counters of one search or batch. */
+typedef struct {
+    uint64_t windows;      /* seedable query windows */
+    uint64_t raw_hits;     /* table entries visited over all variants */
+    uint64_t candidates;   /* hits that pass or run past the screen's column cap */
+    uint64_t hsps;         /* HSPs returned */
+    double device_ms;      /* CUDA-event time of the call's device work */
+    double screen_ms;      /* CUDA-event time of the screen kernel alone */
+} gxy_stats;
+
+const char* gxy_status_string(gxy_status s);
+const char* gxy_last_error(void);
+uint32_t gxy_abi_version(void);
+
+/* ---- context ------------------------------------------------------------ */
+gxy_status gxy_ctx_create(int device, gxy_ctx** out);
+gxy_status gxy_ctx_destroy(gxy_ctx* ctx);
+/* Tunables (screen kernel warps per block, column cap per side, queue depth,
+ * walk block size).  Zero leaves a field unchanged. */
+typedef struct {
+    uint32_t screen_warps;
+    uint32_t screen_cap;
+    uint32_t screen_blocks_per_sm;
+    uint32_t walk_warps;
+} gxy_tuning;
+gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
+gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
+
+/* ---- device-resident sequences ------------------------------------------- */
+/* Copies a host PackedSeq to the device. */
+gxy_status gxy_dseq_upload(gxy_ctx* ctx, const gxy_packed_seq* host, gxy_dseq** out);
+/* Packs ASCII bases on the device: PackedSeq::from_ascii / push_ascii with
+ * encode_base (src/sequences.rs:89-131, src/dna.rs:12-20). */
+gxy_status gxy_dseq_from_ascii(gxy_ctx* ctx, const uint8_t* ascii, uint64_t n, gxy_dseq** out);
+/* PackedSeq::reverse_complement on the device (src/sequences.rs:303-318). */
+gxy_status gxy_dseq_reverse_complement(gxy_ctx* ctx, const gxy_dseq* in, gxy_dseq** out);
+/* Copies a device sequence back into host buffers of ceil(len/4), ceil(len/8),
+ * ceil(len/8) bytes; any pointer may be NULL. */
+gxy_status gxy_dseq_download(const gxy_dseq* s, uint8_t* codes, uint8_t* valid, uint8_t* mask);
+uint64_t gxy_dseq_len(const gxy_dseq* s);
+gxy_status gxy_dseq_free(gxy_dseq* s);
+
+/* ---- position table (src/pos_table.rs) --------------------------------- */
+/* PosTable::build(seq, pattern, step) followed, when max_word_count > 0, by
+ * prune_hot_words(max_word_count) as the driver does (src/driver.rs:212-215).
+ * pattern01 is the 0/1 seed pattern (src/seeds.rs:113-126), at most 32
+ * positions; weight <= 15 (2^30 buckets) is supported. */
+gxy_status gxy_table_build(gxy_ctx* ctx, const gxy_packed_seq* target, const char* pattern01,
+                           uint32_t step, uint32_t max_word_count, gxy_table** out);
+/* Same over a device sequence, restricted to the view [lo, hi) -- the
+ * driver's per-chunk table over chunk.seq (src/driver.rs:178, :212); the
+ * table's positions are view-local like the reference's chunk copy. */
+gxy_status gxy_table_build_view(gxy_ctx* ctx, const gxy_dseq* target, uint64_t lo, uint64_t hi,
+                                const char* pattern01, uint32_t step, uint32_t max_word_count,
+                                gxy_table** out);
+/* PosTable::prune_hot_words(limit) (src/pos_table.rs:113-136) on a built
+ * table: drops every bucket with more than limit positions. */
+gxy_status gxy_table_prune_hot_words(gxy_table* t, uint32_t limit);
+gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_positions,
+                          uint32_t* pattern_len, uint32_t* weight);
+/* Copies starts (num_words + 1 entries) and positions to host buffers; either
+ * may be NULL. */
+gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions);
+gxy_status gxy_table_free(gxy_table* t);
+
+/* ---- the drop-in search (src/seed_search.rs:271-351) --------------------- */
+/* seed_search::search(&table, &target, &query, &matrix, &params).  The
+ * target must be the sequence the table was built from (the reference's
+ * driver and tweener always pass the same one); it is re-read from host only
+ * when its pointers or length differ from the build's.  Thread-safe: calls
+ * from several host threads on one table run on separate streams. */
+gxy_status gxy_search(gxy_ctx* ctx, const gxy_table* table, const gxy_packed_seq* target,
+                      const gxy_packed_seq* query, const gxy_search_params* params,
+                      gxy_hsp_buf* out, gxy_stats* stats);
+/* Same with device-resident sequences (the table's own target is used). */
+gxy_status gxy_search_dseq(gxy_ctx* ctx, const gxy_table* table, const gxy_dseq* query,
+                           const gxy_search_params* params, gxy_hsp_buf* out, gxy_stats* stats);
+void gxy_hsp_buf_free(gxy_hsp_buf* buf);
+
+/* ---- batched: many (table, query, strand) units in one launch ------------ */
+/* One unit is one reference search() call: the driver's
+ * (chunk, query, strand) triple (src/driver.rs:210-240).  strand 1 searches
+ * the reverse complement of the query, computed once per query on the device
+ * (the reference recomputes it per chunk, src/driver.rs:221).  When
+ * primary_hi > primary_lo the unit keeps only HSPs whose t_start lies in
+ * [primary_lo, primary_hi), the driver's chunk filter (src/driver.rs:250-256). */
+typedef struct {
+    uint32_t table;
+    uint32_t query;
+    uint32_t strand;
+    uint32_t primary_lo;
+    uint32_t primary_hi;
+} gxy_unit;
+
+typedef struct {
+    gxy_hsp* hsps;          /* all units' HSPs, unit-major, canonical within a unit */
+    uint64_t* unit_offsets; /* n_units + 1 */
+    uint64_t n_hsps;
+    uint32_t n_units;
+} gxy_batch_result;
+
+typedef struct {
+    uint32_t use_graph;     /* capture the batch's device work in a CUDA graph */
+    uint32_t reserved_[7];
+} gxy_batch_opts;
+
+gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,
+                            uint32_t n_queries, const gxy_dseq* const* queries,
+                            uint32_t n_units, const gxy_unit* units,
+                            const gxy_search_params* params, const gxy_batch_opts* opts,
+                            gxy_batch_result* out, gxy_stats* stats);
+void gxy_batch_result_free(gxy_batch_result* r);
+
+/* chunk_target (src/driver.rs:156-194): writes up to cap chunks as
+ * (chunk_lo, chunk_hi, primary_lo_local, primary_hi_local) quadruples and
+ * returns the count in *n (always set, even when cap is too small). */
+gxy_status gxy_chunk_plan(uint64_t target_len, uint32_t primary_bp, uint32_t halo_bp,
+                          uint64_t* quads, uint64_t cap, uint64_t* n);
+
+/* ---- x-drop extension of given hits (src/hsp.rs:66-148) ------------------ */
+/* Extends n seed hits (t_pos[i], q_pos[i]) of seed_len columns exactly like
+ * extend_hit: ok[i] = 1 and out[i] set when the HSP reaches hspthresh.
+ * mode 0 = one lane per hit, mode 1 = one warp per hit (shuffle prefix-max). */
+gxy_status gxy_extend_hits(gxy_ctx* ctx, const gxy_dseq* target, const gxy_dseq* query,
+                           const gxy_search_params* params, uint64_t n, const uint32_t* t_pos,
+                           const uint32_t* q_pos, uint32_t seed_len, uint32_t mode,
+                           gxy_hsp* out, uint8_t* ok);
+
+/* ---- serving loop ---------------------------------------------------------- */
+/* Keeps the given tables resident, admits submitted queries while device
+ * memory is below max_device_bytes and in-flight units below max_units, and
+ * runs them in overlapping batches on max_streams streams. */
+typedef struct {
+    uint64_t max_device_bytes;
+    uint32_t max_units;
+    uint32_t max_streams;
+    uint32_t max_batch_units;
+    uint32_t both_strands;
+} gxy_server_opts;
+
+gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,
+                             const gxy_search_params* params, const gxy_server_opts* opts,
+                             gxy_server** out);
+/* Copies the query and queues it against table; returns its id. */
+gxy_status gxy_server_submit(gxy_server* s, uint32_t table, const gxy_packed_seq* query,
+                             uint64_t* request_id);
+/* Waits up to timeout_ms for request_id.  On completion fills plus/minus
+ * (library-allocated) and the request's submit->done latency. */
+gxy_status gxy_server_wait(gxy_server* s, uint64_t request_id, uint32_t timeout_ms,
+                           gxy_hsp_buf* plus, gxy_hsp_buf* minus, double* latency_ms);
+typedef struct {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t batches;
+    uint64_t max_inflight_units;
+    uint64_t bytes_in_use;
+} gxy_server_stats;
+gxy_status gxy_server_get_stats(gxy_server* s, gxy_server_stats* st);
+gxy_status gxy_server_destroy(gxy_server* s);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif

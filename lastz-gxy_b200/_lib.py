@@ -1,0 +1,154 @@
+"""ctypes binding of libgxyseed.so, the C ABI declared in include/gxy_seed.h.
+
+The product path runs only through this library: there is no CPU fallback.  If
+the shared object is missing or the device is not a B200, every entry point
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgxyseed.so")
+
+GXY_OK, GXY_EINVAL, GXY_ENOMEM, GXY_EUNSUPPORTED, GXY_ETIMEDOUT, GXY_ECUDA, GXY_ENOTREADY, GXY_EOVERFLOW = range(8)
+
+
+class GxyError(RuntimeError):
+    """A gxy_status other than GXY_OK, with the library's message."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"gxy status {status}: {msg}")
+        self.status = status
+
+
+class PackedSeqC(C.Structure):
+    _fields_ = [("codes", C.c_void_p), ("valid", C.c_void_p), ("mask", C.c_void_p), ("len", C.c_uint64)]
+
+
+class SearchParamsC(C.Structure):
+    _fields_ = [
+        ("sub", C.c_int32 * 16),
+        ("ambig", C.c_int32),
+        ("xdrop", C.c_int32),
+        ("hspthresh", C.c_int32),
+        ("step", C.c_uint32),
+        ("transitions", C.c_uint8),
+        ("has_entropy", C.c_uint8),
+        ("pad_", C.c_uint8 * 2),
+        ("entropy_thr", C.c_int32),
+    ]
+
+
+class HspC(C.Structure):
+    _fields_ = [("t_start", C.c_uint32), ("q_start", C.c_uint32), ("length", C.c_uint32), ("score", C.c_int32)]
+
+
+class HspBufC(C.Structure):
+    _fields_ = [("hsps", C.POINTER(HspC)), ("len", C.c_uint64), ("cap", C.c_uint64)]
+
+
+class StatsC(C.Structure):
+    _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
+                ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double)]
+
+
+class TuningC(C.Structure):
+    _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
+                ("walk_warps", C.c_uint32)]
+
+
+class UnitC(C.Structure):
+    _fields_ = [("table", C.c_uint32), ("query", C.c_uint32), ("strand", C.c_uint32), ("primary_lo", C.c_uint32),
+                ("primary_hi", C.c_uint32)]
+
+
+class BatchResultC(C.Structure):
+    _fields_ = [("hsps", C.POINTER(HspC)), ("unit_offsets", C.POINTER(C.c_uint64)), ("n_hsps", C.c_uint64),
+                ("n_units", C.c_uint32)]
+
+
+class BatchOptsC(C.Structure):
+    _fields_ = [("use_graph", C.c_uint32), ("reserved_", C.c_uint32 * 7)]
+
+
+class ServerOptsC(C.Structure):
+    _fields_ = [("max_device_bytes", C.c_uint64), ("max_units", C.c_uint32), ("max_streams", C.c_uint32),
+                ("max_batch_units", C.c_uint32), ("both_strands", C.c_uint32)]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("max_inflight_units", C.c_uint64), ("bytes_in_use", C.c_uint64)]
+
+
+V = C.c_void_p
+P = C.POINTER
+U32, U64, I32, U8 = C.c_uint32, C.c_uint64, C.c_int32, C.c_uint8
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "gxy_status_string": (C.c_char_p, [C.c_int]),
+    "gxy_last_error": (C.c_char_p, []),
+    "gxy_abi_version": (U32, []),
+    "gxy_ctx_create": (C.c_int, [C.c_int, P(V)]),
+    "gxy_ctx_destroy": (C.c_int, [V]),
+    "gxy_ctx_set_tuning": (C.c_int, [V, P(TuningC)]),
+    "gxy_ctx_get_tuning": (C.c_int, [V, P(TuningC)]),
+    "gxy_dseq_upload": (C.c_int, [V, P(PackedSeqC), P(V)]),
+    "gxy_dseq_from_ascii": (C.c_int, [V, V, U64, P(V)]),
+    "gxy_dseq_reverse_complement": (C.c_int, [V, V, P(V)]),
+    "gxy_dseq_download": (C.c_int, [V, V, V, V]),
+    "gxy_dseq_len": (U64, [V]),
+    "gxy_dseq_free": (C.c_int, [V]),
+    "gxy_table_build": (C.c_int, [V, P(PackedSeqC), C.c_char_p, U32, U32, P(V)]),
+    "gxy_table_build_view": (C.c_int, [V, V, U64, U64, C.c_char_p, U32, U32, P(V)]),
+    "gxy_table_prune_hot_words": (C.c_int, [V, U32]),
+    "gxy_table_info": (C.c_int, [V, P(U64), P(U64), P(U32), P(U32)]),
+    "gxy_table_download": (C.c_int, [V, V, V]),
+    "gxy_table_free": (C.c_int, [V]),
+    "gxy_search": (C.c_int, [V, V, P(PackedSeqC), P(PackedSeqC), P(SearchParamsC), P(HspBufC), P(StatsC)]),
+    "gxy_search_dseq": (C.c_int, [V, V, V, P(SearchParamsC), P(HspBufC), P(StatsC)]),
+    "gxy_hsp_buf_free": (None, [P(HspBufC)]),
+    "gxy_batch_search": (C.c_int, [V, U32, P(V), U32, P(V), U32, P(UnitC), P(SearchParamsC), P(BatchOptsC),
+                                   P(BatchResultC), P(StatsC)]),
+    "gxy_batch_result_free": (None, [P(BatchResultC)]),
+    "gxy_chunk_plan": (C.c_int, [U64, U32, U32, P(U64), U64, P(U64)]),
+    "gxy_extend_hits": (C.c_int, [V, V, V, P(SearchParamsC), U64, V, V, U32, U32, V, V]),
+    "gxy_server_create": (C.c_int, [V, U32, P(V), P(SearchParamsC), P(ServerOptsC), P(V)]),
+    "gxy_server_submit": (C.c_int, [V, U32, P(PackedSeqC), P(U64)]),
+    "gxy_server_wait": (C.c_int, [V, U64, U32, P(HspBufC), P(HspBufC), P(C.c_double)]),
+    "gxy_server_get_stats": (C.c_int, [V, P(ServerStatsC)]),
+    "gxy_server_destroy": (C.c_int, [V]),
+}
+
+_lib = None
+
+
+def build() -> str:
+    """Compiles libgxyseed.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(_HERE, "csrc")], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """Loads libgxyseed.so; raises when it was not built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with lastz_gxy_b200.build() (make -C csrc)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != GXY_OK:
+        msg = lib().gxy_last_error()
+        raise GxyError(status, msg.decode() if msg else "")

@@ -1,0 +1,714 @@
+// gxy_api.cu -- the extern "C" boundary declared in include/gxy_seed.h.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gxy_engine.cuh"
+
+using namespace gxy;
+
+namespace gxy {
+const char* last_error();
+}
+
+#define API_CK(call)                                                                         \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+            return e_ == cudaErrorMemoryAllocation ? GXY_ENOMEM : GXY_ECUDA;                 \
+        }                                                                                    \
+    } while (0)
+
+#define API_TRY(expr)                      \
+    do {                                   \
+        gxy_status s_ = (expr);            \
+        if (s_ != GXY_OK) return s_;       \
+    } while (0)
+
+namespace {
+
+// RAII checkout of a worker.
+struct WorkerLease {
+    gxy_ctx* ctx;
+    Worker* w;
+    gxy_status err;
+    explicit WorkerLease(gxy_ctx* c) : ctx(c), w(nullptr), err(GXY_OK) { w = checkout(c, &err); }
+    ~WorkerLease() {
+        if (w) checkin(ctx, w);
+    }
+};
+
+gxy_status set_device(gxy_ctx* ctx) {
+    API_CK(cudaSetDevice(ctx->device));
+    return GXY_OK;
+}
+
+// SeedPattern::parse (src/seeds.rs:113-126) with the engine's limits.
+gxy_status parse_pattern(const char* s, Pattern& pat) {
+    if (!s) {
+        set_error("pattern is null");
+        return GXY_EINVAL;
+    }
+    memset(&pat, 0, sizeof(pat));
+    uint32_t len = 0, w = 0;
+    for (const char* c = s; *c; c++) {
+        if (*c != '0' && *c != '1') {
+            set_error(std::string("seed pattern character '") + *c + "' is not '0' or '1'");
+            return GXY_EINVAL;
+        }
+        if (len >= 32) {
+            set_error("seed pattern exceeds the 32-position limit (src/seeds.rs:103-107)");
+            return GXY_EINVAL;
+        }
+        if (*c == '1') {
+            if (w >= (uint32_t)kMaxWeight) {
+                set_error("seed weight > 15 needs more than 2^30 buckets; unsupported");
+                return GXY_EUNSUPPORTED;
+            }
+            pat.care[w++] = (uint8_t)len;
+            pat.care_mask |= 1u << len;
+        }
+        len++;
+    }
+    if (len == 0) {
+        set_error("seed pattern is empty");
+        return GXY_EINVAL;
+    }
+    pat.len = len;
+    pat.weight = w;
+    return GXY_OK;
+}
+
+uint32_t n_windows(uint64_t len, uint32_t L, uint32_t step) {
+    // iter_with_stride (src/seeds.rs:226-236): 0, step, ... <= len - L.
+    if (len < L) return 0;
+    return (uint32_t)((len - L) / step + 1);
+}
+
+bool same_host_seq(const gxy_table* t, const gxy_packed_seq* s) {
+    return s->codes == t->hc && s->valid == t->hv && s->mask == t->hm && s->len == t->hlen;
+}
+
+// prune_hot_words (src/pos_table.rs:113-136): counts of kept buckets ->
+// exclusive scan -> copy the kept buckets in word order.
+gxy_status prune_table(gxy_table* t, uint32_t limit, Worker* W) {
+    cudaStream_t st = W->st;
+    const uint64_t nw = t->num_words;
+    uint32_t* new_starts = nullptr;
+    uint32_t* newpos = nullptr;
+    cudaError_t e = cudaMalloc(&new_starts, (nw + 1) * 4);
+    if (e != cudaSuccess) {
+        set_error("table prune allocation");
+        return GXY_ENOMEM;
+    }
+    launch_prune_counts(t->starts, nw, limit, new_starts, st);
+    scan_u32(new_starts, new_starts, nullptr, nw, nw, true, nullptr, W->ps, st);
+    uint32_t total2 = 0;
+    e = cudaMemcpyAsync(&total2, new_starts + nw, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMalloc(&newpos, (size_t)std::max<uint32_t>(total2, 1) * 4);
+    if (e == cudaSuccess) {
+        launch_prune_copy(t->positions, t->starts, nw, new_starts, limit, newpos, st);
+        e = cudaStreamSynchronize(st);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cudaFree(new_starts);
+        if (newpos) cudaFree(newpos);
+        set_error(std::string("table prune: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    cudaFree(t->starts);
+    cudaFree(t->positions);
+    t->starts = new_starts;
+    t->positions = newpos;
+    t->npos = total2;
+    return GXY_OK;
+}
+
+gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t hi, const Pattern& pat,
+                       uint32_t step, uint32_t mwc, gxy_table** out) {
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    Worker* W = L.w;
+    cudaStream_t st = W->st;
+    const uint64_t nw = 1ull << (2 * pat.weight);
+    const uint32_t nwin = n_windows(hi - lo, pat.len, step);
+    gxy_table* t = new gxy_table();
+    t->ctx = ctx;
+    t->seq = seq;
+    t->lo = lo;
+    t->hi = hi;
+    t->num_words = nw;
+    t->pat = pat;
+    t->step = step;
+    DevBuf keys0, vals0, keys1, vals1;
+    auto fail = [&](gxy_status s) {
+        keys0.release(); vals0.release(); keys1.release(); vals1.release();
+        if (t->starts) cudaFree(t->starts);
+        if (t->positions) cudaFree(t->positions);
+        delete t;
+        return s;
+    };
+    cudaError_t e = cudaMalloc(&t->starts, (nw + 1) * 4);
+    if (e == cudaSuccess) e = keys0.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
+    if (e == cudaSuccess) e = vals0.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
+    if (e == cudaSuccess) e = keys1.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
+    if (e == cudaSuccess) e = vals1.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
+    if (e != cudaSuccess) {
+        set_error(std::string("table allocation: ") + cudaGetErrorString(e));
+        return fail(GXY_ENOMEM);
+    }
+    // counts[word] -> exclusive scan in place -> starts (src/pos_table.rs:42-58).
+    e = cudaMemsetAsync(t->starts, 0, (nw + 1) * 4, st);
+    const SeqView view = view_of(seq, lo, hi);
+    launch_seed_words(view, pat, step, nwin, (uint32_t)nw, keys0.as<uint32_t>(), vals0.as<uint32_t>(), t->starts, st);
+    scan_u32(t->starts, t->starts, nullptr, nw, nw, true, nullptr, W->ps, st);
+    // Stable sort of (word, position) by word: positions stay ascending within
+    // a bucket, the order of the reference's scatter (src/pos_table.rs:69-75).
+    RadixPass passes[8];
+    int bits = 0;
+    while ((1ull << bits) <= nw) bits++;   // words and the sentinel nw
+    const int np = plan_radix(0, bits, 0, 0, passes, 8);
+    const int which = radix_sort_u32(keys0.as<uint32_t>(), vals0.as<uint32_t>(), keys1.as<uint32_t>(),
+                                     vals1.as<uint32_t>(), nullptr, nwin, nwin, passes, np, W->ps, st);
+    uint32_t* svals = which ? vals1.as<uint32_t>() : vals0.as<uint32_t>();
+    uint32_t total = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, t->starts + nw, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("table build: ") + cudaGetErrorString(e));
+        return fail(GXY_ECUDA);
+    }
+    t->npos = total;
+    e = cudaMalloc(&t->positions, (size_t)std::max<uint32_t>(total, 1) * 4);
+    if (e == cudaSuccess && total)
+        e = cudaMemcpyAsync(t->positions, svals, (size_t)total * 4, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && mwc > 0) {
+        const gxy_status ps = prune_table(t, mwc, W);
+        if (ps != GXY_OK) return fail(ps);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("table finish: ") + cudaGetErrorString(e));
+        return fail(GXY_ECUDA);
+    }
+    keys0.release(); vals0.release(); keys1.release(); vals1.release();
+    *out = t;
+    return GXY_OK;
+}
+
+gxy_status deliver(const std::vector<gxy_hsp>& v, gxy_hsp_buf* out) {
+    if (!out) return GXY_OK;
+    const uint64_t n = v.size();
+    if (out->hsps == nullptr) {
+        out->hsps = static_cast<gxy_hsp*>(malloc(std::max<uint64_t>(n, 1) * sizeof(gxy_hsp)));
+        if (!out->hsps) {
+            set_error("host allocation of the HSP buffer");
+            return GXY_ENOMEM;
+        }
+        out->cap = n;
+    } else if (out->cap < n) {
+        out->len = n;
+        set_error("caller HSP buffer too small");
+        return GXY_EOVERFLOW;
+    }
+    if (n) memcpy(out->hsps, v.data(), n * sizeof(gxy_hsp));
+    out->len = n;
+    return GXY_OK;
+}
+
+gxy_status search_impl(gxy_ctx* ctx, Worker* W, const gxy_table* table, const SeqView& T, const SeqView& Q,
+                       const gxy_search_params* p, gxy_hsp_buf* out, gxy_stats* stats) {
+    API_TRY(check_params(p, std::min<uint64_t>(T.len, Q.len)));
+    std::vector<SeqView> tsegs{T}, qsegs{Q};
+    std::vector<UnitPlan> units(1);
+    units[0].tseg = 0;
+    units[0].qseg = 0;
+    units[0].starts = table->starts;
+    units[0].positions = table->positions;
+    units[0].nwin = n_windows(Q.len, table->pat.len, p->step);
+    units[0].primary_lo = units[0].primary_hi = 0;
+    RunResult r;
+    API_TRY(run_units(ctx, W, units, tsegs, qsegs, table->pat, *p, false, r));
+    if (stats) *stats = r.stats;
+    return deliver(r.hsps, out);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gxy_status_string(gxy_status s) {
+    switch (s) {
+        case GXY_OK: return "ok";
+        case GXY_EINVAL: return "invalid argument";
+        case GXY_ENOMEM: return "out of memory";
+        case GXY_EUNSUPPORTED: return "unsupported";
+        case GXY_ETIMEDOUT: return "timed out";
+        case GXY_ECUDA: return "CUDA error";
+        case GXY_ENOTREADY: return "not ready";
+        case GXY_EOVERFLOW: return "buffer too small";
+    }
+    return "unknown status";
+}
+
+const char* gxy_last_error(void) { return last_error(); }
+uint32_t gxy_abi_version(void) { return 1; }
+
+gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
+    if (!out) return GXY_EINVAL;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        set_error(std::string("no CUDA device: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    if (device < 0 || device >= n) {
+        set_error("device index out of range");
+        return GXY_EINVAL;
+    }
+    API_CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    API_CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) {
+        set_error(std::string("this library is built for sm_100a; device is ") + prop.name);
+        return GXY_EUNSUPPORTED;
+    }
+    gxy_ctx* c = new gxy_ctx();
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    *out = c;
+    return GXY_OK;
+}
+
+gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
+    if (!ctx) return GXY_OK;
+    cudaSetDevice(ctx->device);
+    for (Worker* w : ctx->all_workers) {
+        cudaStreamSynchronize(w->st);
+        DevBuf* bufs[] = {&w->prim_sums, &w->prim_hist, &w->counters, &w->d_units, &w->d_tsegs, &w->d_qsegs,
+                          &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags, &w->offsets, &w->ohsp,
+                          &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2};
+        for (DevBuf* b : bufs) b->release();
+        dseq_destroy(w->qstage);
+        dseq_destroy(w->tstage);
+        for (gxy_dseq* d : w->rc_tmp) dseq_destroy(d);
+        for (int i = 0; i < 4; i++)
+            if (w->ev[i]) cudaEventDestroy(w->ev[i]);
+        if (w->h_pinned) cudaFreeHost(w->h_pinned);
+        cudaStreamDestroy(w->st);
+        delete w;
+    }
+    delete ctx;
+    return GXY_OK;
+}
+
+gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
+    if (!ctx || !t) return GXY_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (t->screen_warps) {
+        if (t->screen_warps != 4 && t->screen_warps != 8 && t->screen_warps != 16) {
+            set_error("screen_warps must be 4, 8 or 16");
+            return GXY_EINVAL;
+        }
+        ctx->tuning.screen_warps = t->screen_warps;
+    }
+    if (t->screen_cap) ctx->tuning.screen_cap = std::max<uint32_t>(32, t->screen_cap);
+    if (t->screen_blocks_per_sm) ctx->tuning.screen_blocks_per_sm = std::min<uint32_t>(t->screen_blocks_per_sm, 16);
+    if (t->walk_warps) ctx->tuning.walk_warps = t->walk_warps == 4 ? 4 : 8;
+    return GXY_OK;
+}
+
+gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t) {
+    if (!ctx || !t) return GXY_EINVAL;
+    std::lock_guard<std::mutex> g(ctx->mu);
+    *t = ctx->tuning;
+    return GXY_OK;
+}
+
+gxy_status gxy_dseq_upload(gxy_ctx* ctx, const gxy_packed_seq* host, gxy_dseq** out) {
+    if (!ctx || !host || !out || (host->len && (!host->codes || !host->valid || !host->mask))) return GXY_EINVAL;
+    if (host->len >= (1ull << 32)) {
+        set_error("sequences are limited to u32 positions (src/pos_table.rs:56)");
+        return GXY_EUNSUPPORTED;
+    }
+    API_TRY(set_device(ctx));
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    gxy_dseq* d = nullptr;
+    API_TRY(dseq_alloc(ctx, host->len, &d, L.w->st));
+    gxy_status s = dseq_fill_host(d, host, L.w->st);
+    if (s == GXY_OK && cudaStreamSynchronize(L.w->st) != cudaSuccess) s = GXY_ECUDA;
+    if (s != GXY_OK) {
+        dseq_destroy(d);
+        return s;
+    }
+    *out = d;
+    return GXY_OK;
+}
+
+gxy_status gxy_dseq_from_ascii(gxy_ctx* ctx, const uint8_t* ascii, uint64_t n, gxy_dseq** out) {
+    if (!ctx || (!ascii && n) || !out) return GXY_EINVAL;
+    if (n >= (1ull << 32)) return GXY_EUNSUPPORTED;
+    API_TRY(set_device(ctx));
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    gxy_dseq* d = nullptr;
+    API_TRY(dseq_alloc(ctx, n, &d, L.w->st));
+    void* dbuf = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (n) {
+        e = cudaMalloc(&dbuf, n);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dbuf, ascii, n, cudaMemcpyHostToDevice, L.w->st);
+        if (e == cudaSuccess) launch_pack_ascii(static_cast<uint8_t*>(dbuf), n, d->codes, d->valid, d->mask, L.w->st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(L.w->st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (dbuf) cudaFree(dbuf);
+    if (e != cudaSuccess) {
+        dseq_destroy(d);
+        set_error(std::string("pack: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    *out = d;
+    return GXY_OK;
+}
+
+gxy_status gxy_dseq_reverse_complement(gxy_ctx* ctx, const gxy_dseq* in, gxy_dseq** out) {
+    if (!ctx || !in || !out) return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    gxy_dseq* d = nullptr;
+    API_TRY(dseq_alloc(ctx, in->len, &d, L.w->st));
+    launch_reverse_complement(in->codes, in->valid, in->mask, in->len, d->codes, d->valid, d->mask, L.w->st);
+    cudaError_t e = cudaStreamSynchronize(L.w->st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        dseq_destroy(d);
+        set_error(std::string("reverse complement: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    *out = d;
+    return GXY_OK;
+}
+
+gxy_status gxy_dseq_download(const gxy_dseq* s, uint8_t* codes, uint8_t* valid, uint8_t* mask) {
+    if (!s) return GXY_EINVAL;
+    API_TRY(set_device(s->ctx));
+    const uint64_t n = s->len;
+    if (!n) return GXY_OK;
+    if (codes) API_CK(cudaMemcpy(codes, reinterpret_cast<const char*>(s->codes) + kPad / 4, (n + 3) / 4,
+                                 cudaMemcpyDeviceToHost));
+    if (valid) API_CK(cudaMemcpy(valid, reinterpret_cast<const char*>(s->valid) + kPad / 8, (n + 7) / 8,
+                                 cudaMemcpyDeviceToHost));
+    if (mask) API_CK(cudaMemcpy(mask, reinterpret_cast<const char*>(s->mask) + kPad / 8, (n + 7) / 8,
+                                cudaMemcpyDeviceToHost));
+    return GXY_OK;
+}
+
+uint64_t gxy_dseq_len(const gxy_dseq* s) { return s ? s->len : 0; }
+
+gxy_status gxy_dseq_free(gxy_dseq* s) {
+    if (!s) return GXY_OK;
+    cudaSetDevice(s->ctx->device);
+    dseq_destroy(s);
+    return GXY_OK;
+}
+
+gxy_status gxy_table_build(gxy_ctx* ctx, const gxy_packed_seq* target, const char* pattern01, uint32_t step,
+                           uint32_t max_word_count, gxy_table** out) {
+    if (!ctx || !target || !out) return GXY_EINVAL;
+    if (step < 1) {
+        set_error("step must be >= 1 (src/pos_table.rs:36)");
+        return GXY_EINVAL;
+    }
+    Pattern pat;
+    API_TRY(parse_pattern(pattern01, pat));
+    gxy_dseq* d = nullptr;
+    API_TRY(gxy_dseq_upload(ctx, target, &d));
+    gxy_table* t = nullptr;
+    gxy_status s = build_table(ctx, d, 0, d->len, pat, step, max_word_count, &t);
+    if (s != GXY_OK) {
+        dseq_destroy(d);
+        return s;
+    }
+    t->owned = d;
+    t->hc = target->codes;
+    t->hv = target->valid;
+    t->hm = target->mask;
+    t->hlen = target->len;
+    *out = t;
+    return GXY_OK;
+}
+
+gxy_status gxy_table_build_view(gxy_ctx* ctx, const gxy_dseq* target, uint64_t lo, uint64_t hi,
+                                const char* pattern01, uint32_t step, uint32_t max_word_count, gxy_table** out) {
+    if (!ctx || !target || !out || lo > hi || hi > target->len) return GXY_EINVAL;
+    if (step < 1) {
+        set_error("step must be >= 1 (src/pos_table.rs:36)");
+        return GXY_EINVAL;
+    }
+    Pattern pat;
+    API_TRY(parse_pattern(pattern01, pat));
+    API_TRY(set_device(ctx));
+    return build_table(ctx, target, lo, hi, pat, step, max_word_count, out);
+}
+
+gxy_status gxy_table_prune_hot_words(gxy_table* t, uint32_t limit) {
+    if (!t) return GXY_EINVAL;
+    API_TRY(set_device(t->ctx));
+    WorkerLease L(t->ctx);
+    if (!L.w) return L.err;
+    return prune_table(t, limit, L.w);
+}
+
+gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_positions, uint32_t* pattern_len,
+                          uint32_t* weight) {
+    if (!t) return GXY_EINVAL;
+    if (num_words) *num_words = t->num_words;
+    if (n_positions) *n_positions = t->npos;
+    if (pattern_len) *pattern_len = t->pat.len;
+    if (weight) *weight = t->pat.weight;
+    return GXY_OK;
+}
+
+gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions) {
+    if (!t) return GXY_EINVAL;
+    API_TRY(set_device(t->ctx));
+    if (starts) API_CK(cudaMemcpy(starts, t->starts, (t->num_words + 1) * 4, cudaMemcpyDeviceToHost));
+    if (positions && t->npos) API_CK(cudaMemcpy(positions, t->positions, t->npos * 4, cudaMemcpyDeviceToHost));
+    return GXY_OK;
+}
+
+gxy_status gxy_table_free(gxy_table* t) {
+    if (!t) return GXY_OK;
+    cudaSetDevice(t->ctx->device);
+    if (t->starts) cudaFree(t->starts);
+    if (t->positions) cudaFree(t->positions);
+    dseq_destroy(t->owned);
+    delete t;
+    return GXY_OK;
+}
+
+gxy_status gxy_search(gxy_ctx* ctx, const gxy_table* table, const gxy_packed_seq* target,
+                      const gxy_packed_seq* query, const gxy_search_params* params, gxy_hsp_buf* out,
+                      gxy_stats* stats) {
+    if (!ctx || !table || !target || !query || !params) return GXY_EINVAL;
+    if (query->len && (!query->codes || !query->valid || !query->mask)) return GXY_EINVAL;
+    if (query->len >= (1ull << 32)) return GXY_EUNSUPPORTED;
+    API_TRY(set_device(ctx));
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    Worker* W = L.w;
+    SeqView T = view_of(table->seq, table->lo, table->hi);
+    if (!same_host_seq(table, target)) {
+        if (target->len != table->hi - table->lo) {
+            set_error("target length differs from the sequence the table was built on");
+            return GXY_EINVAL;
+        }
+        if (!W->tstage || W->tstage->len < target->len) {
+            dseq_destroy(W->tstage);
+            W->tstage = nullptr;
+            API_TRY(dseq_alloc(ctx, target->len, &W->tstage, W->st));
+        }
+        API_TRY(dseq_fill_host(W->tstage, target, W->st));
+        T = view_of(W->tstage, 0, target->len);
+    }
+    if (!W->qstage || W->qstage->len < query->len || W->qstage->len > 2 * query->len + (1u << 20)) {
+        dseq_destroy(W->qstage);
+        W->qstage = nullptr;
+        API_TRY(dseq_alloc(ctx, query->len, &W->qstage, W->st));
+    }
+    API_TRY(dseq_fill_host(W->qstage, query, W->st));
+    const SeqView Q = view_of(W->qstage, 0, query->len);
+    return search_impl(ctx, W, table, T, Q, params, out, stats);
+}
+
+gxy_status gxy_search_dseq(gxy_ctx* ctx, const gxy_table* table, const gxy_dseq* query,
+                           const gxy_search_params* params, gxy_hsp_buf* out, gxy_stats* stats) {
+    if (!ctx || !table || !query || !params) return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    const SeqView T = view_of(table->seq, table->lo, table->hi);
+    const SeqView Q = view_of(query, 0, query->len);
+    return search_impl(ctx, L.w, table, T, Q, params, out, stats);
+}
+
+void gxy_hsp_buf_free(gxy_hsp_buf* buf) {
+    if (!buf) return;
+    free(buf->hsps);
+    buf->hsps = nullptr;
+    buf->len = buf->cap = 0;
+}
+
+gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables, uint32_t n_queries,
+                            const gxy_dseq* const* queries, uint32_t n_units, const gxy_unit* units,
+                            const gxy_search_params* params, const gxy_batch_opts* opts, gxy_batch_result* out,
+                            gxy_stats* stats) {
+    if (!ctx || (!tables && n_tables) || (!queries && n_queries) || (!units && n_units) || !params || !out)
+        return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    memset(out, 0, sizeof(*out));
+    if (n_units == 0) {
+        out->unit_offsets = static_cast<uint64_t*>(calloc(1, sizeof(uint64_t)));
+        return GXY_OK;
+    }
+    const Pattern& pat = tables[units[0].table]->pat;
+    uint64_t max_cols = 0;
+    for (uint32_t i = 0; i < n_units; i++) {
+        const gxy_unit& u = units[i];
+        if (u.table >= n_tables || u.query >= n_queries || u.strand > 1) {
+            set_error("unit references a missing table or query, or a strand other than 0/1");
+            return GXY_EINVAL;
+        }
+        const gxy_table* t = tables[u.table];
+        if (t->pat.len != pat.len || t->pat.care_mask != pat.care_mask) {
+            set_error("all tables of a batch must share one seed pattern");
+            return GXY_EINVAL;
+        }
+        max_cols = std::max<uint64_t>(max_cols, std::min<uint64_t>(t->hi - t->lo, queries[u.query]->len));
+    }
+    API_TRY(check_params(params, max_cols));
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    Worker* W = L.w;
+    // Reverse complements once per query that needs one.
+    for (gxy_dseq* d : W->rc_tmp) dseq_destroy(d);
+    W->rc_tmp.clear();
+    std::vector<int> qseg_of(2 * (size_t)n_queries, -1);
+    std::vector<int> tseg_of(n_tables, -1);
+    std::vector<SeqView> tsegs, qsegs;
+    std::vector<UnitPlan> plan(n_units);
+    for (uint32_t i = 0; i < n_units; i++) {
+        const gxy_unit& u = units[i];
+        const gxy_table* t = tables[u.table];
+        if (tseg_of[u.table] < 0) {
+            tseg_of[u.table] = (int)tsegs.size();
+            tsegs.push_back(view_of(t->seq, t->lo, t->hi));
+        }
+        const size_t qi = 2 * (size_t)u.query + u.strand;
+        if (qseg_of[qi] < 0) {
+            const gxy_dseq* q = queries[u.query];
+            if (u.strand == 1) {
+                gxy_dseq* rc = nullptr;
+                API_TRY(dseq_alloc(ctx, q->len, &rc, W->st));
+                launch_reverse_complement(q->codes, q->valid, q->mask, q->len, rc->codes, rc->valid, rc->mask, W->st);
+                W->rc_tmp.push_back(rc);
+                q = rc;
+            }
+            qseg_of[qi] = (int)qsegs.size();
+            qsegs.push_back(view_of(q, 0, q->len));
+        }
+        plan[i].tseg = (uint32_t)tseg_of[u.table];
+        plan[i].qseg = (uint32_t)qseg_of[qi];
+        plan[i].starts = t->starts;
+        plan[i].positions = t->positions;
+        plan[i].nwin = n_windows(queries[u.query]->len, pat.len, params->step);
+        plan[i].primary_lo = u.primary_lo;
+        plan[i].primary_hi = u.primary_hi;
+    }
+    RunResult r;
+    API_TRY(run_units(ctx, W, plan, tsegs, qsegs, pat, *params, opts && opts->use_graph, r));
+    if (stats) *stats = r.stats;
+    const uint64_t n = r.hsps.size();
+    out->hsps = static_cast<gxy_hsp*>(malloc(std::max<uint64_t>(n, 1) * sizeof(gxy_hsp)));
+    out->unit_offsets = static_cast<uint64_t*>(calloc((size_t)n_units + 1, sizeof(uint64_t)));
+    if (!out->hsps || !out->unit_offsets) {
+        gxy_batch_result_free(out);
+        set_error("host allocation of the batch result");
+        return GXY_ENOMEM;
+    }
+    if (n) memcpy(out->hsps, r.hsps.data(), n * sizeof(gxy_hsp));
+    for (uint64_t i = 0; i < n; i++) out->unit_offsets[r.unit[i] + 1]++;
+    for (uint32_t u = 0; u < n_units; u++) out->unit_offsets[u + 1] += out->unit_offsets[u];
+    out->n_hsps = n;
+    out->n_units = n_units;
+    return GXY_OK;
+}
+
+void gxy_batch_result_free(gxy_batch_result* r) {
+    if (!r) return;
+    free(r->hsps);
+    free(r->unit_offsets);
+    memset(r, 0, sizeof(*r));
+}
+
+gxy_status gxy_chunk_plan(uint64_t target_len, uint32_t primary_bp, uint32_t halo_bp, uint64_t* quads, uint64_t cap,
+                          uint64_t* n) {
+    if (!n) return GXY_EINVAL;
+    // chunk_target, src/driver.rs:156-194 (u32 arithmetic as the reference).
+    const uint32_t t_len = (uint32_t)target_len;
+    uint64_t k = 0;
+    auto put = [&](uint64_t a, uint64_t b, uint64_t c, uint64_t d) {
+        if (quads && k < cap) {
+            quads[4 * k + 0] = a;
+            quads[4 * k + 1] = b;
+            quads[4 * k + 2] = c;
+            quads[4 * k + 3] = d;
+        }
+        k++;
+    };
+    if (primary_bp == 0 || (uint64_t)t_len <= (uint64_t)primary_bp + halo_bp) {
+        put(0, t_len, 0, t_len);
+    } else {
+        uint32_t ps = 0;
+        while (ps < t_len) {
+            const uint32_t pe = (uint32_t)std::min<uint64_t>((uint64_t)ps + primary_bp, t_len);
+            const uint32_t lo = ps > halo_bp ? ps - halo_bp : 0;
+            const uint32_t hi = (uint32_t)std::min<uint64_t>((uint64_t)pe + halo_bp, t_len);
+            put(lo, hi, ps - lo, pe - lo);
+            if (pe == t_len) break;
+            ps = pe;
+        }
+    }
+    *n = k;
+    return (quads && k > cap) ? GXY_EOVERFLOW : GXY_OK;
+}
+
+gxy_status gxy_extend_hits(gxy_ctx* ctx, const gxy_dseq* target, const gxy_dseq* query,
+                           const gxy_search_params* params, uint64_t n, const uint32_t* t_pos, const uint32_t* q_pos,
+                           uint32_t seed_len, uint32_t mode, gxy_hsp* out, uint8_t* ok) {
+    if (!ctx || !target || !query || !params || (n && (!t_pos || !q_pos || !out || !ok)) || seed_len > 32)
+        return GXY_EINVAL;
+    API_TRY(check_params(params, std::min<uint64_t>(target->len, query->len)));
+    API_TRY(set_device(ctx));
+    if (!n) return GXY_OK;
+    WorkerLease L(ctx);
+    if (!L.w) return L.err;
+    cudaStream_t st = L.w->st;
+    DevBuf bt, bq, bo, bk;
+    cudaError_t e = bt.ensure(n * 4);
+    if (e == cudaSuccess) e = bq.ensure(n * 4);
+    if (e == cudaSuccess) e = bo.ensure(n * sizeof(Hsp));
+    if (e == cudaSuccess) e = bk.ensure(n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bt.p, t_pos, n * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(bq.p, q_pos, n * 4, cudaMemcpyHostToDevice, st);
+    Score sc;
+    memcpy(sc.sub, params->sub, sizeof(sc.sub));
+    sc.ambig = params->ambig;
+    sc.xdrop = params->xdrop;
+    sc.hspthresh = params->hspthresh;
+    if (e == cudaSuccess)
+        launch_extend_hits(view_of(target, 0, target->len), view_of(query, 0, query->len), sc, bt.as<uint32_t>(),
+                           bq.as<uint32_t>(), n, seed_len, mode, bo.as<Hsp>(), bk.as<uint8_t>(), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, bo.p, n * sizeof(Hsp), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ok, bk.p, n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    bt.release(); bq.release(); bo.release(); bk.release();
+    if (e != cudaSuccess) {
+        set_error(std::string("extend_hits: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    return GXY_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,391 @@
+// gxy_engine.cu -- the host engine: device sequences, workers, and the
+// screen -> sort -> walk -> compaction pipeline over a list of units.
+#include "gxy_engine.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace gxy {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+#define GXY_CK(call)                                                                         \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+            return e_ == cudaErrorMemoryAllocation ? GXY_ENOMEM : GXY_ECUDA;                 \
+        }                                                                                    \
+    } while (0)
+
+cudaError_t DevBuf::ensure(size_t need) {
+    if (need <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t b = need < 256 ? 256 : need;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t st) {
+    gxy_dseq* d = new gxy_dseq();
+    d->ctx = ctx;
+    d->len = len;
+    uint64_t nw = (kPad + len + kTailPad + 31) / 32;
+    nw = (nw + 3) & ~3ull;   // each array a multiple of 16 bytes
+    d->nwords = nw;
+    const size_t cb = align256(nw * 8), vb = align256(nw * 4);
+    d->bytes = cb + 2 * vb;
+    cudaError_t e = cudaMalloc(&d->alloc, d->bytes);
+    if (e != cudaSuccess) {
+        delete d;
+        set_error(std::string("cudaMalloc(sequence): ") + cudaGetErrorString(e));
+        return GXY_ENOMEM;
+    }
+    d->codes = static_cast<uint64_t*>(d->alloc);
+    d->valid = reinterpret_cast<uint32_t*>(static_cast<char*>(d->alloc) + cb);
+    d->mask = reinterpret_cast<uint32_t*>(static_cast<char*>(d->alloc) + cb + vb);
+    e = cudaMemsetAsync(d->alloc, 0, d->bytes, st);
+    if (e != cudaSuccess) {
+        cudaFree(d->alloc);
+        delete d;
+        set_error(std::string("cudaMemsetAsync(sequence): ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    *out = d;
+    return GXY_OK;
+}
+
+void dseq_destroy(gxy_dseq* s) {
+    if (!s) return;
+    if (s->alloc) cudaFree(s->alloc);
+    delete s;
+}
+
+gxy_status dseq_fill_host(gxy_dseq* d, const gxy_packed_seq* h, cudaStream_t st) {
+    const uint64_t n = h->len;
+    if (!n) return GXY_OK;
+    GXY_CK(cudaMemcpyAsync(reinterpret_cast<char*>(d->codes) + kPad / 4, h->codes, (n + 3) / 4,
+                           cudaMemcpyHostToDevice, st));
+    GXY_CK(cudaMemcpyAsync(reinterpret_cast<char*>(d->valid) + kPad / 8, h->valid, (n + 7) / 8,
+                           cudaMemcpyHostToDevice, st));
+    GXY_CK(cudaMemcpyAsync(reinterpret_cast<char*>(d->mask) + kPad / 8, h->mask, (n + 7) / 8,
+                           cudaMemcpyHostToDevice, st));
+    return GXY_OK;
+}
+
+SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi) {
+    SeqView v;
+    v.codes = s->codes;
+    v.valid = s->valid;
+    v.mask = s->mask;
+    v.base = kPad + lo;
+    v.len = (uint32_t)(hi - lo);
+    v.key_base = 0;
+    return v;
+}
+
+Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        if (!ctx->free_workers.empty()) {
+            Worker* w = ctx->free_workers.back();
+            ctx->free_workers.pop_back();
+            *err = GXY_OK;
+            return w;
+        }
+    }
+    Worker* w = new Worker();
+    cudaError_t e = cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
+    w->ps.grid = ctx->sm_count * 2;
+    if (e == cudaSuccess) e = w->prim_sums.ensure((w->ps.grid + 1) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = w->prim_hist.ensure(((size_t)kRadixMax * w->ps.grid + 1) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = w->counters.ensure(256);
+    if (e == cudaSuccess) e = cudaMallocHost(&w->h_pinned, 1 << 16);
+    if (e != cudaSuccess) {
+        set_error(std::string("worker setup: ") + cudaGetErrorString(e));
+        *err = e == cudaErrorMemoryAllocation ? GXY_ENOMEM : GXY_ECUDA;
+        return nullptr;
+    }
+    w->h_pinned_bytes = 1 << 16;
+    w->ps.block_sums = w->prim_sums.as<uint32_t>();
+    w->ps.hist = w->prim_hist.as<uint32_t>();
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        ctx->all_workers.push_back(w);
+    }
+    *err = GXY_OK;
+    return w;
+}
+
+void checkin(gxy_ctx* ctx, Worker* w) {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    ctx->free_workers.push_back(w);
+}
+
+gxy_status check_params(const gxy_search_params* p, uint64_t max_cols) {
+    if (!p) {
+        set_error("params is null");
+        return GXY_EINVAL;
+    }
+    if (p->step < 1) {
+        set_error("step must be >= 1 (src/pos_table.rs:36)");
+        return GXY_EINVAL;
+    }
+    int64_t m = p->ambig < 0 ? -(int64_t)p->ambig : p->ambig;
+    for (int i = 0; i < 16; i++) {
+        const int64_t a = p->sub[i] < 0 ? -(int64_t)p->sub[i] : p->sub[i];
+        m = std::max(m, a);
+    }
+    // Every partial sum is bounded by m * columns; the x-drop gap by
+    // |xdrop| + 33 m.  Within this envelope i32 adds never saturate, so the
+    // device's plain adds equal the reference's saturating ones.
+    const int64_t lim = 0x7fffffffLL;
+    const int64_t xd = p->xdrop < 0 ? -(int64_t)p->xdrop : p->xdrop;
+    if (m * (int64_t)(max_cols + 64) >= lim || xd + 33 * m >= lim) {
+        set_error("scores x sequence length can overflow i32; outside the exact envelope");
+        return GXY_EUNSUPPORTED;
+    }
+    return GXY_OK;
+}
+
+static int bits_for(uint64_t x) {
+    int b = 0;
+    while (b < 64 && (1ull << b) <= x) b++;
+    return b;   // smallest b with x < 2^b
+}
+
+static void build_variants(const Pattern& pat, uint32_t transitions, uint32_t* vx, uint32_t& nv) {
+    // src/seed_search.rs:289, :303-316.
+    const uint32_t w = pat.weight;
+    uint32_t shifts[16];
+    for (uint32_t i = 0; i < w; i++) shifts[i] = 2 * (w - 1 - i);
+    nv = 0;
+    vx[nv++] = 0;
+    if (transitions >= 1)
+        for (uint32_t i = 0; i < w; i++) vx[nv++] = 2u << shifts[i];
+    if (transitions >= 2)
+        for (uint32_t i = 0; i < w; i++)
+            for (uint32_t j = i + 1; j < w; j++) vx[nv++] = (2u << shifts[i]) ^ (2u << shifts[j]);
+}
+
+gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units, std::vector<SeqView>& tsegs,
+                     std::vector<SeqView>& qsegs, const Pattern& pat, const gxy_search_params& p, bool use_graph,
+                     RunResult& out) {
+    cudaStream_t st = W->st;
+    out.hsps.clear();
+    out.unit.clear();
+    out.stats = gxy_stats{};
+    const uint32_t nu = (uint32_t)units.size();
+    // Key axes: every target and query segment gets a private key range.
+    uint64_t tk = 0, qk = 0;
+    for (auto& s : tsegs) {
+        s.key_base = (uint32_t)tk;
+        tk += s.len;
+    }
+    for (auto& s : qsegs) {
+        s.key_base = (uint32_t)qk;
+        qk += s.len;
+    }
+    if (tk + qk >= (1ull << 32)) {
+        set_error("batch too large: total target + query length must be < 2^32");
+        return GXY_EUNSUPPORTED;
+    }
+    std::vector<UnitDev> ud(nu);
+    uint64_t tiles = 0;
+    for (uint32_t i = 0; i < nu; i++) {
+        const UnitPlan& u = units[i];
+        ud[i].tseg = u.tseg;
+        ud[i].qseg = u.qseg;
+        ud[i].starts = u.starts;
+        ud[i].positions = u.positions;
+        ud[i].nwin = u.nwin;
+        ud[i].tile_base = (uint32_t)tiles;
+        ud[i].primary_lo = u.primary_lo;
+        ud[i].primary_hi = u.primary_hi;
+        tiles += (u.nwin + 31) / 32;
+    }
+    if (tiles >= (1ull << 32)) {
+        set_error("too many query windows");
+        return GXY_EUNSUPPORTED;
+    }
+    if (nu == 0 || tiles == 0) return GXY_OK;
+
+    GXY_CK(W->d_units.ensure(nu * sizeof(UnitDev)));
+    GXY_CK(W->d_tsegs.ensure(tsegs.size() * sizeof(SeqView)));
+    GXY_CK(W->d_qsegs.ensure(qsegs.size() * sizeof(SeqView)));
+    GXY_CK(cudaMemcpyAsync(W->d_units.p, ud.data(), nu * sizeof(UnitDev), cudaMemcpyHostToDevice, st));
+    GXY_CK(cudaMemcpyAsync(W->d_tsegs.p, tsegs.data(), tsegs.size() * sizeof(SeqView), cudaMemcpyHostToDevice, st));
+    GXY_CK(cudaMemcpyAsync(W->d_qsegs.p, qsegs.data(), qsegs.size() * sizeof(SeqView), cudaMemcpyHostToDevice, st));
+
+    ScreenArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.units = W->d_units.as<UnitDev>();
+    sa.tsegs = W->d_tsegs.as<SeqView>();
+    sa.qsegs = W->d_qsegs.as<SeqView>();
+    sa.n_units = nu;
+    sa.n_tiles = (uint32_t)tiles;
+    sa.pat = pat;
+    sa.step = p.step;
+    build_variants(pat, p.transitions, sa.var_xor, sa.n_var);
+    memcpy(sa.sc.sub, p.sub, sizeof(p.sub));
+    sa.sc.ambig = p.ambig;
+    sa.sc.xdrop = p.xdrop;
+    sa.sc.hspthresh = p.hspthresh;
+    sa.cap = std::max<uint32_t>(32, ctx->tuning.screen_cap);
+    sa.qkey_total = (uint32_t)qk;
+
+    RadixPass passes[16];
+    const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
+
+    uint32_t* cnt = W->counters.as<uint32_t>();           // [0] tiles [1] cands [2] hsps
+    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);   // [0] windows [1] raw
+    if (W->cand_cap == 0) W->cand_cap = 1u << 20;
+    const int blocks_screen = ctx->sm_count * (int)std::max<uint32_t>(1, ctx->tuning.screen_blocks_per_sm);
+    const int blocks_misc = ctx->sm_count * 4;
+    const int walk_warps = ctx->tuning.walk_warps == 4 ? 4 : 8;
+
+    for (int attempt = 0; attempt < 8; attempt++) {
+        const uint32_t cap = W->cand_cap;
+        GXY_CK(W->ck0.ensure((size_t)cap * 8));
+        GXY_CK(W->ck1.ensure((size_t)cap * 8));
+        GXY_CK(W->cv0.ensure((size_t)cap * 4));
+        GXY_CK(W->cv1.ensure((size_t)cap * 4));
+        GXY_CK(W->cands.ensure((size_t)cap * sizeof(Cand)));
+        GXY_CK(W->flags.ensure((size_t)cap));
+        GXY_CK(W->offsets.ensure((size_t)cap * 4 + 4));
+        GXY_CK(W->ohsp.ensure((size_t)cap * sizeof(Hsp)));
+        GXY_CK(W->rhsp.ensure((size_t)cap * sizeof(Hsp)));
+        GXY_CK(W->runit.ensure((size_t)cap * 4));
+        GXY_CK(W->rhsp2.ensure((size_t)cap * sizeof(Hsp)));
+        GXY_CK(W->runit2.ensure((size_t)cap * 4));
+        GXY_CK(W->perm.ensure((size_t)cap * 4));
+        GXY_CK(W->perm2.ensure((size_t)cap * 4));
+        sa.tile_counter = cnt + 0;
+        sa.cand_count = cnt + 1;
+        sa.stats = st64;
+        sa.cand_keys = W->ck0.as<uint64_t>();
+        sa.cand_vals = W->cv0.as<uint32_t>();
+        sa.cands = W->cands.as<Cand>();
+        sa.cand_cap = cap;
+
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t gexec = nullptr;
+        if (use_graph) GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+
+        GXY_CK(cudaMemsetAsync(W->counters.p, 0, 256, st));
+        GXY_CK(cudaEventRecord(W->ev[0], st));
+        launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
+        GXY_CK(cudaEventRecord(W->ev[1], st));
+        const int which = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
+                                         W->cv1.as<uint32_t>(), cnt + 1, 0, cap, passes, npass, W->ps, st);
+        const uint64_t* skeys = which ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
+        const uint32_t* sidx = which ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
+        GXY_CK(cudaMemsetAsync(W->flags.p, 0, cap, st));
+        WalkArgs wa;
+        memset(&wa, 0, sizeof(wa));
+        wa.keys = skeys;
+        wa.idx = sidx;
+        wa.cands = W->cands.as<Cand>();
+        wa.n_dev = cnt + 1;
+        wa.n_cap = cap;
+        wa.units = sa.units;
+        wa.tsegs = sa.tsegs;
+        wa.qsegs = sa.qsegs;
+        wa.seed_len = pat.len;
+        wa.sc = sa.sc;
+        wa.has_entropy = p.has_entropy;
+        wa.entropy_thr = p.entropy_thr;
+        wa.out_flag = W->flags.as<uint8_t>();
+        wa.out_hsp = W->ohsp.as<Hsp>();
+        launch_walk(wa, walk_warps, blocks_misc, st);
+        scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + 1, 0, cap, false, cnt + 2, W->ps, st);
+        launch_compact(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), W->ohsp.as<Hsp>(), sidx,
+                       W->cands.as<Cand>(), cnt + 1, cap, W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), blocks_misc, st);
+        Hsp* fin = W->rhsp.as<Hsp>();
+        uint32_t* fin_unit = W->runit.as<uint32_t>();
+        if (nu > 1) {
+            // Group by unit, keeping each unit's (diagonal, t) order: stable sort.
+            RadixPass up[4];
+            const int nup = plan_radix(0, bits_for(nu - 1), 0, 0, up, 4);
+            launch_iota(W->perm.as<uint32_t>(), cnt + 2, cap, blocks_misc, st);
+            GXY_CK(cudaMemcpyAsync(W->runit2.p, W->runit.p, (size_t)cap * 4, cudaMemcpyDeviceToDevice, st));
+            const int w2 = radix_sort_u32(W->runit2.as<uint32_t>(), W->perm.as<uint32_t>(), W->offsets.as<uint32_t>(),
+                                          W->perm2.as<uint32_t>(), cnt + 2, 0, cap, up, nup, W->ps, st);
+            const uint32_t* perm = w2 ? W->perm2.as<uint32_t>() : W->perm.as<uint32_t>();
+            launch_gather_hsp(W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), perm, cnt + 2, cap, W->rhsp2.as<Hsp>(),
+                              W->runit2.as<uint32_t>(), blocks_misc, st);
+            fin = W->rhsp2.as<Hsp>();
+            fin_unit = W->runit2.as<uint32_t>();
+        }
+        launch_fixup(fin, fin_unit, cnt + 2, cap, W->flags.as<uint8_t>(), blocks_misc, st);
+        GXY_CK(cudaEventRecord(W->ev[2], st));
+        GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, 256, cudaMemcpyDeviceToHost, st));
+
+        if (use_graph) {
+            GXY_CK(cudaStreamEndCapture(st, &graph));
+            cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(graph);
+                set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+                return GXY_ECUDA;
+            }
+            e = cudaGraphLaunch(gexec, st);
+            cudaGraphExecDestroy(gexec);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                set_error(std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
+                return GXY_ECUDA;
+            }
+        }
+        GXY_CK(cudaGetLastError());
+        GXY_CK(cudaStreamSynchronize(st));
+        const uint32_t* hc = static_cast<const uint32_t*>(W->h_pinned);
+        const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + 8);
+        const uint32_t ncand = hc[1];
+        if (ncand > cap) {
+            // Candidate buffer overflowed: grow and rerun (results so far are void).
+            uint64_t nc = (uint64_t)ncand + ncand / 4 + 1024;
+            if (nc >= (1ull << 31)) {
+                set_error("candidate count exceeds 2^31");
+                return GXY_EUNSUPPORTED;
+            }
+            W->cand_cap = (uint32_t)nc;
+            continue;
+        }
+        const uint32_t nh = hc[2];
+        out.stats.windows = hs[0];
+        out.stats.raw_hits = hs[1];
+        out.stats.candidates = ncand;
+        out.stats.hsps = nh;
+        float ms = 0.f, ms_screen = 0.f;
+        cudaEventElapsedTime(&ms, W->ev[0], W->ev[2]);
+        cudaEventElapsedTime(&ms_screen, W->ev[0], W->ev[1]);
+        out.stats.device_ms = ms;
+        out.stats.screen_ms = ms_screen;
+        out.hsps.resize(nh);
+        out.unit.resize(nh);
+        if (nh) {
+            GXY_CK(cudaMemcpyAsync(out.hsps.data(), fin, (size_t)nh * sizeof(Hsp), cudaMemcpyDeviceToHost, st));
+            GXY_CK(cudaMemcpyAsync(out.unit.data(), fin_unit, (size_t)nh * 4, cudaMemcpyDeviceToHost, st));
+            GXY_CK(cudaStreamSynchronize(st));
+        }
+        return GXY_OK;
+    }
+    set_error("candidate buffer did not converge");
+    return GXY_ENOMEM;
+}
+
+}  // namespace gxy

@@ -1,0 +1,124 @@
+// gxy_engine.cuh -- host-side engine shared by the plain, batched and serving
+// entry points.
+#pragma once
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gxy_device.cuh"
+#include "gxy_kernels.cuh"
+#include "gxy_prims.cuh"
+#include "gxy_seed.h"
+
+namespace gxy {
+
+void set_error(const std::string& msg);
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need);
+    void release();
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct Worker {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    PrimScratch ps{};
+    DevBuf prim_sums, prim_hist;
+    DevBuf counters;              // u32[8] + u64[4]
+    DevBuf d_units, d_tsegs, d_qsegs;
+    DevBuf ck0, ck1, cv0, cv1, cands, flags, offsets, ohsp;
+    DevBuf rhsp, runit, rhsp2, runit2, perm, perm2;
+    uint32_t cand_cap = 0;
+    uint32_t res_cap = 0;
+    void* h_pinned = nullptr;     // small host staging
+    size_t h_pinned_bytes = 0;
+    // Host-query staging for gxy_search.
+    gxy_dseq* qstage = nullptr;
+    gxy_dseq* tstage = nullptr;
+    std::vector<gxy_dseq*> rc_tmp;
+};
+
+// One unit as the engine plans it (host side).
+struct UnitPlan {
+    uint32_t tseg;
+    uint32_t qseg;
+    const uint32_t* starts;
+    const uint32_t* positions;
+    uint32_t nwin;
+    uint32_t primary_lo;
+    uint32_t primary_hi;
+};
+
+struct RunResult {
+    std::vector<gxy_hsp> hsps;
+    std::vector<uint32_t> unit;
+    gxy_stats stats{};
+};
+
+}  // namespace gxy
+
+struct gxy_dseq {
+    gxy_ctx* ctx = nullptr;
+    void* alloc = nullptr;
+    size_t bytes = 0;
+    uint64_t* codes = nullptr;
+    uint32_t* valid = nullptr;
+    uint32_t* mask = nullptr;
+    uint64_t len = 0;
+    uint64_t nwords = 0;   // 32-position words, pads included
+};
+
+struct gxy_table {
+    gxy_ctx* ctx = nullptr;
+    gxy_dseq* owned = nullptr;
+    const gxy_dseq* seq = nullptr;
+    uint64_t lo = 0, hi = 0;
+    uint32_t* starts = nullptr;
+    uint32_t* positions = nullptr;
+    uint64_t num_words = 0;
+    uint64_t npos = 0;
+    gxy::Pattern pat{};
+    uint32_t step = 1;
+    const void* hc = nullptr;
+    const void* hv = nullptr;
+    const void* hm = nullptr;
+    uint64_t hlen = 0;
+};
+
+struct gxy_ctx {
+    int device = 0;
+    int sm_count = 148;
+    std::mutex mu;
+    std::vector<gxy::Worker*> free_workers;
+    std::vector<gxy::Worker*> all_workers;
+    gxy_tuning tuning{8, 64, 2, 8};
+};
+
+namespace gxy {
+
+Worker* checkout(gxy_ctx* ctx, gxy_status* err);
+void checkin(gxy_ctx* ctx, Worker* w);
+
+gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t st);
+void dseq_destroy(gxy_dseq* s);
+gxy_status dseq_fill_host(gxy_dseq* d, const gxy_packed_seq* h, cudaStream_t st);
+SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi);
+
+// Validates params and the i32 envelope for a search over sequences whose
+// diagonal spans are at most max_cols columns.
+gxy_status check_params(const gxy_search_params* p, uint64_t max_cols);
+
+// Runs units through screen -> sort -> walk -> compaction on worker W.
+gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units, std::vector<SeqView>& tsegs,
+                     std::vector<SeqView>& qsegs, const Pattern& pat, const gxy_search_params& p, bool use_graph,
+                     RunResult& out);
+
+}  // namespace gxy

@@ -1,0 +1,104 @@
+// gxy_kernels.cuh -- launch interfaces of the seed->HSP kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gxy_device.cuh"
+
+namespace gxy {
+
+// Seed pattern as the kernels read it (src/seeds.rs:20-100).
+struct Pattern {
+    uint32_t len;         // L <= 32
+    uint32_t weight;      // care positions, <= kMaxWeight
+    uint32_t care_mask;   // bit i set when offset i is a care position
+    uint8_t care[16];     // care offsets, leftmost first
+};
+
+// --- packing -----------------------------------------------------------------
+// PackedSeq::from_ascii (src/sequences.rs:89-131): n ASCII bytes -> a device
+// sequence laid out as gxy_device.cuh describes.
+void launch_pack_ascii(const uint8_t* ascii, uint64_t n, uint64_t* codes, uint32_t* valid, uint32_t* mask,
+                       cudaStream_t st);
+// PackedSeq::reverse_complement (src/sequences.rs:303-318).
+void launch_reverse_complement(const uint64_t* icodes, const uint32_t* ivalid, const uint32_t* imask,
+                               uint64_t n, uint64_t* ocodes, uint32_t* ovalid, uint32_t* omask,
+                               cudaStream_t st);
+
+// --- table build (src/pos_table.rs:35-136) -----------------------------------
+// Seed words of the windows k*step of a view; key = word, or num_words for a
+// window that is not seedable; val = view-local position.  counts[word]++.
+void launch_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t num_words_sentinel,
+                       uint32_t* keys, uint32_t* vals, uint32_t* counts, cudaStream_t st);
+// prune_hot_words: counts2[w] = bucket size when <= limit, else 0.
+void launch_prune_counts(const uint32_t* starts, uint64_t num_words, uint32_t limit, uint32_t* counts2,
+                         cudaStream_t st);
+// Moves the kept buckets into the compacted table (one thread per bucket;
+// kept buckets hold at most `limit` positions).
+void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64_t num_words,
+                       const uint32_t* new_starts, uint32_t limit, uint32_t* new_positions, cudaStream_t st);
+
+// --- search ------------------------------------------------------------------
+struct ScreenArgs {
+    const UnitDev* units;
+    const SeqView* tsegs;
+    const SeqView* qsegs;
+    uint32_t n_units;
+    uint32_t n_tiles;
+    uint32_t* tile_counter;
+    Pattern pat;
+    uint32_t step;
+    uint32_t n_var;
+    uint32_t var_xor[kMaxVariants];
+    Score sc;
+    uint32_t cap;          // columns per side before a hit is deferred
+    uint32_t qkey_total;   // size of the query key axis
+    uint64_t* cand_keys;
+    uint32_t* cand_vals;
+    Cand* cands;
+    uint32_t cand_cap;
+    uint32_t* cand_count;
+    unsigned long long* stats;   // [0] windows, [1] raw hits
+};
+// Fused hit enumeration and capped lane-per-hit x-drop.  grid = persistent.
+void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);
+
+struct WalkArgs {
+    const uint64_t* keys;      // candidate keys in sorted order
+    const uint32_t* idx;       // candidate index per sorted position
+    const Cand* cands;
+    const uint32_t* n_dev;     // candidate count (clamped to n_cap)
+    uint32_t n_cap;
+    const UnitDev* units;
+    const SeqView* tsegs;
+    const SeqView* qsegs;
+    uint32_t seed_len;
+    Score sc;
+    uint32_t has_entropy;
+    int32_t entropy_thr;
+    uint8_t* out_flag;         // per sorted position: 1 = emitted and kept
+    Hsp* out_hsp;              // per sorted position
+};
+// Diagonal suppression (src/diag_hash.rs:34-53 as used at
+// src/seed_search.rs:318-342) over the candidates sorted by (diagonal, t),
+// one warp per diagonal segment.
+void launch_walk(const WalkArgs& a, int warps_per_block, int blocks, cudaStream_t st);
+
+// Gathers the kept HSPs: out[offsets[i]] = hsp[i], out_unit likewise.
+void launch_compact(const uint8_t* flag, const uint32_t* offsets, const Hsp* hsp, const uint32_t* idx,
+                    const Cand* cands, const uint32_t* n_dev, uint32_t n_cap, Hsp* out, uint32_t* out_unit,
+                    int blocks, cudaStream_t st);
+// Orders each (unit, diagonal) run by (t_start, length, score).
+void launch_fixup(Hsp* hsp, const uint32_t* unit, const uint32_t* n_dev, uint32_t n_cap, uint8_t* head_scratch,
+                  int blocks, cudaStream_t st);
+// Gathers records by a permutation.
+void launch_gather_hsp(const Hsp* in, const uint32_t* in_unit, const uint32_t* perm, const uint32_t* n_dev,
+                       uint32_t n_cap, Hsp* out, uint32_t* out_unit, int blocks, cudaStream_t st);
+void launch_iota(uint32_t* v, const uint32_t* n_dev, uint32_t n_cap, int blocks, cudaStream_t st);
+
+// --- x-drop of given hits (test entry) ---------------------------------------
+void launch_extend_hits(SeqView T, SeqView Q, Score sc, const uint32_t* tpos, const uint32_t* qpos, uint64_t n,
+                        uint32_t seed_len, uint32_t mode, Hsp* out, uint8_t* ok, cudaStream_t st);
+
+}  // namespace gxy

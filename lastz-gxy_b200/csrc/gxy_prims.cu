@@ -1,0 +1,317 @@
+// gxy_prims.cu -- fixed-grid scan and stable LSD radix sort (see gxy_prims.cuh).
+#include "gxy_prims.cuh"
+
+#include "gxy_device.cuh"
+
+namespace gxy {
+
+namespace {
+
+__device__ __forceinline__ uint64_t read_n(const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap) {
+    if (!n_dev) return n_host;
+    uint64_t n = *n_dev;
+    return n < n_cap ? n : n_cap;
+}
+
+// The contiguous range [beg, end) of block b when n items are split into
+// `grid` ranges of whole `tile`s.
+__device__ __forceinline__ void block_range(uint64_t n, uint64_t tile, uint64_t& beg, uint64_t& end) {
+    const uint64_t ntiles = (n + tile - 1) / tile;
+    const uint64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
+    beg = min(n, (uint64_t)blockIdx.x * per * tile);
+    end = min(n, beg + per * tile);
+}
+
+// Block-wide exclusive scan of one u32 per thread; returns the exclusive
+// prefix and writes the block total to *total_out (shared).
+template <int NT>
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t* total_out) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = lane < NT / 32 ? s_warp[lane] : 0;
+        uint32_t t = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < NT / 32) s_warp[lane] = t - s;
+        if (lane == NT / 32 - 1) *total_out = t;
+    }
+    __syncthreads();
+    const uint32_t r = s_warp[w] + x - v;
+    __syncthreads();
+    return r;
+}
+
+template <typename T>
+__global__ __launch_bounds__(kScanThreads) void k_scan_reduce(const T* in, const uint32_t* n_dev,
+                                                               uint64_t n_host, uint64_t n_cap,
+                                                               uint32_t* block_sums) {
+    const uint64_t n = read_n(n_dev, n_host, n_cap);
+    uint64_t beg, end;
+    block_range(n, (uint64_t)kScanThreads * kScanItems, beg, end);
+    uint32_t s = 0;
+    for (uint64_t i = beg + threadIdx.x; i < end; i += kScanThreads) s += (uint32_t)in[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    __shared__ uint32_t s_w[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int i = 0; i < kScanThreads / 32; i++) t += s_w[i];
+        block_sums[blockIdx.x] = t;
+    }
+}
+
+// Single-block exclusive scan of a short array in place; a[n] = total.
+__global__ __launch_bounds__(1024) void k_scan_small(uint32_t* a, int n) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
+    uint32_t carry = 0;
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + threadIdx.x;
+        const uint32_t v = i < n ? a[i] : 0;
+        const uint32_t ex = block_excl_scan<1024>(v, s_warp, &s_total);
+        if (i < n) a[i] = carry + ex;
+        carry += s_total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) a[n] = carry;
+}
+
+template <typename T>
+__global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_t* out, const uint32_t* n_dev,
+                                                             uint64_t n_host, uint64_t n_cap,
+                                                             const uint32_t* block_sums,
+                                                             int write_total_at_n, uint32_t* total) {
+    const uint64_t n = read_n(n_dev, n_host, n_cap);
+    uint64_t beg, end;
+    block_range(n, (uint64_t)kScanThreads * kScanItems, beg, end);
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
+    uint32_t carry = block_sums[blockIdx.x];
+    for (uint64_t base = beg; base < end; base += (uint64_t)kScanThreads * kScanItems) {
+        // Each thread takes kScanItems consecutive items.
+        const uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
+        uint32_t v[kScanItems];
+        uint32_t s = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            v[k] = (i0 + k < end) ? (uint32_t)in[i0 + k] : 0u;
+            s += v[k];
+        }
+        uint32_t ex = block_excl_scan<kScanThreads>(s, s_warp, &s_total) + carry;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            if (i0 + k < end) out[i0 + k] = ex;
+            ex += v[k];
+        }
+        carry += s_total;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+        const uint32_t t = block_sums[gridDim.x];   // total from k_scan_small
+        if (write_total_at_n) out[n] = t;
+        if (total) *total = t;
+    }
+}
+
+template <typename T>
+void scan_impl(const T* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
+               bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
+    k_scan_reduce<T><<<ps.grid, kScanThreads, 0, st>>>(in, n_dev, n_host, n_cap, ps.block_sums);
+    k_scan_small<<<1, 1024, 0, st>>>(ps.block_sums, ps.grid);
+    k_scan_down<T><<<ps.grid, kScanThreads, 0, st>>>(in, out, n_dev, n_host, n_cap, ps.block_sums,
+                                                      write_total_at_n ? 1 : 0, total);
+}
+
+// ---------------------------------------------------------------------------
+// Radix sort.
+// ---------------------------------------------------------------------------
+template <typename K>
+__global__ __launch_bounds__(kSortThreads) void k_radix_hist(const K* keys, const uint32_t* n_dev, uint64_t n_host,
+                                                              uint64_t n_cap, int shift, int bits, uint32_t* hist) {
+    const uint64_t n = read_n(n_dev, n_host, n_cap);
+    __shared__ uint32_t s_hist[kSortWarps][kRadixMax];
+    const int radix = 1 << bits;
+    const uint32_t dmask = (uint32_t)radix - 1;
+    const int w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kSortWarps * kRadixMax; i += kSortThreads) (&s_hist[0][0])[i] = 0;
+    __syncthreads();
+    uint64_t beg, end;
+    block_range(n, kSortTile, beg, end);
+    for (uint64_t i = beg + threadIdx.x; i < end; i += kSortThreads) {
+        const uint32_t d = (uint32_t)(keys[i] >> shift) & dmask;
+        atomicAdd(&s_hist[w][d], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < radix; d += kSortThreads) {
+        uint32_t s = 0;
+        for (int k = 0; k < kSortWarps; k++) s += s_hist[k][d];
+        hist[(uint64_t)d * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+template <typename K>
+struct SortSmem {
+    K keys[kSortTile];
+    uint32_t vals[kSortTile];
+    uint32_t wcnt[kSortWarps][kRadixMax];
+    uint32_t tile_excl[kRadixMax];
+    uint32_t tile_tot[kRadixMax];
+    uint32_t off[kRadixMax];
+    uint32_t warp_tmp[32];
+    uint32_t total;
+};
+
+template <typename K>
+__global__ __launch_bounds__(kSortThreads) void k_radix_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                                 K* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                                 const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
+                                                                 int shift, int bits, const uint32_t* hist) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
+    const uint64_t n = read_n(n_dev, n_host, n_cap);
+    const int radix = 1 << bits;
+    const uint32_t dmask = (uint32_t)radix - 1;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t lt = lanemask_lt();
+    uint64_t beg, end;
+    block_range(n, kSortTile, beg, end);
+    for (int d = threadIdx.x; d < kRadixMax; d += kSortThreads)
+        S.off[d] = d < radix ? hist[(uint64_t)d * gridDim.x + blockIdx.x] : 0u;
+    for (uint64_t tb = beg; tb < end; tb += kSortTile) {
+        for (int i = threadIdx.x; i < kSortWarps * kRadixMax; i += kSortThreads) (&S.wcnt[0][0])[i] = 0;
+        __syncthreads();
+        K k[kSortItems];
+        uint32_t v[kSortItems], d[kSortItems], rk[kSortItems];
+#pragma unroll
+        for (int it = 0; it < kSortItems; it++) {
+            const uint64_t idx = tb + (uint64_t)w * 32 * kSortItems + (uint64_t)it * 32 + lane;
+            const bool ok = idx < end;
+            k[it] = ok ? kin[idx] : (K)0;
+            v[it] = ok ? vin[idx] : 0u;
+            d[it] = ok ? ((uint32_t)(k[it] >> shift) & dmask) : (uint32_t)kRadixMax;
+        }
+#pragma unroll
+        for (int it = 0; it < kSortItems; it++) {
+            const uint32_t peers = __match_any_sync(kFull, d[it]);
+            uint32_t base = 0;
+            if (d[it] < (uint32_t)kRadixMax) base = S.wcnt[w][d[it]];
+            __syncwarp();
+            if (d[it] < (uint32_t)kRadixMax && (peers & lt) == 0) S.wcnt[w][d[it]] = base + __popc(peers);
+            __syncwarp();
+            rk[it] = base + __popc(peers & lt);
+        }
+        __syncthreads();
+        // Per digit: exclusive prefix over warps and the tile total.
+        {
+            const int dd = threadIdx.x;   // kSortThreads == kRadixMax
+            uint32_t run = 0;
+#pragma unroll
+            for (int ww = 0; ww < kSortWarps; ww++) {
+                const uint32_t c = S.wcnt[ww][dd];
+                S.wcnt[ww][dd] = run;
+                run += c;
+            }
+            S.tile_tot[dd] = run;
+            const uint32_t ex = block_excl_scan<kSortThreads>(run, S.warp_tmp, &S.total);
+            S.tile_excl[dd] = ex;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < kSortItems; it++) {
+            if (d[it] < (uint32_t)kRadixMax) {
+                const uint32_t p = S.tile_excl[d[it]] + S.wcnt[w][d[it]] + rk[it];
+                S.keys[p] = k[it];
+                S.vals[p] = v[it];
+            }
+        }
+        __syncthreads();
+        const uint32_t cnt = (uint32_t)min((uint64_t)kSortTile, end - tb);
+        for (uint32_t j = threadIdx.x; j < cnt; j += kSortThreads) {
+            const K key = S.keys[j];
+            const uint32_t dd = (uint32_t)(key >> shift) & dmask;
+            const uint32_t g = S.off[dd] + (j - S.tile_excl[dd]);
+            kout[g] = key;
+            vout[g] = S.vals[j];
+        }
+        __syncthreads();
+        S.off[threadIdx.x] += S.tile_tot[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+template <typename K>
+int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
+               const RadixPass* passes, int npass, const PrimScratch& ps, cudaStream_t st) {
+    static bool attr_set = false;
+    const size_t smem = sizeof(SortSmem<K>);
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    K* kin = ka;
+    uint32_t* vin = va;
+    K* kout = kb;
+    uint32_t* vout = vb;
+    for (int p = 0; p < npass; p++) {
+        const int radix = 1 << passes[p].bits;
+        k_radix_hist<K><<<ps.grid, kSortThreads, 0, st>>>(kin, n_dev, n_host, n_cap, passes[p].shift,
+                                                          passes[p].bits, ps.hist);
+        k_scan_small<<<1, 1024, 0, st>>>(ps.hist, radix * ps.grid);
+        k_radix_scatter<K><<<ps.grid, kSortThreads, smem, st>>>(kin, vin, kout, vout, n_dev, n_host, n_cap,
+                                                                passes[p].shift, passes[p].bits, ps.hist);
+        K* tk = kin; kin = kout; kout = tk;
+        uint32_t* tv = vin; vin = vout; vout = tv;
+    }
+    return (npass & 1) ? 1 : 0;
+}
+
+}  // namespace
+
+void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
+              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
+    scan_impl<uint32_t>(in, out, n_dev, n_host, n_cap, write_total_at_n, total, ps, st);
+}
+void scan_u8(const uint8_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
+             bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
+    scan_impl<uint8_t>(in, out, n_dev, n_host, n_cap, write_total_at_n, total, ps, st);
+}
+
+int plan_radix(int lo0, int w0, int lo1, int w1, RadixPass* passes, int max_passes) {
+    int np = 0;
+    const int lo[2] = {lo0, lo1}, wd[2] = {w0, w1};
+    for (int f = 0; f < 2; f++) {
+        if (wd[f] <= 0) continue;
+        const int k = (wd[f] + 7) / 8;
+        int shift = lo[f];
+        for (int i = 0; i < k; i++) {
+            const int b = wd[f] / k + (i < wd[f] % k ? 1 : 0);
+            if (np < max_passes) passes[np] = RadixPass{shift, b};
+            np++;
+            shift += b;
+        }
+    }
+    return np;
+}
+
+int radix_sort_u64(uint64_t* ka, uint32_t* va, uint64_t* kb, uint32_t* vb, const uint32_t* n_dev, uint64_t n_host,
+                   uint64_t n_cap, const RadixPass* passes, int npass, const PrimScratch& ps, cudaStream_t st) {
+    return radix_impl<uint64_t>(ka, va, kb, vb, n_dev, n_host, n_cap, passes, npass, ps, st);
+}
+int radix_sort_u32(uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, const uint32_t* n_dev, uint64_t n_host,
+                   uint64_t n_cap, const RadixPass* passes, int npass, const PrimScratch& ps, cudaStream_t st) {
+    return radix_impl<uint32_t>(ka, va, kb, vb, n_dev, n_host, n_cap, passes, npass, ps, st);
+}
+
+}  // namespace gxy

@@ -1,0 +1,654 @@
+/*
+ * oracle.c -- CPU restatement of the lastz-gxy seed->HSP path.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the timed CPU
+ * baseline.  Each function cites the reference file:line it restates.  The
+ * arithmetic is kept in the reference's order and widths: i32 saturating adds
+ * for scores, u32 positions, i64 diagonals.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <pthread.h>
+
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* PackedSeq accessors (src/sequences.rs:136-150).                          */
+/* ------------------------------------------------------------------------ */
+static inline uint32_t s_code(const orc_seq* s, uint64_t i) {
+    return (s->codes[i >> 2] >> ((i & 3) * 2)) & 3u;
+}
+static inline int s_valid(const orc_seq* s, uint64_t i) { return (s->valid[i >> 3] >> (i & 7)) & 1; }
+static inline int s_masked(const orc_seq* s, uint64_t i) { return (s->mask[i >> 3] >> (i & 7)) & 1; }
+
+static inline int32_t sat_add(int32_t a, int32_t b) {
+    int64_t r = (int64_t)a + (int64_t)b;
+    if (r > INT32_MAX) return INT32_MAX;
+    if (r < INT32_MIN) return INT32_MIN;
+    return (int32_t)r;
+}
+static inline int32_t sat_sub(int32_t a, int32_t b) {
+    int64_t r = (int64_t)a - (int64_t)b;
+    if (r > INT32_MAX) return INT32_MAX;
+    if (r < INT32_MIN) return INT32_MIN;
+    return (int32_t)r;
+}
+
+/* encode_base, src/dna.rs:12-20. */
+static inline void encode_base(uint8_t b, uint32_t* code, int* valid) {
+    switch (b) {
+        case 'A': case 'a': *code = 0; *valid = 1; return;
+        case 'C': case 'c': *code = 1; *valid = 1; return;
+        case 'G': case 'g': *code = 2; *valid = 1; return;
+        case 'T': case 't': case 'U': case 'u': *code = 3; *valid = 1; return;
+        default: *code = 0; *valid = 0; return;
+    }
+}
+
+/* PackedSeq::push_ascii, src/sequences.rs:107-131, applied over a buffer
+ * (from_ascii, :89-95).  Output buffers must be zeroed by the caller's size:
+ * codes ceil(n/4), valid and mask ceil(n/8) bytes. */
+void orc_pack_ascii(const uint8_t* ascii, uint64_t n, uint8_t* codes, uint8_t* valid,
+                    uint8_t* mask) {
+    memset(codes, 0, (n + 3) / 4);
+    memset(valid, 0, (n + 7) / 8);
+    memset(mask, 0, (n + 7) / 8);
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t c; int v;
+        uint8_t b = ascii[i];
+        encode_base(b, &c, &v);
+        codes[i >> 2] |= (uint8_t)((c & 3u) << ((i & 3) * 2));
+        if (v) valid[i >> 3] |= (uint8_t)(1u << (i & 7));
+        if (v && b >= 'a' && b <= 'z') mask[i >> 3] |= (uint8_t)(1u << (i & 7));
+    }
+}
+
+/* PackedSeq::reverse_complement, src/sequences.rs:303-318: position len-1-i of
+ * the output is the complement (!c & 3) of input position i; an invalid input
+ * position is pushed as 'N' (code 0, not valid, not masked); the mask bit
+ * moves with its base. */
+void orc_reverse_complement(const orc_seq* in, uint8_t* codes, uint8_t* valid, uint8_t* mask) {
+    uint64_t n = in->len;
+    memset(codes, 0, (n + 3) / 4);
+    memset(valid, 0, (n + 7) / 8);
+    memset(mask, 0, (n + 7) / 8);
+    for (uint64_t o = 0; o < n; o++) {
+        uint64_t i = n - 1 - o;
+        if (!s_valid(in, i)) continue;
+        uint32_t c = (~s_code(in, i)) & 3u;
+        codes[o >> 2] |= (uint8_t)(c << ((o & 3) * 2));
+        valid[o >> 3] |= (uint8_t)(1u << (o & 7));
+        if (s_masked(in, i)) mask[o >> 3] |= (uint8_t)(1u << (o & 7));
+    }
+}
+
+/* PackedSeq::slice_to_new, src/sequences.rs:277-298: invalid positions become
+ * 'N' (code 0, mask 0); valid positions keep their code and mask bit. */
+void orc_slice(const orc_seq* in, uint64_t start, uint64_t end, uint8_t* codes, uint8_t* valid,
+               uint8_t* mask) {
+    uint64_t n = end - start;
+    memset(codes, 0, (n + 3) / 4);
+    memset(valid, 0, (n + 7) / 8);
+    memset(mask, 0, (n + 7) / 8);
+    for (uint64_t o = 0; o < n; o++) {
+        uint64_t i = start + o;
+        if (!s_valid(in, i)) continue;
+        codes[o >> 2] |= (uint8_t)(s_code(in, i) << ((o & 3) * 2));
+        valid[o >> 3] |= (uint8_t)(1u << (o & 7));
+        if (s_masked(in, i)) mask[o >> 3] |= (uint8_t)(1u << (o & 7));
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Seeds (src/seeds.rs).                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* SeedPattern::parse + SeedPattern::new (src/seeds.rs:101-126), and
+ * SeedExtractor::new's care-offset list (:187-195). */
+int orc_pattern_parse(const char* pattern01, uint8_t* care, uint32_t* weight) {
+    int len = 0;
+    uint32_t w = 0;
+    for (const char* c = pattern01; *c; c++) {
+        if (*c != '0' && *c != '1') return -1;
+        if (len >= 32) return -1;
+        if (*c == '1') care[w++] = (uint8_t)len;
+        len++;
+    }
+    if (len == 0) return -1;
+    *weight = w;
+    return len;
+}
+
+/* SeedExtractor::word_at, src/seeds.rs:208-222: None when the window runs past
+ * the end or any care position is invalid or soft-masked; the leftmost care
+ * position lands in the most significant bits. */
+static inline int word_at(const orc_seq* s, const uint8_t* care, uint32_t weight, uint32_t plen,
+                          uint64_t pos, uint64_t* word) {
+    uint64_t end = pos + plen;
+    if (end > s->len) return 0;
+    uint64_t w = 0;
+    for (uint32_t i = 0; i < weight; i++) {
+        uint64_t p = pos + care[i];
+        if (!s_valid(s, p) || s_masked(s, p)) return 0;
+        w = (w << 2) | s_code(s, p);
+    }
+    *word = w;
+    return 1;
+}
+
+int orc_word_at(const orc_seq* s, const char* pattern01, uint64_t pos, uint64_t* word) {
+    uint8_t care[32]; uint32_t weight;
+    int plen = orc_pattern_parse(pattern01, care, &weight);
+    if (plen < 0) return 0;
+    return word_at(s, care, weight, (uint32_t)plen, pos, word);
+}
+
+/* ------------------------------------------------------------------------ */
+/* PosTable (src/pos_table.rs).                                             */
+/* ------------------------------------------------------------------------ */
+
+/* PosTable::build, src/pos_table.rs:35-83.  Windows come from
+ * iter_with_stride (src/seeds.rs:226-236): pos = 0, step, ... <= len-L (with
+ * len-L saturating at 0).  Count per word, exclusive prefix into starts,
+ * then scatter in ascending position order. */
+int orc_table_build(const orc_seq* s, const char* pattern01, uint32_t step, orc_table* out) {
+    memset(out, 0, sizeof(*out));
+    int plen = orc_pattern_parse(pattern01, out->care, &out->weight);
+    if (plen < 0 || out->weight > 15) return -1;
+    if (step < 1) return -2;
+    out->pattern_len = (uint32_t)plen;
+    uint64_t nw = 1ull << (2 * out->weight);
+    out->num_words = nw;
+    uint32_t* counts = (uint32_t*)calloc(nw, sizeof(uint32_t));
+    out->starts = (uint32_t*)malloc((nw + 1) * sizeof(uint32_t));
+    if (!counts || !out->starts) { free(counts); free(out->starts); return -4; }
+    uint64_t max_start = s->len > (uint64_t)plen ? s->len - (uint64_t)plen : 0;
+    uint64_t nwin = 0;
+    for (uint64_t pos = 0; pos <= max_start; pos += step) {
+        uint64_t w;
+        if (word_at(s, out->care, out->weight, (uint32_t)plen, pos, &w)) { counts[w]++; nwin++; }
+    }
+    if (nwin > 0xFFFFFFFFull) { free(counts); free(out->starts); return -3; }
+    uint32_t acc = 0;
+    for (uint64_t i = 0; i < nw; i++) { out->starts[i] = acc; acc += counts[i]; }
+    out->starts[nw] = acc;
+    out->positions = (uint32_t*)malloc((acc ? acc : 1) * sizeof(uint32_t));
+    if (!out->positions) { free(counts); free(out->starts); return -4; }
+    for (uint64_t i = 0; i < nw; i++) counts[i] = out->starts[i];
+    for (uint64_t pos = 0; pos <= max_start; pos += step) {
+        uint64_t w;
+        if (word_at(s, out->care, out->weight, (uint32_t)plen, pos, &w))
+            out->positions[counts[w]++] = (uint32_t)pos;
+    }
+    free(counts);
+    return 0;
+}
+
+/* PosTable::prune_hot_words, src/pos_table.rs:113-136: drop every bucket
+ * whose multiplicity exceeds limit and rebuild starts/positions compactly. */
+void orc_table_prune(orc_table* t, uint32_t limit) {
+    uint64_t nw = t->num_words;
+    uint32_t acc = 0;
+    uint32_t prev_start = t->starts[0];
+    for (uint64_t w = 0; w < nw; w++) {
+        uint32_t s = prev_start, e = t->starts[w + 1];
+        prev_start = e;
+        t->starts[w] = acc;
+        if (e - s <= limit) {
+            memmove(t->positions + acc, t->positions + s, (size_t)(e - s) * sizeof(uint32_t));
+            acc += e - s;
+        }
+    }
+    t->starts[nw] = acc;
+}
+
+void orc_table_free(orc_table* t) {
+    free(t->starts);
+    free(t->positions);
+    t->starts = NULL;
+    t->positions = NULL;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Scalar x-drop extension (src/hsp.rs).                                    */
+/* ------------------------------------------------------------------------ */
+
+/* column_score, src/hsp.rs:198-211. */
+static inline int32_t column_score(const orc_seq* t, const orc_seq* q, const orc_params* p,
+                                   int64_t ti, int64_t qi) {
+    if (!s_valid(t, (uint64_t)ti) || !s_valid(q, (uint64_t)qi)) return p->ambig;
+    return p->sub[s_code(t, (uint64_t)ti) * 4 + s_code(q, (uint64_t)qi)];
+}
+
+/* extend_one_side, src/hsp.rs:160-195. */
+static void extend_one_side(const orc_seq* t, const orc_seq* q, const orc_params* p, int64_t st,
+                            int64_t sq, int64_t dir, int32_t* best_out, uint32_t* ext_out) {
+    int64_t tl = (int64_t)t->len, ql = (int64_t)q->len;
+    int32_t running = 0, best = 0;
+    uint32_t best_ext = 0, ext = 0;
+    int64_t ti = st, qi = sq;
+    for (;;) {
+        if (ti < 0 || qi < 0 || ti >= tl || qi >= ql) break;
+        ext++;
+        running = sat_add(running, column_score(t, q, p, ti, qi));
+        if (running > best) {
+            best = running;
+            best_ext = ext;
+        } else if ((int64_t)best - (int64_t)running > (int64_t)p->xdrop) {
+            break;
+        }
+        ti += dir;
+        qi += dir;
+    }
+    *best_out = best;
+    *ext_out = best_ext;
+}
+
+/* extend_hit_scalar, src/hsp.rs:98-148. */
+int orc_extend_hit_scalar(const orc_seq* t, const orc_seq* q, const orc_params* p,
+                          uint32_t t_pos, uint32_t q_pos, uint32_t seed_len, orc_hsp* out) {
+    int64_t tp = t_pos, qp = q_pos, L = seed_len;
+    if (tp + L > (int64_t)t->len || qp + L > (int64_t)q->len) return 0;
+    int32_t seed = 0;
+    for (int64_t k = 0; k < L; k++) seed = sat_add(seed, column_score(t, q, p, tp + k, qp + k));
+    int32_t rb, lb;
+    uint32_t re, le;
+    extend_one_side(t, q, p, tp + L, qp + L, 1, &rb, &re);
+    extend_one_side(t, q, p, tp - 1, qp - 1, -1, &lb, &le);
+    int32_t score = sat_add(sat_add(seed, lb), rb);
+    if (score < p->hspthresh) return 0;
+    out->t_start = (uint32_t)(tp - le);
+    out->q_start = (uint32_t)(qp - le);
+    out->length = (uint32_t)(L + le + re);
+    out->score = score;
+    return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* AVX2 x-drop extension (src/hsp_simd.rs) -- the CPU baseline's extender.  */
+/* ------------------------------------------------------------------------ */
+
+#if defined(__x86_64__)
+/* PackedSeq::codes_batch, src/sequences.rs:174-212 (LUT-free but identical
+ * output: up to 16 codes from start). */
+static inline uint32_t codes_batch(const orc_seq* s, uint64_t start, uint8_t out[16]) {
+    uint64_t n = s->len > start ? s->len - start : 0;
+    if (n > 16) n = 16;
+    for (uint64_t i = 0; i < n; i++) out[i] = (uint8_t)s_code(s, start + i);
+    return (uint32_t)n;
+}
+/* PackedSeq::valid_mask_batch, src/sequences.rs:220-240. */
+static inline uint32_t valid_mask_batch(const orc_seq* s, uint64_t start) {
+    uint64_t n = s->len > start ? s->len - start : 0;
+    if (n > 16) n = 16;
+    uint32_t m = 0;
+    uint64_t i = 0;
+    while (i < n) {
+        uint64_t pos = start + i;
+        uint32_t byte = s->valid[pos >> 3];
+        uint32_t off = pos & 7;
+        uint64_t take = n - i < 8 - off ? n - i : 8 - off;
+        uint32_t chunk = (byte >> off) & ((1u << take) - 1u);
+        m |= chunk << i;
+        i += take;
+    }
+    return m;
+}
+
+/* extend_side, src/hsp_simd.rs:113-243: PSHUFB lookup of 16 columns against
+ * the i8 LUT (src/scoring.rs:102-112), blend invalid columns to the i8 ambig
+ * score, then the scalar prefix/x-drop scan. */
+__attribute__((target("avx2,sse4.1,ssse3")))
+static void extend_side_avx2(const orc_seq* t, const orc_seq* q, __m128i lut, int8_t ambig_i8,
+                             int32_t xdrop, int64_t st, int64_t sq, int64_t dir,
+                             int32_t* best_out, uint32_t* ext_out) {
+    int64_t tl = (int64_t)t->len, ql = (int64_t)q->len;
+    uint64_t max_ext;
+    if (dir > 0) {
+        if (st >= tl || sq >= ql) max_ext = 0;
+        else max_ext = (uint64_t)((tl - st) < (ql - sq) ? (tl - st) : (ql - sq));
+    } else {
+        if (st < 0 || sq < 0) max_ext = 0;
+        else max_ext = (uint64_t)((st + 1) < (sq + 1) ? (st + 1) : (sq + 1));
+    }
+    *best_out = 0;
+    *ext_out = 0;
+    if (max_ext == 0) return;
+    const __m128i ambig_v = _mm_set1_epi8(ambig_i8);
+    const __m128i low4 = _mm_set1_epi8(0x0F);
+    int32_t running = 0, best = 0;
+    uint32_t best_ext = 0, ext = 0;
+    uint64_t off = 0;
+    while (off < max_ext) {
+        uint64_t chunk = max_ext - off < 16 ? max_ext - off : 16;
+        uint8_t tc[16] = {0}, qc[16] = {0}, inv[16] = {0};
+        if (dir > 0) {
+            uint64_t ts = (uint64_t)(st + (int64_t)off), qs = (uint64_t)(sq + (int64_t)off);
+            codes_batch(t, ts, tc);
+            codes_batch(q, qs, qc);
+            uint32_t both = valid_mask_batch(t, ts) & valid_mask_batch(q, qs);
+            for (uint64_t i = 0; i < chunk; i++)
+                if (((both >> i) & 1u) == 0) inv[i] = 0xFF;
+        } else {
+            for (uint64_t i = 0; i < chunk; i++) {
+                int64_t ti = st - (int64_t)(off + i), qi = sq - (int64_t)(off + i);
+                tc[i] = (uint8_t)s_code(t, (uint64_t)ti);
+                qc[i] = (uint8_t)s_code(q, (uint64_t)qi);
+                if (!s_valid(t, (uint64_t)ti) || !s_valid(q, (uint64_t)qi)) inv[i] = 0xFF;
+            }
+        }
+        for (uint64_t i = chunk; i < 16; i++) inv[i] = 0xFF;
+        __m128i tv = _mm_loadu_si128((const __m128i*)tc);
+        __m128i qv = _mm_loadu_si128((const __m128i*)qc);
+        __m128i idx = _mm_and_si128(_mm_or_si128(_mm_slli_epi16(tv, 2), qv), low4);
+        __m128i sc = _mm_shuffle_epi8(lut, idx);
+        __m128i blended = _mm_blendv_epi8(sc, ambig_v, _mm_loadu_si128((const __m128i*)inv));
+        int8_t d[16];
+        _mm_storeu_si128((__m128i*)d, blended);
+        for (uint64_t i = 0; i < chunk; i++) {
+            ext++;
+            running = sat_add(running, (int32_t)d[i]);
+            if (running > best) {
+                best = running;
+                best_ext = ext;
+            } else if (sat_sub(best, running) > xdrop) {
+                *best_out = best;
+                *ext_out = best_ext;
+                return;
+            }
+        }
+        off += chunk;
+    }
+    *best_out = best;
+    *ext_out = best_ext;
+}
+
+static int i8_safe(const orc_params* p) {
+    for (int i = 0; i < 16; i++)
+        if (p->sub[i] < -128 || p->sub[i] > 127) return 0;
+    return p->ambig >= -128 && p->ambig <= 127;
+}
+
+/* extend_hit_avx2, src/hsp_simd.rs:27-95. */
+__attribute__((target("avx2,sse4.1,ssse3")))
+int orc_extend_hit_avx2(const orc_seq* t, const orc_seq* q, const orc_params* p,
+                        uint32_t t_pos, uint32_t q_pos, uint32_t seed_len, orc_hsp* out) {
+    int64_t tp = t_pos, qp = q_pos, L = seed_len;
+    if (tp + L > (int64_t)t->len || qp + L > (int64_t)q->len) return 0;
+    int8_t lutb[16];
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) lutb[(r << 2) | c] = (int8_t)p->sub[r * 4 + c];
+    __m128i lut = _mm_loadu_si128((const __m128i*)lutb);
+    int32_t seed = 0;
+    for (int64_t k = 0; k < L; k++) seed = sat_add(seed, column_score(t, q, p, tp + k, qp + k));
+    int32_t rb, lb;
+    uint32_t re, le;
+    extend_side_avx2(t, q, lut, (int8_t)p->ambig, p->xdrop, tp + L, qp + L, 1, &rb, &re);
+    extend_side_avx2(t, q, lut, (int8_t)p->ambig, p->xdrop, tp - 1, qp - 1, -1, &lb, &le);
+    int32_t score = sat_add(sat_add(seed, lb), rb);
+    if (score < p->hspthresh) return 0;
+    out->t_start = (uint32_t)(tp - le);
+    out->q_start = (uint32_t)(qp - le);
+    out->length = (uint32_t)(L + le + re);
+    out->score = score;
+    return 1;
+}
+
+int orc_has_avx2(void) { return __builtin_cpu_supports("avx2") ? 1 : 0; }
+#else
+int orc_extend_hit_avx2(const orc_seq* t, const orc_seq* q, const orc_params* p,
+                        uint32_t t_pos, uint32_t q_pos, uint32_t seed_len, orc_hsp* out) {
+    return orc_extend_hit_scalar(t, q, p, t_pos, q_pos, seed_len, out);
+}
+int orc_has_avx2(void) { return 0; }
+static int i8_safe(const orc_params* p) { (void)p; return 0; }
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Entropy gate (src/entropy.rs:27-67).                                     */
+/* ------------------------------------------------------------------------ */
+double orc_shannon_entropy(const orc_seq* s, uint64_t start, uint64_t end) {
+    uint32_t counts[4] = {0, 0, 0, 0};
+    uint32_t total = 0;
+    uint64_t e = end < s->len ? end : s->len;
+    for (uint64_t i = start; i < e; i++)
+        if (s_valid(s, i)) { counts[s_code(s, i)]++; total++; }
+    if (total == 0) return 0.0;
+    double tt = (double)total, h = 0.0;
+    for (int k = 0; k < 4; k++) {
+        if (counts[k] == 0) continue;
+        double pk = (double)counts[k] / tt;
+        h -= pk * log2(pk);
+    }
+    return h;
+}
+
+int orc_passes_entropy_gate(const orc_seq* s, uint32_t t_start, uint32_t t_end, int32_t score,
+                            int32_t threshold) {
+    double h = orc_shannon_entropy(s, t_start, t_end);
+    double scaled = (double)score * (h / 2.0);
+    return scaled >= (double)threshold;
+}
+
+/* ------------------------------------------------------------------------ */
+/* DiagHash (src/diag_hash.rs:19-53): map diagonal -> next admissible t.     */
+/* Open addressing over i64 keys; only get/insert are used, as in the       */
+/* reference, so the container's iteration order never matters.            */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int64_t* keys;
+    uint32_t* vals;
+    uint8_t* used;
+    uint64_t cap, n;
+} diag_hash;
+
+static inline uint64_t mix64(uint64_t x) {
+    x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27; x *= 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+static int dh_init(diag_hash* h, uint64_t cap) {
+    h->cap = cap; h->n = 0;
+    h->keys = (int64_t*)malloc(cap * sizeof(int64_t));
+    h->vals = (uint32_t*)malloc(cap * sizeof(uint32_t));
+    h->used = (uint8_t*)calloc(cap, 1);
+    return h->keys && h->vals && h->used ? 0 : -1;
+}
+static void dh_free(diag_hash* h) { free(h->keys); free(h->vals); free(h->used); }
+static inline uint64_t dh_find(const diag_hash* h, int64_t k) {
+    uint64_t i = mix64((uint64_t)k) & (h->cap - 1);
+    while (h->used[i] && h->keys[i] != k) i = (i + 1) & (h->cap - 1);
+    return i;
+}
+/* admit, src/diag_hash.rs:34-37. */
+static inline int dh_admit(const diag_hash* h, uint32_t t, uint32_t q) {
+    int64_t d = (int64_t)t - (int64_t)q;
+    uint64_t i = dh_find(h, d);
+    return !h->used[i] || t >= h->vals[i];
+}
+static int dh_grow(diag_hash* h) {
+    diag_hash g;
+    if (dh_init(&g, h->cap * 2)) return -1;
+    for (uint64_t i = 0; i < h->cap; i++)
+        if (h->used[i]) {
+            uint64_t j = dh_find(&g, h->keys[i]);
+            g.used[j] = 1; g.keys[j] = h->keys[i]; g.vals[j] = h->vals[i]; g.n++;
+        }
+    dh_free(h);
+    *h = g;
+    return 0;
+}
+/* mark_covered, src/diag_hash.rs:43-53. */
+static inline int dh_mark_covered(diag_hash* h, uint32_t t_end, uint32_t q_end) {
+    if ((h->n + 1) * 2 > h->cap && dh_grow(h)) return -1;
+    int64_t d = (int64_t)t_end - (int64_t)q_end;
+    uint64_t i = dh_find(h, d);
+    if (h->used[i]) {
+        if (t_end > h->vals[i]) h->vals[i] = t_end;
+    } else {
+        h->used[i] = 1; h->keys[i] = d; h->vals[i] = t_end; h->n++;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* search (src/seed_search.rs:271-351).                                     */
+/* ------------------------------------------------------------------------ */
+static int hsp_cmp(const void* a, const void* b) {
+    const orc_hsp* x = (const orc_hsp*)a;
+    const orc_hsp* y = (const orc_hsp*)b;
+    int64_t dx = (int64_t)x->t_start - (int64_t)x->q_start;
+    int64_t dy = (int64_t)y->t_start - (int64_t)y->q_start;
+    if (dx != dy) return dx < dy ? -1 : 1;
+    if (x->t_start != y->t_start) return x->t_start < y->t_start ? -1 : 1;
+    if (x->length != y->length) return x->length < y->length ? -1 : 1;
+    if (x->score != y->score) return x->score < y->score ? -1 : 1;
+    return 0;
+}
+
+int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* query,
+               const orc_params* p, int use_avx2, orc_hsp** out, uint64_t* n_out,
+               orc_stats* stats) {
+    const uint32_t L = table->pattern_len, w = table->weight;
+    orc_stats st = {0, 0, 0, 0};
+    *out = NULL;
+    *n_out = 0;
+    /* shifts, src/seed_search.rs:289. */
+    uint32_t shifts[32];
+    for (uint32_t i = 0; i < w; i++) shifts[i] = 2 * (w - 1 - i);
+    /* variants capacity, src/seed_search.rs:295-299. */
+    uint32_t vcap = p->transitions == 0 ? 1 : (p->transitions == 1 ? 1 + w : 1 + w + w * (w ? w - 1 : 0) / 2);
+    uint64_t* variants = (uint64_t*)malloc(vcap * sizeof(uint64_t));
+    uint64_t cap = 1024, n = 0;
+    orc_hsp* res = (orc_hsp*)malloc(cap * sizeof(orc_hsp));
+    diag_hash dh;
+    if (!variants || !res || dh_init(&dh, 1024)) { free(variants); free(res); return -1; }
+    if (use_avx2 && !(orc_has_avx2() && i8_safe(p))) use_avx2 = 0;
+    uint32_t step = p->step ? p->step : 1;
+    uint64_t max_start = query->len > L ? query->len - L : 0;
+    for (uint64_t qpos = 0; qpos <= max_start; qpos += step) {
+        uint64_t word;
+        if (!word_at(query, table->care, w, L, qpos, &word)) continue;
+        st.windows++;
+        /* variant order, src/seed_search.rs:303-316. */
+        uint32_t nv = 0;
+        variants[nv++] = word;
+        if (p->transitions >= 1)
+            for (uint32_t i = 0; i < w; i++) variants[nv++] = word ^ (2ull << shifts[i]);
+        if (p->transitions >= 2)
+            for (uint32_t i = 0; i < w; i++)
+                for (uint32_t j = i + 1; j < w; j++)
+                    variants[nv++] = word ^ (2ull << shifts[i]) ^ (2ull << shifts[j]);
+        /* src/seed_search.rs:318-342. */
+        for (uint32_t v = 0; v < nv; v++) {
+            uint64_t vw = variants[v];
+            uint32_t b = table->starts[vw], e = table->starts[vw + 1];
+            st.raw_hits += e - b;
+            for (uint32_t j = b; j < e; j++) {
+                uint32_t tpos = table->positions[j];
+                if (!dh_admit(&dh, tpos, (uint32_t)qpos)) continue;
+                st.extended++;
+                orc_hsp h;
+                int ok = use_avx2 ? orc_extend_hit_avx2(target, query, p, tpos, (uint32_t)qpos, L, &h)
+                                  : orc_extend_hit_scalar(target, query, p, tpos, (uint32_t)qpos, L, &h);
+                if (!ok) continue;
+                if (p->has_entropy &&
+                    !orc_passes_entropy_gate(target, h.t_start, h.t_start + h.length, h.score,
+                                             p->entropy_thr))
+                    continue;
+                if (dh_mark_covered(&dh, h.t_start + h.length, h.q_start + h.length)) goto oom;
+                if (n == cap) {
+                    cap *= 2;
+                    orc_hsp* r2 = (orc_hsp*)realloc(res, cap * sizeof(orc_hsp));
+                    if (!r2) goto oom;
+                    res = r2;
+                }
+                res[n++] = h;
+                st.hsps++;
+            }
+        }
+    }
+    /* sort by (diagonal, t_start) + dedup, src/seed_search.rs:348-349; the
+     * oracle breaks key ties by (length, score) so its order is canonical. */
+    qsort(res, n, sizeof(orc_hsp), hsp_cmp);
+    {
+        uint64_t m = 0;
+        for (uint64_t i = 0; i < n; i++)
+            if (m == 0 || hsp_cmp(&res[m - 1], &res[i]) != 0) res[m++] = res[i];
+        n = m;
+    }
+    dh_free(&dh);
+    free(variants);
+    *out = res;
+    *n_out = n;
+    if (stats) *stats = st;
+    return 0;
+oom:
+    dh_free(&dh);
+    free(variants);
+    free(res);
+    return -1;
+}
+
+typedef struct {
+    int n_units;
+    const orc_table* const* tables;
+    const orc_seq* targets;
+    const orc_seq* queries;
+    const orc_params* p;
+    int use_avx2;
+    orc_hsp** out;
+    uint64_t* n_out;
+    orc_stats* stats;
+    int next;       /* next unit to run; taken under the lock */
+    int err;
+    pthread_mutex_t mu;
+} units_job;
+
+static void* units_worker(void* arg) {
+    units_job* j = (units_job*)arg;
+    for (;;) {
+        pthread_mutex_lock(&j->mu);
+        int u = j->next++;
+        pthread_mutex_unlock(&j->mu);
+        if (u >= j->n_units) break;
+        orc_stats s;
+        int r = orc_search(j->tables[u], &j->targets[u], &j->queries[u], j->p, j->use_avx2, &j->out[u],
+                           &j->n_out[u], &s);
+        if (j->stats) j->stats[u] = s;
+        if (r) {
+            pthread_mutex_lock(&j->mu);
+            j->err = 1;
+            pthread_mutex_unlock(&j->mu);
+        }
+    }
+    return NULL;
+}
+
+int orc_search_units(int n_units, const orc_table* const* tables, const orc_seq* targets,
+                     const orc_seq* queries, const orc_params* p, int use_avx2, int n_threads,
+                     orc_hsp** out, uint64_t* n_out, orc_stats* stats) {
+    units_job j;
+    j.n_units = n_units; j.tables = tables; j.targets = targets; j.queries = queries; j.p = p;
+    j.use_avx2 = use_avx2; j.out = out; j.n_out = n_out; j.stats = stats; j.next = 0; j.err = 0;
+    pthread_mutex_init(&j.mu, NULL);
+    if (n_threads < 1) n_threads = 1;
+    if (n_threads > n_units) n_threads = n_units > 0 ? n_units : 1;
+    pthread_t th[256];
+    if (n_threads > 256) n_threads = 256;
+    int started = 0;
+    for (int i = 1; i < n_threads; i++)
+        if (pthread_create(&th[started], NULL, units_worker, &j) == 0) started++;
+    units_worker(&j);
+    for (int i = 0; i < started; i++) pthread_join(th[i], NULL);
+    pthread_mutex_destroy(&j.mu);
+    return j.err ? -1 : 0;
+}
+
+void orc_free(void* ptr) { free(ptr); }

@@ -1,0 +1,263 @@
+"""ctypes view of liboracle.so -- the CPU restatement of the reference's seed->HSP path.
+
+TEST INFRASTRUCTURE ONLY.  tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline legs load this module as the checker / the timed CPU baseline; the
+product path never imports it.  Every wrapped function restates a reference
+function, cited in oracle/oracle.c.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+
+def build() -> str:
+    """Compiles liboracle.so from oracle.c with the Makefile beside it."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+class OrcSeq(C.Structure):
+    _fields_ = [("codes", C.c_void_p), ("valid", C.c_void_p), ("mask", C.c_void_p), ("len", C.c_uint64)]
+
+
+class OrcHsp(C.Structure):
+    _fields_ = [("t_start", C.c_uint32), ("q_start", C.c_uint32), ("length", C.c_uint32), ("score", C.c_int32)]
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("sub", C.c_int32 * 16),
+        ("ambig", C.c_int32),
+        ("xdrop", C.c_int32),
+        ("hspthresh", C.c_int32),
+        ("step", C.c_uint32),
+        ("transitions", C.c_uint8),
+        ("has_entropy", C.c_uint8),
+        ("pad_", C.c_uint8 * 2),
+        ("entropy_thr", C.c_int32),
+    ]
+
+
+class OrcTable(C.Structure):
+    _fields_ = [
+        ("starts", C.POINTER(C.c_uint32)),
+        ("positions", C.POINTER(C.c_uint32)),
+        ("num_words", C.c_uint64),
+        ("pattern_len", C.c_uint32),
+        ("weight", C.c_uint32),
+        ("care", C.c_uint8 * 32),
+    ]
+
+
+class OrcStats(C.Structure):
+    _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("extended", C.c_uint64), ("hsps", C.c_uint64)]
+
+
+HSP_DTYPE = np.dtype([("t_start", "<u4"), ("q_start", "<u4"), ("length", "<u4"), ("score", "<i4")])
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        P = C.POINTER
+        L.orc_pack_ascii.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_reverse_complement.argtypes = [P(OrcSeq), C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_slice.argtypes = [P(OrcSeq), C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_word_at.argtypes = [P(OrcSeq), C.c_char_p, C.c_uint64, P(C.c_uint64)]
+        L.orc_word_at.restype = C.c_int
+        L.orc_table_build.argtypes = [P(OrcSeq), C.c_char_p, C.c_uint32, P(OrcTable)]
+        L.orc_table_build.restype = C.c_int
+        L.orc_table_prune.argtypes = [P(OrcTable), C.c_uint32]
+        L.orc_table_free.argtypes = [P(OrcTable)]
+        for f in (L.orc_extend_hit_scalar, L.orc_extend_hit_avx2):
+            f.argtypes = [P(OrcSeq), P(OrcSeq), P(OrcParams), C.c_uint32, C.c_uint32, C.c_uint32, P(OrcHsp)]
+            f.restype = C.c_int
+        L.orc_has_avx2.restype = C.c_int
+        L.orc_shannon_entropy.argtypes = [P(OrcSeq), C.c_uint64, C.c_uint64]
+        L.orc_shannon_entropy.restype = C.c_double
+        L.orc_passes_entropy_gate.argtypes = [P(OrcSeq), C.c_uint32, C.c_uint32, C.c_int32, C.c_int32]
+        L.orc_passes_entropy_gate.restype = C.c_int
+        L.orc_search.argtypes = [P(OrcTable), P(OrcSeq), P(OrcSeq), P(OrcParams), C.c_int, P(P(OrcHsp)),
+                                 P(C.c_uint64), P(OrcStats)]
+        L.orc_search.restype = C.c_int
+        L.orc_search_units.argtypes = [C.c_int, P(P(OrcTable)), P(OrcSeq), P(OrcSeq), P(OrcParams), C.c_int,
+                                       C.c_int, P(P(OrcHsp)), P(C.c_uint64), P(OrcStats)]
+        L.orc_search_units.restype = C.c_int
+        L.orc_free.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+# ---------------------------------------------------------------------------
+# Sequences: (codes, valid, mask, len) numpy byte arrays in the PackedSeq layout.
+# ---------------------------------------------------------------------------
+@dataclass
+class Seq:
+    codes: np.ndarray
+    valid: np.ndarray
+    mask: np.ndarray
+    len: int
+
+    def c(self) -> OrcSeq:
+        return OrcSeq(self.codes.ctypes.data, self.valid.ctypes.data, self.mask.ctypes.data, self.len)
+
+
+def _alloc(n: int):
+    return (np.zeros((n + 3) // 4 + 8, np.uint8), np.zeros((n + 7) // 8 + 8, np.uint8),
+            np.zeros((n + 7) // 8 + 8, np.uint8))
+
+
+def pack_ascii(ascii: bytes | str) -> Seq:
+    """PackedSeq::from_ascii (src/sequences.rs:89-95)."""
+    if isinstance(ascii, str):
+        ascii = ascii.encode()
+    buf = np.frombuffer(ascii, np.uint8) if len(ascii) else np.zeros(1, np.uint8)
+    n = len(ascii)
+    c, v, m = _alloc(n)
+    lib().orc_pack_ascii(buf.ctypes.data, n, c.ctypes.data, v.ctypes.data, m.ctypes.data)
+    return Seq(c, v, m, n)
+
+
+def reverse_complement(s: Seq) -> Seq:
+    c, v, m = _alloc(s.len)
+    lib().orc_reverse_complement(C.byref(s.c()), c.ctypes.data, v.ctypes.data, m.ctypes.data)
+    return Seq(c, v, m, s.len)
+
+
+def slice_to_new(s: Seq, start: int, end: int) -> Seq:
+    c, v, m = _alloc(end - start)
+    lib().orc_slice(C.byref(s.c()), start, end, c.ctypes.data, v.ctypes.data, m.ctypes.data)
+    return Seq(c, v, m, end - start)
+
+
+def word_at(s: Seq, pattern: str, pos: int):
+    w = C.c_uint64(0)
+    ok = lib().orc_word_at(C.byref(s.c()), pattern.encode(), pos, C.byref(w))
+    return int(w.value) if ok else None
+
+
+HOXD70 = [91, -114, -31, -123, -114, 100, -125, -31, -31, -125, 100, -114, -123, -31, -114, 91]
+
+
+def params(xdrop=910, hspthresh=3000, step=1, transitions=1, entropy=None, sub=None, ambig=-100) -> OrcParams:
+    p = OrcParams()
+    for i, x in enumerate(sub if sub is not None else HOXD70):
+        p.sub[i] = x
+    p.ambig = ambig
+    p.xdrop = xdrop
+    p.hspthresh = hspthresh
+    p.step = step
+    p.transitions = transitions
+    p.has_entropy = 1 if entropy is not None else 0
+    p.entropy_thr = entropy if entropy is not None else 0
+    return p
+
+
+class Table:
+    """PosTable::build (+ prune_hot_words), src/pos_table.rs:35-136."""
+
+    def __init__(self, seq: Seq, pattern: str, step: int = 1, max_word_count: int = 0):
+        self._t = OrcTable()
+        self._seq = seq
+        r = lib().orc_table_build(C.byref(seq.c()), pattern.encode(), step, C.byref(self._t))
+        if r != 0:
+            raise ValueError(f"orc_table_build failed ({r})")
+        if max_word_count > 0:
+            lib().orc_table_prune(C.byref(self._t), max_word_count)
+        self.pattern = pattern
+        self.pattern_len = self._t.pattern_len
+
+    @property
+    def num_words(self) -> int:
+        return int(self._t.num_words)
+
+    def starts(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._t.starts, shape=(self.num_words + 1,)).copy()
+
+    def positions(self) -> np.ndarray:
+        n = int(self._t.starts[self.num_words])
+        if n == 0:
+            return np.zeros(0, np.uint32)
+        return np.ctypeslib.as_array(self._t.positions, shape=(n,)).copy()
+
+    def lookup(self, word: int) -> list[int]:
+        s = self._t.starts
+        return [int(self._t.positions[i]) for i in range(s[word], s[word + 1])]
+
+    def __del__(self):
+        try:
+            lib().orc_table_free(C.byref(self._t))
+        except Exception:
+            pass
+
+
+def extend_hit(t: Seq, q: Seq, p: OrcParams, tpos: int, qpos: int, seed_len: int, avx2: bool = False):
+    h = OrcHsp()
+    f = lib().orc_extend_hit_avx2 if avx2 else lib().orc_extend_hit_scalar
+    ok = f(C.byref(t.c()), C.byref(q.c()), C.byref(p), tpos, qpos, seed_len, C.byref(h))
+    return (h.t_start, h.q_start, h.length, h.score) if ok else None
+
+
+def shannon_entropy(s: Seq, start: int, end: int) -> float:
+    return float(lib().orc_shannon_entropy(C.byref(s.c()), start, end))
+
+
+def passes_entropy_gate(s: Seq, t_start: int, t_end: int, score: int, thr: int) -> bool:
+    return bool(lib().orc_passes_entropy_gate(C.byref(s.c()), t_start, t_end, score, thr))
+
+
+def _to_array(ptr, n: int) -> np.ndarray:
+    if n == 0:
+        return np.zeros(0, HSP_DTYPE)
+    raw = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(n * 16,))
+    return raw.view(HSP_DTYPE).copy()
+
+
+def search(table: Table, target: Seq, query: Seq, p: OrcParams, avx2: bool = False):
+    """seed_search::search (src/seed_search.rs:271-351).  Returns (hsps, stats)."""
+    out = C.POINTER(OrcHsp)()
+    n = C.c_uint64(0)
+    st = OrcStats()
+    r = lib().orc_search(C.byref(table._t), C.byref(target.c()), C.byref(query.c()), C.byref(p), 1 if avx2 else 0,
+                         C.byref(out), C.byref(n), C.byref(st))
+    if r != 0:
+        raise MemoryError("orc_search failed")
+    arr = _to_array(out, n.value)
+    lib().orc_free(out)
+    return arr, {"windows": st.windows, "raw_hits": st.raw_hits, "extended": st.extended, "hsps": st.hsps}
+
+
+def search_units(units, p: OrcParams, avx2: bool = True, threads: int = 1):
+    """Runs search over [(table, target, query)] units on `threads` POSIX threads."""
+    nu = len(units)
+    if nu == 0:
+        return [], []
+    tabs = (C.POINTER(OrcTable) * nu)(*[C.pointer(u[0]._t) for u in units])
+    ts = (OrcSeq * nu)(*[u[1].c() for u in units])
+    qs = (OrcSeq * nu)(*[u[2].c() for u in units])
+    outs = (C.POINTER(OrcHsp) * nu)()
+    ns = (C.c_uint64 * nu)()
+    sts = (OrcStats * nu)()
+    r = lib().orc_search_units(nu, tabs, ts, qs, C.byref(p), 1 if avx2 else 0, threads, outs, ns, sts)
+    if r != 0:
+        raise MemoryError("orc_search_units failed")
+    res, stats = [], []
+    for i in range(nu):
+        res.append(_to_array(outs[i], ns[i]))
+        lib().orc_free(outs[i])
+        stats.append({"windows": sts[i].windows, "raw_hits": sts[i].raw_hits, "extended": sts[i].extended,
+                      "hsps": sts[i].hsps})
+    return res, stats

@@ -1,0 +1,226 @@
+"""GPU parity: the CUDA path against the oracle, bit for bit.
+
+Shapes follow the reference's own tests (src/seed_search.rs:137-280,
+src/pos_table.rs:139-225, src/hsp.rs:213-324, tests/fixture_smoke.rs) plus the
+seeded synthetic workloads."""
+import zlib
+
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import as_tuples, homologous_pair, oracle_search, oracle_seq, orc_params, rand_ascii
+
+pytestmark = pytest.mark.gpu
+
+P12 = "1110100110010101111"
+
+
+def gpu_search(gxy, ctx, target: bytes, query: bytes, pattern, sp, matrix=None, max_word_count=0, stats=None):
+    matrix = matrix or gxy.ScoringMatrix.hoxd70()
+    T = gxy.PackedSeq.from_ascii(target)
+    Q = gxy.PackedSeq.from_ascii(query)
+    tab = gxy.PosTable.build(T, pattern, sp.step, ctx=ctx)
+    if max_word_count:
+        tab.prune_hot_words(max_word_count)
+    return gxy.search(tab, T, Q, matrix, sp, stats=stats)
+
+
+def both(gxy, ctx, target, query, pattern, sp, matrix=None, max_word_count=0):
+    matrix = matrix or gxy.ScoringMatrix.hoxd70()
+    g = gpu_search(gxy, ctx, target, query, pattern, sp, matrix, max_word_count)
+    o, _ = oracle_search(target, query, pattern, matrix, sp, max_word_count)
+    return as_tuples(g), as_tuples(o)
+
+
+# ---- known answers of src/seed_search.rs:137-280 --------------------------------
+def test_exact_match_coordinates(gxy, ctx):
+    sp = gxy.SearchParams(1, gxy.HspParams(500, 1000), 0)
+    g, o = both(gxy, ctx, b"AAAAAGATTACACATGGCATGAAAAA", b"GATTACACATGGCATG", "1" * 8, sp)
+    assert g == o
+    assert len(g) == 1 and g[0][:3] == (5, 0, 16)
+
+
+def test_transition_variants(gxy, ctx):
+    hp = gxy.HspParams(500, 50)
+    g0, o0 = both(gxy, ctx, b"AAAAACGTAAAAA", b"ACATA", "1" * 5, gxy.SearchParams(1, hp, 0))
+    g1, o1 = both(gxy, ctx, b"AAAAACGTAAAAA", b"ACATA", "1" * 5, gxy.SearchParams(1, hp, 1))
+    assert g0 == o0 == []
+    assert g1 == o1 and len(g1) > 0
+
+
+def test_no_match(gxy, ctx):
+    g, o = both(gxy, ctx, b"AAAAAAAAAA", b"CCCCCCCCCC", "1" * 5, gxy.SearchParams(1, gxy.HspParams(100, 100), 0))
+    assert g == o == []
+
+
+def test_diag_collapse(gxy, ctx):
+    sp = gxy.SearchParams(1, gxy.HspParams(500, 500), 0)
+    g, o = both(gxy, ctx, b"AAAAAGATTACACATGGCATGTCGAAAAAA", b"GATTACACATGGCATGTCGA", "1" * 7, sp)
+    assert g == o
+    assert (5, 0, 20) in [x[:3] for x in g]
+    assert len({x[0] - x[1] for x in g}) == len(g)
+
+
+def test_two_diagonals(gxy, ctx):
+    sp = gxy.SearchParams(1, gxy.HspParams(500, 500), 0)
+    g, o = both(gxy, ctx, b"AAAAGATTACACATGGAAAAAAAAAAAAGATTACACATGGTTTTT", b"GATTACACATGG", "1" * 8, sp)
+    assert g == o and len({x[0] - x[1] for x in g}) >= 2
+
+
+def test_fixture_tiny(gxy, ctx):
+    # tests/fixture_smoke.rs:15-51 at the HSP level: t_start 11, span 20.
+    sp = gxy.SearchParams(1, gxy.HspParams(910, 500), 1)
+    g, o = both(gxy, ctx, b"AAAAAAAAAAAGATTACACATGGCATGTCGAATTTTTTTTTTT", b"GATTACACATGGCATGTCGA", "1" * 12, sp)
+    assert g == o
+    assert (11, 0, 20) in [x[:3] for x in g]
+
+
+# ---- table build (src/pos_table.rs) -------------------------------------------
+@pytest.mark.parametrize("pattern,step,mwc", [("111", 1, 0), ("1111", 1, 0), ("111", 3, 0), ("1101", 2, 0),
+                                               (P12, 1, 0), (P12, 3, 0), ("111", 1, 4), (P12, 1, 2),
+                                               ("11111111101111111111"[:14], 1, 0)])
+def test_table_bit_exact(gxy, ctx, pattern, step, mwc):
+    rng = np.random.default_rng(zlib.crc32(f"{pattern}/{step}/{mwc}".encode()))
+    s = rand_ascii(rng, 20000, b"ACGTACGTacgtN", None) + b"AAAAAAAAAAAAAAAAAAAAAAAACG"
+    T = gxy.PackedSeq.from_ascii(s)
+    tab = gxy.PosTable.build(T, pattern, step, ctx=ctx)
+    if mwc:
+        tab.prune_hot_words(mwc)
+    starts, pos = tab.arrays()
+    ot = O.Table(O.pack_ascii(s), pattern, step, mwc)
+    assert np.array_equal(starts, ot.starts())
+    assert np.array_equal(pos, ot.positions())
+
+
+def test_table_known_buckets(gxy, ctx):
+    # src/pos_table.rs:144-161, :177-187, :190-197, :200-211
+    T = gxy.PackedSeq.from_ascii(b"ACGTACGT")
+    tab = gxy.PosTable.build(T, "111", 1, ctx=ctx)
+    acg = O.word_at(O.pack_ascii(b"ACGTACGT"), "111", 0)
+    assert list(tab.lookup(acg)) == [0, 4]
+    tab3 = gxy.PosTable.build(gxy.PackedSeq.from_ascii(b"ACGTACGTACGTACGT"), "111", 3, ctx=ctx)
+    assert list(tab3.lookup(acg)) == [0, 12]
+    tabn = gxy.PosTable.build(gxy.PackedSeq.from_ascii(b"ACGNACG"), "111", 1, ctx=ctx)
+    assert list(tabn.lookup(acg)) == [0, 4]
+    tp = gxy.PosTable.build(gxy.PackedSeq.from_ascii(b"AAAAAAAAAAACG"), "111", 1, ctx=ctx)
+    assert len(tp.lookup(0)) >= 9
+    tp.prune_hot_words(4)
+    assert len(tp.lookup(0)) == 0
+    assert list(tp.lookup(acg)) == [10]
+
+
+# ---- packing ------------------------------------------------------------------
+@pytest.mark.parametrize("n", [0, 1, 7, 31, 32, 33, 100, 4096, 100003])
+def test_pack_and_revcomp(gxy, ctx, n):
+    rng = np.random.default_rng(n)
+    s = rand_ascii(rng, n, b"ACGTUacgtuNnRYx-", None)
+    d = gxy.DeviceSeq.from_ascii(s, ctx=ctx)
+    h = d.to_host()
+    o = O.pack_ascii(s)
+    nb4, nb8 = (n + 3) // 4, (n + 7) // 8
+    assert bytes(h.codes[:nb4]) == bytes(o.codes[:nb4])
+    assert bytes(h.valid[:nb8]) == bytes(o.valid[:nb8])
+    assert bytes(h.mask[:nb8]) == bytes(o.mask[:nb8])
+    r = d.reverse_complement().to_host()
+    orr = O.reverse_complement(o)
+    assert bytes(r.codes[:nb4]) == bytes(orr.codes[:nb4])
+    assert bytes(r.valid[:nb8]) == bytes(orr.valid[:nb8])
+    assert bytes(r.mask[:nb8]) == bytes(orr.mask[:nb8])
+
+
+# ---- x-drop differential, the shape of src/hsp.rs:283-314 ------------------------
+@pytest.mark.parametrize("mode", [0, 1])
+def test_extend_matches_scalar(gxy, ctx, mode):
+    rng = np.random.default_rng(283 + mode)
+    m = gxy.ScoringMatrix.hoxd70()
+    for case in range(200):
+        tb = rand_ascii(rng, int(rng.integers(32, 200)), b"ACGTN")
+        qb = rand_ascii(rng, int(rng.integers(32, 200)), b"ACGTN")
+        L = int(rng.integers(4, 12))
+        xd = int(rng.integers(50, 2000))
+        tmax, qmax = len(tb) - L, len(qb) - L
+        tp, qp = tmax // 2, qmax // 2
+        T = gxy.DeviceSeq.from_ascii(tb, ctx=ctx)
+        Q = gxy.DeviceSeq.from_ascii(qb, ctx=ctx)
+        h, ok = gxy.extend_hits(T, Q, m, gxy.HspParams(xd, 0), [tp], [qp], L, mode)
+        o = O.extend_hit(O.pack_ascii(tb), O.pack_ascii(qb), O.params(xdrop=xd, hspthresh=0), tp, qp, L)
+        got = (int(h[0]["t_start"]), int(h[0]["q_start"]), int(h[0]["length"]), int(h[0]["score"])) if ok[0] else None
+        assert got == o, (case, tb, qb, L, xd)
+
+
+def test_extend_long_homology(gxy, ctx):
+    # Long extensions cross many 32-column steps and warp stage refills.
+    rng = np.random.default_rng(5)
+    m = gxy.ScoringMatrix.hoxd70()
+    for ident in (1.0, 0.97, 0.9, 0.8):
+        t, q = homologous_pair(rng, 6000, ident)
+        L = 12
+        n = min(len(t), len(q)) - L
+        tp = rng.integers(0, n, 64)
+        T, Q = gxy.DeviceSeq.from_ascii(t, ctx=ctx), gxy.DeviceSeq.from_ascii(q, ctx=ctx)
+        OT, OQ = O.pack_ascii(t), O.pack_ascii(q)
+        for mode in (0, 1):
+            h, ok = gxy.extend_hits(T, Q, m, gxy.HspParams(910, 0), tp, tp, L, mode)
+            for i in range(len(tp)):
+                o = O.extend_hit(OT, OQ, O.params(xdrop=910, hspthresh=0), int(tp[i]), int(tp[i]), L)
+                got = tuple(int(h[i][k]) for k in ("t_start", "q_start", "length", "score")) if ok[i] else None
+                assert got == o
+
+
+# ---- whole searches -------------------------------------------------------------
+@pytest.mark.parametrize("seed,transitions,step,lower,nfrac", [(1, 1, 1, 0.0, 0.0), (2, 0, 1, 0.2, 0.01),
+                                                                (3, 2, 1, 0.1, 0.0), (4, 1, 3, 0.0, 0.02),
+                                                                (5, 1, 2, 0.3, 0.005)])
+def test_random_homology(gxy, ctx, seed, transitions, step, lower, nfrac):
+    rng = np.random.default_rng(seed)
+    t, q = homologous_pair(rng, 40000, 0.8, lower=lower, nfrac=nfrac)
+    sp = gxy.SearchParams(step, gxy.HspParams(910, 3000), transitions)
+    g, o = both(gxy, ctx, t, q, P12, sp)
+    assert g == o
+    assert len(o) > 0
+
+
+def test_entropy_gate(gxy, ctx):
+    rng = np.random.default_rng(11)
+    t, q = homologous_pair(rng, 30000, 0.85)
+    t = t + b"ATATATATATATATATATATATATATATATATATATATATATATATATATATATAT" * 4
+    q = q + b"ATATATATATATATATATATATATATATATATATATATATATATATATATATATAT" * 4
+    sp = gxy.SearchParams(1, gxy.HspParams(910, 2000), 1, entropy_threshold=2500)
+    g, o = both(gxy, ctx, t, q, P12, sp)
+    assert g == o
+
+
+def test_max_word_count(gxy, ctx):
+    rng = np.random.default_rng(12)
+    t, q = homologous_pair(rng, 30000, 0.85)
+    sp = gxy.SearchParams(1, gxy.HspParams(910, 3000), 1)
+    g, o = both(gxy, ctx, t, q, P12, sp, max_word_count=1)
+    assert g == o
+
+
+def test_edge_cases(gxy, ctx):
+    sp = gxy.SearchParams(1, gxy.HspParams(910, 100), 1)
+    cases = [(b"ACGT" * 10, b""), (b"ACGT" * 10, b"ACG"), (b"", b"ACGT" * 10), (b"N" * 500, b"N" * 500),
+             (b"acgt" * 200, b"ACGT" * 200), (b"ACGTACGTACGTACGTACG", b"ACGTACGTACGTACGTACG")]
+    for t, q in cases:
+        g, o = both(gxy, ctx, t, q, P12, sp)
+        assert g == o, (t[:20], q[:20])
+
+
+def test_c1_both_strands(gxy, ctx):
+    from lastz_gxy_b200 import synth
+    pr = synth.c1()
+    t, q = pr.target.tobytes(), pr.query.tobytes()
+    sp = gxy.SearchParams()
+    T = gxy.PackedSeq.from_ascii(t)
+    Q = gxy.PackedSeq.from_ascii(q)
+    tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    Qr = Q.reverse_complement(ctx)
+    m = gxy.ScoringMatrix.hoxd70()
+    OT, OQ = O.pack_ascii(t), O.pack_ascii(q)
+    ot = O.Table(OT, P12, 1)
+    for qq, oq in ((Q, OQ), (Qr, O.reverse_complement(OQ))):
+        g = as_tuples(gxy.search(tab, T, qq, m, sp))
+        o = as_tuples(O.search(ot, OT, oq, orc_params(m, sp))[0])
+        assert g == o
