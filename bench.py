@@ -1,0 +1,332 @@
+"""Seed->HSP throughput on B200 (Mbp^2/s), one JSON line on rank 0.
+
+Workload (default): the 10 Mbp chromosome-scale plain configuration -- a 10 Mbp
+target at 41% GC with 2,000 planted repeat families, 45% soft-masked, 20
+N-blocks, against a query evolved from it to ~70% identity; seed 12of19 with
+one transition, HOXD70, xdrop 910, hspthresh 3000, both strands.  One step is
+the reference driver's per-(target, query) work: PosTable::build on the target,
+the reverse complement of the query, and one search() launch per strand.
+
+    Mbp^2 = (target Mbp) x (query Mbp) x (strands)
+
+value: device-resident inputs, CUDA-event time of each step on the library's
+primary stream, L2 flushed between steps (the step's working set, ~100 MB,
+fits in the 126 MB L2).  e2e: the same step through the public C ABI from host
+buffers (target and query PackedSeq copied in each step, HSPs copied out).
+
+Multi-GPU (torchrun): every rank runs its own independent copy of the workload
+(a different synthetic chromosome per rank, no collective on the data path);
+value is all ranks' Mbp^2 over the slowest rank's time ("scaling": "weak").
+--impl reference times the reference's CPU path (the oracle's AVX2 restatement
+of seed_search / PosTable, src/hsp_simd.rs via src/hsp.rs:66-87) on host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+P12 = "1110100110010101111"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _pkg():
+    if "lastz_gxy_b200" in sys.modules:
+        return sys.modules["lastz_gxy_b200"]
+    d = os.path.join(ROOT, "lastz-gxy_b200")
+    spec = importlib.util.spec_from_file_location("lastz_gxy_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["lastz_gxy_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks() -> tuple[float, str]:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the screen kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "screen_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def workload(rank: int):
+    _pkg()
+    from lastz_gxy_b200 import synth
+    pr = synth.c2(seed=2 + rank)
+    return pr.target.tobytes(), pr.query.tobytes()
+
+
+def mbp2(lt: int, lq: int, strands: int = 2) -> float:
+    return (lt / 1e6) * (lq / 1e6) * strands
+
+
+def screen_bytes(st: dict, lq: int, n_var: int) -> float:
+    """Algorithmic bytes of one screen launch (enumeration fused with x-drop):
+    0.5 B/bp query read + 8 B of starts per (window, variant) + 4 B per raw hit
+    (positions) + 3/8 B x 2 per examined column (codes + valid bits of both
+    sequences) + 44 B per candidate written (record, key, index)."""
+    return 0.5 * lq + 8.0 * n_var * st["windows"] + 4.0 * st["raw_hits"] + 0.75 * st["columns"] \
+        + 44.0 * st["candidates"]
+
+
+def run_ours(args, rank: int, world: int, device: int):
+    import torch
+    g = _pkg()
+    torch.cuda.set_device(device)
+    ctx = g.Context(device)
+    tgt, qry = workload(rank)
+    T = g.PackedSeq.from_ascii(tgt)
+    Q = g.PackedSeq.from_ascii(qry)
+    lt, lq = len(T), len(Q)
+    m, sp = g.ScoringMatrix.hoxd70(), g.SearchParams()
+    n_var = 1 + 12
+    dT = T.to_device(ctx)
+    dQ = Q.to_device(ctx)
+    flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=f"cuda:{device}")
+
+    def step_device(collect):
+        tab = g.PosTable.build(dT, P12, 1, ctx=ctx)
+        dQr = dQ.reverse_complement()
+        for q in (dQ, dQr):
+            st = {}
+            h = g.search_device(tab, q, m, sp, stats=st)
+            collect.append((st, len(h)))
+        dQr.free()
+        tab.free()
+
+    def step_e2e(collect):
+        tab = g.PosTable.build(T, P12, 1, ctx=ctx)          # host target -> device, PosTable::build
+        dq = Q.to_device(ctx)                                 # host query -> device
+        dqr = dq.reverse_complement()
+        n = 0
+        for q in (dq, dqr):
+            h = g.search_device(tab, q, m, sp)               # HSPs come back to host
+            n += len(h)
+        collect.append(n)
+        dqr.free()
+        dq.free()
+        tab.free()
+
+    def timed(fn, k, flush_l2=True):
+        times, col = [], []
+        for _ in range(k):
+            if flush_l2:
+                flush.zero_()
+            torch.cuda.synchronize(device)
+            ctx.mark(0)
+            fn(col)
+            ctx.mark(1)
+            times.append(ctx.elapsed_ms(0, 1))
+        return times, col
+
+    barrier = (lambda: torch.distributed.barrier()) if world > 1 else (lambda: None)
+    for _ in range(args.warmup):
+        step_device([])
+        step_e2e([])
+    launches0 = g.lib().gxy_kernel_launches()
+    with ClockSampler(device) as clk:
+        barrier()
+        torch.cuda.synchronize(device)
+        dev_times, dev_col = timed(step_device, args.steps)
+        torch.cuda.synchronize(device)
+        barrier()
+        launches = (g.lib().gxy_kernel_launches() - launches0) // args.steps
+        e2e_times, e2e_col = timed(step_e2e, args.steps)
+        torch.cuda.synchronize(device)
+        barrier()
+    total_ms = sum(dev_times)
+    e2e_ms = sum(e2e_times)
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=f"cuda:{device}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+    per_step = mbp2(lt, lq)
+    value = world * per_step * args.steps / (total_ms / 1e3)
+    e2e_value = world * per_step * args.steps / (e2e_ms / 1e3)
+    # Roofline of the dominant kernel (the screen), from the timed steps.
+    stats = [s for s, _ in dev_col]
+    scr_ms = statistics.mean(s["screen_ms"] for s in stats)
+    scr_bytes = statistics.mean(screen_bytes(s, lq, n_var) for s in stats)
+    peak, peak_kind = peaks()
+    achieved = scr_bytes / (scr_ms / 1e3) / 1e9
+    tr = profiled_traffic()
+    raw = statistics.mean(s["raw_hits"] for s in stats)
+    nh = sum(n for _, n in dev_col) / args.steps
+    h2d = (T.codes.nbytes + T.valid.nbytes + T.mask.nbytes) + (Q.codes.nbytes + Q.valid.nbytes + Q.mask.nbytes)
+    d2h = int(sum(e2e_col) / args.steps) * 16
+    out = {
+        "metric": "seed->HSP Mbp^2/s (12of19 + 1 transition, HOXD70 910/3000, both strands, bit-exact)",
+        "value": round(value, 2), "unit": "Mbp^2/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, lastz_gxy_b200/synth.py)",
+        "config": {"workload": "plain 10 Mbp target x 10 Mbp query at ~70% identity, one launch per (target, strand)",
+                   "target_bp": lt, "query_bp": lq, "strands": 2, "seed": "12of19", "transitions": 1,
+                   "step": "PosTable::build + reverse complement + 2 search() launches",
+                   "mbp2_per_step": round(per_step, 4), "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "seed_hits_per_s": round(world * raw * 2 * args.steps / (total_ms / 1e3), 1),
+        "hsps_per_s": round(world * nh * args.steps / (total_ms / 1e3), 1),
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mbp^2/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms / args.steps, 3)},
+        "gpu_launches": int(launches * args.steps),
+        "roofline": {"bound": "hbm", "kernel": "k_screen", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": tr.get("bytes_per_launch") if tr else None,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback 6.65 TB/s",
+                     "screen_ms": round(scr_ms, 3), "algorithmic_bytes_per_launch": int(scr_bytes)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(tgt, qry, args.cpu_sample_bp, threads=2)
+    return out
+
+
+def cpu_baseline(tgt: bytes, qry: bytes, sample_bp: int, threads: int) -> dict:
+    """The oracle's AVX2 restatement of the reference path on host cores, on a bounded sample:
+    PosTable::build of the whole target plus search() of the first `sample_bp` of the query on
+    both strands (one thread per strand, the reference's unit of parallelism); the table build is
+    amortised over the query's share the sample covers."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    T = O.pack_ascii(tgt)
+    qs = O.pack_ascii(qry[:sample_bp])
+    qr = O.reverse_complement(qs)
+    t0 = time.perf_counter()
+    tab = O.Table(T, P12, 1)
+    t_table = time.perf_counter() - t0
+    p = O.params()
+    t0 = time.perf_counter()
+    O.search_units([(tab, T, qs), (tab, T, qr)], p, avx2=True, threads=threads)
+    t_search = time.perf_counter() - t0
+    frac = sample_bp / len(qry)
+    secs = t_search + t_table * frac
+    v = mbp2(len(tgt), sample_bp) / secs
+    return {"value": round(v, 3), "unit": "Mbp^2/s", "cores": threads, "kind": "port",
+            "sample": f"table of the full {len(tgt)} bp target + first {sample_bp} bp of the query, both strands; "
+                      f"table time amortised by {frac:.3f}; table {t_table:.2f}s, search {t_search:.2f}s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (oracle AVX2 port) on the same workload."""
+    tgt, qry = workload(0)
+    threads = 2
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(tgt, qry, args.cpu_sample_bp, threads)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.mean(x["value"] for x in vals)
+    per_step = mbp2(len(tgt), args.cpu_sample_bp)
+    return {
+        "impl": "reference",
+        "metric": "seed->HSP Mbp^2/s (12of19 + 1 transition, HOXD70 910/3000, both strands, bit-exact)",
+        "value": round(v, 3), "unit": "Mbp^2/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(per_step / v * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, lastz_gxy_b200/synth.py)",
+        "config": {"workload": "plain 10 Mbp target x 10 Mbp query at ~70% identity, one launch per (target, strand)",
+                   "target_bp": len(tgt), "query_bp": len(qry), "strands": 2},
+        "cpu_baseline": {"value": round(v, 3), "unit": "Mbp^2/s", "cores": threads, "kind": "port",
+                         "sample": vals[0]["sample"]},
+        "e2e": {"value": round(v, 3), "unit": "Mbp^2/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-bp", type=int, default=500_000)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, local)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -103,11 +103,14 @@ typedef struct {
     uint64_t hsps;         /* HSPs returned */
     double device_ms;      /* CUDA-event time of the call's device work */
     double screen_ms;      /* CUDA-event time of the screen kernel alone */
+    uint64_t columns;      /* alignment columns the screen examined (seed + both sides) */
 } gxy_stats;
 
 const char* gxy_status_string(gxy_status s);
 const char* gxy_last_error(void);
 uint32_t gxy_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process. */
+uint64_t gxy_kernel_launches(void);
 
 /* ---- context ------------------------------------------------------------ */
 gxy_status gxy_ctx_create(int device, gxy_ctx** out);
@@ -122,6 +125,12 @@ typedef struct {
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
+/* Device timing on the context's primary stream -- the stream every call
+ * made from one host thread at a time runs on.  gxy_ctx_mark records CUDA
+ * event `slot` (0..15) there; gxy_ctx_elapsed_ms waits for event b and
+ * returns the milliseconds between events a and b. */
+gxy_status gxy_ctx_mark(gxy_ctx* ctx, uint32_t slot);
+gxy_status gxy_ctx_elapsed_ms(gxy_ctx* ctx, uint32_t a, uint32_t b, double* ms);
 
 /* ---- device-resident sequences ------------------------------------------- */
 /* Copies a host PackedSeq to the device. */

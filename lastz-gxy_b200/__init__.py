@@ -67,6 +67,15 @@ class Context:
         return {"screen_warps": t.screen_warps, "screen_cap": t.screen_cap,
                 "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps}
 
+    def mark(self, slot: int) -> None:
+        """Records CUDA event `slot` on the context's primary stream."""
+        check(lib().gxy_ctx_mark(self.h, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_double()
+        check(lib().gxy_ctx_elapsed_ms(self.h, a, b, C.byref(ms)))
+        return ms.value
+
     def close(self) -> None:
         if self.h:
             lib().gxy_ctx_destroy(self.h)
@@ -392,7 +401,7 @@ class PosTable:
 # ---------------------------------------------------------------------------
 def _stats(st: _lib.StatsC) -> dict:
     return {"windows": st.windows, "raw_hits": st.raw_hits, "candidates": st.candidates, "hsps": st.hsps,
-            "device_ms": st.device_ms, "screen_ms": st.screen_ms}
+            "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns}
 
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:

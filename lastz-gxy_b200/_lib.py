@@ -52,7 +52,8 @@ class HspBufC(C.Structure):
 
 class StatsC(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
-                ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double)]
+                ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double),
+                ("columns", C.c_uint64)]
 
 
 class TuningC(C.Structure):
@@ -93,10 +94,13 @@ SIGNATURES = {
     "gxy_status_string": (C.c_char_p, [C.c_int]),
     "gxy_last_error": (C.c_char_p, []),
     "gxy_abi_version": (U32, []),
+    "gxy_kernel_launches": (U64, []),
     "gxy_ctx_create": (C.c_int, [C.c_int, P(V)]),
     "gxy_ctx_destroy": (C.c_int, [V]),
     "gxy_ctx_set_tuning": (C.c_int, [V, P(TuningC)]),
     "gxy_ctx_get_tuning": (C.c_int, [V, P(TuningC)]),
+    "gxy_ctx_mark": (C.c_int, [V, U32]),
+    "gxy_ctx_elapsed_ms": (C.c_int, [V, U32, U32, P(C.c_double)]),
     "gxy_dseq_upload": (C.c_int, [V, P(PackedSeqC), P(V)]),
     "gxy_dseq_from_ascii": (C.c_int, [V, V, U64, P(V)]),
     "gxy_dseq_reverse_complement": (C.c_int, [V, V, P(V)]),

@@ -11,6 +11,7 @@ using namespace gxy;
 
 namespace gxy {
 const char* last_error();
+uint64_t launches();
 }
 
 #define API_CK(call)                                                                         \
@@ -99,7 +100,7 @@ gxy_status prune_table(gxy_table* t, uint32_t limit, Worker* W) {
     const uint64_t nw = t->num_words;
     uint32_t* new_starts = nullptr;
     uint32_t* newpos = nullptr;
-    cudaError_t e = cudaMalloc(&new_starts, (nw + 1) * 4);
+    cudaError_t e = dev_alloc((void**)&new_starts, (nw + 1) * 4, st);
     if (e != cudaSuccess) {
         set_error("table prune allocation");
         return GXY_ENOMEM;
@@ -109,20 +110,20 @@ gxy_status prune_table(gxy_table* t, uint32_t limit, Worker* W) {
     uint32_t total2 = 0;
     e = cudaMemcpyAsync(&total2, new_starts + nw, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = cudaMalloc(&newpos, (size_t)std::max<uint32_t>(total2, 1) * 4);
+    if (e == cudaSuccess) e = dev_alloc((void**)&newpos, (size_t)std::max<uint32_t>(total2, 1) * 4, st);
     if (e == cudaSuccess) {
         launch_prune_copy(t->positions, t->starts, nw, new_starts, limit, newpos, st);
         e = cudaStreamSynchronize(st);
     }
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
-        cudaFree(new_starts);
-        if (newpos) cudaFree(newpos);
+        dev_free(new_starts);
+        dev_free(newpos);
         set_error(std::string("table prune: ") + cudaGetErrorString(e));
         return GXY_ECUDA;
     }
-    cudaFree(t->starts);
-    cudaFree(t->positions);
+    dev_free(t->starts);
+    dev_free(t->positions);
     t->starts = new_starts;
     t->positions = newpos;
     t->npos = total2;
@@ -145,15 +146,17 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
     t->num_words = nw;
     t->pat = pat;
     t->step = step;
-    DevBuf keys0, vals0, keys1, vals1;
+    DevBuf& keys0 = W->tk0;
+    DevBuf& vals0 = W->tv0;
+    DevBuf& keys1 = W->tk1;
+    DevBuf& vals1 = W->tv1;
     auto fail = [&](gxy_status s) {
-        keys0.release(); vals0.release(); keys1.release(); vals1.release();
-        if (t->starts) cudaFree(t->starts);
-        if (t->positions) cudaFree(t->positions);
+        dev_free(t->starts);
+        dev_free(t->positions);
         delete t;
         return s;
     };
-    cudaError_t e = cudaMalloc(&t->starts, (nw + 1) * 4);
+    cudaError_t e = dev_alloc((void**)&t->starts, (nw + 1) * 4, st);
     if (e == cudaSuccess) e = keys0.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
     if (e == cudaSuccess) e = vals0.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
     if (e == cudaSuccess) e = keys1.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
@@ -185,7 +188,7 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
         return fail(GXY_ECUDA);
     }
     t->npos = total;
-    e = cudaMalloc(&t->positions, (size_t)std::max<uint32_t>(total, 1) * 4);
+    e = dev_alloc((void**)&t->positions, (size_t)std::max<uint32_t>(total, 1) * 4, st);
     if (e == cudaSuccess && total)
         e = cudaMemcpyAsync(t->positions, svals, (size_t)total * 4, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -198,7 +201,6 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
         set_error(std::string("table finish: ") + cudaGetErrorString(e));
         return fail(GXY_ECUDA);
     }
-    keys0.release(); vals0.release(); keys1.release(); vals1.release();
     *out = t;
     return GXY_OK;
 }
@@ -260,6 +262,7 @@ const char* gxy_status_string(gxy_status s) {
 
 const char* gxy_last_error(void) { return last_error(); }
 uint32_t gxy_abi_version(void) { return 1; }
+uint64_t gxy_kernel_launches(void) { return launches(); }
 
 gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
     if (!out) return GXY_EINVAL;
@@ -280,9 +283,22 @@ gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
         set_error(std::string("this library is built for sm_100a; device is ") + prop.name);
         return GXY_EUNSUPPORTED;
     }
+    // Keep freed pool memory reserved so repeated allocations stay cheap.
+    cudaMemPool_t pool;
+    API_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = ~0ull;
+    API_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     gxy_ctx* c = new gxy_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
+    for (int i = 0; i < 16; i++) API_CK(cudaEventCreate(&c->marks[i]));
+    gxy_status err;
+    Worker* w = checkout(c, &err);   // the primary worker
+    if (!w) {
+        delete c;
+        return err;
+    }
+    checkin(c, w);
     *out = c;
     return GXY_OK;
 }
@@ -299,13 +315,34 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         dseq_destroy(w->qstage);
         dseq_destroy(w->tstage);
         for (gxy_dseq* d : w->rc_tmp) dseq_destroy(d);
+        DevBuf* tb[] = {&w->tk0, &w->tv0, &w->tk1, &w->tv1};
+        for (DevBuf* b : tb) b->release();
         for (int i = 0; i < 4; i++)
             if (w->ev[i]) cudaEventDestroy(w->ev[i]);
         if (w->h_pinned) cudaFreeHost(w->h_pinned);
         cudaStreamDestroy(w->st);
         delete w;
     }
+    for (int i = 0; i < 16; i++)
+        if (ctx->marks[i]) cudaEventDestroy(ctx->marks[i]);
     delete ctx;
+    return GXY_OK;
+}
+
+gxy_status gxy_ctx_mark(gxy_ctx* ctx, uint32_t slot) {
+    if (!ctx || slot >= 16 || ctx->all_workers.empty()) return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    API_CK(cudaEventRecord(ctx->marks[slot], ctx->all_workers[0]->st));
+    return GXY_OK;
+}
+
+gxy_status gxy_ctx_elapsed_ms(gxy_ctx* ctx, uint32_t a, uint32_t b, double* ms) {
+    if (!ctx || a >= 16 || b >= 16 || !ms) return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    API_CK(cudaEventSynchronize(ctx->marks[b]));
+    float f = 0.f;
+    API_CK(cudaEventElapsedTime(&f, ctx->marks[a], ctx->marks[b]));
+    *ms = f;
     return GXY_OK;
 }
 
@@ -490,8 +527,8 @@ gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* po
 gxy_status gxy_table_free(gxy_table* t) {
     if (!t) return GXY_OK;
     cudaSetDevice(t->ctx->device);
-    if (t->starts) cudaFree(t->starts);
-    if (t->positions) cudaFree(t->positions);
+    dev_free(t->starts);
+    dev_free(t->positions);
     dseq_destroy(t->owned);
     delete t;
     return GXY_OK;

@@ -19,6 +19,9 @@ constexpr int kMaxWeight = 15;        // 4^15 buckets; starts[] is u32 x (2^30 +
 constexpr int kMaxVariants = 1 + 15 + 105;
 constexpr uint32_t kFull = 0xffffffffu;
 
+// Process-wide count of kernels this library launched (gxy_kernel_launches).
+void count_launch(uint64_t n = 1);
+
 // One sequence segment as the kernels see it.  `base` is the global position
 // of local position 0 (a chunk view of a target starts at kPad + chunk_lo);
 // `key_base` places the segment on a private axis of the candidate sort key

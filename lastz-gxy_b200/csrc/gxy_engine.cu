@@ -3,11 +3,15 @@
 #include "gxy_engine.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 namespace gxy {
 
 static thread_local std::string g_err;
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 void set_error(const std::string& msg) { g_err = msg; }
 const char* last_error() { return g_err.c_str(); }
 
@@ -38,6 +42,18 @@ void DevBuf::release() {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st) {
+    return cudaMallocAsync(p, bytes ? bytes : 256, st);
+}
+
+void dev_free(void* p) {
+    if (!p) return;
+    // Pool memory goes back after every stream that may still use it is done.
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, 0);
+    cudaStreamSynchronize(0);
+}
+
 gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t st) {
     gxy_dseq* d = new gxy_dseq();
     d->ctx = ctx;
@@ -47,18 +63,19 @@ gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t s
     d->nwords = nw;
     const size_t cb = align256(nw * 8), vb = align256(nw * 4);
     d->bytes = cb + 2 * vb;
-    cudaError_t e = cudaMalloc(&d->alloc, d->bytes);
+    cudaError_t e = dev_alloc(&d->alloc, d->bytes, st);
     if (e != cudaSuccess) {
         delete d;
-        set_error(std::string("cudaMalloc(sequence): ") + cudaGetErrorString(e));
+        set_error(std::string("cudaMallocAsync(sequence): ") + cudaGetErrorString(e));
         return GXY_ENOMEM;
     }
+    d->st = st;
     d->codes = static_cast<uint64_t*>(d->alloc);
     d->valid = reinterpret_cast<uint32_t*>(static_cast<char*>(d->alloc) + cb);
     d->mask = reinterpret_cast<uint32_t*>(static_cast<char*>(d->alloc) + cb + vb);
     e = cudaMemsetAsync(d->alloc, 0, d->bytes, st);
     if (e != cudaSuccess) {
-        cudaFree(d->alloc);
+        dev_free(d->alloc);
         delete d;
         set_error(std::string("cudaMemsetAsync(sequence): ") + cudaGetErrorString(e));
         return GXY_ECUDA;
@@ -69,7 +86,7 @@ gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t s
 
 void dseq_destroy(gxy_dseq* s) {
     if (!s) return;
-    if (s->alloc) cudaFree(s->alloc);
+    dev_free(s->alloc);
     delete s;
 }
 
@@ -100,8 +117,12 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     {
         std::lock_guard<std::mutex> g(ctx->mu);
         if (!ctx->free_workers.empty()) {
-            Worker* w = ctx->free_workers.back();
-            ctx->free_workers.pop_back();
+            // Prefer the primary worker so single-threaded callers share one stream.
+            auto it = ctx->free_workers.begin();
+            for (auto j = ctx->free_workers.begin(); j != ctx->free_workers.end(); ++j)
+                if (*j == ctx->all_workers[0]) it = j;
+            Worker* w = *it;
+            ctx->free_workers.erase(it);
             *err = GXY_OK;
             return w;
         }
@@ -251,7 +272,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
 
     uint32_t* cnt = W->counters.as<uint32_t>();           // [0] tiles [1] cands [2] hsps
-    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);   // [0] windows [1] raw
+    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);   // [0] windows [1] raw [2] cols
     if (W->cand_cap == 0) W->cand_cap = 1u << 20;
     const int blocks_screen = ctx->sm_count * (int)std::max<uint32_t>(1, ctx->tuning.screen_blocks_per_sm);
     const int blocks_misc = ctx->sm_count * 4;
@@ -368,6 +389,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         const uint32_t nh = hc[2];
         out.stats.windows = hs[0];
         out.stats.raw_hits = hs[1];
+        out.stats.columns = hs[2];
         out.stats.candidates = ncand;
         out.stats.hsps = nh;
         float ms = 0.f, ms_screen = 0.f;

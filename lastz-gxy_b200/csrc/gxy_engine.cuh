@@ -29,6 +29,7 @@ struct DevBuf {
 
 struct Worker {
     cudaStream_t st = nullptr;
+    DevBuf tk0, tv0, tk1, tv1;    // table-build temporaries
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     PrimScratch ps{};
     DevBuf prim_sums, prim_hist;
@@ -74,6 +75,7 @@ struct gxy_dseq {
     uint32_t* mask = nullptr;
     uint64_t len = 0;
     uint64_t nwords = 0;   // 32-position words, pads included
+    cudaStream_t st = nullptr;   // stream the allocation is ordered on
 };
 
 struct gxy_table {
@@ -97,12 +99,17 @@ struct gxy_ctx {
     int device = 0;
     int sm_count = 148;
     std::mutex mu;
-    std::vector<gxy::Worker*> free_workers;
+    std::vector<gxy::Worker*> free_workers;   // the primary worker (all_workers[0]) is taken first
     std::vector<gxy::Worker*> all_workers;
     gxy_tuning tuning{8, 64, 2, 8};
+    cudaEvent_t marks[16] = {};
 };
 
 namespace gxy {
+
+// Stream-ordered pool allocation; dev_free waits for the device first.
+cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st);
+void dev_free(void* p);
 
 Worker* checkout(gxy_ctx* ctx, gxy_status* err);
 void checkin(gxy_ctx* ctx, Worker* w);

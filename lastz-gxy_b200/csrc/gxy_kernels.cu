@@ -58,6 +58,7 @@ void launch_pack_ascii(const uint8_t* ascii, uint64_t n, uint64_t* codes, uint32
     const uint64_t nw = (n + 31) / 32;
     if (!nw) return;
     const int blocks = (int)umin64((nw + 255) / 256, 148 * 16);
+    count_launch();
     k_pack_ascii<<<blocks, 256, 0, st>>>(ascii, n, codes, valid, mask);
 }
 
@@ -112,6 +113,7 @@ void launch_reverse_complement(const uint64_t* icodes, const uint32_t* ivalid, c
     const uint64_t nw = (n + 31) / 32;
     if (!nw) return;
     const int blocks = (int)umin64((nw + 255) / 256, 148 * 16);
+    count_launch();
     k_reverse_complement<<<blocks, 256, 0, st>>>(icodes, ivalid, imask, n, ocodes, ovalid, omask);
 }
 
@@ -156,6 +158,7 @@ void launch_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, 
                        uint32_t* vals, uint32_t* counts, cudaStream_t st) {
     if (!nwin) return;
     const int blocks = (int)umin64((nwin + 255) / 256, 148 * 16);
+    count_launch();
     k_seed_words<<<blocks, 256, 0, st>>>(view, pat, step, nwin, sentinel, keys, vals, counts);
 }
 
@@ -168,6 +171,7 @@ __global__ void k_prune_counts(const uint32_t* starts, uint64_t nw, uint32_t lim
 
 void launch_prune_counts(const uint32_t* starts, uint64_t num_words, uint32_t limit, uint32_t* counts2,
                          cudaStream_t st) {
+    count_launch();
     k_prune_counts<<<148 * 8, 256, 0, st>>>(starts, num_words, limit, counts2);
 }
 
@@ -183,178 +187,351 @@ __global__ void k_prune_copy(const uint32_t* pos, const uint32_t* starts, uint64
 
 void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64_t num_words,
                        const uint32_t* new_starts, uint32_t limit, uint32_t* new_positions, cudaStream_t st) {
+    count_launch();
     k_prune_copy<<<148 * 8, 256, 0, st>>>(positions, starts, num_words, new_starts, limit, new_positions);
 }
 
 // ---------------------------------------------------------------------------
 // Screen: fused hit enumeration + capped lane-per-hit x-drop.
 //
-// One warp takes a tile of 32 consecutive query windows of one unit from a
-// global work counter.  Each lane forms its window's seed word and its
-// transition variants (src/seed_search.rs:303-316) and looks up their buckets
-// (src/pos_table.rs:102-108).  The buckets' hits are queued in shared memory
-// and drained 32 at a time, one lane per hit, so lanes share the work evenly.
-// A hit is extended with the lane x-drop up to `cap` columns per side:
+// Each warp runs a producer and 32 consumers over a shared-memory queue of
+// hits (t, q, unit).
+//  - Producer (warp-cooperative): takes tiles of 32 consecutive query windows
+//    of one unit from a global work counter, forms each window's seed word
+//    and its transition variants (src/seed_search.rs:303-316), and pushes the
+//    hits of each variant's bucket (src/pos_table.rs:102-108) into the queue.
+//  - Consumers (one lane per hit): every iteration an idle lane takes the
+//    next queued hit, and every busy lane advances its own hit by one chunk of
+//    up to 32 columns -- the seed footprint, then the right side, then the
+//    left side of extend_hit (src/hsp.rs:98-195).  All phases run the same
+//    chunk code, so lanes in different phases do not diverge.
+// A hit is extended up to `cap` columns per side:
 //  - ended below hspthresh: dropped.  Such a hit can never change the output:
 //    search() only records diagonal cover for a hit whose HSP passes
 //    (src/seed_search.rs:321-340), so whether it was admitted is irrelevant.
 //  - ended at or above hspthresh, or still running at the cap: kept as a
 //    candidate for the walk, which applies the diagonal rule in order.
 // ---------------------------------------------------------------------------
-constexpr int kQCap = 256;   // queued hits per warp
+constexpr int kRefillBelow = 96;  // the producer runs while fewer hits are queued
 
-template <int WARPS>
-__global__ __launch_bounds__(WARPS * 32) void k_screen(const __grid_constant__ ScreenArgs a) {
+enum : uint32_t { kIdle = 0, kSeed = 1, kRight = 2, kLeft = 3 };
+
+__device__ __forceinline__ uint64_t rev_pairs64(uint64_t c) {
+    c = __brevll(c);
+    return ((c >> 1) & 0x5555555555555555ull) | ((c & 0x5555555555555555ull) << 1);
+}
+
+template <int WARPS, int MINB>
+__global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_constant__ ScreenArgs a) {
+    constexpr int kQCap = WARPS >= 16 ? 128 : 256;   // queued hits per warp
     __shared__ int32_t s_lut[16];
     __shared__ uint32_t s_qt[WARPS][kQCap];
-    __shared__ uint8_t s_ql[WARPS][kQCap];
+    __shared__ uint32_t s_qq[WARPS][kQCap];
+    __shared__ uint32_t s_qu[WARPS][kQCap];
     __shared__ uint32_t s_ex[WARPS][32];
     __shared__ uint32_t s_b[WARPS][32];
+    __shared__ uint32_t s_qw[WARPS][32];
     if (threadIdx.x < 16) s_lut[threadIdx.x] = a.sc.sub[threadIdx.x];
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t lt = lanemask_lt();
     const uint32_t L = a.pat.len;
-    unsigned long long n_windows = 0, n_raw = 0;
+    const int32_t ambig = a.sc.ambig, xdrop = a.sc.xdrop, thresh = a.sc.hspthresh;
+    unsigned long long n_windows = 0, n_raw = 0, n_cols = 0;
+
+    // ---- producer state (warp-uniform, except the per-lane window data) ----
+    uint32_t head = 0, tail = 0;
+    bool exhausted = false, have_tile = false;
+    uint32_t pu = 0, v = 0, done_v = 0, total_v = 0, maxc = 0;
+    const uint32_t* p_starts = nullptr;
+    const uint32_t* p_pos = nullptr;
+    uint32_t word = 0, qwin = 0, my_b = 0, my_cnt = 0, my_ex = 0;
+    bool wv = false;
+
+    // ---- consumer state (per lane) ----
+    uint32_t phase = kIdle, ht = 0, hq = 0, hu = 0xffffffffu;
+    uint32_t pos_t = 0, pos_q = 0, rem = 0, ext = 0, bext = 0, rext = 0;
+    int32_t run = 0, best = 0, seed = 0, rbest = 0;
+    SeqView T{}, Q{};
+    uint32_t cur_unit = 0xffffffffu;
+
+    auto load_variant = [&]() {
+        my_b = 0;
+        my_cnt = 0;
+        if (wv) {
+            const uint32_t vw = word ^ a.var_xor[v];
+            my_b = __ldg(p_starts + vw);
+            my_cnt = __ldg(p_starts + vw + 1) - my_b;
+        }
+        uint32_t incl = my_cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        total_v = __shfl_sync(kFull, incl, 31);
+        my_ex = incl - my_cnt;
+        maxc = my_cnt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(kFull, maxc, o));
+        done_v = 0;
+        n_raw += lane == 0 ? total_v : 0;
+    };
 
     for (;;) {
-        uint32_t tile = 0;
-        if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
-        tile = __shfl_sync(kFull, tile, 0);
-        if (tile >= a.n_tiles) break;
-        // Unit owning this tile: last unit with tile_base <= tile.
-        uint32_t lo = 0, hi = a.n_units;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (a.units[mid].tile_base <= tile) lo = mid;
-            else hi = mid;
-        }
-        const uint32_t u = lo;
-        const UnitDev U = a.units[u];
-        const SeqView T = a.tsegs[U.tseg];
-        const SeqView Q = a.qsegs[U.qseg];
-        const uint32_t k0 = (tile - U.tile_base) * 32;
-        const uint32_t k = k0 + lane;
-        uint32_t word = 0;
-        bool wv = k < U.nwin && word_at(Q, a.pat, k * a.step, word);
-        n_windows += wv ? 1 : 0;
-
-        uint32_t fill = 0;
-        // Drains the queue: one lane per hit.
-        auto drain = [&](uint32_t cnt) {
-            for (uint32_t base = 0; base < cnt; base += 32) {
-                const uint32_t i = base + lane;
-                const bool act = i < cnt;
-                bool cand = false;
-                uint32_t t = 0, q = 0;
-                LaneExt r;
-                r.score = 0; r.lext = 0; r.rext = 0; r.done = true;
-                if (act) {
-                    t = s_qt[w][i];
-                    q = (k0 + s_ql[w][i]) * a.step;
-                    r = extend_lane(T, Q, t, q, L, a.cap, a.sc.xdrop, s_lut, a.sc.ambig);
-                    cand = !r.done || r.score >= a.sc.hspthresh;
+        // ---------------- produce ----------------
+        while (!exhausted && tail - head < (uint32_t)kRefillBelow) {
+            if (!have_tile) {
+                uint32_t tile = 0;
+                if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+                tile = __shfl_sync(kFull, tile, 0);
+                if (tile >= a.n_tiles) {
+                    exhausted = true;
+                    break;
                 }
-                const uint32_t m = __ballot_sync(kFull, cand);
-                if (m) {
-                    uint32_t slot0 = 0;
-                    if (lane == 0) slot0 = atomicAdd(a.cand_count, (uint32_t)__popc(m));
-                    slot0 = __shfl_sync(kFull, slot0, 0);
-                    if (cand) {
-                        const uint32_t slot = slot0 + __popc(m & lt);
-                        if (slot < a.cand_cap) {
-                            const uint32_t tk = T.key_base + t, qk = Q.key_base + q;
-                            a.cand_keys[slot] = ((uint64_t)(tk - qk + a.qkey_total) << 32) | tk;
-                            a.cand_vals[slot] = slot;
-                            Cand c;
-                            c.unit = u; c.t = t; c.q = q;
-                            c.flags = r.done ? 0u : kCandLong;
-                            c.lext = r.lext; c.rext = r.rext; c.score = r.score; c.pad_ = 0;
-                            a.cands[slot] = c;
-                        }
+                uint32_t lo = 0, hi = a.n_units;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (a.units[mid].tile_base <= tile) lo = mid;
+                    else hi = mid;
+                }
+                pu = lo;
+                const UnitDev U = a.units[pu];
+                p_starts = U.starts;
+                p_pos = U.positions;
+                const uint32_t k = (tile - U.tile_base) * 32 + lane;
+                qwin = k * a.step;
+                wv = false;
+                if (k < U.nwin) wv = word_at(a.qsegs[U.qseg], a.pat, qwin, word);
+                n_windows += wv ? 1 : 0;
+                s_qw[w][lane] = qwin;
+                v = 0;
+                load_variant();
+                have_tile = true;
+            }
+            while (done_v == total_v) {
+                if (++v == a.n_var) {
+                    have_tile = false;
+                    break;
+                }
+                load_variant();
+            }
+            if (!have_tile) continue;
+            const uint32_t room = (uint32_t)kQCap - (tail - head);
+            const uint32_t np = min(room, total_v - done_v);
+            if (done_v == 0 && np == total_v && maxc <= 8) {
+                // Typical case: each lane copies its own short bucket.
+                for (uint32_t j = 0; j < my_cnt; j++) {
+                    const uint32_t slot = (tail + my_ex + j) % kQCap;
+                    s_qt[w][slot] = __ldg(p_pos + my_b + j);
+                    s_qq[w][slot] = qwin;
+                    s_qu[w][slot] = pu;
+                }
+            } else {
+                // Hot buckets: all lanes copy; owner = last lane with ex <= idx.
+                s_ex[w][lane] = my_ex;
+                s_b[w][lane] = my_b;
+                __syncwarp();
+                for (uint32_t j = lane; j < np; j += 32) {
+                    const uint32_t idx = done_v + j;
+                    uint32_t lo2 = 0, hi2 = 32;
+                    while (hi2 - lo2 > 1) {
+                        const uint32_t mid = (lo2 + hi2) >> 1;
+                        if (s_ex[w][mid] <= idx) lo2 = mid;
+                        else hi2 = mid;
                     }
+                    const uint32_t slot = (tail + j) % kQCap;
+                    s_qt[w][slot] = __ldg(p_pos + s_b[w][lo2] + (idx - s_ex[w][lo2]));
+                    s_qq[w][slot] = s_qw[w][lo2];
+                    s_qu[w][slot] = pu;
                 }
             }
             __syncwarp();
-        };
+            tail += np;
+            done_v += np;
+        }
 
-        for (uint32_t v = 0; v < a.n_var; v++) {
-            uint32_t b = 0, cnt = 0;
-            if (wv) {
-                const uint32_t vw = word ^ a.var_xor[v];
-                b = __ldg(U.starts + vw);
-                cnt = __ldg(U.starts + vw + 1) - b;
-            }
-            uint32_t incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(kFull, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            if (total == 0) continue;
-            n_raw += (lane == 0) ? total : 0;
-            const uint32_t ex = incl - cnt;
-            if (fill + total > kQCap) {
-                drain(fill);
-                fill = 0;
-            }
-            uint32_t maxc = cnt;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(kFull, maxc, o));
-            if (total <= kQCap && maxc <= 8) {
-                // Typical case: each lane copies its own (short) bucket.
-                for (uint32_t j = 0; j < cnt; j++) {
-                    s_qt[w][fill + ex + j] = __ldg(U.positions + b + j);
-                    s_ql[w][fill + ex + j] = (uint8_t)lane;
+        // ---------------- assign ----------------
+        const bool idle = phase == kIdle;
+        const uint32_t im = __ballot_sync(kFull, idle);
+        const uint32_t avail = tail - head;
+        const uint32_t take = min((uint32_t)__popc(im), avail);
+        if (idle) {
+            const uint32_t rk = __popc(im & lt);
+            if (rk < take) {
+                const uint32_t slot = (head + rk) % kQCap;
+                ht = s_qt[w][slot];
+                hq = s_qq[w][slot];
+                hu = s_qu[w][slot];
+                if (hu != cur_unit) {
+                    cur_unit = hu;
+                    const UnitDev U = a.units[hu];
+                    T = a.tsegs[U.tseg];
+                    Q = a.qsegs[U.qseg];
                 }
-                __syncwarp();
-                fill += total;
-            } else {
-                // Hot buckets: all lanes copy, QCap hits at a time.
-                s_ex[w][lane] = ex;
-                s_b[w][lane] = b;
-                __syncwarp();
-                uint32_t ps = 0;
-                while (ps < total) {
-                    const uint32_t np = min(kQCap - fill, total - ps);
-                    for (uint32_t j = lane; j < np; j += 32) {
-                        const uint32_t idx = ps + j;
-                        uint32_t lo2 = 0, hi2 = 32;   // owner: last lane with ex <= idx
-                        while (hi2 - lo2 > 1) {
-                            const uint32_t mid = (lo2 + hi2) >> 1;
-                            if (s_ex[w][mid] <= idx) lo2 = mid;
-                            else hi2 = mid;
-                        }
-                        s_qt[w][fill + j] = __ldg(U.positions + s_b[w][lo2] + (idx - s_ex[w][lo2]));
-                        s_ql[w][fill + j] = (uint8_t)lo2;
-                    }
-                    __syncwarp();
-                    fill += np;
-                    ps += np;
-                    if (fill == kQCap) {
-                        drain(fill);
-                        fill = 0;
+                phase = kSeed;
+            }
+        }
+        head += take;
+        const bool busy = phase != kIdle;
+        if (!__any_sync(kFull, busy)) {
+            if (exhausted && tail == head) break;
+            continue;
+        }
+
+        // ---------------- one chunk ----------------
+        uint64_t tg = 0, qg = 0;
+        uint32_t n = 0;
+        int32_t xd = INT32_MAX;
+        const bool fwd = phase != kLeft;
+        if (phase == kSeed) {
+            tg = T.base + ht;
+            qg = Q.base + hq;
+            n = L;
+        } else if (phase == kRight) {
+            tg = T.base + pos_t;
+            qg = Q.base + pos_q;
+            n = min(32u, rem);
+            xd = xdrop;
+        } else if (phase == kLeft) {
+            tg = T.base + pos_t - 31;
+            qg = Q.base + pos_q - 31;
+            n = min(32u, rem);
+            xd = xdrop;
+        }
+        uint64_t tc = 0, qc = 0;
+        uint32_t vv = 0;
+        if (busy) {
+            tc = load_codes32(T.codes, tg);
+            qc = load_codes32(Q.codes, qg);
+            vv = load_bits32(T.valid, tg) & load_bits32(Q.valid, qg);
+            if (!fwd) {
+                tc = rev_pairs64(tc);
+                qc = rev_pairs64(qc);
+                vv = __brev(vv);
+            }
+        }
+        int32_t r = phase == kSeed ? 0 : run;
+        int32_t b = best;
+        uint32_t be = bext;
+        bool alive = busy;
+        bool ended = false;
+#pragma unroll
+        for (int g = 0; g < 4; g++) {
+            if (!__any_sync(kFull, alive && (uint32_t)(g * 8) < n)) break;
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int k = g * 8 + i;
+                if (alive && (uint32_t)k < n) {
+                    r += col_score(tc, qc, vv, k, s_lut, ambig);
+                    if (r > b) {
+                        b = r;
+                        be = ext + k + 1;
+                    } else if (b - r > xd) {
+                        alive = false;
+                        ended = true;
+                        n_cols += (unsigned long long)(k + 1);
                     }
                 }
             }
         }
-        drain(fill);
+
+        // Columns examined this chunk (the break column included), for the
+        // algorithmic byte count.
+        if (busy) n_cols += phase == kSeed ? n : (ended ? 0 : n);
+        // ---------------- bookkeeping ----------------
+        bool finish = false, cand = false, is_long = false;
+        int32_t score = 0;
+        uint32_t lext_out = 0;
+        if (busy) {
+            if (phase == kSeed) {
+                seed = r;
+                phase = kRight;
+                pos_t = ht + L;
+                pos_q = hq + L;
+                rem = min(T.len - ht - L, Q.len - hq - L);
+                run = 0; best = 0; bext = 0; ext = 0;
+            } else {
+                run = r; best = b; bext = be;
+                ext += n;
+                rem -= n;
+                const bool side_done = ended || rem == 0;
+                if (!side_done && ext >= a.cap) {
+                    finish = true;      // still extending at the cap: defer to the walk
+                    cand = true;
+                    is_long = true;
+                } else if (!side_done) {
+                    if (phase == kRight) { pos_t += n; pos_q += n; }
+                    else { pos_t -= n; pos_q -= n; }
+                } else if (phase == kRight) {
+                    rbest = best;
+                    rext = bext;
+                    phase = kLeft;
+                    pos_t = ht - 1;
+                    pos_q = hq - 1;
+                    rem = min(ht, hq);
+                    run = 0; best = 0; bext = 0; ext = 0;
+                } else {
+                    finish = true;
+                    score = seed + best + rbest;
+                    lext_out = bext;
+                    cand = score >= thresh;
+                }
+            }
+            // An empty right side goes straight to the left; an empty left side finishes.
+            if (!finish && phase == kRight && rem == 0) {
+                rbest = 0; rext = 0;
+                phase = kLeft;
+                pos_t = ht - 1;
+                pos_q = hq - 1;
+                rem = min(ht, hq);
+                run = 0; best = 0; bext = 0; ext = 0;
+            }
+            if (!finish && phase == kLeft && rem == 0) {
+                finish = true;
+                score = seed + rbest;
+                lext_out = 0;
+                cand = score >= thresh;
+            }
+        }
+        const uint32_t m = __ballot_sync(kFull, finish && cand);
+        if (m) {
+            uint32_t slot0 = 0;
+            if (lane == 0) slot0 = atomicAdd(a.cand_count, (uint32_t)__popc(m));
+            slot0 = __shfl_sync(kFull, slot0, 0);
+            if (finish && cand) {
+                const uint32_t slot = slot0 + __popc(m & lt);
+                if (slot < a.cand_cap) {
+                    const uint32_t tk = T.key_base + ht, qk = Q.key_base + hq;
+                    a.cand_keys[slot] = ((uint64_t)(tk - qk + a.qkey_total) << 32) | tk;
+                    a.cand_vals[slot] = slot;
+                    Cand c;
+                    c.unit = hu; c.t = ht; c.q = hq;
+                    c.flags = is_long ? kCandLong : 0u;
+                    c.lext = lext_out; c.rext = rext; c.score = score; c.pad_ = 0;
+                    a.cands[slot] = c;
+                }
+            }
+        }
+        if (finish) phase = kIdle;
     }
-    // Per-warp counters, one atomic each.
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n_windows += __shfl_xor_sync(kFull, n_windows, o);
+    for (int o = 16; o > 0; o >>= 1) {
+        n_windows += __shfl_xor_sync(kFull, n_windows, o);
+        n_cols += __shfl_xor_sync(kFull, n_cols, o);
+    }
     if (lane == 0) {
         atomicAdd(&a.stats[0], n_windows);
         atomicAdd(&a.stats[1], n_raw);
+        atomicAdd(&a.stats[2], n_cols);
     }
 }
 
 void launch_screen(const ScreenArgs& a, int warps, int blocks, cudaStream_t st) {
     switch (warps) {
-        case 4: k_screen<4><<<blocks, 128, 0, st>>>(a); break;
-        case 16: k_screen<16><<<blocks, 512, 0, st>>>(a); break;
-        default: k_screen<8><<<blocks, 256, 0, st>>>(a); break;
+        case 4: count_launch(); k_screen<4, 4><<<blocks, 128, 0, st>>>(a); break;
+        case 16: count_launch(); k_screen<16, 1><<<blocks, 512, 0, st>>>(a); break;
+        default: count_launch(); k_screen<8, 2><<<blocks, 256, 0, st>>>(a); break;
     }
 }
 
@@ -489,8 +666,8 @@ __global__ __launch_bounds__(WARPS * 32) void k_walk(const __grid_constant__ Wal
 
 void launch_walk(const WalkArgs& a, int warps, int blocks, cudaStream_t st) {
     switch (warps) {
-        case 4: k_walk<4><<<blocks, 128, 0, st>>>(a); break;
-        default: k_walk<8><<<blocks, 256, 0, st>>>(a); break;
+        case 4: count_launch(); k_walk<4><<<blocks, 128, 0, st>>>(a); break;
+        default: count_launch(); k_walk<8><<<blocks, 256, 0, st>>>(a); break;
     }
 }
 
@@ -508,6 +685,7 @@ __global__ void k_compact(const uint8_t* flag, const uint32_t* off, const Hsp* h
 void launch_compact(const uint8_t* flag, const uint32_t* offsets, const Hsp* hsp, const uint32_t* idx,
                     const Cand* cands, const uint32_t* n_dev, uint32_t n_cap, Hsp* out, uint32_t* out_unit,
                     int blocks, cudaStream_t st) {
+    count_launch();
     k_compact<<<blocks, 256, 0, st>>>(flag, offsets, hsp, idx, cands, n_dev, n_cap, out, out_unit);
 }
 
@@ -554,7 +732,9 @@ __global__ void k_fixup(Hsp* hsp, const uint8_t* head, const uint32_t* n_dev, ui
 
 void launch_fixup(Hsp* hsp, const uint32_t* unit, const uint32_t* n_dev, uint32_t n_cap, uint8_t* head_scratch,
                   int blocks, cudaStream_t st) {
+    count_launch();
     k_mark_runs<<<blocks, 256, 0, st>>>(hsp, unit, n_dev, n_cap, head_scratch);
+    count_launch();
     k_fixup<<<blocks, 256, 0, st>>>(hsp, head_scratch, n_dev, n_cap);
 }
 
@@ -570,6 +750,7 @@ __global__ void k_gather_hsp(const Hsp* in, const uint32_t* in_unit, const uint3
 
 void launch_gather_hsp(const Hsp* in, const uint32_t* in_unit, const uint32_t* perm, const uint32_t* n_dev,
                        uint32_t n_cap, Hsp* out, uint32_t* out_unit, int blocks, cudaStream_t st) {
+    count_launch();
     k_gather_hsp<<<blocks, 256, 0, st>>>(in, in_unit, perm, n_dev, n_cap, out, out_unit);
 }
 
@@ -579,6 +760,7 @@ __global__ void k_iota(uint32_t* v, const uint32_t* n_dev, uint32_t n_cap) {
 }
 
 void launch_iota(uint32_t* v, const uint32_t* n_dev, uint32_t n_cap, int blocks, cudaStream_t st) {
+    count_launch();
     k_iota<<<blocks, 256, 0, st>>>(v, n_dev, n_cap);
 }
 
@@ -634,9 +816,11 @@ void launch_extend_hits(SeqView T, SeqView Q, Score sc, const uint32_t* tpos, co
     if (!n) return;
     if (mode == 1) {
         const int blocks = (int)umin64((n + 7) / 8, 148 * 8);
+        count_launch();
         k_extend_warp<<<blocks, 256, 0, st>>>(T, Q, sc, tpos, qpos, n, seed_len, out, ok);
     } else {
         const int blocks = (int)umin64((n + 255) / 256, 148 * 8);
+        count_launch();
         k_extend_lane<<<blocks, 256, 0, st>>>(T, Q, sc, tpos, qpos, n, seed_len, out, ok);
     }
 }

@@ -59,7 +59,7 @@ struct ScreenArgs {
     Cand* cands;
     uint32_t cand_cap;
     uint32_t* cand_count;
-    unsigned long long* stats;   // [0] windows, [1] raw hits
+    unsigned long long* stats;   // [0] windows, [1] raw hits, [2] columns examined
 };
 // Fused hit enumeration and capped lane-per-hit x-drop.  grid = persistent.
 void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);

@@ -128,8 +128,11 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_
 template <typename T>
 void scan_impl(const T* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
                bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
+    count_launch();
     k_scan_reduce<T><<<ps.grid, kScanThreads, 0, st>>>(in, n_dev, n_host, n_cap, ps.block_sums);
+    count_launch();
     k_scan_small<<<1, 1024, 0, st>>>(ps.block_sums, ps.grid);
+    count_launch();
     k_scan_down<T><<<ps.grid, kScanThreads, 0, st>>>(in, out, n_dev, n_host, n_cap, ps.block_sums,
                                                       write_total_at_n ? 1 : 0, total);
 }
@@ -266,9 +269,12 @@ int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, 
     uint32_t* vout = vb;
     for (int p = 0; p < npass; p++) {
         const int radix = 1 << passes[p].bits;
+        count_launch();
         k_radix_hist<K><<<ps.grid, kSortThreads, 0, st>>>(kin, n_dev, n_host, n_cap, passes[p].shift,
                                                           passes[p].bits, ps.hist);
+        count_launch();
         k_scan_small<<<1, 1024, 0, st>>>(ps.hist, radix * ps.grid);
+        count_launch();
         k_radix_scatter<K><<<ps.grid, kSortThreads, smem, st>>>(kin, vin, kout, vout, n_dev, n_host, n_cap,
                                                                 passes[p].shift, passes[p].bits, ps.hist);
         K* tk = kin; kin = kout; kout = tk;

@@ -275,12 +275,38 @@ int orc_extend_hit_scalar(const orc_seq* t, const orc_seq* q, const orc_params* 
 /* ------------------------------------------------------------------------ */
 
 #if defined(__x86_64__)
-/* PackedSeq::codes_batch, src/sequences.rs:174-212 (LUT-free but identical
- * output: up to 16 codes from start). */
+/* UNPACK_LUT, src/sequences.rs:24-35: byte -> its four 2-bit codes. */
+static uint8_t g_unpack_lut[256][4];
+static int g_unpack_ready = 0;
+static void unpack_lut_init(void) {
+    if (g_unpack_ready) return;
+    for (int i = 0; i < 256; i++)
+        for (int k = 0; k < 4; k++) g_unpack_lut[i][k] = (uint8_t)((i >> (2 * k)) & 3);
+    g_unpack_ready = 1;
+}
+
+/* PackedSeq::codes_batch, src/sequences.rs:174-212: up to 16 codes from
+ * start -- the head of an unaligned first byte, then 4 codes per LUT load,
+ * then a per-position tail. */
 static inline uint32_t codes_batch(const orc_seq* s, uint64_t start, uint8_t out[16]) {
     uint64_t n = s->len > start ? s->len - start : 0;
     if (n > 16) n = 16;
-    for (uint64_t i = 0; i < n; i++) out[i] = (uint8_t)s_code(s, start + i);
+    if (n == 0) return 0;
+    uint64_t off = start & 3, base = start >> 2, filled = 0;
+    if (off != 0) {
+        uint8_t byte = s->codes[base];
+        for (uint64_t k = off; k < 4 && k < off + n; k++) out[filled++] = (byte >> (k * 2)) & 3;
+        base++;
+    }
+    while (filled + 4 <= n) {
+        memcpy(out + filled, g_unpack_lut[s->codes[base]], 4);
+        base++;
+        filled += 4;
+    }
+    while (filled < n) {
+        uint64_t pos = start + filled;
+        out[filled++] = (s->codes[pos >> 2] >> ((pos & 3) * 2)) & 3;
+    }
     return (uint32_t)n;
 }
 /* PackedSeq::valid_mask_batch, src/sequences.rs:220-240. */
@@ -381,6 +407,7 @@ int orc_extend_hit_avx2(const orc_seq* t, const orc_seq* q, const orc_params* p,
                         uint32_t t_pos, uint32_t q_pos, uint32_t seed_len, orc_hsp* out) {
     int64_t tp = t_pos, qp = q_pos, L = seed_len;
     if (tp + L > (int64_t)t->len || qp + L > (int64_t)q->len) return 0;
+    unpack_lut_init();
     int8_t lutb[16];
     for (int r = 0; r < 4; r++)
         for (int c = 0; c < 4; c++) lutb[(r << 2) | c] = (int8_t)p->sub[r * 4 + c];
@@ -525,6 +552,7 @@ int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* que
     /* variants capacity, src/seed_search.rs:295-299. */
     uint32_t vcap = p->transitions == 0 ? 1 : (p->transitions == 1 ? 1 + w : 1 + w + w * (w ? w - 1 : 0) / 2);
     uint64_t* variants = (uint64_t*)malloc(vcap * sizeof(uint64_t));
+    uint32_t bounds[2 * (1 + 15 + 105)];
     uint64_t cap = 1024, n = 0;
     orc_hsp* res = (orc_hsp*)malloc(cap * sizeof(orc_hsp));
     diag_hash dh;
@@ -545,10 +573,16 @@ int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* que
             for (uint32_t i = 0; i < w; i++)
                 for (uint32_t j = i + 1; j < w; j++)
                     variants[nv++] = word ^ (2ull << shifts[i]) ^ (2ull << shifts[j]);
-        /* src/seed_search.rs:318-342. */
+        /* src/seed_search.rs:318-342.  The bucket bounds of all variants are
+         * read first (independent loads the CPU can overlap); the hits are
+         * then visited in the reference's order. */
         for (uint32_t v = 0; v < nv; v++) {
             uint64_t vw = variants[v];
-            uint32_t b = table->starts[vw], e = table->starts[vw + 1];
+            bounds[2 * v] = table->starts[vw];
+            bounds[2 * v + 1] = table->starts[vw + 1];
+        }
+        for (uint32_t v = 0; v < nv; v++) {
+            uint32_t b = bounds[2 * v], e = bounds[2 * v + 1];
             st.raw_hits += e - b;
             for (uint32_t j = b; j < e; j++) {
                 uint32_t tpos = table->positions[j];
