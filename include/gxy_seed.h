@@ -102,8 +102,11 @@ typedef struct {
     uint64_t candidates;   /* hits that pass or run past the screen's column cap */
     uint64_t hsps;         /* HSPs returned */
     double device_ms;      /* CUDA-event time of the call's device work */
-    double screen_ms;      /* CUDA-event time of the screen kernel alone */
-    uint64_t columns;      /* alignment columns the screen examined (seed + both sides) */
+    double screen_ms;      /* CUDA-event time of the x-drop screen kernel (with enumeration when passes > 1) */
+    uint64_t columns;      /* alignment columns the screen scanned on the two sides */
+    double enum_ms;        /* CUDA-event time of the hit enumeration kernel (single pass) */
+    uint32_t passes;       /* window-range passes the raw hits needed */
+    uint32_t reserved_;
 } gxy_stats;
 
 const char* gxy_status_string(gxy_status s);
@@ -115,13 +118,15 @@ uint64_t gxy_kernel_launches(void);
 /* ---- context ------------------------------------------------------------ */
 gxy_status gxy_ctx_create(int device, gxy_ctx** out);
 gxy_status gxy_ctx_destroy(gxy_ctx* ctx);
-/* Tunables (screen kernel warps per block, column cap per side, queue depth,
- * walk block size).  Zero leaves a field unchanged. */
+/* Tunables (screen kernel warps per block, column cap per side, screen blocks
+ * per SM, walk warps per block, raw hits per pass).  Zero leaves a field
+ * unchanged. */
 typedef struct {
     uint32_t screen_warps;
     uint32_t screen_cap;
     uint32_t screen_blocks_per_sm;
     uint32_t walk_warps;
+    uint32_t max_hits_per_pass;   /* raw-hit buffer bound; larger searches run in window passes */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);

@@ -57,15 +57,17 @@ class Context:
             cls._default[device] = Context(device)
         return cls._default[device]
 
-    def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0) -> None:
-        t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps)
+    def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0,
+                   max_hits_per_pass=0) -> None:
+        t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass)
         check(lib().gxy_ctx_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
         t = _lib.TuningC()
         check(lib().gxy_ctx_get_tuning(self.h, C.byref(t)))
         return {"screen_warps": t.screen_warps, "screen_cap": t.screen_cap,
-                "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps}
+                "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps,
+                "max_hits_per_pass": t.max_hits_per_pass}
 
     def mark(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's primary stream."""
@@ -401,7 +403,8 @@ class PosTable:
 # ---------------------------------------------------------------------------
 def _stats(st: _lib.StatsC) -> dict:
     return {"windows": st.windows, "raw_hits": st.raw_hits, "candidates": st.candidates, "hsps": st.hsps,
-            "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns}
+            "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns, "enum_ms": st.enum_ms,
+            "passes": st.passes}
 
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:

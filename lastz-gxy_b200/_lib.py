@@ -53,12 +53,12 @@ class HspBufC(C.Structure):
 class StatsC(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
                 ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double),
-                ("columns", C.c_uint64)]
+                ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reserved_", C.c_uint32)]
 
 
 class TuningC(C.Structure):
     _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
-                ("walk_warps", C.c_uint32)]
+                ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32)]
 
 
 class UnitC(C.Structure):

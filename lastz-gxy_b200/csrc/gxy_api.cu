@@ -310,7 +310,7 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         cudaStreamSynchronize(w->st);
         DevBuf* bufs[] = {&w->prim_sums, &w->prim_hist, &w->counters, &w->d_units, &w->d_tsegs, &w->d_qsegs,
                           &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags, &w->offsets, &w->ohsp,
-                          &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2};
+                          &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2, &w->hits};
         for (DevBuf* b : bufs) b->release();
         dseq_destroy(w->qstage);
         dseq_destroy(w->tstage);
@@ -359,6 +359,7 @@ gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
     if (t->screen_cap) ctx->tuning.screen_cap = std::max<uint32_t>(32, t->screen_cap);
     if (t->screen_blocks_per_sm) ctx->tuning.screen_blocks_per_sm = std::min<uint32_t>(t->screen_blocks_per_sm, 16);
     if (t->walk_warps) ctx->tuning.walk_warps = t->walk_warps == 4 ? 4 : 8;
+    if (t->max_hits_per_pass) ctx->tuning.max_hits_per_pass = std::max<uint32_t>(4096, t->max_hits_per_pass);
     return GXY_OK;
 }
 

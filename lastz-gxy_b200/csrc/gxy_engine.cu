@@ -15,6 +15,12 @@ uint64_t launches() { return g_launches.load(std::memory_order_relaxed); }
 void set_error(const std::string& msg) { g_err = msg; }
 const char* last_error() { return g_err.c_str(); }
 
+#define API_TRY_ENGINE(expr)          \
+    do {                              \
+        gxy_status s_ = (expr);       \
+        if (s_ != GXY_OK) return s_;  \
+    } while (0)
+
 #define GXY_CK(call)                                                                         \
     do {                                                                                     \
         cudaError_t e_ = (call);                                                             \
@@ -257,7 +263,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     sa.tsegs = W->d_tsegs.as<SeqView>();
     sa.qsegs = W->d_qsegs.as<SeqView>();
     sa.n_units = nu;
-    sa.n_tiles = (uint32_t)tiles;
+    sa.tile_lo = 0;
+    sa.tile_hi = (uint32_t)tiles;
     sa.pat = pat;
     sa.step = p.step;
     build_variants(pat, p.transitions, sa.var_xor, sa.n_var);
@@ -271,15 +278,41 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     RadixPass passes[16];
     const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
 
-    uint32_t* cnt = W->counters.as<uint32_t>();           // [0] tiles [1] cands [2] hsps
-    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);   // [0] windows [1] raw [2] cols
+    // Device counters: u32 [0] tile, [1] candidates, [2] HSPs, [3] hit cursor;
+    // u64 at byte 32: [0] windows, [1] raw hits, [2] columns; u64 at byte 64: hits.
+    uint32_t* cnt = W->counters.as<uint32_t>();
+    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);
+    unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + 16);
     if (W->cand_cap == 0) W->cand_cap = 1u << 20;
+    if (W->hit_cap == 0) W->hit_cap = 32ull << 20;
+    const uint64_t kMaxHitCap = std::max<uint32_t>(4096, ctx->tuning.max_hits_per_pass);
+    if (W->hit_cap > kMaxHitCap) {
+        W->hits.release();
+        W->hit_cap = kMaxHitCap;
+    }
+    uint32_t pass_tiles = (uint32_t)tiles;
     const int blocks_screen = ctx->sm_count * (int)std::max<uint32_t>(1, ctx->tuning.screen_blocks_per_sm);
+    const int blocks_enum = ctx->sm_count * 8;
     const int blocks_misc = ctx->sm_count * 4;
     const int walk_warps = ctx->tuning.walk_warps == 4 ? 4 : 8;
 
-    for (int attempt = 0; attempt < 8; attempt++) {
+    // One pass: enumerate tiles [t0, t1) into the hit buffer, then screen them.
+    bool single_pass_timing = false;
+    auto pass = [&](uint32_t t0, uint32_t t1) -> gxy_status {
+        GXY_CK(cudaMemsetAsync(cnt + 0, 0, 4, st));
+        GXY_CK(cudaMemsetAsync(cnt + 3, 0, 4, st));
+        GXY_CK(cudaMemsetAsync(hitc, 0, 8, st));
+        sa.tile_lo = t0;
+        sa.tile_hi = t1;
+        launch_enumerate(sa, blocks_enum, st);
+        if (single_pass_timing) GXY_CK(cudaEventRecord(W->ev[3], st));
+        launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
+        return GXY_OK;
+    };
+
+    for (int attempt = 0; attempt < 16; attempt++) {
         const uint32_t cap = W->cand_cap;
+        GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
         GXY_CK(W->ck0.ensure((size_t)cap * 8));
         GXY_CK(W->ck1.ensure((size_t)cap * 8));
         GXY_CK(W->cv0.ensure((size_t)cap * 4));
@@ -296,20 +329,55 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(W->perm2.ensure((size_t)cap * 4));
         sa.tile_counter = cnt + 0;
         sa.cand_count = cnt + 1;
+        sa.hit_next = cnt + 3;
+        sa.hit_count = hitc;
+        sa.hits = W->hits.as<Hit>();
+        sa.hit_cap = W->hit_cap;
         sa.stats = st64;
         sa.cand_keys = W->ck0.as<uint64_t>();
         sa.cand_vals = W->cv0.as<uint32_t>();
         sa.cands = W->cands.as<Cand>();
         sa.cand_cap = cap;
 
+        const bool single = pass_tiles >= tiles;
+        const bool graph_now = use_graph && single;
+        single_pass_timing = single;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t gexec = nullptr;
-        if (use_graph) GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-
         GXY_CK(cudaMemsetAsync(W->counters.p, 0, 256, st));
-        GXY_CK(cudaEventRecord(W->ev[0], st));
-        launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
-        GXY_CK(cudaEventRecord(W->ev[1], st));
+        if (!single) {
+            // Passes over window ranges, each checked for hit-buffer overflow.
+            GXY_CK(cudaEventRecord(W->ev[0], st));
+            for (uint32_t t0 = 0; t0 < tiles;) {
+                const uint32_t t1 = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)t0 + pass_tiles);
+                uint32_t before[24];   // counters before this pass, restored if it is redone
+                GXY_CK(cudaMemcpyAsync(before, cnt, sizeof(before), cudaMemcpyDeviceToHost, st));
+                GXY_CK(cudaStreamSynchronize(st));
+                API_TRY_ENGINE(pass(t0, t1));
+                unsigned long long nh = 0;
+                GXY_CK(cudaMemcpyAsync(&nh, hitc, 8, cudaMemcpyDeviceToHost, st));
+                GXY_CK(cudaStreamSynchronize(st));
+                if (nh > W->hit_cap) {
+                    if (t1 - t0 == 1) {
+                        set_error("one tile of 32 query windows has more raw hits than the hit buffer holds");
+                        return GXY_ENOMEM;
+                    }
+                    // Undo this pass's candidates and counters; redo it over fewer tiles.
+                    GXY_CK(cudaMemcpyAsync(cnt, before, sizeof(before), cudaMemcpyHostToDevice, st));
+                    pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)(t1 - t0) * W->hit_cap / nh * 0.8));
+                    continue;
+                }
+                t0 = t1;
+            }
+            GXY_CK(cudaEventRecord(W->ev[3], st));
+            GXY_CK(cudaEventRecord(W->ev[1], st));
+        } else {
+            if (graph_now) GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            GXY_CK(cudaMemsetAsync(W->counters.p, 0, 256, st));
+            GXY_CK(cudaEventRecord(W->ev[0], st));
+            API_TRY_ENGINE(pass(0, (uint32_t)tiles));
+            GXY_CK(cudaEventRecord(W->ev[1], st));
+        }
         const int which = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
                                          W->cv1.as<uint32_t>(), cnt + 1, 0, cap, passes, npass, W->ps, st);
         const uint64_t* skeys = which ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
@@ -355,7 +423,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(cudaEventRecord(W->ev[2], st));
         GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, 256, cudaMemcpyDeviceToHost, st));
 
-        if (use_graph) {
+        if (graph_now) {
             GXY_CK(cudaStreamEndCapture(st, &graph));
             cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
             if (e != cudaSuccess) {
@@ -375,7 +443,20 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(cudaStreamSynchronize(st));
         const uint32_t* hc = static_cast<const uint32_t*>(W->h_pinned);
         const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + 8);
+        const unsigned long long nhits = *reinterpret_cast<const unsigned long long*>(hc + 16);
         const uint32_t ncand = hc[1];
+        if (single && nhits > W->hit_cap) {
+            // Raw hits overflowed the hit buffer: grow it, or split into passes.
+            if (nhits + nhits / 8 <= kMaxHitCap) {
+                W->hits.release();
+                W->hit_cap = nhits + nhits / 8 + 1024;
+            } else {
+                W->hits.release();
+                W->hit_cap = kMaxHitCap;
+                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / nhits * 0.8));
+            }
+            continue;
+        }
         if (ncand > cap) {
             // Candidate buffer overflowed: grow and rerun (results so far are void).
             uint64_t nc = (uint64_t)ncand + ncand / 4 + 1024;
@@ -392,11 +473,14 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.columns = hs[2];
         out.stats.candidates = ncand;
         out.stats.hsps = nh;
-        float ms = 0.f, ms_screen = 0.f;
+        float ms = 0.f, ms_enum = 0.f, ms_screen = 0.f;
         cudaEventElapsedTime(&ms, W->ev[0], W->ev[2]);
-        cudaEventElapsedTime(&ms_screen, W->ev[0], W->ev[1]);
+        cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[3]);
+        cudaEventElapsedTime(&ms_screen, W->ev[3], W->ev[1]);
         out.stats.device_ms = ms;
-        out.stats.screen_ms = ms_screen;
+        out.stats.enum_ms = single ? ms_enum : 0.0;
+        out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;
+        out.stats.passes = single ? 1 : (uint32_t)((tiles + pass_tiles - 1) / pass_tiles);
         out.hsps.resize(nh);
         out.unit.resize(nh);
         if (nh) {

@@ -37,6 +37,8 @@ struct Worker {
     DevBuf d_units, d_tsegs, d_qsegs;
     DevBuf ck0, ck1, cv0, cv1, cands, flags, offsets, ohsp;
     DevBuf rhsp, runit, rhsp2, runit2, perm, perm2;
+    DevBuf hits;                  // raw hits of one pass
+    uint64_t hit_cap = 0;
     uint32_t cand_cap = 0;
     uint32_t res_cap = 0;
     void* h_pinned = nullptr;     // small host staging
@@ -101,7 +103,7 @@ struct gxy_ctx {
     std::mutex mu;
     std::vector<gxy::Worker*> free_workers;   // the primary worker (all_workers[0]) is taken first
     std::vector<gxy::Worker*> all_workers;
-    gxy_tuning tuning{8, 64, 2, 8};
+    gxy_tuning tuning{8, 128, 4, 8, 256u << 20};
     cudaEvent_t marks[16] = {};
 };
 

@@ -200,11 +200,12 @@ void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64
 //    of one unit from a global work counter, forms each window's seed word
 //    and its transition variants (src/seed_search.rs:303-316), and pushes the
 //    hits of each variant's bucket (src/pos_table.rs:102-108) into the queue.
-//  - Consumers (one lane per hit): every iteration an idle lane takes the
-//    next queued hit, and every busy lane advances its own hit by one chunk of
-//    up to 32 columns -- the seed footprint, then the right side, then the
-//    left side of extend_hit (src/hsp.rs:98-195).  All phases run the same
-//    chunk code, so lanes in different phases do not diverge.
+//  - Consumers (one lane per hit): an idle lane takes the next queued hit and
+//    loads one 128-position window of the target and of the query around it;
+//    from those registers it scores the seed footprint and the first 32
+//    columns of both sides of extend_hit (src/hsp.rs:98-195) -- the sides are
+//    independent.  A side still running after 32 columns continues one chunk
+//    per iteration with fresh loads, while the other lanes take new hits.
 // A hit is extended up to `cap` columns per side:
 //  - ended below hspthresh: dropped.  Such a hit can never change the output:
 //    search() only records diagonal cover for a hit whose HSP passes
@@ -212,286 +213,458 @@ void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64
 //  - ended at or above hspthresh, or still running at the cap: kept as a
 //    candidate for the walk, which applies the diagonal rule in order.
 // ---------------------------------------------------------------------------
-constexpr int kRefillBelow = 96;  // the producer runs while fewer hits are queued
-
-enum : uint32_t { kIdle = 0, kSeed = 1, kRight = 2, kLeft = 3 };
 
 __device__ __forceinline__ uint64_t rev_pairs64(uint64_t c) {
     c = __brevll(c);
     return ((c >> 1) & 0x5555555555555555ull) | ((c & 0x5555555555555555ull) << 1);
 }
 
-template <int WARPS, int MINB>
-__global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_constant__ ScreenArgs a) {
-    constexpr int kQCap = WARPS >= 16 ? 128 : 256;   // queued hits per warp
-    __shared__ int32_t s_lut[16];
-    __shared__ uint32_t s_qt[WARPS][kQCap];
-    __shared__ uint32_t s_qq[WARPS][kQCap];
-    __shared__ uint32_t s_qu[WARPS][kQCap];
-    __shared__ uint32_t s_ex[WARPS][32];
-    __shared__ uint32_t s_b[WARPS][32];
-    __shared__ uint32_t s_qw[WARPS][32];
-    if (threadIdx.x < 16) s_lut[threadIdx.x] = a.sc.sub[threadIdx.x];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t lt = lanemask_lt();
-    const uint32_t L = a.pat.len;
-    const int32_t ambig = a.sc.ambig, xdrop = a.sc.xdrop, thresh = a.sc.hspthresh;
-    unsigned long long n_windows = 0, n_raw = 0, n_cols = 0;
+// 32 positions starting at offset o of a 4-word window (o <= 96).
+__device__ __forceinline__ uint64_t win_codes(const uint64_t (&w)[4], uint32_t o) {
+    const uint32_t i = o >> 5, s = (o & 31) * 2;
+    const uint64_t lo = i == 0 ? w[0] : (i == 1 ? w[1] : w[2]);
+    const uint64_t hi = i == 0 ? w[1] : (i == 1 ? w[2] : w[3]);
+    return s ? ((lo >> s) | (hi << (64 - s))) : lo;
+}
+__device__ __forceinline__ uint32_t win_bits(const uint32_t (&w)[4], uint32_t o) {
+    const uint32_t i = o >> 5;
+    const uint32_t lo = i == 0 ? w[0] : (i == 1 ? w[1] : w[2]);
+    const uint32_t hi = i == 0 ? w[1] : (i == 1 ? w[2] : w[3]);
+    return __funnelshift_r(lo, hi, o & 31);
+}
 
-    // ---- producer state (warp-uniform, except the per-lane window data) ----
-    uint32_t head = 0, tail = 0;
-    bool exhausted = false, have_tile = false;
-    uint32_t pu = 0, v = 0, done_v = 0, total_v = 0, maxc = 0;
-    const uint32_t* p_starts = nullptr;
-    const uint32_t* p_pos = nullptr;
-    uint32_t word = 0, qwin = 0, my_b = 0, my_cnt = 0, my_ex = 0;
-    bool wv = false;
+// Spreads the 2-bit codes of 16 columns (32 bits) into 16 nibbles (64 bits).
+__device__ __forceinline__ uint64_t spread16(uint32_t x) {
+    uint64_t v = x;
+    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    v = (v | (v << 2)) & 0x3333333333333333ull;
+    return v;
+}
 
-    // ---- consumer state (per lane) ----
-    uint32_t phase = kIdle, ht = 0, hq = 0, hu = 0xffffffffu;
-    uint32_t pos_t = 0, pos_q = 0, rem = 0, ext = 0, bext = 0, rext = 0;
-    int32_t run = 0, best = 0, seed = 0, rbest = 0;
-    SeqView T{}, Q{};
-    uint32_t cur_unit = 0xffffffffu;
-
-    auto load_variant = [&]() {
-        my_b = 0;
-        my_cnt = 0;
-        if (wv) {
-            const uint32_t vw = word ^ a.var_xor[v];
-            my_b = __ldg(p_starts + vw);
-            my_cnt = __ldg(p_starts + vw + 1) - my_b;
+// The x-drop scan of extend_one_side (src/hsp.rs:179-193) over up to 32
+// columns whose codes and validity are in registers (column k at bits 2k /
+// bit k).  Continues a side from (run, best, bext) after ext0 columns; n = 0
+// is a no-op.  Sets ended when the x-drop break fired; used = columns consumed.
+template <bool kCheckValid>
+__device__ __forceinline__ void scan32(uint64_t tc, uint64_t qc, uint32_t vv, uint32_t n, int32_t xd,
+                                       const int32_t* lut, int32_t ambig, uint32_t ext0, int32_t& run,
+                                       int32_t& best, uint32_t& bext, bool& ended, uint32_t& used) {
+    // idx_k = (t_k << 2) | q_k as nibble k of nib[k / 16].
+    const uint64_t nib0 = (spread16((uint32_t)tc) << 2) | spread16((uint32_t)qc);
+    const uint64_t nib1 = (spread16((uint32_t)(tc >> 32)) << 2) | spread16((uint32_t)(qc >> 32));
+    int32_t r = run, b = best;
+    uint32_t be = bext, lim = n, brk = n;
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+        if (!__any_sync(kFull, (uint32_t)(g * 8) < lim)) break;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int k = g * 8 + i;
+            if ((uint32_t)k < lim) {
+                const uint32_t idx = (uint32_t)(((k < 16 ? nib0 : nib1) >> (4 * (k & 15))) & 15u);
+                int32_t sc = lut[idx];
+                if (kCheckValid) sc = ((vv >> k) & 1u) ? sc : ambig;
+                r += sc;
+                if (r > b) {
+                    b = r;
+                    be = ext0 + k + 1;
+                } else if (b - r > xd) {
+                    brk = k;
+                    lim = 0;
+                }
+            }
         }
-        uint32_t incl = my_cnt;
+    }
+    ended = brk < n;
+    used = ended ? brk + 1 : n;
+    run = r;
+    best = b;
+    bext = be;
+}
+
+// One side's scan state for the interleaved scans below.
+struct SideScan {
+    uint64_t nib0, nib1;   // (t << 2 | q) nibbles of columns 0-15 and 16-31
+    uint32_t vv;           // column validity
+    uint32_t lim;          // columns still to scan (0 once the side broke)
+    uint32_t brk;          // break column, or n when the side did not break
+    uint32_t ext0;         // columns of this side already scanned
+    int32_t r, b;          // running score, best
+    uint32_t be;           // best extent
+};
+
+__device__ __forceinline__ void side_init(SideScan& S, uint64_t tc, uint64_t qc, uint32_t vv, uint32_t n,
+                                          uint32_t ext0, int32_t run, int32_t best, uint32_t bext) {
+    S.nib0 = (spread16((uint32_t)tc) << 2) | spread16((uint32_t)qc);
+    S.nib1 = (spread16((uint32_t)(tc >> 32)) << 2) | spread16((uint32_t)(qc >> 32));
+    S.vv = vv;
+    S.lim = n;
+    S.brk = n;
+    S.ext0 = ext0;
+    S.r = run;
+    S.b = best;
+    S.be = bext;
+}
+
+template <bool kCheckValid, int k>
+__device__ __forceinline__ void side_step(SideScan& S, int32_t xd, const int32_t* lut, int32_t ambig) {
+    if ((uint32_t)k < S.lim) {
+        const uint32_t idx = (uint32_t)(((k < 16 ? S.nib0 : S.nib1) >> (4 * (k & 15))) & 15u);
+        int32_t sc = lut[idx];
+        if (kCheckValid) sc = ((S.vv >> k) & 1u) ? sc : ambig;
+        S.r += sc;
+        if (S.r > S.b) {
+            S.b = S.r;
+            S.be = S.ext0 + k + 1;
+        } else if (S.b - S.r > xd) {
+            S.brk = k;
+            S.lim = 0;
+        }
+    }
+}
+
+// Two independent sides scanned column by column in lockstep: the x-drop
+// recurrence of each side is a serial chain, and interleaving two chains
+// lets the scheduler issue from both.
+template <bool kCheckValid>
+__device__ __forceinline__ void scan_pair(SideScan& A, SideScan& B, int32_t xd, const int32_t* lut,
+                                          int32_t ambig) {
+#define GXY_STEP8(g)                                                             \
+    side_step<kCheckValid, g * 8 + 0>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 0>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 1>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 1>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 2>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 2>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 3>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 3>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 4>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 4>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 5>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 5>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 6>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 6>(B, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 7>(A, xd, lut, ambig);                        \
+    side_step<kCheckValid, g * 8 + 7>(B, xd, lut, ambig);
+    if (!__any_sync(kFull, A.lim > 0 || B.lim > 0)) return;
+    GXY_STEP8(0)
+    if (!__any_sync(kFull, A.lim > 8 || B.lim > 8)) return;
+    GXY_STEP8(1)
+    if (!__any_sync(kFull, A.lim > 16 || B.lim > 16)) return;
+    GXY_STEP8(2)
+    if (!__any_sync(kFull, A.lim > 24 || B.lim > 24)) return;
+    GXY_STEP8(3)
+#undef GXY_STEP8
+}
+
+__device__ __forceinline__ void scan_pair_any(SideScan& A, SideScan& B, uint32_t na, uint32_t nb, int32_t xd,
+                                              const int32_t* lut, int32_t ambig) {
+    const uint32_t need_a = na >= 32 ? 0xffffffffu : ((1u << na) - 1u);
+    const uint32_t need_b = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
+    if (__any_sync(kFull, (A.vv & need_a) != need_a || (B.vv & need_b) != need_b))
+        scan_pair<true>(A, B, xd, lut, ambig);
+    else
+        scan_pair<false>(A, B, xd, lut, ambig);
+}
+
+// ---------------------------------------------------------------------------
+// Enumeration: one warp per tile of 32 consecutive query windows of one unit.
+// Each lane forms its window's seed word and transition variants
+// (src/seed_search.rs:303-316); the warp reserves room for all hits of the
+// tile with one atomic and writes (t, q, unit) for every position of every
+// variant's bucket (src/pos_table.rs:102-108).  Large buckets are copied by
+// the whole warp.
+// ---------------------------------------------------------------------------
+__global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ ScreenArgs a) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t ntile = a.tile_hi - a.tile_lo;
+    unsigned long long n_windows = 0, n_raw = 0;
+    for (;;) {
+        uint32_t tile = 0;
+        if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+        tile = __shfl_sync(kFull, tile, 0);
+        if (tile >= ntile) break;
+        tile += a.tile_lo;
+        uint32_t lo = 0, hi = a.n_units;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (a.units[mid].tile_base <= tile) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t u = lo;
+        const UnitDev U = a.units[u];
+        const uint32_t k = (tile - U.tile_base) * 32 + lane;
+        const uint32_t q = k * a.step;
+        uint32_t word = 0;
+        bool wv = false;
+        if (k < U.nwin) wv = word_at(a.qsegs[U.qseg], a.pat, q, word);
+        n_windows += wv ? 1 : 0;
+        // Pass 1: this lane's hit count over all variants.  The bucket
+        // bounds of the first kRegVar variants stay in registers for pass 2.
+        constexpr uint32_t kRegVar = 16;
+        uint32_t rb[kRegVar], rc[kRegVar];
+        uint32_t tot = 0;
+#pragma unroll
+        for (uint32_t v = 0; v < kRegVar; v++) {
+            rb[v] = 0;
+            rc[v] = 0;
+            if (wv && v < a.n_var) {
+                const uint32_t vw = word ^ a.var_xor[v];
+                rb[v] = __ldg(U.starts + vw);
+                rc[v] = __ldg(U.starts + vw + 1) - rb[v];
+                tot += rc[v];
+            }
+        }
+        if (wv) {
+            for (uint32_t v = kRegVar; v < a.n_var; v++) {
+                const uint32_t vw = word ^ a.var_xor[v];
+                tot += __ldg(U.starts + vw + 1) - __ldg(U.starts + vw);
+            }
+        }
+        uint32_t incl = tot;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(kFull, incl, o);
             if (lane >= o) incl += y;
         }
-        total_v = __shfl_sync(kFull, incl, 31);
-        my_ex = incl - my_cnt;
-        maxc = my_cnt;
+        const uint32_t wtot = __shfl_sync(kFull, incl, 31);
+        if (wtot == 0) continue;
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(a.hit_count, (unsigned long long)wtot);
+        base = __shfl_sync(kFull, base, 0);
+        n_raw += lane == 0 ? wtot : 0;
+        if (base + wtot > a.hit_cap) continue;   // overflow: the pass is redone with fewer tiles
+        // Pass 2: write.  dst = this lane's next slot.
+        uint64_t dst = base + (incl - tot);
+        for (uint32_t v = 0; v < a.n_var; v++) {
+            uint32_t b = 0, c = 0;
+            if (v < kRegVar) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(kFull, maxc, o));
-        done_v = 0;
-        n_raw += lane == 0 ? total_v : 0;
-    };
+                for (uint32_t x = 0; x < kRegVar; x++)
+                    if (x == v) {
+                        b = rb[x];
+                        c = rc[x];
+                    }
+            } else if (wv) {
+                const uint32_t vw = word ^ a.var_xor[v];
+                b = __ldg(U.starts + vw);
+                c = __ldg(U.starts + vw + 1) - b;
+            }
+            const bool big = c > 16;
+            if (!big) {
+                for (uint32_t j = 0; j < c; j++) {
+                    Hit h;
+                    h.t = __ldg(U.positions + b + j);
+                    h.q = q;
+                    h.unit = u;
+                    a.hits[dst + j] = h;
+                }
+            }
+            uint32_t bm = __ballot_sync(kFull, big);
+            while (bm) {
+                const int src = __ffs(bm) - 1;
+                bm &= bm - 1;
+                const uint32_t bb = __shfl_sync(kFull, b, src), cc = __shfl_sync(kFull, c, src);
+                const uint32_t qq = __shfl_sync(kFull, q, src);
+                const uint64_t dd = __shfl_sync(kFull, dst, src);
+                for (uint32_t j = lane; j < cc; j += 32) {
+                    Hit h;
+                    h.t = __ldg(U.positions + bb + j);
+                    h.q = qq;
+                    h.unit = u;
+                    a.hits[dd + j] = h;
+                }
+            }
+            dst += c;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_windows += __shfl_xor_sync(kFull, n_windows, o);
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_windows);
+        atomicAdd(&a.stats[1], n_raw);
+    }
+}
+
+void launch_enumerate(const ScreenArgs& a, int blocks, cudaStream_t st) {
+    count_launch();
+    k_enumerate<<<blocks, 256, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Screen: capped lane-per-hit x-drop over the enumerated hits.
+//
+// Each idle lane takes the next hit from the pass's hit array and loads one
+// 128-position window of the target and of the query around it; from those
+// registers it scores the seed footprint and the first 32 columns of both
+// sides of extend_hit (src/hsp.rs:98-195) -- the sides are independent and
+// are scanned in lockstep.  A side still running after 32 columns continues
+// one chunk per iteration with fresh loads while the other lanes take new
+// hits.  A hit is extended up to `cap` columns per side:
+//  - ended below hspthresh: dropped.  Such a hit can never change the output:
+//    search() only records diagonal cover for a hit whose HSP passes
+//    (src/seed_search.rs:321-340), so whether it was admitted is irrelevant.
+//  - ended at or above hspthresh, or still running at the cap: kept as a
+//    candidate for the walk, which applies the diagonal rule in order.
+// ---------------------------------------------------------------------------
+template <int WARPS, int MINB>
+__global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_constant__ ScreenArgs a) {
+    __shared__ int32_t s_lut[16];
+    if (threadIdx.x < 16) s_lut[threadIdx.x] = a.sc.sub[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    const uint32_t L = a.pat.len;
+    const int32_t ambig = a.sc.ambig, xdrop = a.sc.xdrop, thresh = a.sc.hspthresh;
+    const unsigned long long hc = *a.hit_count;
+    const uint32_t n_hits = (uint32_t)(hc < a.hit_cap ? hc : a.hit_cap);
+    unsigned long long n_cols = 0;
+    bool exhausted = false;
+
+    bool busy = false, rdone = true, ldone = true;
+    uint32_t ht = 0, hq = 0, hu = 0xffffffffu;
+    int32_t seed = 0;
+    int32_t rrun = 0, rbest = 0, lrun = 0, lbest = 0;
+    uint32_t rbext = 0, lbext = 0, rext = 0, lext = 0, rrem = 0, lrem = 0;
+    SeqView T{}, Q{};
+    uint32_t cur_unit = 0xffffffffu;
 
     for (;;) {
-        // ---------------- produce ----------------
-        while (!exhausted && tail - head < (uint32_t)kRefillBelow) {
-            if (!have_tile) {
-                uint32_t tile = 0;
-                if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
-                tile = __shfl_sync(kFull, tile, 0);
-                if (tile >= a.n_tiles) {
-                    exhausted = true;
-                    break;
-                }
-                uint32_t lo = 0, hi = a.n_units;
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (a.units[mid].tile_base <= tile) lo = mid;
-                    else hi = mid;
-                }
-                pu = lo;
-                const UnitDev U = a.units[pu];
-                p_starts = U.starts;
-                p_pos = U.positions;
-                const uint32_t k = (tile - U.tile_base) * 32 + lane;
-                qwin = k * a.step;
-                wv = false;
-                if (k < U.nwin) wv = word_at(a.qsegs[U.qseg], a.pat, qwin, word);
-                n_windows += wv ? 1 : 0;
-                s_qw[w][lane] = qwin;
-                v = 0;
-                load_variant();
-                have_tile = true;
-            }
-            while (done_v == total_v) {
-                if (++v == a.n_var) {
-                    have_tile = false;
-                    break;
-                }
-                load_variant();
-            }
-            if (!have_tile) continue;
-            const uint32_t room = (uint32_t)kQCap - (tail - head);
-            const uint32_t np = min(room, total_v - done_v);
-            if (done_v == 0 && np == total_v && maxc <= 8) {
-                // Typical case: each lane copies its own short bucket.
-                for (uint32_t j = 0; j < my_cnt; j++) {
-                    const uint32_t slot = (tail + my_ex + j) % kQCap;
-                    s_qt[w][slot] = __ldg(p_pos + my_b + j);
-                    s_qq[w][slot] = qwin;
-                    s_qu[w][slot] = pu;
-                }
-            } else {
-                // Hot buckets: all lanes copy; owner = last lane with ex <= idx.
-                s_ex[w][lane] = my_ex;
-                s_b[w][lane] = my_b;
-                __syncwarp();
-                for (uint32_t j = lane; j < np; j += 32) {
-                    const uint32_t idx = done_v + j;
-                    uint32_t lo2 = 0, hi2 = 32;
-                    while (hi2 - lo2 > 1) {
-                        const uint32_t mid = (lo2 + hi2) >> 1;
-                        if (s_ex[w][mid] <= idx) lo2 = mid;
-                        else hi2 = mid;
-                    }
-                    const uint32_t slot = (tail + j) % kQCap;
-                    s_qt[w][slot] = __ldg(p_pos + s_b[w][lo2] + (idx - s_ex[w][lo2]));
-                    s_qq[w][slot] = s_qw[w][lo2];
-                    s_qu[w][slot] = pu;
-                }
-            }
-            __syncwarp();
-            tail += np;
-            done_v += np;
-        }
-
         // ---------------- assign ----------------
-        const bool idle = phase == kIdle;
-        const uint32_t im = __ballot_sync(kFull, idle);
-        const uint32_t avail = tail - head;
-        const uint32_t take = min((uint32_t)__popc(im), avail);
-        if (idle) {
+        const uint32_t im = __ballot_sync(kFull, !busy);
+        uint32_t base = 0, take = 0;
+        if (!exhausted && im) {
+            if (lane == 0) base = atomicAdd(a.hit_next, (uint32_t)__popc(im));
+            base = __shfl_sync(kFull, base, 0);
+            take = base < n_hits ? min((uint32_t)__popc(im), n_hits - base) : 0u;
+            if (base + (uint32_t)__popc(im) >= n_hits) exhausted = true;
+        }
+        bool fresh = false;
+        if (!busy) {
             const uint32_t rk = __popc(im & lt);
             if (rk < take) {
-                const uint32_t slot = (head + rk) % kQCap;
-                ht = s_qt[w][slot];
-                hq = s_qq[w][slot];
-                hu = s_qu[w][slot];
+                const Hit h = a.hits[base + rk];
+                ht = h.t;
+                hq = h.q;
+                hu = h.unit;
                 if (hu != cur_unit) {
                     cur_unit = hu;
                     const UnitDev U = a.units[hu];
                     T = a.tsegs[U.tseg];
                     Q = a.qsegs[U.qseg];
                 }
-                phase = kSeed;
+                fresh = true;
+                busy = true;
             }
         }
-        head += take;
-        const bool busy = phase != kIdle;
         if (!__any_sync(kFull, busy)) {
-            if (exhausted && tail == head) break;
+            if (exhausted) break;
             continue;
         }
 
-        // ---------------- one chunk ----------------
-        uint64_t tg = 0, qg = 0;
-        uint32_t n = 0;
-        int32_t xd = INT32_MAX;
-        const bool fwd = phase != kLeft;
-        if (phase == kSeed) {
-            tg = T.base + ht;
-            qg = Q.base + hq;
-            n = L;
-        } else if (phase == kRight) {
-            tg = T.base + pos_t;
-            qg = Q.base + pos_q;
-            n = min(32u, rem);
-            xd = xdrop;
-        } else if (phase == kLeft) {
-            tg = T.base + pos_t - 31;
-            qg = Q.base + pos_q - 31;
-            n = min(32u, rem);
-            xd = xdrop;
-        }
-        uint64_t tc = 0, qc = 0;
-        uint32_t vv = 0;
-        if (busy) {
-            tc = load_codes32(T.codes, tg);
-            qc = load_codes32(Q.codes, qg);
-            vv = load_bits32(T.valid, tg) & load_bits32(Q.valid, qg);
-            if (!fwd) {
-                tc = rev_pairs64(tc);
-                qc = rev_pairs64(qc);
-                vv = __brev(vv);
+        // ---------------- chunk data ----------------
+        // Scan A: a fresh hit's first right chunk, or a continuing side's next chunk.
+        // Scan B: a fresh hit's first left chunk.
+        uint64_t atc = 0, aqc = 0, btc = 0, bqc = 0;
+        uint32_t avv = 0, bvv = 0, an = 0, bn = 0;
+        const bool a_right = fresh || !rdone;   // which side scan A advances
+        if (fresh) {
+            const uint64_t tb = T.base + ht, qb = Q.base + hq;
+            const uint64_t tw = (tb - 32) & ~31ull, qw = (qb - 32) & ~31ull;
+            uint64_t twc[4], qwc[4];
+            uint32_t twv[4], qwv[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                twc[j] = __ldg(T.codes + (tw >> 5) + j);
+                qwc[j] = __ldg(Q.codes + (qw >> 5) + j);
+                twv[j] = __ldg(T.valid + (tw >> 5) + j);
+                qwv[j] = __ldg(Q.valid + (qw >> 5) + j);
             }
-        }
-        int32_t r = phase == kSeed ? 0 : run;
-        int32_t b = best;
-        uint32_t be = bext;
-        bool alive = busy;
-        bool ended = false;
+            const uint32_t ot = (uint32_t)(tb - tw), oq = (uint32_t)(qb - qw);   // both in [32, 63]
+            // Seed footprint: all L columns (src/hsp.rs:119-123).
+            {
+                const uint64_t tc = win_codes(twc, ot), qc = win_codes(qwc, oq);
+                const uint32_t vv = win_bits(twv, ot) & win_bits(qwv, oq);
+                int32_t sd = 0;
 #pragma unroll
-        for (int g = 0; g < 4; g++) {
-            if (!__any_sync(kFull, alive && (uint32_t)(g * 8) < n)) break;
-#pragma unroll
-            for (int i = 0; i < 8; i++) {
-                const int k = g * 8 + i;
-                if (alive && (uint32_t)k < n) {
-                    r += col_score(tc, qc, vv, k, s_lut, ambig);
-                    if (r > b) {
-                        b = r;
-                        be = ext + k + 1;
-                    } else if (b - r > xd) {
-                        alive = false;
-                        ended = true;
-                        n_cols += (unsigned long long)(k + 1);
-                    }
+                for (int k = 0; k < 32; k++) {
+                    if ((uint32_t)k >= L) break;
+                    sd += col_score(tc, qc, vv, k, s_lut, ambig);
                 }
+                seed = sd;
+            }
+            rrem = min(T.len - ht - L, Q.len - hq - L);
+            lrem = min(ht, hq);
+            rrun = rbest = lrun = lbest = 0;
+            rbext = lbext = rext = lext = 0;
+            rdone = rrem == 0;
+            ldone = lrem == 0;
+            an = min(32u, rrem);
+            atc = win_codes(twc, ot + L);
+            aqc = win_codes(qwc, oq + L);
+            avv = win_bits(twv, ot + L) & win_bits(qwv, oq + L);
+            bn = min(32u, lrem);
+            btc = rev_pairs64(win_codes(twc, ot - 32));
+            bqc = rev_pairs64(win_codes(qwc, oq - 32));
+            bvv = __brev(win_bits(twv, ot - 32) & win_bits(qwv, oq - 32));
+        } else if (busy) {
+            if (!rdone) {
+                const uint64_t tg = T.base + ht + L + rext, qg = Q.base + hq + L + rext;
+                atc = load_codes32(T.codes, tg);
+                aqc = load_codes32(Q.codes, qg);
+                avv = load_bits32(T.valid, tg) & load_bits32(Q.valid, qg);
+                an = min(32u, rrem);
+            } else {
+                // Left side continues below position ht - 1 - lext.
+                const uint64_t tg = T.base + ht - lext - 32, qg = Q.base + hq - lext - 32;
+                atc = rev_pairs64(load_codes32(T.codes, tg));
+                aqc = rev_pairs64(load_codes32(Q.codes, qg));
+                avv = __brev(load_bits32(T.valid, tg) & load_bits32(Q.valid, qg));
+                an = min(32u, lrem);
             }
         }
 
-        // Columns examined this chunk (the break column included), for the
-        // algorithmic byte count.
-        if (busy) n_cols += phase == kSeed ? n : (ended ? 0 : n);
+        // ---------------- scans ----------------
+        {
+            if (!busy) an = 0;
+            if (!fresh) bn = 0;
+            SideScan A, B;
+            side_init(A, atc, aqc, avv, an, a_right ? rext : lext, a_right ? rrun : lrun, a_right ? rbest : lbest,
+                      a_right ? rbext : lbext);
+            side_init(B, btc, bqc, bvv, bn, 0, lrun, lbest, lbext);
+            scan_pair_any(A, B, an, bn, xdrop, s_lut, ambig);
+            const bool aend = A.brk < an, bend = B.brk < bn;
+            const uint32_t aused = aend ? A.brk + 1 : an, bused = bend ? B.brk + 1 : bn;
+            n_cols += aused + bused;
+            if (busy) {
+                if (a_right) {
+                    rrun = A.r; rbest = A.b; rbext = A.be; rext += aused; rrem -= aused;
+                    rdone = rdone || aend || rrem == 0;
+                } else {
+                    lrun = A.r; lbest = A.b; lbext = A.be; lext += aused; lrem -= aused;
+                    ldone = ldone || aend || lrem == 0;
+                }
+            }
+            if (fresh) {
+                lrun = B.r; lbest = B.b; lbext = B.be; lext += bused; lrem -= bused;
+                ldone = ldone || bend || lrem == 0;
+            }
+        }
+
         // ---------------- bookkeeping ----------------
         bool finish = false, cand = false, is_long = false;
         int32_t score = 0;
-        uint32_t lext_out = 0;
         if (busy) {
-            if (phase == kSeed) {
-                seed = r;
-                phase = kRight;
-                pos_t = ht + L;
-                pos_q = hq + L;
-                rem = min(T.len - ht - L, Q.len - hq - L);
-                run = 0; best = 0; bext = 0; ext = 0;
-            } else {
-                run = r; best = b; bext = be;
-                ext += n;
-                rem -= n;
-                const bool side_done = ended || rem == 0;
-                if (!side_done && ext >= a.cap) {
-                    finish = true;      // still extending at the cap: defer to the walk
-                    cand = true;
-                    is_long = true;
-                } else if (!side_done) {
-                    if (phase == kRight) { pos_t += n; pos_q += n; }
-                    else { pos_t -= n; pos_q -= n; }
-                } else if (phase == kRight) {
-                    rbest = best;
-                    rext = bext;
-                    phase = kLeft;
-                    pos_t = ht - 1;
-                    pos_q = hq - 1;
-                    rem = min(ht, hq);
-                    run = 0; best = 0; bext = 0; ext = 0;
-                } else {
-                    finish = true;
-                    score = seed + best + rbest;
-                    lext_out = bext;
-                    cand = score >= thresh;
-                }
-            }
-            // An empty right side goes straight to the left; an empty left side finishes.
-            if (!finish && phase == kRight && rem == 0) {
-                rbest = 0; rext = 0;
-                phase = kLeft;
-                pos_t = ht - 1;
-                pos_q = hq - 1;
-                rem = min(ht, hq);
-                run = 0; best = 0; bext = 0; ext = 0;
-            }
-            if (!finish && phase == kLeft && rem == 0) {
+            if (rdone && ldone) {
                 finish = true;
-                score = seed + rbest;
-                lext_out = 0;
+                score = seed + rbest + lbest;
                 cand = score >= thresh;
+            } else if ((!rdone && rext >= a.cap) || (!ldone && lext >= a.cap)) {
+                finish = true;      // still extending at the cap: defer to the walk
+                cand = true;
+                is_long = true;
             }
         }
         const uint32_t m = __ballot_sync(kFull, finish && cand);
@@ -508,30 +681,31 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
                     Cand c;
                     c.unit = hu; c.t = ht; c.q = hq;
                     c.flags = is_long ? kCandLong : 0u;
-                    c.lext = lext_out; c.rext = rext; c.score = score; c.pad_ = 0;
+                    c.lext = lbext; c.rext = rbext; c.score = score; c.pad_ = 0;
                     a.cands[slot] = c;
                 }
             }
         }
-        if (finish) phase = kIdle;
+        if (finish) busy = false;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        n_windows += __shfl_xor_sync(kFull, n_windows, o);
-        n_cols += __shfl_xor_sync(kFull, n_cols, o);
-    }
-    if (lane == 0) {
-        atomicAdd(&a.stats[0], n_windows);
-        atomicAdd(&a.stats[1], n_raw);
-        atomicAdd(&a.stats[2], n_cols);
-    }
+    for (int o = 16; o > 0; o >>= 1) n_cols += __shfl_xor_sync(kFull, n_cols, o);
+    if (lane == 0) atomicAdd(&a.stats[2], n_cols);
 }
 
 void launch_screen(const ScreenArgs& a, int warps, int blocks, cudaStream_t st) {
+    // blocks = SMs x blocks-per-SM; for 8-warp blocks the register budget
+    // follows the requested blocks per SM (2: 128, 3: 85, 4: 64 registers).
+    const int per_sm = blocks / 148 > 0 ? blocks / 148 : 1;
     switch (warps) {
         case 4: count_launch(); k_screen<4, 4><<<blocks, 128, 0, st>>>(a); break;
         case 16: count_launch(); k_screen<16, 1><<<blocks, 512, 0, st>>>(a); break;
-        default: count_launch(); k_screen<8, 2><<<blocks, 256, 0, st>>>(a); break;
+        default:
+            count_launch();
+            if (per_sm >= 4) k_screen<8, 4><<<blocks, 256, 0, st>>>(a);
+            else if (per_sm == 3) k_screen<8, 3><<<blocks, 256, 0, st>>>(a);
+            else k_screen<8, 2><<<blocks, 256, 0, st>>>(a);
+            break;
     }
 }
 

@@ -40,12 +40,20 @@ void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64
                        const uint32_t* new_starts, uint32_t limit, uint32_t* new_positions, cudaStream_t st);
 
 // --- search ------------------------------------------------------------------
+// A raw seed hit: target position t, query window q, unit.
+struct Hit {
+    uint32_t t;
+    uint32_t q;
+    uint32_t unit;
+};
+
 struct ScreenArgs {
     const UnitDev* units;
     const SeqView* tsegs;
     const SeqView* qsegs;
     uint32_t n_units;
-    uint32_t n_tiles;
+    uint32_t tile_lo;      // this pass enumerates tiles [tile_lo, tile_hi)
+    uint32_t tile_hi;
     uint32_t* tile_counter;
     Pattern pat;
     uint32_t step;
@@ -54,6 +62,10 @@ struct ScreenArgs {
     Score sc;
     uint32_t cap;          // columns per side before a hit is deferred
     uint32_t qkey_total;   // size of the query key axis
+    Hit* hits;             // raw hits of this pass
+    uint64_t hit_cap;
+    unsigned long long* hit_count;   // hits enumerated (may exceed hit_cap: then the pass is redone smaller)
+    uint32_t* hit_next;    // x-drop work counter
     uint64_t* cand_keys;
     uint32_t* cand_vals;
     Cand* cands;
@@ -61,7 +73,10 @@ struct ScreenArgs {
     uint32_t* cand_count;
     unsigned long long* stats;   // [0] windows, [1] raw hits, [2] columns examined
 };
-// Fused hit enumeration and capped lane-per-hit x-drop.  grid = persistent.
+// Seed-hit enumeration: one warp per tile of 32 query windows; writes the
+// hits of every (window, variant) bucket to a.hits.
+void launch_enumerate(const ScreenArgs& a, int blocks, cudaStream_t st);
+// Capped lane-per-hit x-drop over a.hits; keeps the candidates.  grid = persistent.
 void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);
 
 struct WalkArgs {

@@ -73,20 +73,22 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_reduce(const T* in, const
     }
 }
 
-// Single-block exclusive scan of a short array in place; a[n] = total.
+// Single-block exclusive scan of a short array in place; a[n] = total.  Each
+// thread owns one contiguous segment: sum it, scan the 1024 sums, write.
 __global__ __launch_bounds__(1024) void k_scan_small(uint32_t* a, int n) {
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_total;
-    uint32_t carry = 0;
-    for (int base = 0; base < n; base += 1024) {
-        const int i = base + threadIdx.x;
-        const uint32_t v = i < n ? a[i] : 0;
-        const uint32_t ex = block_excl_scan<1024>(v, s_warp, &s_total);
-        if (i < n) a[i] = carry + ex;
-        carry += s_total;
-        __syncthreads();
+    const int per = (n + 1023) / 1024;
+    const int beg = min(n, (int)threadIdx.x * per), end = min(n, beg + per);
+    uint32_t s = 0;
+    for (int i = beg; i < end; i++) s += a[i];
+    uint32_t run = block_excl_scan<1024>(s, s_warp, &s_total);
+    for (int i = beg; i < end; i++) {
+        const uint32_t x = a[i];
+        a[i] = run;
+        run += x;
     }
-    if (threadIdx.x == 0) a[n] = carry;
+    if (threadIdx.x == 0) a[n] = s_total;
 }
 
 template <typename T>

@@ -224,3 +224,28 @@ def test_c1_both_strands(gxy, ctx):
         g = as_tuples(gxy.search(tab, T, qq, m, sp))
         o = as_tuples(O.search(ot, OT, oq, orc_params(m, sp))[0])
         assert g == o
+
+
+def test_window_passes_match_single_pass(gxy):
+    # A tiny raw-hit buffer forces the search into many window-range passes,
+    # including redone passes; the HSPs must not change.
+    rng = np.random.default_rng(21)
+    t, q = homologous_pair(rng, 400000, 0.8, lower=0.1)
+    sp = gxy.SearchParams()
+    c2 = gxy.Context(0)
+    try:
+        T, Q = gxy.PackedSeq.from_ascii(t), gxy.PackedSeq.from_ascii(q)
+        tab = gxy.PosTable.build(T, P12, 1, ctx=c2)
+        m = gxy.ScoringMatrix.hoxd70()
+        st1 = {}
+        ref = gxy.search(tab, T, Q, m, sp, stats=st1)
+        assert st1["raw_hits"] > 3 * 4096
+        c2.set_tuning(max_hits_per_pass=4096)
+        st2 = {}
+        got = gxy.search(tab, T, Q, m, sp, stats=st2)
+        assert st2["passes"] > 1
+        assert got.tobytes() == ref.tobytes()
+        assert st1["raw_hits"] == st2["raw_hits"] and st1["windows"] == st2["windows"]
+        tab.free()
+    finally:
+        c2.close()
