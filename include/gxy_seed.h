@@ -167,6 +167,27 @@ gxy_status gxy_table_build_view(gxy_ctx* ctx, const gxy_dseq* target, uint64_t l
 /* PosTable::prune_hot_words(limit) (src/pos_table.rs:113-136) on a built
  * table: drops every bucket with more than limit positions. */
 gxy_status gxy_table_prune_hot_words(gxy_table* t, uint32_t limit);
+/* PosTable::build(seq, pattern, step) for callers that cannot allocate
+ * device memory -- their memory belongs to another allocator (a framework's
+ * caching allocator or a fixed serving arena) or they cannot afford the
+ * device synchronisation an allocation implies.  This entry point has no
+ * counterpart in the reference; it exists only for those callers.
+ * It allocates nothing: the caller passes device buffers starts_out
+ * (starts_cap >= 4^weight + 1 entries) and positions_out (positions_cap >=
+ * the target's window count), and the staged target and every intermediate
+ * live in one fixed device array of about 17 MiB inside this library, held
+ * by each GPU that loads it until the process exits.  Limits: target length
+ * at most 1,048,576 bp (longer targets are rejected with GXY_EINVAL); no hot
+ * word pruning.  Runs on the calling thread's current device and the legacy
+ * default stream and returns when the table is complete; *n_positions
+ * receives starts[num_words].  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the array: builds from one process
+ * are serialised per device, and calls from elsewhere that overlap on the
+ * GPU would race on it. */
+gxy_status gxy_table_build_static(const gxy_packed_seq* target, const char* pattern01, uint32_t step,
+                                  uint32_t* starts_out, uint64_t starts_cap, uint32_t* positions_out,
+                                  uint64_t positions_cap, uint64_t* n_positions);
 gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_positions,
                           uint32_t* pattern_len, uint32_t* weight);
 /* Copies starts (num_words + 1 entries) and positions to host buffers; either
