@@ -685,4 +685,18 @@ int orc_search_units(int n_units, const orc_table* const* tables, const orc_seq*
     return j.err ? -1 : 0;
 }
 
+void* orc_diag_new(void) {
+    diag_hash* h = (diag_hash*)malloc(sizeof(diag_hash));
+    if (!h) return NULL;
+    if (dh_init(h, 64)) { free(h); return NULL; }
+    return h;
+}
+int orc_diag_admit(void* h, uint32_t t_pos, uint32_t q_pos) { return dh_admit((diag_hash*)h, t_pos, q_pos); }
+void orc_diag_mark_covered(void* h, uint32_t t_end, uint32_t q_end) { dh_mark_covered((diag_hash*)h, t_end, q_end); }
+void orc_diag_free(void* h) {
+    if (!h) return;
+    dh_free((diag_hash*)h);
+    free(h);
+}
+
 void orc_free(void* ptr) { free(ptr); }

@@ -122,6 +122,12 @@ int orc_search_units(int n_units, const orc_table* const* tables, const orc_seq*
                      const orc_seq* queries, const orc_params* p, int use_avx2, int n_threads,
                      orc_hsp** out, uint64_t* n_out, orc_stats* stats);
 
+/* DiagHash (src/diag_hash.rs:19-53) on its own, for the reference's KATs. */
+void* orc_diag_new(void);
+int orc_diag_admit(void* h, uint32_t t_pos, uint32_t q_pos);
+void orc_diag_mark_covered(void* h, uint32_t t_end, uint32_t q_end);
+void orc_diag_free(void* h);
+
 void orc_free(void* p);
 
 #ifdef __cplusplus

@@ -97,6 +97,11 @@ def lib():
                                        C.c_int, P(P(OrcHsp)), P(C.c_uint64), P(OrcStats)]
         L.orc_search_units.restype = C.c_int
         L.orc_free.argtypes = [C.c_void_p]
+        L.orc_diag_new.restype = C.c_void_p
+        L.orc_diag_admit.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        L.orc_diag_admit.restype = C.c_int
+        L.orc_diag_mark_covered.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+        L.orc_diag_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -261,3 +266,22 @@ def search_units(units, p: OrcParams, avx2: bool = True, threads: int = 1):
         stats.append({"windows": sts[i].windows, "raw_hits": sts[i].raw_hits, "extended": sts[i].extended,
                       "hsps": sts[i].hsps})
     return res, stats
+
+
+class DiagHash:
+    """DiagHash (src/diag_hash.rs:19-53)."""
+
+    def __init__(self):
+        self.h = lib().orc_diag_new()
+
+    def admit(self, t: int, q: int) -> bool:
+        return bool(lib().orc_diag_admit(self.h, t, q))
+
+    def mark_covered(self, t_end: int, q_end: int) -> None:
+        lib().orc_diag_mark_covered(self.h, t_end, q_end)
+
+    def __del__(self):
+        try:
+            lib().orc_diag_free(self.h)
+        except Exception:
+            pass

@@ -1,0 +1,99 @@
+"""Host-side logic that needs no GPU: the C ABI's exports, chunk planning, the
+Python mirror of the reference types, and unit sharding across ranks."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "gxy_seed.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(gxy_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(gxy):
+    lib = gxy.lib()
+    names = header_functions()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(lib, n), n
+    # and the Python binding declares every one of them
+    assert set(names) == set(gxy._lib.SIGNATURES)
+
+
+def chunk_target_ref(t_len, primary, halo):
+    # src/driver.rs:156-194 restated for the check.
+    if primary == 0 or t_len <= primary + halo:
+        return [(0, t_len, 0, t_len)]
+    out, ps = [], 0
+    while ps < t_len:
+        pe = min(ps + primary, t_len)
+        lo = max(ps - halo, 0)
+        hi = min(pe + halo, t_len)
+        out.append((lo, hi, ps - lo, pe - lo))
+        if pe == t_len:
+            break
+        ps = pe
+    return out
+
+
+@pytest.mark.parametrize("t_len,primary,halo", [(2032, 600, 200), (250_000_000, 10_000_000, 50_000),
+                                               (100, 0, 50_000), (10_050_000, 10_000_000, 50_000),
+                                               (10_050_001, 10_000_000, 50_000), (1, 1, 0)])
+def test_chunk_plan(gxy, t_len, primary, halo):
+    assert gxy.chunk_target(t_len, primary, halo) == chunk_target_ref(t_len, primary, halo)
+
+
+def test_chunk_plan_250mbp_has_25_chunks(gxy):
+    assert len(gxy.chunk_target(250_000_000, 10_000_000, 50_000)) == 25
+
+
+def test_reference_types(gxy):
+    p = gxy.SeedPattern.twelve_of_nineteen()
+    assert len(p) == 19 and p.weight() == 12 and p.bit_width() == 24 and p.num_words() == 1 << 24
+    assert gxy.SeedPattern.nineteen_of_twenty().weight() == 19
+    assert str(gxy.SeedPattern.parse("custom", "1101")) == "1101"
+    with pytest.raises(ValueError):
+        gxy.SeedPattern.parse("x", "11X0")
+    m = gxy.ScoringMatrix.hoxd70()
+    assert m.score(0, 0) == 91 and m.score(1, 1) == 100 and m.ambig_score == -100
+    sp = gxy.SearchParams()
+    assert (sp.step, sp.hsp.x_drop, sp.hsp.hsp_threshold, sp.transitions) == (1, 910, 3000, 1)
+    s = gxy.PackedSeq.from_ascii(b"ACgtNACGT")
+    assert s.to_ascii() == b"ACGTNACGT" and s.is_masked(2) and not s.is_valid(4)
+
+
+def test_packing_matches_oracle(gxy):
+    import numpy as np
+    import oracle as O
+    from helpers import rand_ascii
+    rng = np.random.default_rng(3)
+    for n in (0, 1, 7, 33, 1000, 4099):
+        b = rand_ascii(rng, n, b"ACGTUacgtuNRY-")
+        a, o = gxy.PackedSeq.from_ascii(b), O.pack_ascii(b)
+        assert bytes(a.codes[:(n + 3) // 4]) == bytes(o.codes[:(n + 3) // 4])
+        assert bytes(a.valid[:(n + 7) // 8]) == bytes(o.valid[:(n + 7) // 8])
+        assert bytes(a.mask[:(n + 7) // 8]) == bytes(o.mask[:(n + 7) // 8])
+
+
+def test_no_gpu_fails_loudly(gxy):
+    # Without a CUDA device the context cannot be created: no silent CPU path.
+    from conftest import has_gpu
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    with pytest.raises(gxy.GxyError):
+        gxy.Context(0)
+
+
+def test_shard_units_partition():
+    from lastz_gxy_b200.shard import shard_units
+    for world in (1, 2, 3, 8):
+        w = [((i * 7919) % 97) + 1 for i in range(50)]
+        parts = [shard_units(50, r, world, w) for r in range(world)]
+        assert sorted(sum(parts, [])) == list(range(50))
+        parts = [shard_units(50, r, world) for r in range(world)]
+        assert sorted(sum(parts, [])) == list(range(50))

@@ -1,0 +1,192 @@
+"""The oracle against the reference's own known-answer tests (CPU only).
+
+Each test names the reference test it ports (file:line).  These pin the C
+restatement in oracle/oracle.c; the GPU tests then compare the CUDA path with
+the oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import rand_ascii
+
+HOX = O.params
+
+
+# ---- src/dna.rs:43-74 via packing -------------------------------------------------
+def test_encode_and_case():
+    s = O.pack_ascii(b"ACGTacgtUuN")
+    codes = [(int(s.codes[i >> 2]) >> ((i & 3) * 2)) & 3 for i in range(11)]
+    valid = [(int(s.valid[i >> 3]) >> (i & 7)) & 1 for i in range(11)]
+    mask = [(int(s.mask[i >> 3]) >> (i & 7)) & 1 for i in range(11)]
+    assert codes[:10] == [0, 1, 2, 3, 0, 1, 2, 3, 3, 3]
+    assert valid == [1] * 10 + [0]
+    assert mask == [0, 0, 0, 0, 1, 1, 1, 1, 0, 1, 0]
+
+
+def test_ambiguous_bases_are_invalid():
+    s = O.pack_ascii(b"NnRrYyMmKkSsWwBbDdHhVv?-")
+    assert not any((int(s.valid[i >> 3]) >> (i & 7)) & 1 for i in range(24))
+
+
+# ---- src/sequences.rs:396-577 -------------------------------------------------------
+def to_ascii(s):
+    out = []
+    for i in range(s.len):
+        if (int(s.valid[i >> 3]) >> (i & 7)) & 1:
+            out.append(b"ACGT"[(int(s.codes[i >> 2]) >> ((i & 3) * 2)) & 3])
+        else:
+            out.append(ord("N"))
+    return bytes(out)
+
+
+def masked(s, i):
+    return bool((int(s.mask[i >> 3]) >> (i & 7)) & 1)
+
+
+def test_packed_roundtrip_and_rc():
+    assert to_ascii(O.pack_ascii(b"ACGTACGTNACG")) == b"ACGTACGTNACG"          # :396-402
+    rc = O.reverse_complement(O.pack_ascii(b"ACGTACGT"))
+    assert to_ascii(rc) == b"ACGTACGT"                                            # :413-419
+    assert to_ascii(O.reverse_complement(rc)) == b"ACGTACGT"
+    assert to_ascii(O.reverse_complement(O.pack_ascii(b"ACCGTTNAG"))) == b"CTNAACGGT"  # :422-426
+
+
+def test_soft_mask_and_slice():
+    p = O.pack_ascii(b"ACgtAC")                                                   # :457-465
+    assert [masked(p, i) for i in range(6)] == [False, False, True, True, False, False]
+    s = O.slice_to_new(O.pack_ascii(b"ACgtNACGT"), 2, 7)                          # :478-488
+    assert s.len == 5 and to_ascii(s) == b"GTNAC"
+    assert masked(s, 0) and masked(s, 1) and not masked(s, 3) and not masked(s, 4)
+    rc = O.reverse_complement(O.pack_ascii(b"ACgtAC"))                            # :567-577
+    assert masked(rc, 2) and masked(rc, 3) and not any(masked(rc, i) for i in (0, 1, 4, 5))
+
+
+# ---- src/seeds.rs:260-356 -----------------------------------------------------------
+def test_seed_words():
+    assert O.word_at(O.pack_ascii(b"ACGT"), "1111", 0) == 0x1B                  # :291-299
+    assert O.word_at(O.pack_ascii(b"ACGT"), "1001", 0) == 0b0011                # :301-309
+    assert O.word_at(O.pack_ascii(b"AcG"), "111", 0) is None                    # :311-318
+    assert O.word_at(O.pack_ascii(b"AcG"), "101", 0) is not None                # :320-328
+    assert O.word_at(O.pack_ascii(b"ACG"), "1111", 0) is None                   # :330-336
+
+
+def test_iter_with_stride():
+    s = O.pack_ascii(b"ACGNNACGT")                                              # :338-347
+    assert [p for p in range(7) if O.word_at(s, "111", p) is not None] == [0, 5, 6]
+    t = O.Table(O.pack_ascii(b"ACGTACGT"), "11", 3)                             # :349-356
+    pos = sorted(t.positions().tolist())
+    assert pos == [0, 3, 6]
+
+
+# ---- src/pos_table.rs:143-225 -------------------------------------------------------
+def test_pos_table_known_buckets():
+    s = O.pack_ascii(b"ACGTACGT")
+    t = O.Table(s, "111", 1)
+    w = {k: O.word_at(s, "111", p) for k, p in (("acg", 0), ("cgt", 1), ("gta", 2), ("tac", 3))}
+    assert t.lookup(w["acg"]) == [0, 4] and t.lookup(w["cgt"]) == [1, 5]          # :144-161
+    assert t.lookup(w["gta"]) == [2] and t.lookup(w["tac"]) == [3]
+    a = O.Table(O.pack_ascii(b"ACGACGACGACG"), "111", 1)                          # :164-175
+    st, pos = a.starts(), a.positions()
+    for i in range(a.num_words):
+        b = pos[st[i]:st[i + 1]]
+        assert all(b[k] < b[k + 1] for k in range(len(b) - 1))
+    s16 = O.pack_ascii(b"ACGTACGTACGTACGT")                                       # :177-187
+    assert len(O.Table(s16, "111", 3).positions()) < len(O.Table(s16, "111", 1).positions())
+    assert O.Table(s16, "111", 3).lookup(w["acg"]) == [0, 12]
+    assert O.Table(O.pack_ascii(b"ACGNACG"), "111", 1).lookup(w["acg"]) == [0, 4]  # :190-197
+    hot = O.pack_ascii(b"AAAAAAAAAAACG")                                          # :200-211
+    assert len(O.Table(hot, "111", 1).lookup(0)) >= 9
+    pr = O.Table(hot, "111", 1, max_word_count=4)
+    assert pr.lookup(0) == [] and pr.lookup(O.word_at(hot, "111", 10)) == [10]
+    m = O.Table(O.pack_ascii(b"ACGTACGTACGT"), "1111", 1)                         # :214-225
+    st = m.starts()
+    assert np.all(np.diff(st.astype(np.int64)) >= 0) and st[-1] == len(m.positions())
+
+
+# ---- src/diag_hash.rs:73-102 --------------------------------------------------------
+def test_diag_hash():
+    assert O.DiagHash().admit(10, 5)
+    h = O.DiagHash()
+    h.mark_covered(100, 50)
+    assert not h.admit(80, 30) and h.admit(200, 150)
+    assert h.admit(100, 49)
+    g = O.DiagHash()
+    g.mark_covered(200, 100)
+    g.mark_covered(150, 50)
+    assert not g.admit(199, 99) and g.admit(200, 100)
+
+
+# ---- src/hsp.rs:222-324 -------------------------------------------------------------
+def test_extend_hit_known_answers():
+    s = O.pack_ascii(b"ACGTACGTACGTACGT")
+    h = O.extend_hit(s, s, HOX(xdrop=100, hspthresh=100), 2, 2, 4)               # :222-232
+    assert h[0] == 0 and h[1] == 0 and h[2] == 16 and h[3] >= 100
+    t, q = O.pack_ascii(b"TTTACGTTTT"), O.pack_ascii(b"AAAACGAAAA")              # :234-245
+    assert O.extend_hit(t, q, HOX(xdrop=50, hspthresh=50), 3, 3, 3)[:3] == (3, 3, 3)
+    assert O.extend_hit(O.pack_ascii(b"ACGT"), O.pack_ascii(b"TTTT"),            # :247-253
+                        HOX(xdrop=100, hspthresh=10000), 0, 0, 4) is None
+    a = O.pack_ascii(b"ACGT")                                                     # :255-261
+    assert O.extend_hit(a, a, HOX(), 2, 2, 10) is None
+    hh = O.extend_hit(O.pack_ascii(b"ACGTACGT"), O.pack_ascii(b"ACNTACGT"),      # :263-271
+                      HOX(xdrop=500, hspthresh=200), 4, 4, 4)
+    assert hh is not None and hh[2] >= 4
+    c = O.pack_ascii(b"CCCCCCAAAAAACCCCCC")                                       # :316-324
+    h2 = O.extend_hit(c, c, HOX(xdrop=500, hspthresh=100), 8, 8, 2)
+    assert 8 - h2[0] == h2[0] + h2[2] - 10
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_avx2_matches_scalar(seed):
+    # The shape of the proptest simd_matches_scalar, src/hsp.rs:283-314.
+    if not O.lib().orc_has_avx2():
+        pytest.skip("no AVX2 on this host")
+    rng = np.random.default_rng(seed)
+    for _ in range(200):
+        tb = rand_ascii(rng, int(rng.integers(32, 200)), b"ACGTN")
+        qb = rand_ascii(rng, int(rng.integers(32, 200)), b"ACGTN")
+        L = int(rng.integers(4, 12))
+        xd = int(rng.integers(50, 2000))
+        T, Q = O.pack_ascii(tb), O.pack_ascii(qb)
+        p = HOX(xdrop=xd, hspthresh=0)
+        tp, qp = (len(tb) - L) // 2, (len(qb) - L) // 2
+        assert O.extend_hit(T, Q, p, tp, qp, L) == O.extend_hit(T, Q, p, tp, qp, L, avx2=True)
+
+
+# ---- src/seed_search.rs:362-506 -----------------------------------------------------
+def search(t, q, pattern, xdrop, thresh, transitions):
+    T, Q = O.pack_ascii(t), O.pack_ascii(q)
+    h, _ = O.search(O.Table(T, pattern, 1), T, Q, HOX(xdrop=xdrop, hspthresh=thresh, transitions=transitions))
+    return [tuple(int(x) for x in r) for r in h]
+
+
+def test_search_known_answers():
+    h = search(b"AAAAAGATTACACATGGCATGAAAAA", b"GATTACACATGGCATG", "1" * 8, 500, 1000, 0)   # :362-387
+    assert len(h) == 1 and h[0][:3] == (5, 0, 16)
+    assert search(b"AAAAACGTAAAAA", b"ACATA", "1" * 5, 500, 50, 0) == []                 # :389-426
+    assert search(b"AAAAACGTAAAAA", b"ACATA", "1" * 5, 500, 50, 1) != []
+    assert search(b"AAAAAAAAAA", b"CCCCCCCCCC", "1" * 5, 100, 100, 0) == []              # :428-447
+    d = search(b"AAAAAGATTACACATGGCATGTCGAAAAAA", b"GATTACACATGGCATGTCGA", "1" * 7, 500, 500, 0)
+    assert len(d) == len({x[0] - x[1] for x in d}) and (5, 0, 20) in [x[:3] for x in d]  # :449-479
+    two = search(b"AAAAGATTACACATGGAAAAAAAAAAAAGATTACACATGGTTTTT", b"GATTACACATGG", "1" * 8, 500, 500, 0)
+    assert len({x[0] - x[1] for x in two}) >= 2                                          # :481-506
+
+
+def test_fixture_smoke_hsp_level():
+    # tests/fixture_smoke.rs:15-51 (t_start 11, q_start 0, span 20) before gapped extension.
+    h = search(b"AAAAAAAAAAAGATTACACATGGCATGTCGAATTTTTTTTTTT", b"GATTACACATGGCATGTCGA", "1" * 12,
+               910, 500, 1)
+    assert (11, 0, 20) in [x[:3] for x in h]
+
+
+# ---- src/entropy.rs:72-122 ----------------------------------------------------------
+def test_entropy():
+    assert abs(O.shannon_entropy(O.pack_ascii(b"ACGTACGTACGTACGT"), 0, 16) - 2.0) < 1e-9
+    assert O.shannon_entropy(O.pack_ascii(b"AAAAAAAAAA"), 0, 10) == 0.0
+    assert abs(O.shannon_entropy(O.pack_ascii(b"ATATATATAT"), 0, 10) - 1.0) < 1e-9
+    s = O.pack_ascii(b"NNNNACGTACGT")
+    assert abs(O.shannon_entropy(s, 0, 12) - 2.0) < 1e-9
+    assert not O.passes_entropy_gate(O.pack_ascii(b"AAAAAAAAAA"), 0, 10, 10_000, 1_000)
+    b = O.pack_ascii(b"ACGTACGTACGT")
+    assert O.passes_entropy_gate(b, 0, 12, 1_000, 1_000) and not O.passes_entropy_gate(b, 0, 12, 999, 1_000)
+    a = O.pack_ascii(b"ATATATATAT")
+    assert not O.passes_entropy_gate(a, 0, 10, 1_000, 1_000) and O.passes_entropy_gate(a, 0, 10, 2_000, 1_000)
