@@ -288,6 +288,7 @@ gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
     API_CK(cudaDeviceGetDefaultMemPool(&pool, device));
     uint64_t thr = ~0ull;
     API_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    prims_init();
     gxy_ctx* c = new gxy_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;

@@ -298,6 +298,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
 
     // One pass: enumerate tiles [t0, t1) into the hit buffer, then screen them.
     bool single_pass_timing = false;
+    bool in_capture = false;
     auto pass = [&](uint32_t t0, uint32_t t1) -> gxy_status {
         GXY_CK(cudaMemsetAsync(cnt + 0, 0, 4, st));
         GXY_CK(cudaMemsetAsync(cnt + 3, 0, 4, st));
@@ -305,7 +306,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         sa.tile_lo = t0;
         sa.tile_hi = t1;
         launch_enumerate(sa, blocks_enum, st);
-        if (single_pass_timing) GXY_CK(cudaEventRecord(W->ev[3], st));
+        if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
         launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
         return GXY_OK;
     };
@@ -341,6 +342,18 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
 
         const bool single = pass_tiles >= tiles;
         const bool graph_now = use_graph && single;
+        // Ends an open capture if this attempt leaves early with an error.
+        struct CaptureGuard {
+            cudaStream_t st;
+            bool active = false;
+            ~CaptureGuard() {
+                if (!active) return;
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(st, &g);
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+            }
+        } capture{st};
         single_pass_timing = single;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t gexec = nullptr;
@@ -372,11 +385,16 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             GXY_CK(cudaEventRecord(W->ev[3], st));
             GXY_CK(cudaEventRecord(W->ev[1], st));
         } else {
-            if (graph_now) GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            // In graph mode the timing events sit around the graph launch.
+            in_capture = graph_now;
+            if (graph_now) {
+                GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                capture.active = true;
+            }
             GXY_CK(cudaMemsetAsync(W->counters.p, 0, 256, st));
-            GXY_CK(cudaEventRecord(W->ev[0], st));
+            if (!graph_now) GXY_CK(cudaEventRecord(W->ev[0], st));
             API_TRY_ENGINE(pass(0, (uint32_t)tiles));
-            GXY_CK(cudaEventRecord(W->ev[1], st));
+            if (!graph_now) GXY_CK(cudaEventRecord(W->ev[1], st));
         }
         const int which = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
                                          W->cv1.as<uint32_t>(), cnt + 1, 0, cap, passes, npass, W->ps, st);
@@ -420,10 +438,11 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             fin_unit = W->runit2.as<uint32_t>();
         }
         launch_fixup(fin, fin_unit, cnt + 2, cap, W->flags.as<uint8_t>(), blocks_misc, st);
-        GXY_CK(cudaEventRecord(W->ev[2], st));
+        if (!graph_now) GXY_CK(cudaEventRecord(W->ev[2], st));
         GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, 256, cudaMemcpyDeviceToHost, st));
 
         if (graph_now) {
+            capture.active = false;
             GXY_CK(cudaStreamEndCapture(st, &graph));
             cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
             if (e != cudaSuccess) {
@@ -431,7 +450,10 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                 set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
                 return GXY_ECUDA;
             }
-            e = cudaGraphLaunch(gexec, st);
+            in_capture = false;
+            e = cudaEventRecord(W->ev[0], st);
+            if (e == cudaSuccess) e = cudaGraphLaunch(gexec, st);
+            if (e == cudaSuccess) e = cudaEventRecord(W->ev[2], st);
             cudaGraphExecDestroy(gexec);
             cudaGraphDestroy(graph);
             if (e != cudaSuccess) {
@@ -474,9 +496,11 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.candidates = ncand;
         out.stats.hsps = nh;
         float ms = 0.f, ms_enum = 0.f, ms_screen = 0.f;
-        cudaEventElapsedTime(&ms, W->ev[0], W->ev[2]);
-        cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[3]);
-        cudaEventElapsedTime(&ms_screen, W->ev[3], W->ev[1]);
+        GXY_CK(cudaEventElapsedTime(&ms, W->ev[0], W->ev[2]));
+        if (!graph_now) {
+            GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[3]));
+            GXY_CK(cudaEventElapsedTime(&ms_screen, W->ev[3], W->ev[1]));
+        }
         out.stats.device_ms = ms;
         out.stats.enum_ms = single ? ms_enum : 0.0;
         out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;

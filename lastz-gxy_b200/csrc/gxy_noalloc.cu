@@ -65,6 +65,7 @@ gxy_status scratch_address(int dev, DeviceSlot& slot) {
     int sms = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return fail(GXY_ECUDA, std::string("device attribute: ") + cudaGetErrorString(e));
+    prims_init();
     slot.sm_count = sms;
     slot.ptr = static_cast<unsigned char*>(p);
     return GXY_OK;

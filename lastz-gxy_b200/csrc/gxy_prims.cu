@@ -257,14 +257,15 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(const K* __restr
 }
 
 template <typename K>
+void radix_attr() {
+    cudaFuncSetAttribute(k_radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(SortSmem<K>));
+}
+
+template <typename K>
 int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
                const RadixPass* passes, int npass, const PrimScratch& ps, cudaStream_t st) {
-    static bool attr_set = false;
     const size_t smem = sizeof(SortSmem<K>);
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
     K* kin = ka;
     uint32_t* vin = va;
     K* kout = kb;
@@ -286,6 +287,11 @@ int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, 
 }
 
 }  // namespace
+
+void prims_init() {
+    radix_attr<uint32_t>();
+    radix_attr<uint64_t>();
+}
 
 void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
               bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {

@@ -36,6 +36,10 @@ void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t
 void scan_u8(const uint8_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st);
 
+// Per-device kernel attributes of the primitives; call once with the device
+// current, before any stream capture.
+void prims_init();
+
 // One digit pass: shift/bits select the digit (bits <= 8).
 struct RadixPass {
     int shift;

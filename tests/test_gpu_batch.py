@@ -1,0 +1,120 @@
+"""Batched launches: many (table, query, strand) units in one pass through the
+pipeline must give each unit exactly the reference search() result.
+
+Shapes: uneven query lengths, both strands, several targets, the driver's
+chunk/halo split with its primary-region filter (src/driver.rs:156-256), and
+the CUDA-graph capture of the batch."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import homologous_pair, rand_ascii
+
+pytestmark = pytest.mark.gpu
+P12 = "1110100110010101111"
+
+
+def make_queries(rng, target: bytes, n: int, lo=1000, hi=30000):
+    from lastz_gxy_b200 import synth
+    t = np.frombuffer(target, np.uint8)
+    out = []
+    for i in range(n):
+        L = int(rng.integers(lo, hi))
+        s = int(rng.integers(0, len(t) - L))
+        ident = float(rng.uniform(0.65, 0.95))
+        out.append(synth.evolve(rng, t[s:s + L].copy(), ident, 0.005).tobytes())
+    return out
+
+
+def oracle_units(target: bytes, queries, units, pattern=P12, mwc=0, sp=None):
+    T = O.pack_ascii(target)
+    tab = O.Table(T, pattern, 1, mwc)
+    p = O.params() if sp is None else sp
+    res = []
+    for (ti, qi, strand) in units:
+        Q = O.pack_ascii(queries[qi])
+        if strand:
+            Q = O.reverse_complement(Q)
+        h, _ = O.search(tab, T, Q, p)
+        res.append(h)
+    return res
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_matches_per_unit_search(gxy, ctx, use_graph):
+    rng = np.random.default_rng(31)
+    target = rand_ascii(rng, 200_000, b"ACGTACGTACGTacgtN")
+    queries = make_queries(rng, target, 12)
+    T = gxy.PackedSeq.from_ascii(target)
+    tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    dq = [gxy.PackedSeq.from_ascii(q).to_device(ctx) for q in queries]
+    units = [(0, qi, s) for qi in range(len(queries)) for s in (0, 1)]
+    st = {}
+    got = gxy.batch_search([tab], dq, units, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams(),
+                           use_graph=use_graph, stats=st)
+    want = oracle_units(target, queries, units)
+    assert sum(len(w) for w in want) > 0
+    for u, (g, w) in enumerate(zip(got, want)):
+        assert g.tobytes() == w.tobytes(), u
+
+
+def test_batch_graph_repeat_is_identical(gxy, ctx):
+    rng = np.random.default_rng(32)
+    target = rand_ascii(rng, 100_000, b"ACGT")
+    queries = make_queries(rng, target, 6, 2000, 20000)
+    tab = gxy.PosTable.build(gxy.PackedSeq.from_ascii(target), P12, 1, ctx=ctx)
+    dq = [gxy.PackedSeq.from_ascii(q).to_device(ctx) for q in queries]
+    units = [(0, qi, s) for qi in range(len(queries)) for s in (0, 1)]
+    m, sp = gxy.ScoringMatrix.hoxd70(), gxy.SearchParams()
+    a = gxy.batch_search([tab], dq, units, m, sp, use_graph=True)
+    b = gxy.batch_search([tab], dq, units, m, sp, use_graph=True)
+    c = gxy.batch_search([tab], dq, units, m, sp, use_graph=False)
+    for x, y, z in zip(a, b, c):
+        assert x.tobytes() == y.tobytes() == z.tobytes()
+
+
+def test_batch_several_targets(gxy, ctx):
+    rng = np.random.default_rng(33)
+    targets = [rand_ascii(rng, n, b"ACGTACGTacgt") for n in (60_000, 150_000, 90_000)]
+    queries, units = [], []
+    for ti, t in enumerate(targets):
+        for q in make_queries(rng, t, 3, 1000, 20000):
+            units.append((ti, len(queries), 0))
+            units.append((ti, len(queries), 1))
+            queries.append(q)
+    tabs = [gxy.PosTable.build(gxy.PackedSeq.from_ascii(t), P12, 1, ctx=ctx) for t in targets]
+    dq = [gxy.PackedSeq.from_ascii(q).to_device(ctx) for q in queries]
+    got = gxy.batch_search(tabs, dq, units, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams())
+    for u, (ti, qi, s) in enumerate(units):
+        want = oracle_units(targets[ti], queries, [(0, qi, s)])[0]
+        assert got[u].tobytes() == want.tobytes(), u
+
+
+@pytest.mark.parametrize("transitions,mwc", [(1, 0), (0, 0), (1, 3)])
+def test_chunked_batch_matches_driver_semantics(gxy, ctx, transitions, mwc):
+    # driver.rs:156-256: per chunk a table over the chunk copy (extension stops
+    # at the chunk edges), per (chunk, query, strand) a search, then the
+    # primary-region filter on t_start.
+    rng = np.random.default_rng(40 + transitions + mwc)
+    target, query = homologous_pair(rng, 130_000, 0.85, lower=0.1, nfrac=0.002)
+    primary, halo = 30_000, 5_000
+    chunks = gxy.chunk_target(len(target), primary, halo)
+    assert len(chunks) > 3
+    dT = gxy.PackedSeq.from_ascii(target).to_device(ctx)
+    tabs = [gxy.PosTable.build_view(dT, lo, hi, P12, 1, max_word_count=mwc, ctx=ctx) for lo, hi, _, _ in chunks]
+    dq = [gxy.PackedSeq.from_ascii(query).to_device(ctx)]
+    units = [(ci, 0, s, chunks[ci][2], chunks[ci][3]) for ci in range(len(chunks)) for s in (0, 1)]
+    sp = gxy.SearchParams(transitions=transitions)
+    got = gxy.batch_search(tabs, dq, units, gxy.ScoringMatrix.hoxd70(), sp)
+    OT = O.pack_ascii(target)
+    OQ = O.pack_ascii(query)
+    total = 0
+    for u, (ci, _, s, plo, phi) in enumerate(units):
+        lo, hi = chunks[ci][0], chunks[ci][1]
+        CS = O.slice_to_new(OT, lo, hi)
+        tab = O.Table(CS, P12, 1, mwc)
+        h, _ = O.search(tab, CS, O.reverse_complement(OQ) if s else OQ, O.params(transitions=transitions))
+        h = h[(h["t_start"] >= plo) & (h["t_start"] < phi)]
+        total += len(h)
+        assert got[u].tobytes() == h.tobytes(), u
+    assert total > 0
