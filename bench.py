@@ -127,13 +127,21 @@ def mbp2(lt: int, lq: int, strands: int = 2) -> float:
     return (lt / 1e6) * (lq / 1e6) * strands
 
 
-def screen_bytes(st: dict, lq: int, n_var: int) -> float:
-    """Algorithmic bytes of one screen launch (enumeration fused with x-drop):
-    0.5 B/bp query read + 8 B of starts per (window, variant) + 4 B per raw hit
-    (positions) + 3/8 B x 2 per examined column (codes + valid bits of both
-    sequences) + 44 B per candidate written (record, key, index)."""
-    return 0.5 * lq + 8.0 * n_var * st["windows"] + 4.0 * st["raw_hits"] + 0.75 * st["columns"] \
-        + 44.0 * st["candidates"]
+def screen_bytes(st: dict, seed_len: int) -> float:
+    """Algorithmic bytes of one x-drop screen launch: 8 B per raw hit read
+    (t, q), 3/8 B x 2 per examined column -- codes + valid bits of both
+    sequences over the seed footprint and the columns both sides scanned,
+    break columns included -- and 44 B per candidate written (record, key,
+    index)."""
+    cols = st["columns"] + seed_len * st["raw_hits"]
+    return 8.0 * st["raw_hits"] + 0.75 * cols + 44.0 * st["candidates"]
+
+
+def enum_bytes(st: dict, lq: int, n_var: int) -> float:
+    """Algorithmic bytes of one enumeration launch: 0.5 B/bp of query read,
+    8 B of starts per (seedable window, variant), 4 B of positions per raw hit,
+    8 B per raw hit written."""
+    return 0.5 * lq + 8.0 * n_var * st["windows"] + 12.0 * st["raw_hits"]
 
 
 def run_ours(args, rank: int, world: int, device: int):
@@ -213,9 +221,12 @@ def run_ours(args, rank: int, world: int, device: int):
     # Roofline of the dominant kernel (the screen), from the timed steps.
     stats = [s for s, _ in dev_col]
     scr_ms = statistics.mean(s["screen_ms"] for s in stats)
-    scr_bytes = statistics.mean(screen_bytes(s, lq, n_var) for s in stats)
+    scr_bytes = statistics.mean(screen_bytes(s, 19) for s in stats)
+    en_ms = statistics.mean(s["enum_ms"] for s in stats)
+    en_bytes = statistics.mean(enum_bytes(s, lq, n_var) for s in stats)
     peak, peak_kind = peaks()
     achieved = scr_bytes / (scr_ms / 1e3) / 1e9
+    en_achieved = en_bytes / (en_ms / 1e3) / 1e9
     tr = profiled_traffic()
     raw = statistics.mean(s["raw_hits"] for s in stats)
     nh = sum(n for _, n in dev_col) / args.steps
@@ -241,7 +252,11 @@ def run_ours(args, rank: int, world: int, device: int):
                      "traffic": tr.get("bytes_per_launch") if tr else None,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s",
-                     "screen_ms": round(scr_ms, 3), "algorithmic_bytes_per_launch": int(scr_bytes)},
+                     "kernel_ms": round(scr_ms, 3), "algorithmic_bytes_per_launch": int(scr_bytes)},
+        "roofline_enumerate": {"bound": "hbm", "kernel": "k_enumerate", "achieved": round(en_achieved, 1),
+                               "peak": peak, "unit": "GB/s", "frac": round(en_achieved / peak, 4),
+                               "kernel_ms": round(en_ms, 3), "algorithmic_bytes_per_launch": int(en_bytes),
+                               "traffic": tr.get("enumerate_bytes_per_launch") if tr else None},
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -299,6 +314,71 @@ def run_reference(args):
     }
 
 
+def run_batched(args):
+    """Uneven batch: one 50 Mbp chromosome-style target and 4,096 log-normal query
+    contigs (~200 Mbp), both strands -- one batched launch per pass against the
+    plain per-(query, strand) search() loop on the same GPU; results must match."""
+    import torch
+    g = _pkg()
+    from lastz_gxy_b200 import synth
+    from lastz_gxy_b200.autotune import autotune
+    s = args.scale
+    t0 = time.time()
+    tgt, queries = synth.c3(target_len=int(50_000_000 * s), n_queries=max(8, int(4096 * s)),
+                            total=int(200_000_000 * s))
+    gen_s = time.time() - t0
+    ctx = g.Context(0)
+    m, sp = g.ScoringMatrix.hoxd70(), g.SearchParams()
+    dT = g.PackedSeq.from_ascii(tgt.tobytes()).to_device(ctx)
+    ctx.mark(0)
+    tab = g.PosTable.build(dT, P12, 1, ctx=ctx)
+    ctx.mark(1)
+    table_ms = ctx.elapsed_ms(0, 1)
+    dq = [g.PackedSeq.from_ascii(q.tobytes()).to_device(ctx) for q in queries]
+    units = [(0, qi, st) for qi in range(len(queries)) for st in (0, 1)]
+    tune = autotune(ctx, [tab], dq, units, m, sp, workload="uneven-batch", sample_units=256, use_cache=False)
+    # Batched: every unit in one call (graph-captured when it fits one pass).
+    batched = None
+    b_times = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        st = {}
+        ctx.mark(2)
+        out = g.batch_search([tab], dq, units, m, sp, use_graph=True, stats=st, ctx=ctx)
+        ctx.mark(3)
+        if i >= args.warmup:
+            b_times.append(ctx.elapsed_ms(2, 3))
+        batched = (out, st)
+    # Plain: the driver's loop, one search() per (query, strand), reverse complement per query.
+    plain = []
+    ctx.mark(4)
+    for q in dq:
+        qr = q.reverse_complement()
+        plain.append(g.search_device(tab, q, m, sp))
+        plain.append(g.search_device(tab, qr, m, sp))
+        qr.free()
+    ctx.mark(5)
+    plain_ms = ctx.elapsed_ms(4, 5)
+    same = all(a.tobytes() == b.tobytes() for a, b in zip(batched[0], plain))
+    lt = len(tgt)
+    mbp2_total = sum(mbp2(lt, len(q), 1) for q in queries) * 2
+    b_ms = statistics.mean(b_times)
+    st = batched[1]
+    return {
+        "workload": "uneven batch: %d bp target x %d query contigs (%d bp, log-normal), both strands"
+                    % (lt, len(queries), sum(len(q) for q in queries)),
+        "metric": "seed->HSP Mbp^2/s", "unit": "Mbp^2/s", "mbp2": round(mbp2_total, 2),
+        "batched": {"value": round(mbp2_total / (b_ms / 1e3), 2), "ms": round(b_ms, 2), "steps": args.steps,
+                    "passes": st.get("passes"), "raw_hits": st["raw_hits"], "candidates": st["candidates"],
+                    "hsps": st["hsps"]},
+        "plain": {"value": round(mbp2_total / (plain_ms / 1e3), 2), "ms": round(plain_ms, 2),
+                  "launches": 2 * len(queries)},
+        "speedup_batched_vs_plain": round(plain_ms / b_ms, 3),
+        "bit_identical": same, "table_ms": round(table_ms, 3), "generate_s": round(gen_s, 1),
+        "autotune": tune["tuning"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -307,6 +387,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-bp", type=int, default=500_000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--scale", type=float, default=1.0, help="batched workload size factor")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -314,6 +396,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)
+        return
+    if args.workload == "batched":
+        print(json.dumps(run_batched(args)), flush=True)
         return
     if world > 1:
         import datetime
