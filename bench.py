@@ -379,6 +379,24 @@ def run_batched(args):
     }
 
 
+def run_case(args):
+    """One plus-strand search on the chromosome-style workload of --length bp
+    (target and query both that long): the small case the ncu captures use."""
+    g = _pkg()
+    from lastz_gxy_b200 import synth
+    pr = synth.c2(length=args.length)
+    ctx = g.Context(0)
+    dT = g.PackedSeq.from_ascii(pr.target.tobytes()).to_device(ctx)
+    dQ = g.PackedSeq.from_ascii(pr.query.tobytes()).to_device(ctx)
+    tab = g.PosTable.build(dT, P12, 1, ctx=ctx)
+    out = []
+    for _ in range(max(1, args.steps)):
+        st = {}
+        h = g.search_device(tab, dQ, g.ScoringMatrix.hoxd70(), g.SearchParams(), stats=st)
+        out.append({"hsps": len(h), **st})
+    return {"workload": f"case {args.length} bp", "runs": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,7 +405,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-bp", type=int, default=500_000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "case"])
+    ap.add_argument("--length", type=int, default=4_000_000, help="case workload length (bp)")
     ap.add_argument("--scale", type=float, default=1.0, help="batched workload size factor")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -399,6 +418,9 @@ def main():
         return
     if args.workload == "batched":
         print(json.dumps(run_batched(args)), flush=True)
+        return
+    if args.workload == "case":
+        print(json.dumps(run_case(args)), flush=True)
         return
     if world > 1:
         import datetime

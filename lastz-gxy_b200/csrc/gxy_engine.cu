@@ -90,6 +90,12 @@ gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t s
     return GXY_OK;
 }
 
+void dseq_destroy_async(gxy_dseq* s, cudaStream_t st) {
+    if (!s) return;
+    if (s->alloc) cudaFreeAsync(s->alloc, st);
+    delete s;
+}
+
 void dseq_destroy(gxy_dseq* s) {
     if (!s) return;
     dev_free(s->alloc);

@@ -118,6 +118,8 @@ void checkin(gxy_ctx* ctx, Worker* w);
 
 gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t st);
 void dseq_destroy(gxy_dseq* s);
+// Frees in stream order on st: for sequences only st has used.
+void dseq_destroy_async(gxy_dseq* s, cudaStream_t st);
 gxy_status dseq_fill_host(gxy_dseq* d, const gxy_packed_seq* h, cudaStream_t st);
 SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi);
 

@@ -74,16 +74,36 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_reduce(const T* in, const
 }
 
 // Single-block exclusive scan of a short array in place; a[n] = total.  Each
-// thread owns one contiguous segment: sum it, scan the 1024 sums, write.
+// thread owns one contiguous segment: sum it (eight independent loads at a
+// time), scan the 1024 sums, write.
 __global__ __launch_bounds__(1024) void k_scan_small(uint32_t* a, int n) {
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_total;
     const int per = (n + 1023) / 1024;
     const int beg = min(n, (int)threadIdx.x * per), end = min(n, beg + per);
     uint32_t s = 0;
-    for (int i = beg; i < end; i++) s += a[i];
+    int i = beg;
+    for (; i + 8 <= end; i += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = a[i + k];
+#pragma unroll
+        for (int k = 0; k < 8; k++) s += v[k];
+    }
+    for (; i < end; i++) s += a[i];
     uint32_t run = block_excl_scan<1024>(s, s_warp, &s_total);
-    for (int i = beg; i < end; i++) {
+    i = beg;
+    for (; i + 8 <= end; i += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = a[i + k];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            a[i + k] = run;
+            run += v[k];
+        }
+    }
+    for (; i < end; i++) {
         const uint32_t x = a[i];
         a[i] = run;
         run += x;

@@ -1,15 +1,342 @@
-// gxy_server.cu -- serving loop (placeholder until the loop lands).
+// gxy_server.cu -- serving loop over resident position tables.
+//
+// Requests (a query against one resident table, one or both strands) are
+// copied in by gxy_server_submit and queued.  max_streams dispatcher threads
+// each own a worker stream; a free dispatcher forms a batch from the queue,
+// admitting requests in arrival order while the device-memory budget
+// (max_device_bytes, and the device's actually free memory) and the unit
+// limits allow, runs it through the same pipeline as gxy_batch_search, and
+// hands each request its HSPs.  Requests that arrive while batches run are
+// admitted by the next free dispatcher, so batches overlap on the device.
+// Every unit's result is computed exactly as a lone search() would compute it
+// (units never share diagonal state), so a request's HSPs are the same alone
+// and in any mix.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <thread>
+#include <vector>
+
 #include "gxy_engine.cuh"
 
+namespace gxy {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    uint32_t table = 0;
+    std::vector<uint8_t> codes, valid, mask;
+    uint64_t len = 0;
+    uint64_t bytes = 0;                 // admission estimate
+    Clock::time_point submitted;
+    Clock::time_point done_at;
+    bool done = false;
+    gxy_status status = GXY_OK;
+    std::vector<gxy_hsp> plus, minus;
+};
+
+uint32_t windows_of(uint64_t len, uint32_t L, uint32_t step) {
+    if (len < L) return 0;
+    return (uint32_t)((len - L) / step + 1);
+}
+
+}  // namespace
+}  // namespace gxy
+
+using namespace gxy;
+
+struct gxy_server {
+    gxy_ctx* ctx = nullptr;
+    std::vector<const gxy_table*> tables;
+    gxy_search_params params{};
+    gxy_server_opts opts{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> pending;
+    std::map<uint64_t, Request*> requests;
+    std::vector<std::thread> threads;
+    bool stop = false;
+    uint64_t next_id = 1;
+    uint64_t bytes_in_use = 0;
+    uint64_t units_in_flight = 0;
+    gxy_server_stats st{};
+};
+
+namespace {
+
+// Runs one batch of requests on worker W.  Called without the server lock.
+gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
+    cudaStream_t stream = W->st;
+    const Pattern& pat = s->tables[0]->pat;
+    std::vector<gxy_dseq*> owned;
+    auto cleanup = [&]() {
+        // Only this worker's stream used them: no device-wide sync.
+        for (gxy_dseq* d : owned) dseq_destroy_async(d, stream);
+    };
+    std::vector<SeqView> tsegs, qsegs;
+    std::vector<int> tseg_of(s->tables.size(), -1);
+    std::vector<UnitPlan> plan;
+    std::vector<std::pair<size_t, int>> unit_owner;   // (request index, strand)
+    const int strands = s->opts.both_strands ? 2 : 1;
+    uint64_t max_cols = 0;
+    for (size_t r = 0; r < batch.size(); r++) {
+        Request* q = batch[r];
+        const gxy_table* t = s->tables[q->table];
+        if (tseg_of[q->table] < 0) {
+            tseg_of[q->table] = (int)tsegs.size();
+            tsegs.push_back(view_of(t->seq, t->lo, t->hi));
+        }
+        gxy_dseq* d = nullptr;
+        gxy_status e = dseq_alloc(s->ctx, q->len, &d, stream);
+        if (e != GXY_OK) {
+            cleanup();
+            return e;
+        }
+        owned.push_back(d);
+        gxy_packed_seq h{q->codes.data(), q->valid.data(), q->mask.data(), q->len};
+        e = dseq_fill_host(d, &h, stream);
+        if (e != GXY_OK) {
+            cleanup();
+            return e;
+        }
+        max_cols = std::max<uint64_t>(max_cols, std::min<uint64_t>(t->hi - t->lo, q->len));
+        for (int sd = 0; sd < strands; sd++) {
+            const gxy_dseq* qs = d;
+            if (sd == 1) {
+                gxy_dseq* rc = nullptr;
+                e = dseq_alloc(s->ctx, q->len, &rc, stream);
+                if (e != GXY_OK) {
+                    cleanup();
+                    return e;
+                }
+                owned.push_back(rc);
+                launch_reverse_complement(d->codes, d->valid, d->mask, d->len, rc->codes, rc->valid, rc->mask,
+                                          stream);
+                qs = rc;
+            }
+            UnitPlan u;
+            u.tseg = (uint32_t)tseg_of[q->table];
+            u.qseg = (uint32_t)qsegs.size();
+            qsegs.push_back(view_of(qs, 0, qs->len));
+            u.starts = t->starts;
+            u.positions = t->positions;
+            u.nwin = windows_of(q->len, pat.len, s->params.step);
+            u.primary_lo = u.primary_hi = 0;
+            plan.push_back(u);
+            unit_owner.push_back({r, sd});
+        }
+    }
+    gxy_status e = check_params(&s->params, max_cols);
+    RunResult res;
+    if (e == GXY_OK) e = run_units(s->ctx, W, plan, tsegs, qsegs, pat, s->params, false, res);
+    cleanup();
+    if (e != GXY_OK) return e;
+    for (size_t i = 0; i < res.hsps.size(); i++) {
+        const auto& o = unit_owner[res.unit[i]];
+        (o.second ? batch[o.first]->minus : batch[o.first]->plus).push_back(res.hsps[i]);
+    }
+    return GXY_OK;
+}
+
+void dispatcher(gxy_server* s) {
+    cudaSetDevice(s->ctx->device);
+    gxy_status err;
+    Worker* W = checkout(s->ctx, &err);
+    if (!W) {
+        std::lock_guard<std::mutex> g(s->mu);
+        for (Request* q : s->pending) {
+            q->status = err;
+            q->done = true;
+            q->done_at = Clock::now();
+        }
+        s->pending.clear();
+        s->cv_done.notify_all();
+        return;
+    }
+    const uint32_t strands = s->opts.both_strands ? 2 : 1;
+    for (;;) {
+        std::vector<Request*> batch;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+            if (s->stop && s->pending.empty()) break;
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            uint64_t batch_units = 0;
+            while (!s->pending.empty()) {
+                Request* q = s->pending.front();
+                const bool fits_mem = s->bytes_in_use + q->bytes <= s->opts.max_device_bytes &&
+                                      q->bytes + (64ull << 20) <= free_b;
+                const bool fits_units = s->units_in_flight + strands <= s->opts.max_units &&
+                                        batch_units + strands <= s->opts.max_batch_units;
+                // A request that could never fit alone is still run alone.
+                const bool alone = batch.empty() && s->units_in_flight == 0;
+                if (!(fits_mem && fits_units) && !alone) break;
+                s->pending.pop_front();
+                batch.push_back(q);
+                s->bytes_in_use += q->bytes;
+                s->units_in_flight += strands;
+                batch_units += strands;
+                if (free_b > q->bytes) free_b -= q->bytes;
+            }
+            if (batch.empty()) {
+                // Budget taken by batches in flight: wait for one to finish.
+                s->cv_done.wait_for(lk, std::chrono::milliseconds(2));
+                continue;
+            }
+            s->st.batches++;
+            s->st.max_inflight_units = std::max<uint64_t>(s->st.max_inflight_units, s->units_in_flight);
+            s->st.bytes_in_use = s->bytes_in_use;
+        }
+        const gxy_status e = run_batch(s, W, batch);
+        {
+            std::lock_guard<std::mutex> g(s->mu);
+            const auto now = Clock::now();
+            for (Request* q : batch) {
+                q->status = e;
+                q->done = true;
+                q->done_at = now;
+                q->codes.clear();
+                q->codes.shrink_to_fit();
+                q->valid.clear();
+                q->valid.shrink_to_fit();
+                q->mask.clear();
+                q->mask.shrink_to_fit();
+                s->bytes_in_use -= q->bytes;
+                s->units_in_flight -= strands;
+                s->st.completed++;
+            }
+            s->st.bytes_in_use = s->bytes_in_use;
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+    checkin(s->ctx, W);
+}
+
+gxy_status copy_out(const std::vector<gxy_hsp>& v, gxy_hsp_buf* out) {
+    if (!out) return GXY_OK;
+    out->len = v.size();
+    out->cap = v.size();
+    out->hsps = static_cast<gxy_hsp*>(malloc(std::max<size_t>(v.size(), 1) * sizeof(gxy_hsp)));
+    if (!out->hsps) return GXY_ENOMEM;
+    if (!v.empty()) memcpy(out->hsps, v.data(), v.size() * sizeof(gxy_hsp));
+    return GXY_OK;
+}
+
+}  // namespace
+
 extern "C" {
-gxy_status gxy_server_create(gxy_ctx*, uint32_t, const gxy_table* const*, const gxy_search_params*,
-                             const gxy_server_opts*, gxy_server**) {
-    return GXY_EUNSUPPORTED;
+
+gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,
+                             const gxy_search_params* params, const gxy_server_opts* opts, gxy_server** out) {
+    if (!ctx || !n_tables || !tables || !params || !out) return GXY_EINVAL;
+    for (uint32_t i = 0; i < n_tables; i++) {
+        if (!tables[i]) return GXY_EINVAL;
+        if (tables[i]->pat.len != tables[0]->pat.len || tables[i]->pat.care_mask != tables[0]->pat.care_mask) {
+            set_error("all resident tables of a server must share one seed pattern");
+            return GXY_EINVAL;
+        }
+    }
+    if (params->step < 1) {
+        set_error("step must be >= 1");
+        return GXY_EINVAL;
+    }
+    gxy_server* s = new gxy_server();
+    s->ctx = ctx;
+    s->tables.assign(tables, tables + n_tables);
+    s->params = *params;
+    gxy_server_opts o = opts ? *opts : gxy_server_opts{};
+    if (!o.max_device_bytes) o.max_device_bytes = 16ull << 30;
+    if (!o.max_units) o.max_units = 8192;
+    if (!o.max_streams) o.max_streams = 2;
+    if (!o.max_batch_units) o.max_batch_units = 1024;
+    s->opts = o;
+    for (uint32_t i = 0; i < o.max_streams; i++) s->threads.emplace_back(dispatcher, s);
+    *out = s;
+    return GXY_OK;
 }
-gxy_status gxy_server_submit(gxy_server*, uint32_t, const gxy_packed_seq*, uint64_t*) { return GXY_EUNSUPPORTED; }
-gxy_status gxy_server_wait(gxy_server*, uint64_t, uint32_t, gxy_hsp_buf*, gxy_hsp_buf*, double*) {
-    return GXY_EUNSUPPORTED;
+
+gxy_status gxy_server_submit(gxy_server* s, uint32_t table, const gxy_packed_seq* query, uint64_t* request_id) {
+    if (!s || !query || !request_id || table >= s->tables.size()) return GXY_EINVAL;
+    if (query->len && (!query->codes || !query->valid || !query->mask)) return GXY_EINVAL;
+    if (query->len >= (1ull << 32)) return GXY_EUNSUPPORTED;
+    Request* q = new Request();
+    q->table = table;
+    q->len = query->len;
+    q->codes.assign(query->codes, query->codes + (query->len + 3) / 4);
+    q->valid.assign(query->valid, query->valid + (query->len + 7) / 8);
+    q->mask.assign(query->mask, query->mask + (query->len + 7) / 8);
+    // Device bytes while in flight: the query and its reverse complement
+    // (0.5 B/bp each with pads) plus a per-base share of the raw-hit and
+    // candidate scratch.
+    q->bytes = (uint64_t)q->len * 24 + (1u << 20);
+    q->submitted = Clock::now();
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (s->stop) {
+            delete q;
+            return GXY_EINVAL;
+        }
+        q->id = s->next_id++;
+        s->requests[q->id] = q;
+        s->pending.push_back(q);
+        s->st.submitted++;
+        *request_id = q->id;
+    }
+    s->cv_work.notify_one();
+    return GXY_OK;
 }
-gxy_status gxy_server_get_stats(gxy_server*, gxy_server_stats*) { return GXY_EUNSUPPORTED; }
-gxy_status gxy_server_destroy(gxy_server*) { return GXY_EUNSUPPORTED; }
+
+gxy_status gxy_server_wait(gxy_server* s, uint64_t request_id, uint32_t timeout_ms, gxy_hsp_buf* plus,
+                           gxy_hsp_buf* minus, double* latency_ms) {
+    if (!s) return GXY_EINVAL;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) {
+        set_error("unknown request id");
+        return GXY_EINVAL;
+    }
+    Request* q = it->second;
+    if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; })) {
+        set_error("request still running after the timeout");
+        return GXY_ETIMEDOUT;
+    }
+    s->requests.erase(it);
+    lk.unlock();
+    gxy_status e = q->status;
+    if (e == GXY_OK) e = copy_out(q->plus, plus);
+    if (e == GXY_OK) e = copy_out(q->minus, minus);
+    if (latency_ms) latency_ms[0] = std::chrono::duration<double, std::milli>(q->done_at - q->submitted).count();
+    delete q;
+    return e;
 }
+
+gxy_status gxy_server_get_stats(gxy_server* s, gxy_server_stats* st) {
+    if (!s || !st) return GXY_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    *st = s->st;
+    return GXY_OK;
+}
+
+gxy_status gxy_server_destroy(gxy_server* s) {
+    if (!s) return GXY_OK;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto& t : s->threads) t.join();
+    for (auto& kv : s->requests) delete kv.second;
+    delete s;
+    return GXY_OK;
+}
+
+}  // extern "C"
