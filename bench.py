@@ -379,6 +379,149 @@ def run_batched(args):
     }
 
 
+def _pct(v, q):
+    import numpy as np
+    return round(float(np.percentile(np.asarray(v), q)), 2) if len(v) else None
+
+
+def run_served(args):
+    """Serving: three resident chromosome-style targets; requests arrive as a
+    Poisson process (50/s, seed 7), each a target slice of log-uniform length
+    10 kbp-5 Mbp evolved to 60-95% identity, searched on both strands.  The
+    arrival trace is replayed in real time against the serving loop; the same
+    trace is also run as serial plain launches (one request at a time, FIFO)
+    and their latencies computed on the same arrival times.  HSPs must match."""
+    import threading as th
+    g = _pkg()
+    from lastz_gxy_b200 import synth
+    s = args.scale
+    t0 = time.time()
+    targets = synth.c5_targets(length=int(100_000_000 * s))
+    reqs = synth.c5_requests(targets, n_requests=args.requests, hi=int(5_000_000 * min(1.0, s * 2)) or 10_001)
+    gen_s = time.time() - t0
+    ctx = g.Context(0)
+    m, sp = g.ScoringMatrix.hoxd70(), g.SearchParams()
+    tabs = [g.PosTable.build(g.PackedSeq.from_ascii(t.tobytes()).to_device(ctx), P12, 1, ctx=ctx) for t in targets]
+    packed = [g.PackedSeq.from_ascii(r.query.tobytes()) for r in reqs]
+    mbp2_total = sum(mbp2(len(targets[r.target]), len(r.query), 2) for r in reqs)
+    # warm up the pipeline once
+    srv = g.Server(tabs, m, sp, max_streams=args.streams, max_batch_units=args.batch_units)
+    srv.wait(srv.submit(0, packed[0]))
+    ids = [None] * len(reqs)
+    res = [None] * len(reqs)
+    lat = [None] * len(reqs)
+
+    def waiter():
+        for i in range(len(reqs)):
+            while ids[i] is None:
+                time.sleep(0.0005)
+            p, mi, l = srv.wait(ids[i], timeout_ms=600_000)
+            res[i], lat[i] = (p, mi), l
+            done_t[i] = time.perf_counter()
+    done_t = [0.0] * len(reqs)
+    w = th.Thread(target=waiter)
+    w.start()
+    start = time.perf_counter()
+    for i, r in enumerate(reqs):
+        d = start + r.arrival_s - reqs[0].arrival_s - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids[i] = srv.submit(r.target, packed[i])
+    w.join()
+    makespan = max(done_t) - start
+    st = srv.stats()
+    srv.close()
+    # Serial plain launches on the same trace.
+    service = []
+    same = True
+    for i, r in enumerate(reqs):
+        ctx.mark(6)
+        dq = packed[i].to_device(ctx)
+        dqr = dq.reverse_complement()
+        p = g.search_device(tabs[r.target], dq, m, sp)
+        mi = g.search_device(tabs[r.target], dqr, m, sp)
+        dqr.free()
+        dq.free()
+        ctx.mark(7)
+        service.append(ctx.elapsed_ms(6, 7))
+        same = same and p.tobytes() == res[i][0].tobytes() and mi.tobytes() == res[i][1].tobytes()
+    fin, serial_lat = 0.0, []
+    t_first = reqs[0].arrival_s
+    for r, sv in zip(reqs, service):
+        a = (r.arrival_s - t_first) * 1e3
+        fin = max(fin, a) + sv
+        serial_lat.append(fin - a)
+    serial_span = fin / 1e3
+    return {
+        "workload": "serving: %d resident targets of %d bp, %d requests, Poisson %.0f/s (seed 7), both strands"
+                    % (len(targets), len(targets[0]), len(reqs), 50.0),
+        "mbp2": round(mbp2_total, 2), "query_bp": sum(len(r.query) for r in reqs),
+        "served": {"value": round(mbp2_total / makespan, 2), "unit": "Mbp^2/s", "makespan_s": round(makespan, 3),
+                   "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "p999_ms": _pct(lat, 99.9),
+                   "batches": st["batches"], "max_inflight_units": st["max_inflight_units"]},
+        "serial_plain": {"value": round(mbp2_total / serial_span, 2), "unit": "Mbp^2/s",
+                         "makespan_s": round(serial_span, 3), "p50_ms": _pct(serial_lat, 50),
+                         "p99_ms": _pct(serial_lat, 99), "p999_ms": _pct(serial_lat, 99.9),
+                         "mean_service_ms": round(statistics.mean(service), 2)},
+        "bit_identical": same, "generate_s": round(gen_s, 1),
+        "latency": "submit -> HSPs back on the host, wall clock",
+    }
+
+
+def run_chunked(args):
+    """Chunked single chromosome: a chromosome-style target and a query evolved
+    to ~70% identity, split by --chunk-size 10,000,000 --halo 50,000 into chunks
+    with resident tables; all (chunk, strand) units in batched launches, with the
+    driver's primary-region filter, against plain per-(chunk, strand) launches.
+    Transitions 1 and 0 are tuned and timed separately."""
+    g = _pkg()
+    from lastz_gxy_b200 import synth
+    from lastz_gxy_b200.autotune import autotune
+    s = args.scale
+    t0 = time.time()
+    pr = synth.c4(length=int(250_000_000 * s), families=max(1, int(30_000 * s)), nblocks=max(1, int(500 * s)))
+    gen_s = time.time() - t0
+    ctx = g.Context(0)
+    m = g.ScoringMatrix.hoxd70()
+    dT = g.PackedSeq.from_ascii(pr.target.tobytes()).to_device(ctx)
+    dQ = g.PackedSeq.from_ascii(pr.query.tobytes()).to_device(ctx)
+    chunks = g.chunk_target(len(pr.target), 10_000_000, 50_000)
+    ctx.mark(8)
+    tabs = [g.PosTable.build_view(dT, lo, hi, P12, 1, ctx=ctx) for lo, hi, _, _ in chunks]
+    ctx.mark(9)
+    table_ms = ctx.elapsed_ms(8, 9)
+    units = [(ci, 0, st, chunks[ci][2], chunks[ci][3]) for ci in range(len(chunks)) for st in (0, 1)]
+    mbp2_total = sum(mbp2(c[3] - c[2], len(pr.query), 1) for c in chunks) * 2
+    out = {"workload": "chunked: %d bp target x %d bp query, %d chunks x 2 strands" % (
+        len(pr.target), len(pr.query), len(chunks)), "mbp2": round(mbp2_total, 2), "table_build_ms": round(table_ms, 2),
+        "generate_s": round(gen_s, 1)}
+    for tr in (1, 0):
+        sp = g.SearchParams(transitions=tr)
+        tune = autotune(ctx, tabs, [dQ], units, m, sp, workload="chunked", sample_units=4, reps=1, use_cache=False,
+                        space={"screen_blocks_per_sm": [4, 3], "screen_cap": [128, 64]})
+        st = {}
+        ctx.mark(10)
+        got = g.batch_search(tabs, [dQ], units, m, sp, stats=st, ctx=ctx)
+        ctx.mark(11)
+        b_ms = ctx.elapsed_ms(10, 11)
+        ctx.mark(12)
+        same = True
+        dQr = dQ.reverse_complement()
+        for u, (ci, _, strand, plo, phi) in enumerate(units):
+            h = g.search_device(tabs[ci], dQr if strand else dQ, m, sp)
+            h = h[(h["t_start"] >= plo) & (h["t_start"] < phi)]
+            same = same and h.tobytes() == got[u].tobytes()
+        dQr.free()
+        ctx.mark(13)
+        p_ms = ctx.elapsed_ms(12, 13)
+        out[f"transitions_{tr}"] = {
+            "batched": {"value": round(mbp2_total / (b_ms / 1e3), 2), "ms": round(b_ms, 1), "raw_hits": st["raw_hits"],
+                        "candidates": st["candidates"], "hsps": st["hsps"], "passes": st["passes"]},
+            "plain": {"value": round(mbp2_total / (p_ms / 1e3), 2), "ms": round(p_ms, 1)},
+            "bit_identical": same, "autotune": tune["tuning"]}
+    return out
+
+
 def run_case(args):
     """One plus-strand search on the chromosome-style workload of --length bp
     (target and query both that long): the small case the ncu captures use."""
@@ -405,7 +548,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-bp", type=int, default=500_000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "case"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "chunked", "case"])
+    ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
+    ap.add_argument("--streams", type=int, default=3, help="served workload: dispatcher streams")
+    ap.add_argument("--batch-units", type=int, default=64, help="served workload: units per batch at most")
     ap.add_argument("--length", type=int, default=4_000_000, help="case workload length (bp)")
     ap.add_argument("--scale", type=float, default=1.0, help="batched workload size factor")
     args = ap.parse_args()
@@ -418,6 +564,12 @@ def main():
         return
     if args.workload == "batched":
         print(json.dumps(run_batched(args)), flush=True)
+        return
+    if args.workload == "served":
+        print(json.dumps(run_served(args)), flush=True)
+        return
+    if args.workload == "chunked":
+        print(json.dumps(run_chunked(args)), flush=True)
         return
     if args.workload == "case":
         print(json.dumps(run_case(args)), flush=True)
