@@ -236,6 +236,7 @@ gxy_status search_impl(gxy_ctx* ctx, Worker* W, const gxy_table* table, const Se
     units[0].positions = table->positions;
     units[0].nwin = n_windows(Q.len, table->pat.len, p->step);
     units[0].primary_lo = units[0].primary_hi = 0;
+    units[0].avg_bucket = table->num_words ? (double)table->npos / (double)table->num_words : 0.0;
     RunResult r;
     API_TRY(run_units(ctx, W, units, tsegs, qsegs, table->pat, *p, false, r));
     if (stats) *stats = r.stats;
@@ -653,6 +654,7 @@ gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* co
         plan[i].nwin = n_windows(queries[u.query]->len, pat.len, params->step);
         plan[i].primary_lo = u.primary_lo;
         plan[i].primary_hi = u.primary_hi;
+        plan[i].avg_bucket = t->num_words ? (double)t->npos / (double)t->num_words : 0.0;
     }
     RunResult r;
     API_TRY(run_units(ctx, W, plan, tsegs, qsegs, pat, *params, opts && opts->use_graph, r));

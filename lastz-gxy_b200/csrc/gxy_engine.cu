@@ -32,16 +32,16 @@ const char* last_error() { return g_err.c_str(); }
 
 cudaError_t DevBuf::ensure(size_t need) {
     if (need <= bytes && p) return cudaSuccess;
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     bytes = 0;
     size_t b = need < 256 ? 256 : need;
-    cudaError_t e = cudaMalloc(&p, b);
+    cudaError_t e = cudaMallocAsync(&p, b, st);
     if (e == cudaSuccess) bytes = b;
     return e;
 }
 void DevBuf::release() {
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, st);
     p = nullptr;
     bytes = 0;
 }
@@ -141,6 +141,11 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     }
     Worker* w = new Worker();
     cudaError_t e = cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking);
+    for (DevBuf* b : {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->prim_sums, &w->prim_hist, &w->counters, &w->d_units,
+                      &w->d_tsegs, &w->d_qsegs, &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags,
+                      &w->offsets, &w->ohsp, &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2,
+                      &w->hits})
+        b->st = w->st;
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
     if (e == cudaSuccess) e = w->prim_sums.ensure((w->ps.grid + 1) * sizeof(uint32_t));
@@ -289,7 +294,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     uint32_t* cnt = W->counters.as<uint32_t>();
     unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);
     unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + 16);
-    if (W->cand_cap == 0) W->cand_cap = 1u << 20;
+    if (W->cand_cap == 0) W->cand_cap = 2u << 20;
     if (W->hit_cap == 0) W->hit_cap = 32ull << 20;
     const uint64_t kMaxHitCap = std::max<uint32_t>(4096, ctx->tuning.max_hits_per_pass);
     if (W->hit_cap > kMaxHitCap) {
@@ -297,6 +302,22 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         W->hit_cap = kMaxHitCap;
     }
     uint32_t pass_tiles = (uint32_t)tiles;
+    // Size the raw-hit buffer from the expected hits (windows x variants x mean
+    // bucket, with margin) so that large searches do not run twice.
+    {
+        double est = 1 << 20;
+        for (const UnitPlan& u : units) est += 1.5 * (double)u.nwin * sa.n_var * u.avg_bucket;
+        if (est > (double)W->hit_cap) {
+            if (est <= (double)kMaxHitCap) {
+                W->hits.release();
+                W->hit_cap = (uint64_t)est;
+            } else {
+                W->hits.release();
+                W->hit_cap = kMaxHitCap;
+                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / est));
+            }
+        }
+    }
     const int blocks_screen = ctx->sm_count * (int)std::max<uint32_t>(1, ctx->tuning.screen_blocks_per_sm);
     const int blocks_enum = ctx->sm_count * 8;
     const int blocks_misc = ctx->sm_count * 4;

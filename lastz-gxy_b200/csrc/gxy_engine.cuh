@@ -19,9 +19,13 @@ namespace gxy {
 void set_error(const std::string& msg);
 
 // Grow-only device buffer.
+// Grow-only device buffer, allocated and freed in stream order on `st` (the
+// owning worker's stream; the legacy stream when unset), so growing it never
+// synchronises the whole device.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    cudaStream_t st = nullptr;
     cudaError_t ensure(size_t need);
     void release();
     template <typename T> T* as() const { return static_cast<T*>(p); }
@@ -58,6 +62,7 @@ struct UnitPlan {
     uint32_t nwin;
     uint32_t primary_lo;
     uint32_t primary_hi;
+    double avg_bucket;   // table positions / words: sizes the raw-hit buffer before the first pass
 };
 
 struct RunResult {

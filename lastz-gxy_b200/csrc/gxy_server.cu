@@ -129,6 +129,7 @@ gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
             u.positions = t->positions;
             u.nwin = windows_of(q->len, pat.len, s->params.step);
             u.primary_lo = u.primary_hi = 0;
+            u.avg_bucket = t->num_words ? (double)t->npos / (double)t->num_words : 0.0;
             plan.push_back(u);
             unit_owner.push_back({r, sd});
         }
