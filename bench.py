@@ -384,14 +384,74 @@ def _pct(v, q):
     return round(float(np.percentile(np.asarray(v), q)), 2) if len(v) else None
 
 
-def run_served(args):
-    """Serving: three resident chromosome-style targets; requests arrive as a
-    Poisson process (50/s, seed 7), each a target slice of log-uniform length
-    10 kbp-5 Mbp evolved to 60-95% identity, searched on both strands.  The
-    arrival trace is replayed in real time against the serving loop; the same
-    trace is also run as serial plain launches (one request at a time, FIFO)
-    and their latencies computed on the same arrival times.  HSPs must match."""
-    import threading as th
+def replay_served(g, srv, reqs, packed):
+    """Replays the arrival trace in real time against a Server; returns
+    (results, latencies_ms, makespan_s).  Latency = submit -> HSPs on the host."""
+    ids = [None] * len(reqs)
+    res = [None] * len(reqs)
+    lat = [None] * len(reqs)
+    done_t = [0.0] * len(reqs)
+
+    def waiter():
+        for i in range(len(reqs)):
+            while ids[i] is None:
+                time.sleep(0.0002)
+            p, mi, l = srv.wait(ids[i], timeout_ms=600_000)
+            res[i], lat[i] = (p, mi), l
+            done_t[i] = time.perf_counter()
+    w = threading.Thread(target=waiter)
+    w.start()
+    start = time.perf_counter()
+    for i, r in enumerate(reqs):
+        d = start + r.arrival_s - reqs[0].arrival_s - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids[i] = srv.submit(r.target, packed[i])
+    w.join()
+    return res, lat, max(done_t) - start
+
+
+def replay_serial(g, ctx, tabs, reqs, packed, m, sp):
+    """The same trace served FIFO by plain per-pair launches, one request at a
+    time, in real time: a worker thread takes each request once it has arrived
+    and runs search() on both strands (host query in, HSPs out).  Returns
+    (results, latencies_ms, makespan_s, device_service_ms)."""
+    res = [None] * len(reqs)
+    lat = [None] * len(reqs)
+    service = [None] * len(reqs)
+    arrive = [None] * len(reqs)
+    cv = threading.Condition()
+
+    def worker():
+        for i, r in enumerate(reqs):
+            with cv:
+                cv.wait_for(lambda: arrive[i] is not None)
+            ctx.mark(6)
+            dq = packed[i].to_device(ctx)
+            dqr = dq.reverse_complement()
+            p = g.search_device(tabs[r.target], dq, m, sp)
+            mi = g.search_device(tabs[r.target], dqr, m, sp)
+            dqr.free()
+            dq.free()
+            ctx.mark(7)
+            res[i] = (p, mi)
+            lat[i] = (time.perf_counter() - arrive[i]) * 1e3
+            service[i] = ctx.elapsed_ms(6, 7)
+    w = threading.Thread(target=worker)
+    w.start()
+    start = time.perf_counter()
+    for i, r in enumerate(reqs):
+        d = start + r.arrival_s - reqs[0].arrival_s - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        with cv:
+            arrive[i] = time.perf_counter()
+            cv.notify()
+    w.join()
+    return res, lat, max(arrive[i] + lat[i] / 1e3 for i in range(len(reqs))) - start, service
+
+
+def served_setup(args):
     g = _pkg()
     from lastz_gxy_b200 import synth
     s = args.scale
@@ -403,68 +463,49 @@ def run_served(args):
     m, sp = g.ScoringMatrix.hoxd70(), g.SearchParams()
     tabs = [g.PosTable.build(g.PackedSeq.from_ascii(t.tobytes()).to_device(ctx), P12, 1, ctx=ctx) for t in targets]
     packed = [g.PackedSeq.from_ascii(r.query.tobytes()) for r in reqs]
-    mbp2_total = sum(mbp2(len(targets[r.target]), len(r.query), 2) for r in reqs)
-    # warm up the pipeline once
-    srv = g.Server(tabs, m, sp, max_streams=args.streams, max_batch_units=args.batch_units)
-    srv.wait(srv.submit(0, packed[0]))
-    ids = [None] * len(reqs)
-    res = [None] * len(reqs)
-    lat = [None] * len(reqs)
+    return g, ctx, targets, reqs, tabs, packed, m, sp, gen_s
 
-    def waiter():
-        for i in range(len(reqs)):
-            while ids[i] is None:
-                time.sleep(0.0005)
-            p, mi, l = srv.wait(ids[i], timeout_ms=600_000)
-            res[i], lat[i] = (p, mi), l
-            done_t[i] = time.perf_counter()
-    done_t = [0.0] * len(reqs)
-    w = th.Thread(target=waiter)
-    w.start()
-    start = time.perf_counter()
-    for i, r in enumerate(reqs):
-        d = start + r.arrival_s - reqs[0].arrival_s - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
-        ids[i] = srv.submit(r.target, packed[i])
-    w.join()
-    makespan = max(done_t) - start
-    st = srv.stats()
-    srv.close()
-    # Serial plain launches on the same trace.
-    service = []
-    same = True
-    for i, r in enumerate(reqs):
-        ctx.mark(6)
-        dq = packed[i].to_device(ctx)
-        dqr = dq.reverse_complement()
-        p = g.search_device(tabs[r.target], dq, m, sp)
-        mi = g.search_device(tabs[r.target], dqr, m, sp)
-        dqr.free()
-        dq.free()
-        ctx.mark(7)
-        service.append(ctx.elapsed_ms(6, 7))
-        same = same and p.tobytes() == res[i][0].tobytes() and mi.tobytes() == res[i][1].tobytes()
-    fin, serial_lat = 0.0, []
-    t_first = reqs[0].arrival_s
-    for r, sv in zip(reqs, service):
-        a = (r.arrival_s - t_first) * 1e3
-        fin = max(fin, a) + sv
-        serial_lat.append(fin - a)
-    serial_span = fin / 1e3
+
+def served_run(g, tabs, reqs, packed, m, sp, streams, batch_units, batch_bases):
+    srv = g.Server(tabs, m, sp, max_streams=streams, max_batch_units=batch_units, max_batch_bases=batch_bases)
+    try:
+        # Warm every dispatcher's buffers with the trace's largest request.
+        big = max(range(len(reqs)), key=lambda i: len(reqs[i].query))
+        for rid in [srv.submit(reqs[big].target, packed[big]) for _ in range(streams)]:
+            srv.wait(rid)
+        res, lat, span = replay_served(g, srv, reqs, packed)
+        return res, lat, span, srv.stats()
+    finally:
+        srv.close()
+
+
+def run_served(args):
+    """Serving: three resident chromosome-style targets; requests arrive as a
+    Poisson process (50/s, seed 7), each a target slice of log-uniform length
+    10 kbp-5 Mbp evolved to 60-95% identity, searched on both strands.  The
+    arrival trace is replayed in real time against the serving loop, and again
+    against serial plain launches (FIFO, one request at a time); both
+    latencies are wall clock from arrival to HSPs on the host.  HSPs must match."""
+    g, ctx, targets, reqs, tabs, packed, m, sp, gen_s = served_setup(args)
+    mbp2_total = sum(mbp2(len(targets[r.target]), len(r.query), 2) for r in reqs)
+    res, lat, makespan, st = served_run(g, tabs, reqs, packed, m, sp, args.streams, args.batch_units,
+                                        args.batch_bases)
+    sres, slat, sspan, service = replay_serial(g, ctx, tabs, reqs, packed, m, sp)
+    same = all(a[0].tobytes() == b[0].tobytes() and a[1].tobytes() == b[1].tobytes() for a, b in zip(res, sres))
     return {
         "workload": "serving: %d resident targets of %d bp, %d requests, Poisson %.0f/s (seed 7), both strands"
                     % (len(targets), len(targets[0]), len(reqs), 50.0),
         "mbp2": round(mbp2_total, 2), "query_bp": sum(len(r.query) for r in reqs),
         "served": {"value": round(mbp2_total / makespan, 2), "unit": "Mbp^2/s", "makespan_s": round(makespan, 3),
                    "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99), "p999_ms": _pct(lat, 99.9),
-                   "batches": st["batches"], "max_inflight_units": st["max_inflight_units"]},
-        "serial_plain": {"value": round(mbp2_total / serial_span, 2), "unit": "Mbp^2/s",
-                         "makespan_s": round(serial_span, 3), "p50_ms": _pct(serial_lat, 50),
-                         "p99_ms": _pct(serial_lat, 99), "p999_ms": _pct(serial_lat, 99.9),
-                         "mean_service_ms": round(statistics.mean(service), 2)},
+                   "batches": st["batches"], "max_inflight_units": st["max_inflight_units"],
+                   "streams": args.streams, "max_batch_units": args.batch_units, "max_batch_bases": args.batch_bases},
+        "serial_plain": {"value": round(mbp2_total / sspan, 2), "unit": "Mbp^2/s",
+                         "makespan_s": round(sspan, 3), "p50_ms": _pct(slat, 50),
+                         "p99_ms": _pct(slat, 99), "p999_ms": _pct(slat, 99.9),
+                         "mean_device_service_ms": round(statistics.mean(service), 2)},
         "bit_identical": same, "generate_s": round(gen_s, 1),
-        "latency": "submit -> HSPs back on the host, wall clock",
+        "latency": "arrival -> HSPs back on the host, wall clock, both arms",
     }
 
 
@@ -550,8 +591,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "chunked", "case"])
     ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
-    ap.add_argument("--streams", type=int, default=3, help="served workload: dispatcher streams")
+    ap.add_argument("--streams", type=int, default=2, help="served workload: dispatcher streams")
     ap.add_argument("--batch-units", type=int, default=64, help="served workload: units per batch at most")
+    ap.add_argument("--batch-bases", type=int, default=16 << 20,
+                    help="served workload: query bases (per strand) per batch at most")
     ap.add_argument("--length", type=int, default=4_000_000, help="case workload length (bp)")
     ap.add_argument("--scale", type=float, default=1.0, help="batched workload size factor")
     args = ap.parse_args()

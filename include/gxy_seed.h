@@ -127,6 +127,8 @@ typedef struct {
     uint32_t screen_blocks_per_sm;
     uint32_t walk_warps;
     uint32_t max_hits_per_pass;   /* raw-hit buffer bound; larger searches run in window passes */
+    uint32_t initial_candidates;  /* candidate capacity every search starts from (grown on demand);
+                                     0 in the context = keep what each stream's buffers grew to */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
@@ -268,6 +270,9 @@ typedef struct {
     uint32_t max_streams;
     uint32_t max_batch_units;
     uint32_t both_strands;
+    /* Query bases (counted once per strand) one batch takes at most, so that
+     * a batch stays short and requests behind it wait less; 0 = 16 Mbp. */
+    uint64_t max_batch_bases;
 } gxy_server_opts;
 
 gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,

@@ -58,8 +58,9 @@ class Context:
         return cls._default[device]
 
     def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0,
-                   max_hits_per_pass=0) -> None:
-        t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass)
+                   max_hits_per_pass=0, initial_candidates=0) -> None:
+        t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass,
+                         initial_candidates)
         check(lib().gxy_ctx_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -67,7 +68,7 @@ class Context:
         check(lib().gxy_ctx_get_tuning(self.h, C.byref(t)))
         return {"screen_warps": t.screen_warps, "screen_cap": t.screen_cap,
                 "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps,
-                "max_hits_per_pass": t.max_hits_per_pass}
+                "max_hits_per_pass": t.max_hits_per_pass, "initial_candidates": t.initial_candidates}
 
     def mark(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's primary stream."""

@@ -58,7 +58,7 @@ class StatsC(C.Structure):
 
 class TuningC(C.Structure):
     _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
-                ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32)]
+                ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32), ("initial_candidates", C.c_uint32)]
 
 
 class UnitC(C.Structure):
@@ -77,7 +77,8 @@ class BatchOptsC(C.Structure):
 
 class ServerOptsC(C.Structure):
     _fields_ = [("max_device_bytes", C.c_uint64), ("max_units", C.c_uint32), ("max_streams", C.c_uint32),
-                ("max_batch_units", C.c_uint32), ("both_strands", C.c_uint32)]
+                ("max_batch_units", C.c_uint32), ("both_strands", C.c_uint32),
+                ("max_batch_bases", C.c_uint64)]
 
 
 class ServerStatsC(C.Structure):

@@ -362,6 +362,7 @@ gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
     if (t->screen_blocks_per_sm) ctx->tuning.screen_blocks_per_sm = std::min<uint32_t>(t->screen_blocks_per_sm, 16);
     if (t->walk_warps) ctx->tuning.walk_warps = t->walk_warps == 4 ? 4 : 8;
     if (t->max_hits_per_pass) ctx->tuning.max_hits_per_pass = std::max<uint32_t>(4096, t->max_hits_per_pass);
+    if (t->initial_candidates) ctx->tuning.initial_candidates = std::max<uint32_t>(1024, t->initial_candidates);
     return GXY_OK;
 }
 

@@ -294,6 +294,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     uint32_t* cnt = W->counters.as<uint32_t>();
     unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);
     unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + 16);
+    if (ctx->tuning.initial_candidates) W->cand_cap = ctx->tuning.initial_candidates;
     if (W->cand_cap == 0) W->cand_cap = 2u << 20;
     if (W->hit_cap == 0) W->hit_cap = 32ull << 20;
     const uint64_t kMaxHitCap = std::max<uint32_t>(4096, ctx->tuning.max_hits_per_pass);
@@ -338,8 +339,21 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         return GXY_OK;
     };
 
+    // Grows a buffer to `bytes`, keeping its first `keep` bytes.
+    auto grow_keep = [&](DevBuf& b, size_t bytes, size_t keep) -> cudaError_t {
+        if (bytes <= b.bytes && b.p) return cudaSuccess;
+        void* np = nullptr;
+        cudaError_t e = cudaMallocAsync(&np, bytes, b.st);
+        if (e != cudaSuccess) return e;
+        if (b.p && keep) e = cudaMemcpyAsync(np, b.p, keep, cudaMemcpyDeviceToDevice, b.st);
+        if (b.p) cudaFreeAsync(b.p, b.st);
+        b.p = np;
+        b.bytes = bytes;
+        return e;
+    };
+
     for (int attempt = 0; attempt < 16; attempt++) {
-        const uint32_t cap = W->cand_cap;
+        uint32_t cap = W->cand_cap;
         GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
         GXY_CK(W->ck0.ensure((size_t)cap * 8));
         GXY_CK(W->ck1.ensure((size_t)cap * 8));
@@ -394,9 +408,30 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                 GXY_CK(cudaMemcpyAsync(before, cnt, sizeof(before), cudaMemcpyDeviceToHost, st));
                 GXY_CK(cudaStreamSynchronize(st));
                 API_TRY_ENGINE(pass(t0, t1));
-                unsigned long long nh = 0;
-                GXY_CK(cudaMemcpyAsync(&nh, hitc, 8, cudaMemcpyDeviceToHost, st));
+                uint32_t after[24];
+                GXY_CK(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
                 GXY_CK(cudaStreamSynchronize(st));
+                const unsigned long long nh = *reinterpret_cast<const unsigned long long*>(after + 16);
+                if (after[1] > cap && nh <= W->hit_cap) {
+                    // Candidates overflowed in this pass: grow the candidate
+                    // arrays keeping the earlier passes' entries, redo the pass.
+                    const uint64_t nc = (uint64_t)after[1] + after[1] / 2 + (1u << 20);
+                    if (nc >= (1ull << 31)) {
+                        set_error("candidate count exceeds 2^31");
+                        return GXY_EUNSUPPORTED;
+                    }
+                    const size_t keep = before[1];
+                    GXY_CK(grow_keep(W->ck0, nc * 8, keep * 8));
+                    GXY_CK(grow_keep(W->cv0, nc * 4, keep * 4));
+                    GXY_CK(grow_keep(W->cands, nc * sizeof(Cand), keep * sizeof(Cand)));
+                    W->cand_cap = cap = (uint32_t)nc;
+                    sa.cand_keys = W->ck0.as<uint64_t>();
+                    sa.cand_vals = W->cv0.as<uint32_t>();
+                    sa.cands = W->cands.as<Cand>();
+                    sa.cand_cap = cap;
+                    GXY_CK(cudaMemcpyAsync(cnt, before, sizeof(before), cudaMemcpyHostToDevice, st));
+                    continue;
+                }
                 if (nh > W->hit_cap) {
                     if (t1 - t0 == 1) {
                         set_error("one tile of 32 query windows has more raw hits than the hit buffer holds");
@@ -411,6 +446,17 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             }
             GXY_CK(cudaEventRecord(W->ev[3], st));
             GXY_CK(cudaEventRecord(W->ev[1], st));
+            GXY_CK(W->ck1.ensure((size_t)cap * 8));
+            GXY_CK(W->cv1.ensure((size_t)cap * 4));
+            GXY_CK(W->flags.ensure((size_t)cap));
+            GXY_CK(W->offsets.ensure((size_t)cap * 4 + 4));
+            GXY_CK(W->ohsp.ensure((size_t)cap * sizeof(Hsp)));
+            GXY_CK(W->rhsp.ensure((size_t)cap * sizeof(Hsp)));
+            GXY_CK(W->runit.ensure((size_t)cap * 4));
+            GXY_CK(W->rhsp2.ensure((size_t)cap * sizeof(Hsp)));
+            GXY_CK(W->runit2.ensure((size_t)cap * 4));
+            GXY_CK(W->perm.ensure((size_t)cap * 4));
+            GXY_CK(W->perm2.ensure((size_t)cap * 4));
         } else {
             // In graph mode the timing events sit around the graph launch.
             in_capture = graph_now;

@@ -108,7 +108,7 @@ struct gxy_ctx {
     std::mutex mu;
     std::vector<gxy::Worker*> free_workers;   // the primary worker (all_workers[0]) is taken first
     std::vector<gxy::Worker*> all_workers;
-    gxy_tuning tuning{8, 128, 4, 8, 256u << 20};
+    gxy_tuning tuning{8, 128, 4, 8, 256u << 20, 0};
     cudaEvent_t marks[16] = {};
 };
 

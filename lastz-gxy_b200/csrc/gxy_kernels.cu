@@ -510,7 +510,7 @@ void launch_enumerate(const ScreenArgs& a, int blocks, cudaStream_t st) {
 //    candidate for the walk, which applies the diagonal rule in order.
 // ---------------------------------------------------------------------------
 template <int WARPS, int MINB>
-__global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_constant__ ScreenArgs a) {
+__global__ __launch_bounds__(WARPS * 32, MINB) void k_screen_wide(const __grid_constant__ ScreenArgs a) {
     __shared__ int32_t s_lut[16];
     if (threadIdx.x < 16) s_lut[threadIdx.x] = a.sc.sub[threadIdx.x];
     __syncthreads();
@@ -693,18 +693,325 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     if (lane == 0) atomicAdd(&a.stats[2], n_cols);
 }
 
+// ---------------------------------------------------------------------------
+// Screen, packed form.  The same lane-per-hit screen as k_screen_wide, with
+// the x-drop state of a side packed into two integers:
+//     P = 256 * run  + (255 - columns scanned)
+//     B = 256 * best + (255 - best extent)
+// One column of extend_one_side (src/hsp.rs:179-193) is then
+//     P += 256 * score - 1;  B = max(B, P);  break when B - P >= 256 (xdrop + 1)
+// and this is exact:
+//  - run > best: P exceeds B by at least 1, so B takes P -- best and its
+//    extent move together, as in the reference.
+//  - run <= best: P < B (a later column has a smaller low byte), so B keeps the
+//    first extent that reached the best, as the reference's strict `>` does.
+//  - then B - P = 256 (best - run) + d with 1 <= d <= 255, and
+//    B - P >= 256 (xdrop + 1)  <=>  best - run > xdrop.
+// It needs at most 255 columns per side in the screen (cap <= 192), xdrop in
+// [0, 2^22] and |scores| <= 16383, so that no packed value leaves i32; the
+// host uses k_screen_wide outside that envelope.
+// ---------------------------------------------------------------------------
+struct PkSide {
+    uint64_t nib0, nib1;   // (t << 2 | q) nibbles of columns 0-15 and 16-31
+    uint32_t vv;           // column validity
+    uint32_t n;            // columns present in this chunk
+    int32_t p, b;          // packed run and best
+    bool alive;            // no x-drop break yet, and the side has columns
+};
+
+__device__ __forceinline__ void pk_init(PkSide& S, uint64_t tc, uint64_t qc, uint32_t vv, uint32_t n, int32_t p,
+                                        int32_t b) {
+    S.nib0 = (spread16((uint32_t)tc) << 2) | spread16((uint32_t)qc);
+    S.nib1 = (spread16((uint32_t)(tc >> 32)) << 2) | spread16((uint32_t)(qc >> 32));
+    S.vv = vv;
+    S.n = n;
+    S.p = p;
+    S.b = b;
+    S.alive = n > 0;
+}
+
+// Column k of a side.  kSlow: the chunk may hold invalid bases (scored
+// `ambig`) or end before column 32.
+template <bool kSlow, int k>
+__device__ __forceinline__ void pk_step(PkSide& S, int32_t T, const int32_t* plut, int32_t pamb) {
+    const uint32_t idx = (uint32_t)(((k < 16 ? S.nib0 : S.nib1) >> (4 * (k & 15))) & 15u);
+    int32_t s = plut[idx];
+    bool go = S.alive;
+    if (kSlow) {
+        s = ((S.vv >> k) & 1u) ? s : pamb;
+        go = go && (uint32_t)k < S.n;
+    }
+    if (go) {
+        S.p += s;
+        S.b = max(S.b, S.p);
+        S.alive = S.b - S.p < T;
+    }
+}
+
+// Both sides column by column in lockstep: two independent serial chains.
+template <bool kSlow>
+__device__ __forceinline__ void pk_scan_pair(PkSide& A, PkSide& B, int32_t T, const int32_t* plut, int32_t pamb) {
+#define GXY_PK4(g)                                                         \
+    pk_step<kSlow, g * 4 + 0>(A, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 0>(B, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 1>(A, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 1>(B, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 2>(A, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 2>(B, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 3>(A, T, plut, pamb);                           \
+    pk_step<kSlow, g * 4 + 3>(B, T, plut, pamb);
+    GXY_PK4(0) GXY_PK4(1) GXY_PK4(2) GXY_PK4(3) GXY_PK4(4) GXY_PK4(5) GXY_PK4(6) GXY_PK4(7)
+#undef GXY_PK4
+}
+
+__device__ __forceinline__ int32_t pk_run(int32_t p) { return p >> 8; }            // arithmetic shift
+__device__ __forceinline__ uint32_t pk_ext(int32_t p) { return 255u - ((uint32_t)p & 255u); }
+constexpr int32_t kPkStart = 255;   // run 0, no columns
+
+template <int WARPS, int MINB>
+__global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_constant__ ScreenArgs a) {
+    __shared__ int32_t s_lut[16];     // raw column scores
+    __shared__ int32_t s_plut[16];    // 256 * score - 1
+    __shared__ int32_t s_tri[4096];   // sum of three columns' scores, index (t3 << 6) | q3
+    for (uint32_t i = threadIdx.x; i < 4096; i += blockDim.x) {
+        int32_t v = 0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) v += a.sc.sub[(((i >> (6 + 2 * c)) & 3u) << 2) | ((i >> (2 * c)) & 3u)];
+        s_tri[i] = v;
+    }
+    if (threadIdx.x < 16) {
+        s_lut[threadIdx.x] = a.sc.sub[threadIdx.x];
+        s_plut[threadIdx.x] = a.sc.sub[threadIdx.x] * 256 - 1;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = lanemask_lt();
+    const uint32_t L = a.pat.len;
+    const int32_t ambig = a.sc.ambig, thresh = a.sc.hspthresh;
+    const int32_t pamb = ambig * 256 - 1;
+    const int32_t T = (a.sc.xdrop + 1) * 256;
+    const uint32_t seed_mask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+    const unsigned long long hc = *a.hit_count;
+    const uint32_t n_hits = (uint32_t)(hc < a.hit_cap ? hc : a.hit_cap);
+    unsigned long long n_cols = 0;
+    bool exhausted = false;
+
+    bool busy = false, rdone = true, ldone = true;
+    uint32_t ht = 0, hq = 0, hu = 0xffffffffu;
+    int32_t seed = 0;
+    int32_t rp = kPkStart, rb = kPkStart, lp = kPkStart, lb = kPkStart;
+    uint32_t rrem = 0, lrem = 0;
+    SeqView T_{}, Q_{};
+    uint32_t cur_unit = 0xffffffffu;
+
+    for (;;) {
+        // ---------------- assign ----------------
+        const uint32_t im = __ballot_sync(kFull, !busy);
+        uint32_t base = 0, take = 0;
+        if (!exhausted && im) {
+            if (lane == 0) base = atomicAdd(a.hit_next, (uint32_t)__popc(im));
+            base = __shfl_sync(kFull, base, 0);
+            take = base < n_hits ? min((uint32_t)__popc(im), n_hits - base) : 0u;
+            if (base + (uint32_t)__popc(im) >= n_hits) exhausted = true;
+        }
+        bool fresh = false;
+        if (!busy) {
+            const uint32_t rk = __popc(im & lt);
+            if (rk < take) {
+                const Hit h = a.hits[base + rk];
+                ht = h.t;
+                hq = h.q;
+                hu = h.unit;
+                if (hu != cur_unit) {
+                    cur_unit = hu;
+                    const UnitDev U = a.units[hu];
+                    T_ = a.tsegs[U.tseg];
+                    Q_ = a.qsegs[U.qseg];
+                }
+                fresh = true;
+                busy = true;
+            }
+        }
+        if (!__any_sync(kFull, busy)) {
+            if (exhausted) break;
+            continue;
+        }
+
+        // ---------------- chunk data ----------------
+        // Side A: a fresh hit's first right chunk, or a continuing side's next chunk.
+        // Side B: a fresh hit's first left chunk.
+        uint64_t atc = 0, aqc = 0, btc = 0, bqc = 0;
+        uint32_t avv = 0, bvv = 0, an = 0, bn = 0;
+        const bool a_right = fresh || !rdone;
+        if (fresh) {
+            const uint64_t tb = T_.base + ht, qb = Q_.base + hq;
+            const uint64_t tw = (tb - 32) & ~31ull, qw = (qb - 32) & ~31ull;
+            uint64_t twc[4], qwc[4];
+            uint32_t twv[4], qwv[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                twc[j] = __ldg(T_.codes + (tw >> 5) + j);
+                qwc[j] = __ldg(Q_.codes + (qw >> 5) + j);
+                twv[j] = __ldg(T_.valid + (tw >> 5) + j);
+                qwv[j] = __ldg(Q_.valid + (qw >> 5) + j);
+            }
+            const uint32_t ot = (uint32_t)(tb - tw), oq = (uint32_t)(qb - qw);   // both in [32, 63]
+            // Seed footprint, all L columns (src/hsp.rs:119-123): three
+            // columns per table read, the rest singly, then invalid columns
+            // re-scored as ambig.
+            {
+                const uint64_t tc = win_codes(twc, ot), qc = win_codes(qwc, oq);
+                int32_t sd = 0;
+#pragma unroll
+                for (int k = 0; k + 3 <= 32; k += 3) {
+                    if ((uint32_t)k + 3 > L) break;
+                    const uint32_t i6 = ((((uint32_t)(tc >> (2 * k))) & 63u) << 6) | ((uint32_t)(qc >> (2 * k)) & 63u);
+                    sd += s_tri[i6];
+                }
+                for (uint32_t k = L - L % 3; k < L; k++)
+                    sd += s_lut[((((uint32_t)(tc >> (2 * k))) & 3u) << 2) | ((uint32_t)(qc >> (2 * k)) & 3u)];
+                uint32_t bad = ~(win_bits(twv, ot) & win_bits(qwv, oq)) & seed_mask;
+                while (bad) {
+                    const uint32_t k = __ffs(bad) - 1;
+                    bad &= bad - 1;
+                    sd += ambig - s_lut[((((uint32_t)(tc >> (2 * k))) & 3u) << 2) | ((uint32_t)(qc >> (2 * k)) & 3u)];
+                }
+                seed = sd;
+            }
+            rrem = min(T_.len - ht - L, Q_.len - hq - L);
+            lrem = min(ht, hq);
+            rp = rb = lp = lb = kPkStart;
+            rdone = rrem == 0;
+            ldone = lrem == 0;
+            an = min(32u, rrem);
+            atc = win_codes(twc, ot + L);
+            aqc = win_codes(qwc, oq + L);
+            avv = win_bits(twv, ot + L) & win_bits(qwv, oq + L);
+            bn = min(32u, lrem);
+            btc = rev_pairs64(win_codes(twc, ot - 32));
+            bqc = rev_pairs64(win_codes(qwc, oq - 32));
+            bvv = __brev(win_bits(twv, ot - 32) & win_bits(qwv, oq - 32));
+        } else if (busy) {
+            if (!rdone) {
+                const uint32_t ext = pk_ext(rp);
+                const uint64_t tg = T_.base + ht + L + ext, qg = Q_.base + hq + L + ext;
+                atc = load_codes32(T_.codes, tg);
+                aqc = load_codes32(Q_.codes, qg);
+                avv = load_bits32(T_.valid, tg) & load_bits32(Q_.valid, qg);
+                an = min(32u, rrem);
+            } else {
+                // The left side continues below position ht - 1 - ext.
+                const uint32_t ext = pk_ext(lp);
+                const uint64_t tg = T_.base + ht - ext - 32, qg = Q_.base + hq - ext - 32;
+                atc = rev_pairs64(load_codes32(T_.codes, tg));
+                aqc = rev_pairs64(load_codes32(Q_.codes, qg));
+                avv = __brev(load_bits32(T_.valid, tg) & load_bits32(Q_.valid, qg));
+                an = min(32u, lrem);
+            }
+        }
+
+        // ---------------- scans ----------------
+        {
+            if (!busy) an = 0;
+            if (!fresh) bn = 0;
+            PkSide A, B;
+            pk_init(A, atc, aqc, avv, an, a_right ? rp : lp, a_right ? rb : lb);
+            pk_init(B, btc, bqc, bvv, bn, lp, lb);
+            const bool slow = (an != 0 && (an < 32 || avv != 0xffffffffu)) ||
+                              (bn != 0 && (bn < 32 || bvv != 0xffffffffu));
+            if (__any_sync(kFull, slow)) pk_scan_pair<true>(A, B, T, s_plut, pamb);
+            else pk_scan_pair<false>(A, B, T, s_plut, pamb);
+            const int32_t a0 = a_right ? rp : lp;
+            const uint32_t aused = ((uint32_t)a0 & 255u) - ((uint32_t)A.p & 255u);
+            const uint32_t bused = ((uint32_t)lp & 255u) - ((uint32_t)B.p & 255u);
+            const bool aend = an != 0 && !A.alive, bend = bn != 0 && !B.alive;
+            n_cols += (fresh || busy ? aused : 0u) + (fresh ? bused : 0u);
+            if (busy) {
+                if (a_right) {
+                    rp = A.p; rb = A.b; rrem -= aused;
+                    rdone = rdone || aend || rrem == 0;
+                } else {
+                    lp = A.p; lb = A.b; lrem -= aused;
+                    ldone = ldone || aend || lrem == 0;
+                }
+            }
+            if (fresh) {
+                lp = B.p; lb = B.b; lrem -= bused;
+                ldone = ldone || bend || lrem == 0;
+            }
+        }
+
+        // ---------------- bookkeeping ----------------
+        bool finish = false, cand = false, is_long = false;
+        int32_t score = 0;
+        if (busy) {
+            if (rdone && ldone) {
+                finish = true;
+                score = seed + pk_run(rb) + pk_run(lb);
+                cand = score >= thresh;
+            } else if ((!rdone && pk_ext(rp) >= a.cap) || (!ldone && pk_ext(lp) >= a.cap)) {
+                finish = true;      // still extending at the cap: defer to the walk
+                cand = true;
+                is_long = true;
+            }
+        }
+        const uint32_t m = __ballot_sync(kFull, finish && cand);
+        if (m) {
+            uint32_t slot0 = 0;
+            if (lane == 0) slot0 = atomicAdd(a.cand_count, (uint32_t)__popc(m));
+            slot0 = __shfl_sync(kFull, slot0, 0);
+            if (finish && cand) {
+                const uint32_t slot = slot0 + __popc(m & lt);
+                if (slot < a.cand_cap) {
+                    const uint32_t tk = T_.key_base + ht, qk = Q_.key_base + hq;
+                    a.cand_keys[slot] = ((uint64_t)(tk - qk + a.qkey_total) << 32) | tk;
+                    a.cand_vals[slot] = slot;
+                    Cand c;
+                    c.unit = hu; c.t = ht; c.q = hq;
+                    c.flags = is_long ? kCandLong : 0u;
+                    c.lext = pk_ext(lb); c.rext = pk_ext(rb); c.score = score; c.pad_ = 0;
+                    a.cands[slot] = c;
+                }
+            }
+        }
+        if (finish) busy = false;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_cols += __shfl_xor_sync(kFull, n_cols, o);
+    if (lane == 0) atomicAdd(&a.stats[2], n_cols);
+}
+
+// The packed screen's envelope (see above).
+static bool packed_ok(const ScreenArgs& a) {
+    int64_t m = a.sc.ambig < 0 ? -(int64_t)a.sc.ambig : a.sc.ambig;
+    for (int i = 0; i < 16; i++) m = std::max<int64_t>(m, a.sc.sub[i] < 0 ? -(int64_t)a.sc.sub[i] : a.sc.sub[i]);
+    return a.cap <= 192 && m <= 16383 && a.sc.xdrop >= 0 && a.sc.xdrop <= (1 << 22);
+}
+
 void launch_screen(const ScreenArgs& a, int warps, int blocks, cudaStream_t st) {
     // blocks = SMs x blocks-per-SM; for 8-warp blocks the register budget
     // follows the requested blocks per SM (2: 128, 3: 85, 4: 64 registers).
     const int per_sm = blocks / 148 > 0 ? blocks / 148 : 1;
+    count_launch();
+    if (packed_ok(a)) {
+        switch (warps) {
+            case 4: k_screen<4, 4><<<blocks, 128, 0, st>>>(a); break;
+            case 16: k_screen<16, 1><<<blocks, 512, 0, st>>>(a); break;
+            default:
+                if (per_sm >= 4) k_screen<8, 4><<<blocks, 256, 0, st>>>(a);
+                else if (per_sm == 3) k_screen<8, 3><<<blocks, 256, 0, st>>>(a);
+                else k_screen<8, 2><<<blocks, 256, 0, st>>>(a);
+                break;
+        }
+        return;
+    }
     switch (warps) {
-        case 4: count_launch(); k_screen<4, 4><<<blocks, 128, 0, st>>>(a); break;
-        case 16: count_launch(); k_screen<16, 1><<<blocks, 512, 0, st>>>(a); break;
+        case 4: k_screen_wide<4, 4><<<blocks, 128, 0, st>>>(a); break;
+        case 16: k_screen_wide<16, 1><<<blocks, 512, 0, st>>>(a); break;
         default:
-            count_launch();
-            if (per_sm >= 4) k_screen<8, 4><<<blocks, 256, 0, st>>>(a);
-            else if (per_sm == 3) k_screen<8, 3><<<blocks, 256, 0, st>>>(a);
-            else k_screen<8, 2><<<blocks, 256, 0, st>>>(a);
+            if (per_sm >= 4) k_screen_wide<8, 4><<<blocks, 256, 0, st>>>(a);
+            else if (per_sm == 3) k_screen_wide<8, 3><<<blocks, 256, 0, st>>>(a);
+            else k_screen_wide<8, 2><<<blocks, 256, 0, st>>>(a);
             break;
     }
 }

@@ -170,21 +170,25 @@ void dispatcher(gxy_server* s) {
             if (s->stop && s->pending.empty()) break;
             size_t free_b = 0, total_b = 0;
             cudaMemGetInfo(&free_b, &total_b);
-            uint64_t batch_units = 0;
+            uint64_t batch_units = 0, batch_bases = 0;
             while (!s->pending.empty()) {
                 Request* q = s->pending.front();
                 const bool fits_mem = s->bytes_in_use + q->bytes <= s->opts.max_device_bytes &&
                                       q->bytes + (64ull << 20) <= free_b;
-                const bool fits_units = s->units_in_flight + strands <= s->opts.max_units &&
-                                        batch_units + strands <= s->opts.max_batch_units;
+                const bool fits_units = s->units_in_flight + strands <= s->opts.max_units;
+                // The per-batch limits bound what joins a batch, never its first request.
+                const bool fits_batch = batch.empty() ||
+                                        (batch_units + strands <= s->opts.max_batch_units &&
+                                         batch_bases + (uint64_t)q->len * strands <= s->opts.max_batch_bases);
                 // A request that could never fit alone is still run alone.
                 const bool alone = batch.empty() && s->units_in_flight == 0;
-                if (!(fits_mem && fits_units) && !alone) break;
+                if (!(fits_mem && fits_units && fits_batch) && !alone) break;
                 s->pending.pop_front();
                 batch.push_back(q);
                 s->bytes_in_use += q->bytes;
                 s->units_in_flight += strands;
                 batch_units += strands;
+                batch_bases += (uint64_t)q->len * strands;
                 if (free_b > q->bytes) free_b -= q->bytes;
             }
             if (batch.empty()) {
@@ -259,6 +263,7 @@ gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* c
     if (!o.max_units) o.max_units = 8192;
     if (!o.max_streams) o.max_streams = 2;
     if (!o.max_batch_units) o.max_batch_units = 1024;
+    if (!o.max_batch_bases) o.max_batch_bases = 16ull << 20;
     s->opts = o;
     for (uint32_t i = 0; i < o.max_streams; i++) s->threads.emplace_back(dispatcher, s);
     *out = s;

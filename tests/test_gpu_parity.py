@@ -181,6 +181,37 @@ def test_random_homology(gxy, ctx, seed, transitions, step, lower, nfrac):
     assert len(o) > 0
 
 
+# The screen packs a side's run and extent into one i32 when scores, x-drop
+# and the column cap allow it, else it runs the unpacked kernel: both must
+# equal the oracle, on both sides of each bound.
+@pytest.mark.parametrize("scale,xdrop,thresh,cap", [
+    (1, 0, 300, 0),                 # x-drop 0: breaks on the first non-improving column
+    (1, 1, 300, 0),
+    (1, 910, 3000, 192),            # largest packed cap
+    (1, 910, 3000, 224),            # cap above the packed bound
+    (131, 910 * 131, 3000 * 131, 0),   # |score| 16375: packed
+    (132, 910 * 132, 3000 * 132, 0),   # |score| 16500: unpacked
+    (1, 1 << 22, 3000, 0),          # largest packed x-drop
+    (1, (1 << 22) + 1, 3000, 0),    # unpacked
+    (1, -1, 200, 0),                # negative x-drop: unpacked
+])
+def test_screen_envelopes(gxy, scale, xdrop, thresh, cap):
+    rng = np.random.default_rng(91)
+    t, q = homologous_pair(rng, 30000, 0.8, lower=0.05, nfrac=0.003)
+    base = gxy.ScoringMatrix.hoxd70()
+    m = gxy.ScoringMatrix(sub=[[v * scale for v in row] for row in base.sub], ambig_score=base.ambig_score * scale)
+    sp = gxy.SearchParams(1, gxy.HspParams(xdrop, thresh), 1)
+    c2 = gxy.Context(0)
+    try:
+        if cap:
+            c2.set_tuning(screen_cap=cap)
+        g, o = both(gxy, c2, t, q, P12, sp, matrix=m)
+    finally:
+        c2.close()
+    assert g == o
+    assert len(o) > 0
+
+
 def test_entropy_gate(gxy, ctx):
     rng = np.random.default_rng(11)
     t, q = homologous_pair(rng, 30000, 0.85)
@@ -246,6 +277,19 @@ def test_window_passes_match_single_pass(gxy):
         assert st2["passes"] > 1
         assert got.tobytes() == ref.tobytes()
         assert st1["raw_hits"] == st2["raw_hits"] and st1["windows"] == st2["windows"]
+        # A tiny candidate capacity as well: candidates overflow inside a pass,
+        # the arrays grow keeping earlier passes' candidates and the pass is redone.
+        assert st1["candidates"] > 4 * 1024
+        c2.set_tuning(initial_candidates=1024)
+        st3 = {}
+        got3 = gxy.search(tab, T, Q, m, sp, stats=st3)
+        assert st3["passes"] > 1 and got3.tobytes() == ref.tobytes()
+        assert st3["candidates"] == st1["candidates"]
+        # Single pass with the tiny candidate capacity: grown and rerun whole.
+        c2.set_tuning(max_hits_per_pass=1 << 30)
+        st4 = {}
+        assert gxy.search(tab, T, Q, m, sp, stats=st4).tobytes() == ref.tobytes()
+        assert st4["passes"] == 1 and st4["candidates"] == st1["candidates"]
         tab.free()
     finally:
         c2.close()
