@@ -712,7 +712,7 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen_wide(const __grid_c
 // host uses k_screen_wide outside that envelope.
 // ---------------------------------------------------------------------------
 struct PkSide {
-    uint64_t nib0, nib1;   // (t << 2 | q) nibbles of columns 0-15 and 16-31
+    uint64_t e, o;         // nibble j of e: column 2j, of o: column 2j+1; nibble = q << 2 | t
     uint32_t vv;           // column validity
     uint32_t n;            // columns present in this chunk
     int32_t p, b;          // packed run and best
@@ -721,8 +721,9 @@ struct PkSide {
 
 __device__ __forceinline__ void pk_init(PkSide& S, uint64_t tc, uint64_t qc, uint32_t vv, uint32_t n, int32_t p,
                                         int32_t b) {
-    S.nib0 = (spread16((uint32_t)tc) << 2) | spread16((uint32_t)qc);
-    S.nib1 = (spread16((uint32_t)(tc >> 32)) << 2) | spread16((uint32_t)(qc >> 32));
+    constexpr uint64_t m = 0x3333333333333333ull;
+    S.e = (tc & m) | ((qc << 2) & ~m);
+    S.o = ((tc >> 2) & m) | (qc & ~m);
     S.vv = vv;
     S.n = n;
     S.p = p;
@@ -731,10 +732,10 @@ __device__ __forceinline__ void pk_init(PkSide& S, uint64_t tc, uint64_t qc, uin
 }
 
 // Column k of a side.  kSlow: the chunk may hold invalid bases (scored
-// `ambig`) or end before column 32.
+// `ambig`) or end before column 32.  plut is indexed by (q << 2) | t.
 template <bool kSlow, int k>
 __device__ __forceinline__ void pk_step(PkSide& S, int32_t T, const int32_t* plut, int32_t pamb) {
-    const uint32_t idx = (uint32_t)(((k < 16 ? S.nib0 : S.nib1) >> (4 * (k & 15))) & 15u);
+    const uint32_t idx = (uint32_t)(((k & 1) ? S.o : S.e) >> (4 * (k >> 1))) & 15u;
     int32_t s = plut[idx];
     bool go = S.alive;
     if (kSlow) {
@@ -768,10 +769,39 @@ __device__ __forceinline__ int32_t pk_run(int32_t p) { return p >> 8; }         
 __device__ __forceinline__ uint32_t pk_ext(int32_t p) { return 255u - ((uint32_t)p & 255u); }
 constexpr int32_t kPkStart = 255;   // run 0, no columns
 
+// 64 bits from the 128-bit pair (hi:lo) starting at bit s (0 <= s < 64).
+__device__ __forceinline__ uint64_t funnel64(uint64_t lo, uint64_t hi, uint32_t s) {
+    return s ? ((lo >> s) | (hi << (64 - s))) : lo;
+}
+
+// Seed footprint score, all L columns at t / q (src/hsp.rs:119-123): three
+// columns per table read, the rest singly, invalid columns re-scored ambig.
+__device__ __forceinline__ int32_t seed_score(const SeqView& T, const SeqView& Q, uint32_t t, uint32_t q,
+                                              uint32_t L, uint32_t seed_mask, const int32_t* s_tri,
+                                              const int32_t* s_lut, int32_t ambig) {
+    const uint64_t tc = load_codes32(T.codes, T.base + t), qc = load_codes32(Q.codes, Q.base + q);
+    const uint32_t vv = load_bits32(T.valid, T.base + t) & load_bits32(Q.valid, Q.base + q);
+    int32_t sd = 0;
+#pragma unroll
+    for (int k = 0; k + 3 <= 32; k += 3) {
+        if ((uint32_t)k + 3 > L) break;
+        sd += s_tri[((((uint32_t)(tc >> (2 * k))) & 63u) << 6) | ((uint32_t)(qc >> (2 * k)) & 63u)];
+    }
+    for (uint32_t k = L - L % 3; k < L; k++)
+        sd += s_lut[((((uint32_t)(tc >> (2 * k))) & 3u) << 2) | ((uint32_t)(qc >> (2 * k)) & 3u)];
+    uint32_t bad = ~vv & seed_mask;
+    while (bad) {
+        const uint32_t k = __ffs(bad) - 1;
+        bad &= bad - 1;
+        sd += ambig - s_lut[((((uint32_t)(tc >> (2 * k))) & 3u) << 2) | ((uint32_t)(qc >> (2 * k)) & 3u)];
+    }
+    return sd;
+}
+
 template <int WARPS, int MINB>
 __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_constant__ ScreenArgs a) {
-    __shared__ int32_t s_lut[16];     // raw column scores
-    __shared__ int32_t s_plut[16];    // 256 * score - 1
+    __shared__ int32_t s_lut[16];     // raw column scores, index (t << 2) | q
+    __shared__ int32_t s_plut[16];    // 256 * score - 1, index (q << 2) | t
     __shared__ int32_t s_tri[4096];   // sum of three columns' scores, index (t3 << 6) | q3
     for (uint32_t i = threadIdx.x; i < 4096; i += blockDim.x) {
         int32_t v = 0;
@@ -781,7 +811,7 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     }
     if (threadIdx.x < 16) {
         s_lut[threadIdx.x] = a.sc.sub[threadIdx.x];
-        s_plut[threadIdx.x] = a.sc.sub[threadIdx.x] * 256 - 1;
+        s_plut[threadIdx.x] = a.sc.sub[((threadIdx.x & 3u) << 2) | (threadIdx.x >> 2)] * 256 - 1;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -791,14 +821,19 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     const int32_t pamb = ambig * 256 - 1;
     const int32_t T = (a.sc.xdrop + 1) * 256;
     const uint32_t seed_mask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
+    // No seed footprint scores above this: a hit whose two sides' bests stay
+    // below thresh - seed_ub can never pass, whatever its seed scores.
+    int32_t top = ambig;
+    for (int i = 0; i < 16; i++) top = max(top, a.sc.sub[i]);
+    const int32_t seed_ub = top * (int32_t)L;
     const unsigned long long hc = *a.hit_count;
     const uint32_t n_hits = (uint32_t)(hc < a.hit_cap ? hc : a.hit_cap);
-    unsigned long long n_cols = 0;
+    uint32_t n_cols = 0;
+    unsigned long long n_cols_all = 0;
     bool exhausted = false;
 
     bool busy = false, rdone = true, ldone = true;
     uint32_t ht = 0, hq = 0, hu = 0xffffffffu;
-    int32_t seed = 0;
     int32_t rp = kPkStart, rb = kPkStart, lp = kPkStart, lb = kPkStart;
     uint32_t rrem = 0, lrem = 0;
     SeqView T_{}, Q_{};
@@ -844,53 +879,39 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
         uint32_t avv = 0, bvv = 0, an = 0, bn = 0;
         const bool a_right = fresh || !rdone;
         if (fresh) {
+            // One 128-position window of each sequence: word 0 starts at or
+            // below ht - 32 (offset ot - 32 in [0, 31]), so the left chunk is
+            // in words 0-1 and the right chunk (offset ot + L) in words 1-3.
             const uint64_t tb = T_.base + ht, qb = Q_.base + hq;
-            const uint64_t tw = (tb - 32) & ~31ull, qw = (qb - 32) & ~31ull;
+            const uint64_t tw = (tb - 32) >> 5, qw = (qb - 32) >> 5;
             uint64_t twc[4], qwc[4];
             uint32_t twv[4], qwv[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                twc[j] = __ldg(T_.codes + (tw >> 5) + j);
-                qwc[j] = __ldg(Q_.codes + (qw >> 5) + j);
-                twv[j] = __ldg(T_.valid + (tw >> 5) + j);
-                qwv[j] = __ldg(Q_.valid + (qw >> 5) + j);
+                twc[j] = __ldg(T_.codes + tw + j);
+                qwc[j] = __ldg(Q_.codes + qw + j);
+                twv[j] = __ldg(T_.valid + tw + j);
+                qwv[j] = __ldg(Q_.valid + qw + j);
             }
-            const uint32_t ot = (uint32_t)(tb - tw), oq = (uint32_t)(qb - qw);   // both in [32, 63]
-            // Seed footprint, all L columns (src/hsp.rs:119-123): three
-            // columns per table read, the rest singly, then invalid columns
-            // re-scored as ambig.
-            {
-                const uint64_t tc = win_codes(twc, ot), qc = win_codes(qwc, oq);
-                int32_t sd = 0;
-#pragma unroll
-                for (int k = 0; k + 3 <= 32; k += 3) {
-                    if ((uint32_t)k + 3 > L) break;
-                    const uint32_t i6 = ((((uint32_t)(tc >> (2 * k))) & 63u) << 6) | ((uint32_t)(qc >> (2 * k)) & 63u);
-                    sd += s_tri[i6];
-                }
-                for (uint32_t k = L - L % 3; k < L; k++)
-                    sd += s_lut[((((uint32_t)(tc >> (2 * k))) & 3u) << 2) | ((uint32_t)(qc >> (2 * k)) & 3u)];
-                uint32_t bad = ~(win_bits(twv, ot) & win_bits(qwv, oq)) & seed_mask;
-                while (bad) {
-                    const uint32_t k = __ffs(bad) - 1;
-                    bad &= bad - 1;
-                    sd += ambig - s_lut[((((uint32_t)(tc >> (2 * k))) & 3u) << 2) | ((uint32_t)(qc >> (2 * k)) & 3u)];
-                }
-                seed = sd;
-            }
+            const uint32_t ot = (uint32_t)(tb & 31) + 32, oq = (uint32_t)(qb & 31) + 32;
             rrem = min(T_.len - ht - L, Q_.len - hq - L);
             lrem = min(ht, hq);
             rp = rb = lp = lb = kPkStart;
             rdone = rrem == 0;
             ldone = lrem == 0;
             an = min(32u, rrem);
-            atc = win_codes(twc, ot + L);
-            aqc = win_codes(qwc, oq + L);
-            avv = win_bits(twv, ot + L) & win_bits(qwv, oq + L);
+            {
+                const uint32_t rt = ot + L, rq = oq + L;      // in [32, 95]
+                const bool t2 = rt >= 64, q2 = rq >= 64;
+                atc = funnel64(t2 ? twc[2] : twc[1], t2 ? twc[3] : twc[2], (rt & 31) * 2);
+                aqc = funnel64(q2 ? qwc[2] : qwc[1], q2 ? qwc[3] : qwc[2], (rq & 31) * 2);
+                avv = __funnelshift_r(t2 ? twv[2] : twv[1], t2 ? twv[3] : twv[2], rt & 31) &
+                      __funnelshift_r(q2 ? qwv[2] : qwv[1], q2 ? qwv[3] : qwv[2], rq & 31);
+            }
             bn = min(32u, lrem);
-            btc = rev_pairs64(win_codes(twc, ot - 32));
-            bqc = rev_pairs64(win_codes(qwc, oq - 32));
-            bvv = __brev(win_bits(twv, ot - 32) & win_bits(qwv, oq - 32));
+            btc = rev_pairs64(funnel64(twc[0], twc[1], (ot & 31) * 2));
+            bqc = rev_pairs64(funnel64(qwc[0], qwc[1], (oq & 31) * 2));
+            bvv = __brev(__funnelshift_r(twv[0], twv[1], ot & 31) & __funnelshift_r(qwv[0], qwv[1], oq & 31));
         } else if (busy) {
             if (!rdone) {
                 const uint32_t ext = pk_ext(rp);
@@ -915,17 +936,17 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
             if (!busy) an = 0;
             if (!fresh) bn = 0;
             PkSide A, B;
-            pk_init(A, atc, aqc, avv, an, a_right ? rp : lp, a_right ? rb : lb);
+            const int32_t a0 = a_right ? rp : lp;
+            pk_init(A, atc, aqc, avv, an, a0, a_right ? rb : lb);
             pk_init(B, btc, bqc, bvv, bn, lp, lb);
             const bool slow = (an != 0 && (an < 32 || avv != 0xffffffffu)) ||
                               (bn != 0 && (bn < 32 || bvv != 0xffffffffu));
             if (__any_sync(kFull, slow)) pk_scan_pair<true>(A, B, T, s_plut, pamb);
             else pk_scan_pair<false>(A, B, T, s_plut, pamb);
-            const int32_t a0 = a_right ? rp : lp;
             const uint32_t aused = ((uint32_t)a0 & 255u) - ((uint32_t)A.p & 255u);
             const uint32_t bused = ((uint32_t)lp & 255u) - ((uint32_t)B.p & 255u);
             const bool aend = an != 0 && !A.alive, bend = bn != 0 && !B.alive;
-            n_cols += (fresh || busy ? aused : 0u) + (fresh ? bused : 0u);
+            n_cols += aused + bused;
             if (busy) {
                 if (a_right) {
                     rp = A.p; rb = A.b; rrem -= aused;
@@ -940,6 +961,10 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
                 ldone = ldone || bend || lrem == 0;
             }
         }
+        if (n_cols >= (1u << 30)) {
+            n_cols_all += n_cols;
+            n_cols = 0;
+        }
 
         // ---------------- bookkeeping ----------------
         bool finish = false, cand = false, is_long = false;
@@ -947,12 +972,18 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
         if (busy) {
             if (rdone && ldone) {
                 finish = true;
-                score = seed + pk_run(rb) + pk_run(lb);
-                cand = score >= thresh;
+                score = pk_run(rb) + pk_run(lb);
+                cand = score >= thresh - seed_ub;   // else the seed cannot lift it to thresh
             } else if ((!rdone && pk_ext(rp) >= a.cap) || (!ldone && pk_ext(lp) >= a.cap)) {
                 finish = true;      // still extending at the cap: defer to the walk
                 cand = true;
                 is_long = true;
+            }
+        }
+        if (__any_sync(kFull, finish && cand && !is_long)) {
+            if (finish && cand && !is_long) {
+                score += seed_score(T_, Q_, ht, hq, L, seed_mask, s_tri, s_lut, ambig);
+                cand = score >= thresh;
             }
         }
         const uint32_t m = __ballot_sync(kFull, finish && cand);
@@ -969,16 +1000,17 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
                     Cand c;
                     c.unit = hu; c.t = ht; c.q = hq;
                     c.flags = is_long ? kCandLong : 0u;
-                    c.lext = pk_ext(lb); c.rext = pk_ext(rb); c.score = score; c.pad_ = 0;
+                    c.lext = pk_ext(lb); c.rext = pk_ext(rb); c.score = is_long ? 0 : score; c.pad_ = 0;
                     a.cands[slot] = c;
                 }
             }
         }
         if (finish) busy = false;
     }
+    n_cols_all += n_cols;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n_cols += __shfl_xor_sync(kFull, n_cols, o);
-    if (lane == 0) atomicAdd(&a.stats[2], n_cols);
+    for (int o = 16; o > 0; o >>= 1) n_cols_all += __shfl_xor_sync(kFull, n_cols_all, o);
+    if (lane == 0) atomicAdd(&a.stats[2], n_cols_all);
 }
 
 // The packed screen's envelope (see above).
