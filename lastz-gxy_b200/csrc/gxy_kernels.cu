@@ -436,8 +436,28 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
         base = __shfl_sync(kFull, base, 0);
         n_raw += lane == 0 ? wtot : 0;
         if (base + wtot > a.hit_cap) continue;   // overflow: the pass is redone with fewer tiles
-        // Pass 2: write.  dst = this lane's next slot.
+        // Pass 2: write this lane's hits into its slots [dst, dst + tot).
+        // Their order within the slots is free (candidates are sorted by a
+        // unique (diagonal, t) key later), so the first position of every
+        // small bucket is loaded at once -- up to kRegVar loads in flight --
+        // before the rest.
         uint64_t dst = base + (incl - tot);
+        {
+            uint32_t first[kRegVar];
+#pragma unroll
+            for (uint32_t v = 0; v < kRegVar; v++)
+                first[v] = (rc[v] != 0 && rc[v] <= 16) ? __ldg(U.positions + rb[v]) : 0u;
+#pragma unroll
+            for (uint32_t v = 0; v < kRegVar; v++) {
+                if (rc[v] != 0 && rc[v] <= 16) {
+                    Hit h;
+                    h.t = first[v];
+                    h.q = q;
+                    h.unit = u;
+                    a.hits[dst++] = h;
+                }
+            }
+        }
         for (uint32_t v = 0; v < a.n_var; v++) {
             uint32_t b = 0, c = 0;
             if (v < kRegVar) {
@@ -453,13 +473,15 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
                 c = __ldg(U.starts + vw + 1) - b;
             }
             const bool big = c > 16;
+            // Small buckets of the first kRegVar variants wrote their first position above.
+            const uint32_t j0 = (v < kRegVar && !big) ? 1u : 0u;
             if (!big) {
-                for (uint32_t j = 0; j < c; j++) {
+                for (uint32_t j = j0; j < c; j++) {
                     Hit h;
                     h.t = __ldg(U.positions + b + j);
                     h.q = q;
                     h.unit = u;
-                    a.hits[dst + j] = h;
+                    a.hits[dst++] = h;
                 }
             }
             uint32_t bm = __ballot_sync(kFull, big);
@@ -477,7 +499,7 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
                     a.hits[dd + j] = h;
                 }
             }
-            dst += c;
+            if (big) dst += c;
         }
     }
 #pragma unroll
@@ -716,37 +738,37 @@ struct PkSide {
     uint32_t vv;           // column validity
     uint32_t n;            // columns present in this chunk
     int32_t p, b;          // packed run and best
-    bool alive;            // no x-drop break yet, and the side has columns
 };
 
+// A side with no columns starts dead (b - p = T) so that no column moves it.
 __device__ __forceinline__ void pk_init(PkSide& S, uint64_t tc, uint64_t qc, uint32_t vv, uint32_t n, int32_t p,
-                                        int32_t b) {
+                                        int32_t b, int32_t T) {
     constexpr uint64_t m = 0x3333333333333333ull;
     S.e = (tc & m) | ((qc << 2) & ~m);
     S.o = ((tc >> 2) & m) | (qc & ~m);
     S.vv = vv;
     S.n = n;
-    S.p = p;
     S.b = b;
-    S.alive = n > 0;
+    S.p = n ? p : b - T;
 }
 
-// Column k of a side.  kSlow: the chunk may hold invalid bases (scored
-// `ambig`) or end before column 32.  plut is indexed by (q << 2) | t.
+// Column k of a side, branch-free.  A side is alive while b - p < T; once the
+// x-drop break fires its later columns add 0, so p and b (and b - p >= T)
+// stay as the break left them.  kSlow: the chunk may hold invalid bases
+// (scored `ambig`) or end before column 32 (absent columns add 0 and keep
+// the side alive).  plut is indexed by (q << 2) | t.
 template <bool kSlow, int k>
 __device__ __forceinline__ void pk_step(PkSide& S, int32_t T, const int32_t* plut, int32_t pamb) {
     const uint32_t idx = (uint32_t)(((k & 1) ? S.o : S.e) >> (4 * (k >> 1))) & 15u;
     int32_t s = plut[idx];
-    bool go = S.alive;
+    bool go = S.b - S.p < T;
     if (kSlow) {
         s = ((S.vv >> k) & 1u) ? s : pamb;
         go = go && (uint32_t)k < S.n;
     }
-    if (go) {
-        S.p += s;
-        S.b = max(S.b, S.p);
-        S.alive = S.b - S.p < T;
-    }
+    s = go ? s : 0;
+    S.p += s;
+    S.b = max(S.b, S.p);
 }
 
 // Both sides column by column in lockstep: two independent serial chains.
@@ -873,92 +895,70 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
         }
 
         // ---------------- chunk data ----------------
-        // Side A: a fresh hit's first right chunk, or a continuing side's next chunk.
-        // Side B: a fresh hit's first left chunk.
+        // Side A: the next chunk of the side this hit is on (a fresh hit's
+        // first right chunk); side B: a fresh hit's first left chunk.  Right
+        // chunks read forward from the column after the last one scanned,
+        // left chunks the 32 positions below it, reversed.
         uint64_t atc = 0, aqc = 0, btc = 0, bqc = 0;
         uint32_t avv = 0, bvv = 0, an = 0, bn = 0;
         const bool a_right = fresh || !rdone;
         if (fresh) {
-            // One 128-position window of each sequence: word 0 starts at or
-            // below ht - 32 (offset ot - 32 in [0, 31]), so the left chunk is
-            // in words 0-1 and the right chunk (offset ot + L) in words 1-3.
-            const uint64_t tb = T_.base + ht, qb = Q_.base + hq;
-            const uint64_t tw = (tb - 32) >> 5, qw = (qb - 32) >> 5;
-            uint64_t twc[4], qwc[4];
-            uint32_t twv[4], qwv[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                twc[j] = __ldg(T_.codes + tw + j);
-                qwc[j] = __ldg(Q_.codes + qw + j);
-                twv[j] = __ldg(T_.valid + tw + j);
-                qwv[j] = __ldg(Q_.valid + qw + j);
-            }
-            const uint32_t ot = (uint32_t)(tb & 31) + 32, oq = (uint32_t)(qb & 31) + 32;
             rrem = min(T_.len - ht - L, Q_.len - hq - L);
             lrem = min(ht, hq);
             rp = rb = lp = lb = kPkStart;
             rdone = rrem == 0;
             ldone = lrem == 0;
-            an = min(32u, rrem);
-            {
-                const uint32_t rt = ot + L, rq = oq + L;      // in [32, 95]
-                const bool t2 = rt >= 64, q2 = rq >= 64;
-                atc = funnel64(t2 ? twc[2] : twc[1], t2 ? twc[3] : twc[2], (rt & 31) * 2);
-                aqc = funnel64(q2 ? qwc[2] : qwc[1], q2 ? qwc[3] : qwc[2], (rq & 31) * 2);
-                avv = __funnelshift_r(t2 ? twv[2] : twv[1], t2 ? twv[3] : twv[2], rt & 31) &
-                      __funnelshift_r(q2 ? qwv[2] : qwv[1], q2 ? qwv[3] : qwv[2], rq & 31);
+        }
+        if (busy) {
+            const uint32_t ext = pk_ext(a_right ? rp : lp);
+            const uint64_t ta = a_right ? T_.base + ht + L + ext : T_.base + ht - ext - 32;
+            const uint64_t qa = a_right ? Q_.base + hq + L + ext : Q_.base + hq - ext - 32;
+            atc = load_codes32(T_.codes, ta);
+            aqc = load_codes32(Q_.codes, qa);
+            avv = load_bits32(T_.valid, ta) & load_bits32(Q_.valid, qa);
+            if (!a_right) {
+                atc = rev_pairs64(atc);
+                aqc = rev_pairs64(aqc);
+                avv = __brev(avv);
             }
+            an = min(32u, a_right ? rrem : lrem);
+        }
+        if (fresh) {
+            const uint64_t tb = T_.base + ht - 32, qb = Q_.base + hq - 32;
+            btc = rev_pairs64(load_codes32(T_.codes, tb));
+            bqc = rev_pairs64(load_codes32(Q_.codes, qb));
+            bvv = __brev(load_bits32(T_.valid, tb) & load_bits32(Q_.valid, qb));
             bn = min(32u, lrem);
-            btc = rev_pairs64(funnel64(twc[0], twc[1], (ot & 31) * 2));
-            bqc = rev_pairs64(funnel64(qwc[0], qwc[1], (oq & 31) * 2));
-            bvv = __brev(__funnelshift_r(twv[0], twv[1], ot & 31) & __funnelshift_r(qwv[0], qwv[1], oq & 31));
-        } else if (busy) {
-            if (!rdone) {
-                const uint32_t ext = pk_ext(rp);
-                const uint64_t tg = T_.base + ht + L + ext, qg = Q_.base + hq + L + ext;
-                atc = load_codes32(T_.codes, tg);
-                aqc = load_codes32(Q_.codes, qg);
-                avv = load_bits32(T_.valid, tg) & load_bits32(Q_.valid, qg);
-                an = min(32u, rrem);
-            } else {
-                // The left side continues below position ht - 1 - ext.
-                const uint32_t ext = pk_ext(lp);
-                const uint64_t tg = T_.base + ht - ext - 32, qg = Q_.base + hq - ext - 32;
-                atc = rev_pairs64(load_codes32(T_.codes, tg));
-                aqc = rev_pairs64(load_codes32(Q_.codes, qg));
-                avv = __brev(load_bits32(T_.valid, tg) & load_bits32(Q_.valid, qg));
-                an = min(32u, lrem);
-            }
         }
 
         // ---------------- scans ----------------
         {
-            if (!busy) an = 0;
-            if (!fresh) bn = 0;
             PkSide A, B;
             const int32_t a0 = a_right ? rp : lp;
-            pk_init(A, atc, aqc, avv, an, a0, a_right ? rb : lb);
-            pk_init(B, btc, bqc, bvv, bn, lp, lb);
+            pk_init(A, atc, aqc, avv, an, a0, a_right ? rb : lb, T);
+            pk_init(B, btc, bqc, bvv, bn, lp, lb, T);
             const bool slow = (an != 0 && (an < 32 || avv != 0xffffffffu)) ||
                               (bn != 0 && (bn < 32 || bvv != 0xffffffffu));
             if (__any_sync(kFull, slow)) pk_scan_pair<true>(A, B, T, s_plut, pamb);
             else pk_scan_pair<false>(A, B, T, s_plut, pamb);
-            const uint32_t aused = ((uint32_t)a0 & 255u) - ((uint32_t)A.p & 255u);
-            const uint32_t bused = ((uint32_t)lp & 255u) - ((uint32_t)B.p & 255u);
-            const bool aend = an != 0 && !A.alive, bend = bn != 0 && !B.alive;
-            n_cols += aused + bused;
-            if (busy) {
+            if (an) {
+                const uint32_t used = ((uint32_t)a0 & 255u) - ((uint32_t)A.p & 255u);
+                const bool end = A.b - A.p >= T;
+                n_cols += used;
                 if (a_right) {
-                    rp = A.p; rb = A.b; rrem -= aused;
-                    rdone = rdone || aend || rrem == 0;
+                    rp = A.p; rb = A.b; rrem -= used;
+                    rdone = end || rrem == 0;
                 } else {
-                    lp = A.p; lb = A.b; lrem -= aused;
-                    ldone = ldone || aend || lrem == 0;
+                    lp = A.p; lb = A.b; lrem -= used;
+                    ldone = end || lrem == 0;
                 }
             }
-            if (fresh) {
-                lp = B.p; lb = B.b; lrem -= bused;
-                ldone = ldone || bend || lrem == 0;
+            if (bn) {
+                const uint32_t used = ((uint32_t)lp & 255u) - ((uint32_t)B.p & 255u);
+                const bool end = B.b - B.p >= T;
+                n_cols += used;
+                lp = B.p; lb = B.b; lrem -= used;
+                ldone = end || lrem == 0;
             }
         }
         if (n_cols >= (1u << 30)) {
