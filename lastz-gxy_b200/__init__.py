@@ -410,11 +410,9 @@ def _stats(st: _lib.StatsC) -> dict:
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:
     n = int(buf.len)
-    if n == 0:
-        out = np.zeros(0, HSP_DTYPE)
-    else:
-        raw = np.ctypeslib.as_array(C.cast(buf.hsps, C.POINTER(C.c_uint8)), shape=(n * 16,))
-        out = raw.view(HSP_DTYPE).copy()
+    out = np.empty(n, HSP_DTYPE)
+    if n:
+        C.memmove(out.ctypes.data, buf.hsps, n * HSP_DTYPE.itemsize)
     lib().gxy_hsp_buf_free(C.byref(buf))
     return out
 
@@ -475,12 +473,12 @@ def batch_search(tables: Sequence[PosTable], queries: Sequence[DeviceSeq], units
     if stats is not None:
         stats.update(_stats(st))
     n = int(res.n_hsps)
+    allh = np.empty(n, HSP_DTYPE)
     if n:
-        raw = np.ctypeslib.as_array(C.cast(res.hsps, C.POINTER(C.c_uint8)), shape=(n * 16,))
-        allh = raw.view(HSP_DTYPE).copy()
-    else:
-        allh = np.zeros(0, HSP_DTYPE)
-    offs = np.ctypeslib.as_array(res.unit_offsets, shape=(len(ul) + 1,)).copy() if len(ul) else np.zeros(1, np.uint64)
+        C.memmove(allh.ctypes.data, res.hsps, n * HSP_DTYPE.itemsize)
+    offs = np.zeros(len(ul) + 1, np.uint64)
+    if len(ul):
+        C.memmove(offs.ctypes.data, res.unit_offsets, (len(ul) + 1) * 8)
     lib().gxy_batch_result_free(C.byref(res))
     return [allh[int(offs[i]):int(offs[i + 1])] for i in range(len(ul))]
 

@@ -146,52 +146,40 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
     t->num_words = nw;
     t->pat = pat;
     t->step = step;
-    DevBuf& keys0 = W->tk0;
-    DevBuf& vals0 = W->tv0;
-    DevBuf& keys1 = W->tk1;
-    DevBuf& vals1 = W->tv1;
+    DevBuf& counts_buf = W->tk0;
     auto fail = [&](gxy_status s) {
         dev_free(t->starts);
         dev_free(t->positions);
         delete t;
         return s;
     };
+    // counts[word] -> exclusive scan -> starts (src/pos_table.rs:42-58); then
+    // each window drops its position into its bucket (src/pos_table.rs:69-75)
+    // through an atomic cursor, so bucket order is arbitrary until the table
+    // is made canonical (on download).
     cudaError_t e = dev_alloc((void**)&t->starts, (nw + 1) * 4, st);
-    if (e == cudaSuccess) e = keys0.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
-    if (e == cudaSuccess) e = vals0.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
-    if (e == cudaSuccess) e = keys1.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
-    if (e == cudaSuccess) e = vals1.ensure((size_t)std::max<uint32_t>(nwin, 1) * 4);
+    if (e == cudaSuccess) e = dev_alloc((void**)&t->positions, (size_t)std::max<uint32_t>(nwin, 1) * 4, st);
+    if (e == cudaSuccess) e = counts_buf.ensure((size_t)(nw + 1) * 4);
     if (e != cudaSuccess) {
         set_error(std::string("table allocation: ") + cudaGetErrorString(e));
         return fail(GXY_ENOMEM);
     }
-    // counts[word] -> exclusive scan in place -> starts (src/pos_table.rs:42-58).
-    e = cudaMemsetAsync(t->starts, 0, (nw + 1) * 4, st);
+    uint32_t* counts = counts_buf.as<uint32_t>();
+    e = cudaMemsetAsync(counts, 0, (nw + 1) * 4, st);
     const SeqView view = view_of(seq, lo, hi);
-    launch_seed_words(view, pat, step, nwin, (uint32_t)nw, keys0.as<uint32_t>(), vals0.as<uint32_t>(), t->starts, st);
-    scan_u32(t->starts, t->starts, nullptr, nw, nw, true, nullptr, W->ps, st);
-    // Stable sort of (word, position) by word: positions stay ascending within
-    // a bucket, the order of the reference's scatter (src/pos_table.rs:69-75).
-    RadixPass passes[8];
-    int bits = 0;
-    while ((1ull << bits) <= nw) bits++;   // words and the sentinel nw
-    const int np = plan_radix(0, bits, 0, 0, passes, 8);
-    const int which = radix_sort_u32(keys0.as<uint32_t>(), vals0.as<uint32_t>(), keys1.as<uint32_t>(),
-                                     vals1.as<uint32_t>(), nullptr, nwin, nwin, passes, np, W->ps, st);
-    uint32_t* svals = which ? vals1.as<uint32_t>() : vals0.as<uint32_t>();
-    uint32_t total = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, t->starts + nw, 4, cudaMemcpyDeviceToHost, st);
+    launch_count_words(view, pat, step, nwin, counts, st);
+    scan_u32(counts, t->starts, nullptr, nw, nw, true, nullptr, W->ps, st);
+    launch_fill_buckets(view, pat, step, nwin, t->starts, counts, t->positions, st);
+    uint32_t* total_h = static_cast<uint32_t*>(W->h_pinned);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(total_h, t->starts + nw, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("table build: ") + cudaGetErrorString(e));
         return fail(GXY_ECUDA);
     }
-    t->npos = total;
-    e = dev_alloc((void**)&t->positions, (size_t)std::max<uint32_t>(total, 1) * 4, st);
-    if (e == cudaSuccess && total)
-        e = cudaMemcpyAsync(t->positions, svals, (size_t)total * 4, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    t->npos = *total_h;
+    t->canonical = t->npos == 0;
     if (e == cudaSuccess && mwc > 0) {
         const gxy_status ps = prune_table(t, mwc, W);
         if (ps != GXY_OK) return fail(ps);
@@ -205,9 +193,59 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
     return GXY_OK;
 }
 
-gxy_status deliver(const std::vector<gxy_hsp>& v, gxy_hsp_buf* out) {
+// Puts every bucket in ascending position order, the order of the
+// reference's stable scatter (src/pos_table.rs:69-75): buckets of <= 16 by
+// one thread each, <= kBlockBucket by one block each, larger ones by the
+// radix sort, one bucket at a time.
+gxy_status canonicalize(gxy_table* t, Worker* W) {
+    if (t->canonical) return GXY_OK;
+    cudaStream_t st = W->st;
+    uint32_t cap = 1u << 16;
+    uint32_t* hn = static_cast<uint32_t*>(W->h_pinned);
+    for (;;) {
+        API_CK(W->tk1.ensure(((size_t)cap * 2 + 1) * 4));
+        uint32_t* nbig = W->tk1.as<uint32_t>();
+        API_CK(cudaMemsetAsync(nbig, 0, 4, st));
+        launch_sort_small_buckets(t->starts, t->num_words, t->positions, nbig + 1, nbig, cap, st);
+        API_CK(cudaMemcpyAsync(hn, nbig, 4, cudaMemcpyDeviceToHost, st));
+        API_CK(cudaStreamSynchronize(st));
+        if (*hn > cap) {
+            cap = *hn;   // re-sorting the sorted small buckets is harmless
+            continue;
+        }
+        break;
+    }
+    const uint32_t n_big = *hn;
+    uint32_t* big = W->tk1.as<uint32_t>() + 1;
+    launch_sort_block_buckets(big, n_big, t->positions, st);
+    if (n_big) {
+        std::vector<uint32_t> hb((size_t)n_big * 2);
+        API_CK(cudaMemcpyAsync(hb.data(), big, hb.size() * 4, cudaMemcpyDeviceToHost, st));
+        API_CK(cudaStreamSynchronize(st));
+        int bits = 0;
+        while (bits < 32 && (1ull << bits) < t->hi - t->lo) bits++;
+        RadixPass passes[8];
+        const int np = plan_radix(0, std::max(bits, 1), 0, 0, passes, 8);
+        for (uint32_t i = 0; i < n_big; i++) {
+            const uint32_t b = hb[2 * i], n = hb[2 * i + 1];
+            if (n <= kBlockBucket) continue;
+            API_CK(W->tk0.ensure((size_t)n * 4));
+            API_CK(W->tv0.ensure((size_t)n * 4));
+            API_CK(W->tv1.ensure((size_t)n * 4));
+            const int which = radix_sort_u32(t->positions + b, W->tv0.as<uint32_t>(), W->tk0.as<uint32_t>(),
+                                             W->tv1.as<uint32_t>(), nullptr, n, n, passes, np, W->ps, st);
+            if (which)
+                API_CK(cudaMemcpyAsync(t->positions + b, W->tk0.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    API_CK(cudaStreamSynchronize(st));
+    API_CK(cudaGetLastError());
+    t->canonical = true;
+    return GXY_OK;
+}
+
+gxy_status deliver(const gxy_hsp* v, uint64_t n, gxy_hsp_buf* out) {
     if (!out) return GXY_OK;
-    const uint64_t n = v.size();
     if (out->hsps == nullptr) {
         out->hsps = static_cast<gxy_hsp*>(malloc(std::max<uint64_t>(n, 1) * sizeof(gxy_hsp)));
         if (!out->hsps) {
@@ -220,7 +258,7 @@ gxy_status deliver(const std::vector<gxy_hsp>& v, gxy_hsp_buf* out) {
         set_error("caller HSP buffer too small");
         return GXY_EOVERFLOW;
     }
-    if (n) memcpy(out->hsps, v.data(), n * sizeof(gxy_hsp));
+    if (n) memcpy(out->hsps, v, n * sizeof(gxy_hsp));
     out->len = n;
     return GXY_OK;
 }
@@ -238,9 +276,10 @@ gxy_status search_impl(gxy_ctx* ctx, Worker* W, const gxy_table* table, const Se
     units[0].primary_lo = units[0].primary_hi = 0;
     units[0].avg_bucket = table->num_words ? (double)table->npos / (double)table->num_words : 0.0;
     RunResult r;
+    r.want_view = true;
     API_TRY(run_units(ctx, W, units, tsegs, qsegs, table->pat, *p, false, r));
     if (stats) *stats = r.stats;
-    return deliver(r.hsps, out);
+    return deliver(r.view, r.n_view, out);
 }
 
 }  // namespace
@@ -322,6 +361,7 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         for (int i = 0; i < 4; i++)
             if (w->ev[i]) cudaEventDestroy(w->ev[i]);
         if (w->h_pinned) cudaFreeHost(w->h_pinned);
+        if (w->h_res) cudaFreeHost(w->h_res);
         cudaStreamDestroy(w->st);
         delete w;
     }
@@ -523,6 +563,13 @@ gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_p
 gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions) {
     if (!t) return GXY_EINVAL;
     API_TRY(set_device(t->ctx));
+    if (positions && !t->canonical) {
+        // Bucket order is an internal detail until it is observed here; the
+        // table's contents (and every search on it) are the same either way.
+        WorkerLease L(t->ctx);
+        if (!L.w) return L.err;
+        API_TRY(canonicalize(const_cast<gxy_table*>(t), L.w));
+    }
     if (starts) API_CK(cudaMemcpy(starts, t->starts, (t->num_words + 1) * 4, cudaMemcpyDeviceToHost));
     if (positions && t->npos) API_CK(cudaMemcpy(positions, t->positions, t->npos * 4, cudaMemcpyDeviceToHost));
     return GXY_OK;

@@ -148,8 +148,11 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
         b->st = w->st;
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
+    w->ps.sort_grid_max = ctx->sm_count * 8;
     if (e == cudaSuccess) e = w->prim_sums.ensure((w->ps.grid + 1) * sizeof(uint32_t));
-    if (e == cudaSuccess) e = w->prim_hist.ensure(((size_t)kRadixMax * w->ps.grid + 1) * sizeof(uint32_t));
+    if (e == cudaSuccess)
+        e = w->prim_hist.ensure(((size_t)kRadixMax * std::max(w->ps.grid, w->ps.sort_grid_max) + 1) *
+                                sizeof(uint32_t));
     if (e == cudaSuccess) e = w->counters.ensure(256);
     if (e == cudaSuccess) e = cudaMallocHost(&w->h_pinned, 1 << 16);
     if (e != cudaSuccess) {
@@ -264,9 +267,27 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     GXY_CK(W->d_units.ensure(nu * sizeof(UnitDev)));
     GXY_CK(W->d_tsegs.ensure(tsegs.size() * sizeof(SeqView)));
     GXY_CK(W->d_qsegs.ensure(qsegs.size() * sizeof(SeqView)));
-    GXY_CK(cudaMemcpyAsync(W->d_units.p, ud.data(), nu * sizeof(UnitDev), cudaMemcpyHostToDevice, st));
-    GXY_CK(cudaMemcpyAsync(W->d_tsegs.p, tsegs.data(), tsegs.size() * sizeof(SeqView), cudaMemcpyHostToDevice, st));
-    GXY_CK(cudaMemcpyAsync(W->d_qsegs.p, qsegs.data(), qsegs.size() * sizeof(SeqView), cudaMemcpyHostToDevice, st));
+    {
+        // Descriptors go through the pinned staging when they fit (the
+        // worker's stream is idle here: every call ends synchronized).
+        const size_t bu = nu * sizeof(UnitDev), bt = tsegs.size() * sizeof(SeqView),
+                     bq = qsegs.size() * sizeof(SeqView);
+        const size_t off = 4096;
+        if (off + bu + bt + bq <= W->h_pinned_bytes) {
+            unsigned char* h = static_cast<unsigned char*>(W->h_pinned) + off;
+            memcpy(h, ud.data(), bu);
+            memcpy(h + bu, tsegs.data(), bt);
+            memcpy(h + bu + bt, qsegs.data(), bq);
+            GXY_CK(cudaMemcpyAsync(W->d_units.p, h, bu, cudaMemcpyHostToDevice, st));
+            GXY_CK(cudaMemcpyAsync(W->d_tsegs.p, h + bu, bt, cudaMemcpyHostToDevice, st));
+            GXY_CK(cudaMemcpyAsync(W->d_qsegs.p, h + bu + bt, bq, cudaMemcpyHostToDevice, st));
+        } else {
+            GXY_CK(cudaMemcpyAsync(W->d_units.p, ud.data(), bu, cudaMemcpyHostToDevice, st));
+            GXY_CK(cudaMemcpyAsync(W->d_tsegs.p, tsegs.data(), bt, cudaMemcpyHostToDevice, st));
+            GXY_CK(cudaMemcpyAsync(W->d_qsegs.p, qsegs.data(), bq, cudaMemcpyHostToDevice, st));
+            GXY_CK(cudaStreamSynchronize(st));   // the host vectors die with this call
+        }
+    }
 
     ScreenArgs sa;
     memset(&sa, 0, sizeof(sa));
@@ -578,12 +599,35 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.enum_ms = single ? ms_enum : 0.0;
         out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;
         out.stats.passes = single ? 1 : (uint32_t)((tiles + pass_tiles - 1) / pass_tiles);
-        out.hsps.resize(nh);
-        out.unit.resize(nh);
+        // Results come back through the worker's pinned staging.
+        const size_t hb = (size_t)nh * sizeof(Hsp), ub = nu > 1 ? (size_t)nh * 4 : 0;
+        if (hb + ub > W->h_res_bytes) {
+            if (W->h_res) GXY_CK(cudaFreeHost(W->h_res));
+            W->h_res = nullptr;
+            W->h_res_bytes = 0;
+            const size_t want = std::max<size_t>(1 << 20, (hb + ub) + (hb + ub) / 2);
+            GXY_CK(cudaMallocHost(&W->h_res, want));
+            W->h_res_bytes = want;
+        }
+        unsigned char* hr = static_cast<unsigned char*>(W->h_res);
         if (nh) {
-            GXY_CK(cudaMemcpyAsync(out.hsps.data(), fin, (size_t)nh * sizeof(Hsp), cudaMemcpyDeviceToHost, st));
-            GXY_CK(cudaMemcpyAsync(out.unit.data(), fin_unit, (size_t)nh * 4, cudaMemcpyDeviceToHost, st));
+            GXY_CK(cudaMemcpyAsync(hr, fin, hb, cudaMemcpyDeviceToHost, st));
+            if (ub) GXY_CK(cudaMemcpyAsync(hr + hb, fin_unit, ub, cudaMemcpyDeviceToHost, st));
             GXY_CK(cudaStreamSynchronize(st));
+        }
+        static_assert(sizeof(Hsp) == sizeof(gxy_hsp), "device and ABI HSP layouts differ");
+        const gxy_hsp* hh = reinterpret_cast<const gxy_hsp*>(hr);
+        if (out.want_view && nu == 1) {
+            out.view = hh;
+            out.n_view = nh;
+            return GXY_OK;
+        }
+        out.hsps.assign(hh, hh + nh);
+        if (ub) {
+            const uint32_t* uu = reinterpret_cast<const uint32_t*>(hr + hb);
+            out.unit.assign(uu, uu + nh);
+        } else {
+            out.unit.assign(nh, 0u);
         }
         return GXY_OK;
     }

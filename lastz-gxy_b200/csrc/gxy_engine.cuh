@@ -45,8 +45,10 @@ struct Worker {
     uint64_t hit_cap = 0;
     uint32_t cand_cap = 0;
     uint32_t res_cap = 0;
-    void* h_pinned = nullptr;     // small host staging
+    void* h_pinned = nullptr;     // small host staging: counters, unit and segment descriptors
     size_t h_pinned_bytes = 0;
+    void* h_res = nullptr;        // pinned staging of results (grown on demand)
+    size_t h_res_bytes = 0;
     // Host-query staging for gxy_search.
     gxy_dseq* qstage = nullptr;
     gxy_dseq* tstage = nullptr;
@@ -69,6 +71,12 @@ struct RunResult {
     std::vector<gxy_hsp> hsps;
     std::vector<uint32_t> unit;
     gxy_stats stats{};
+    // With want_view set (single-unit searches), the HSPs are left in the
+    // worker's pinned staging instead: view[0, n_view), valid until the
+    // worker's next call; hsps and unit stay empty.
+    bool want_view = false;
+    const gxy_hsp* view = nullptr;
+    uint64_t n_view = 0;
 };
 
 }  // namespace gxy
@@ -94,6 +102,9 @@ struct gxy_table {
     uint32_t* positions = nullptr;
     uint64_t num_words = 0;
     uint64_t npos = 0;
+    // Positions within a bucket are in ascending order (the reference's
+    // order) only once canonical; searches do not depend on that order.
+    bool canonical = true;
     gxy::Pattern pat{};
     uint32_t step = 1;
     const void* hc = nullptr;

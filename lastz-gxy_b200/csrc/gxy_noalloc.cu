@@ -38,7 +38,7 @@ constexpr uint64_t kOffVals0 = kOffKeys0 + kStaticMaxLen * 4;
 constexpr uint64_t kOffKeys1 = kOffVals0 + kStaticMaxLen * 4;
 constexpr uint64_t kOffVals1 = kOffKeys1 + kStaticMaxLen * 4;
 constexpr uint64_t kOffHist = kOffVals1 + kStaticMaxLen * 4;
-constexpr uint64_t kOffSums = kOffHist + ((uint64_t)kRadixMax * kStaticMaxGrid + 1) * 4;
+constexpr uint64_t kOffSums = (kOffHist + ((uint64_t)kRadixMax * kStaticMaxGrid + 1) * 4 + 255) & ~255ull;
 constexpr uint64_t kStaticScratchBytes = (kOffSums + (kStaticMaxGrid + 1) * 4 + 255) & ~255ull;
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
@@ -148,6 +148,7 @@ extern "C" gxy_status gxy_table_build_static(const gxy_packed_seq* target, const
     if (e != cudaSuccess) return fail(GXY_ECUDA, std::string("static table build staging: ") + cudaGetErrorString(e));
     PrimScratch ps;
     ps.grid = (int)std::min<uint32_t>(kStaticMaxGrid, (uint32_t)slot.sm_count * 2);
+    ps.sort_grid_max = ps.grid;
     ps.hist = reinterpret_cast<uint32_t*>(base + kOffHist);
     ps.block_sums = reinterpret_cast<uint32_t*>(base + kOffSums);
     uint32_t* k0 = reinterpret_cast<uint32_t*>(base + kOffKeys0);

@@ -1,6 +1,8 @@
 // gxy_prims.cu -- fixed-grid scan and stable LSD radix sort (see gxy_prims.cuh).
 #include "gxy_prims.cuh"
 
+#include <algorithm>
+
 #include "gxy_device.cuh"
 
 namespace gxy {
@@ -73,42 +75,86 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_reduce(const T* in, const
     }
 }
 
-// Single-block exclusive scan of a short array in place; a[n] = total.  Each
-// thread owns one contiguous segment: sum it (eight independent loads at a
-// time), scan the 1024 sums, write.
+// Single-block exclusive scan of a short array in place (the block sums of a
+// scan, or the digit-major histograms of a radix pass); a[n] = total.  Each
+// warp owns a contiguous run of 256-element chunks; a lane holds 8
+// consecutive elements (two 16-byte loads when a is 16-byte aligned), so
+// every warp access is one contiguous kilobyte.
 __global__ __launch_bounds__(1024) void k_scan_small(uint32_t* a, int n) {
-    __shared__ uint32_t s_warp[32];
-    __shared__ uint32_t s_total;
-    const int per = (n + 1023) / 1024;
-    const int beg = min(n, (int)threadIdx.x * per), end = min(n, beg + per);
-    uint32_t s = 0;
-    int i = beg;
-    for (; i + 8 <= end; i += 8) {
-        uint32_t v[8];
+    __shared__ uint32_t s_w[33];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool vec = (reinterpret_cast<uintptr_t>(a) & 15u) == 0;
+    const int nch = (n + 255) / 256;
+    const int per = (nch + 31) / 32;
+    const int beg = min(n, w * per * 256), end = min(n, beg + per * 256);
+    auto load8 = [&](int i, uint32_t (&v)[8]) {
+        if (vec && i + 8 <= end) {
+            const uint4 x = *reinterpret_cast<const uint4*>(a + i);
+            const uint4 y = *reinterpret_cast<const uint4*>(a + i + 4);
+            v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+            v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+        } else {
 #pragma unroll
-        for (int k = 0; k < 8; k++) v[k] = a[i + k];
+            for (int k = 0; k < 8; k++) v[k] = i + k < end ? a[i + k] : 0u;
+        }
+    };
+    uint32_t s = 0;
+    for (int i = beg + lane * 8; i < end; i += 256) {
+        uint32_t v[8];
+        load8(i, v);
 #pragma unroll
         for (int k = 0; k < 8; k++) s += v[k];
     }
-    for (; i < end; i++) s += a[i];
-    uint32_t run = block_excl_scan<1024>(s, s_warp, &s_total);
-    i = beg;
-    for (; i + 8 <= end; i += 8) {
-        uint32_t v[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) v[k] = a[i + k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    if (lane == 0) s_w[w] = s;
+    __syncthreads();
+    if (w == 0) {
+        const uint32_t x = s_w[lane];
+        uint32_t incl = x;
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            a[i + k] = run;
-            run += v[k];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
         }
+        s_w[lane] = incl - x;
+        if (lane == 31) s_w[32] = incl;
     }
-    for (; i < end; i++) {
-        const uint32_t x = a[i];
-        a[i] = run;
-        run += x;
+    __syncthreads();
+    uint32_t carry = s_w[w];
+    for (int c = beg; c < end; c += 256) {
+        const int i = c + lane * 8;
+        uint32_t v[8];
+        load8(i, v);
+        uint32_t t = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) t += v[k];
+        uint32_t incl = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint32_t run = carry + incl - t;
+        if (vec && i + 8 <= end) {
+            uint32_t o8[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                o8[k] = run;
+                run += v[k];
+            }
+            *reinterpret_cast<uint4*>(a + i) = make_uint4(o8[0], o8[1], o8[2], o8[3]);
+            *reinterpret_cast<uint4*>(a + i + 4) = make_uint4(o8[4], o8[5], o8[6], o8[7]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                if (i + k < end) a[i + k] = run;
+                run += v[k];
+            }
+        }
+        carry += __shfl_sync(kFull, incl, 31);
     }
-    if (threadIdx.x == 0) a[n] = s_total;
+    if (threadIdx.x == 0) a[n] = s_w[32];
 }
 
 template <typename T>
@@ -286,6 +332,12 @@ template <typename K>
 int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
                const RadixPass* passes, int npass, const PrimScratch& ps, cudaStream_t st) {
     const size_t smem = sizeof(SortSmem<K>);
+    // Blocks: enough for every block to own about two tiles at capacity, so
+    // that large sorts fill the GPU and small ones keep their digit-major
+    // histogram (radix x grid entries, scanned by one block) short.
+    const uint64_t want = (n_cap + 2 * (uint64_t)kSortTile - 1) / (2 * (uint64_t)kSortTile);
+    const int cap_grid = ps.sort_grid_max > 0 ? ps.sort_grid_max : ps.grid;
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)cap_grid));
     K* kin = ka;
     uint32_t* vin = va;
     K* kout = kb;
@@ -293,13 +345,13 @@ int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, 
     for (int p = 0; p < npass; p++) {
         const int radix = 1 << passes[p].bits;
         count_launch();
-        k_radix_hist<K><<<ps.grid, kSortThreads, 0, st>>>(kin, n_dev, n_host, n_cap, passes[p].shift,
-                                                          passes[p].bits, ps.hist);
+        k_radix_hist<K><<<grid, kSortThreads, 0, st>>>(kin, n_dev, n_host, n_cap, passes[p].shift,
+                                                       passes[p].bits, ps.hist);
         count_launch();
-        k_scan_small<<<1, 1024, 0, st>>>(ps.hist, radix * ps.grid);
+        k_scan_small<<<1, 1024, 0, st>>>(ps.hist, radix * grid);
         count_launch();
-        k_radix_scatter<K><<<ps.grid, kSortThreads, smem, st>>>(kin, vin, kout, vout, n_dev, n_host, n_cap,
-                                                                passes[p].shift, passes[p].bits, ps.hist);
+        k_radix_scatter<K><<<grid, kSortThreads, smem, st>>>(kin, vin, kout, vout, n_dev, n_host, n_cap,
+                                                             passes[p].shift, passes[p].bits, ps.hist);
         K* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }

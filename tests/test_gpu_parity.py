@@ -93,6 +93,29 @@ def test_table_bit_exact(gxy, ctx, pattern, step, mwc):
     assert np.array_equal(pos, ot.positions())
 
 
+# Table builds fill buckets through atomic cursors; the download puts every
+# bucket in ascending order by size class (<= 16 one thread, <= 4096 one
+# block, larger the radix sort).  All three against the oracle, after a
+# search on the same table (searches do not need the order).
+@pytest.mark.parametrize("pattern,step", [("111", 1), ("11011", 1), (P12, 1), ("111", 2)])
+def test_table_bucket_orders(gxy, ctx, pattern, step):
+    rng = np.random.default_rng(7 + step + len(pattern))
+    s = (rand_ascii(rng, 30000, b"ACGTacgtN", None) + b"A" * 13000 + b"ACGTT" * 900 +
+         rand_ascii(rng, 5000, b"ACGT", None))
+    T = gxy.PackedSeq.from_ascii(s)
+    tab = gxy.PosTable.build(T, pattern, step, ctx=ctx)
+    q = s[2000:12000]   # random part: few raw hits even for the dense patterns
+    sp = gxy.SearchParams(step, gxy.HspParams(910, 3000), 1)
+    got = gxy.search(tab, T, gxy.PackedSeq.from_ascii(q), gxy.ScoringMatrix.hoxd70(), sp)
+    starts, pos = tab.arrays()
+    ot = O.Table(O.pack_ascii(s), pattern, step)
+    assert np.array_equal(starts, ot.starts())
+    assert np.array_equal(pos, ot.positions())
+    assert int(np.diff(starts.astype(np.int64)).max()) > 4096
+    want, _ = O.search(ot, O.pack_ascii(s), O.pack_ascii(q), orc_params(gxy.ScoringMatrix.hoxd70(), sp))
+    assert as_tuples(got) == as_tuples(want) and len(want) > 0
+
+
 def test_table_known_buckets(gxy, ctx):
     # src/pos_table.rs:144-161, :177-187, :190-197, :200-211
     T = gxy.PackedSeq.from_ascii(b"ACGTACGT")
