@@ -59,13 +59,25 @@ def peaks() -> tuple[float, str]:
 
 
 def profiled_traffic():
-    """Per-launch DRAM bytes of the screen kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "screen_traffic.json")
+    """DRAM bytes of the screen and enumerate kernels from one committed ncu
+    capture (profiles/kernel_traffic.json), with the raw hits of that launch;
+    None when the file is absent."""
+    p = os.path.join(ROOT, "profiles", "kernel_traffic.json")
     try:
         with open(p) as f:
             return json.load(f)
     except Exception:
         return None
+
+
+def scaled_traffic(tr, kernel: str, raw_hits: float):
+    """Per-launch DRAM traffic of `kernel` at this launch's raw hits: the
+    captured read + write bytes scaled by raw hits (both kernels' traffic
+    grows with the hits they enumerate or screen)."""
+    if not tr or kernel not in tr:
+        return None
+    k = tr[kernel]
+    return int((k["dram_read_bytes"] + k["dram_write_bytes"]) * raw_hits / k["raw_hits"])
 
 
 class ClockSampler:
@@ -249,14 +261,16 @@ def run_ours(args, rank: int, world: int, device: int):
         "gpu_launches": int(launches * args.steps),
         "roofline": {"bound": "hbm", "kernel": "k_screen", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": tr.get("bytes_per_launch") if tr else None,
+                     "traffic": scaled_traffic(tr, "k_screen", raw),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_screen launch "
+                                       "(profiles/kernel_traffic.json), scaled to this launch by raw hits",
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s",
                      "kernel_ms": round(scr_ms, 3), "algorithmic_bytes_per_launch": int(scr_bytes)},
         "roofline_enumerate": {"bound": "hbm", "kernel": "k_enumerate", "achieved": round(en_achieved, 1),
                                "peak": peak, "unit": "GB/s", "frac": round(en_achieved / peak, 4),
                                "kernel_ms": round(en_ms, 3), "algorithmic_bytes_per_launch": int(en_bytes),
-                               "traffic": tr.get("enumerate_bytes_per_launch") if tr else None},
+                               "traffic": scaled_traffic(tr, "k_enumerate", raw)},
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -341,7 +341,6 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         }
     }
     const int blocks_screen = ctx->sm_count * (int)std::max<uint32_t>(1, ctx->tuning.screen_blocks_per_sm);
-    const int blocks_enum = ctx->sm_count * 8;
     const int blocks_misc = ctx->sm_count * 4;
     const int walk_warps = ctx->tuning.walk_warps == 4 ? 4 : 8;
 
@@ -354,7 +353,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(cudaMemsetAsync(hitc, 0, 8, st));
         sa.tile_lo = t0;
         sa.tile_hi = t1;
-        launch_enumerate(sa, blocks_enum, st);
+        launch_enumerate(sa, ctx->sm_count, st);
         if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
         launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
         return GXY_OK;
@@ -464,6 +463,12 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                     continue;
                 }
                 t0 = t1;
+                // Hit density varies along the query (repeats): grow the
+                // window range again after a sparse pass, up to twice.
+                if ((double)nh < 0.5 * (double)W->hit_cap) {
+                    const double f = std::min(2.0, 0.8 * (double)W->hit_cap / std::max<double>(1.0, (double)nh));
+                    pass_tiles = (uint32_t)std::min<double>((double)tiles, std::max(1.0, (double)pass_tiles * f));
+                }
             }
             GXY_CK(cudaEventRecord(W->ev[3], st));
             GXY_CK(cudaEventRecord(W->ev[1], st));

@@ -480,6 +480,13 @@ __device__ __forceinline__ void scan_pair_any(SideScan& A, SideScan& B, uint32_t
 // variant's bucket (src/pos_table.rs:102-108).  Large buckets are copied by
 // the whole warp.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void store_hit(Hit* p, uint32_t t, uint32_t q, uint32_t u) {
+    p->t = t;
+    p->q = q;
+    p->unit = u;
+}
+__device__ __forceinline__ Hit load_hit(const Hit* p) { return *p; }
+
 __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ ScreenArgs a) {
     const int lane = threadIdx.x & 31;
     const uint32_t ntile = a.tile_hi - a.tile_lo;
@@ -552,13 +559,7 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
                 first[v] = (rc[v] != 0 && rc[v] <= 16) ? __ldg(U.positions + rb[v]) : 0u;
 #pragma unroll
             for (uint32_t v = 0; v < kRegVar; v++) {
-                if (rc[v] != 0 && rc[v] <= 16) {
-                    Hit h;
-                    h.t = first[v];
-                    h.q = q;
-                    h.unit = u;
-                    a.hits[dst++] = h;
-                }
+                if (rc[v] != 0 && rc[v] <= 16) store_hit(a.hits + dst++, first[v], q, u);
             }
         }
         for (uint32_t v = 0; v < a.n_var; v++) {
@@ -579,13 +580,7 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
             // Small buckets of the first kRegVar variants wrote their first position above.
             const uint32_t j0 = (v < kRegVar && !big) ? 1u : 0u;
             if (!big) {
-                for (uint32_t j = j0; j < c; j++) {
-                    Hit h;
-                    h.t = __ldg(U.positions + b + j);
-                    h.q = q;
-                    h.unit = u;
-                    a.hits[dst++] = h;
-                }
+                for (uint32_t j = j0; j < c; j++) store_hit(a.hits + dst++, __ldg(U.positions + b + j), q, u);
             }
             uint32_t bm = __ballot_sync(kFull, big);
             while (bm) {
@@ -594,13 +589,7 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
                 const uint32_t bb = __shfl_sync(kFull, b, src), cc = __shfl_sync(kFull, c, src);
                 const uint32_t qq = __shfl_sync(kFull, q, src);
                 const uint64_t dd = __shfl_sync(kFull, dst, src);
-                for (uint32_t j = lane; j < cc; j += 32) {
-                    Hit h;
-                    h.t = __ldg(U.positions + bb + j);
-                    h.q = qq;
-                    h.unit = u;
-                    a.hits[dd + j] = h;
-                }
+                for (uint32_t j = lane; j < cc; j += 32) store_hit(a.hits + dd + j, __ldg(U.positions + bb + j), qq, u);
             }
             if (big) dst += c;
         }
@@ -613,9 +602,9 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
     }
 }
 
-void launch_enumerate(const ScreenArgs& a, int blocks, cudaStream_t st) {
+void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st) {
     count_launch();
-    k_enumerate<<<blocks, 256, 0, st>>>(a);
+    k_enumerate<<<sm_count * 8, 256, 0, st>>>(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -644,7 +633,8 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen_wide(const __grid_c
     const uint32_t L = a.pat.len;
     const int32_t ambig = a.sc.ambig, xdrop = a.sc.xdrop, thresh = a.sc.hspthresh;
     const unsigned long long hc = *a.hit_count;
-    const uint32_t n_hits = (uint32_t)(hc < a.hit_cap ? hc : a.hit_cap);
+    if (hc > a.hit_cap) return;   // the pass is redone over fewer tiles
+    const uint32_t n_hits = (uint32_t)hc;
     unsigned long long n_cols = 0;
     bool exhausted = false;
 
@@ -670,7 +660,7 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen_wide(const __grid_c
         if (!busy) {
             const uint32_t rk = __popc(im & lt);
             if (rk < take) {
-                const Hit h = a.hits[base + rk];
+                const Hit h = load_hit(a.hits + base + rk);
                 ht = h.t;
                 hq = h.q;
                 hu = h.unit;
@@ -952,7 +942,16 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     for (int i = 0; i < 16; i++) top = max(top, a.sc.sub[i]);
     const int32_t seed_ub = top * (int32_t)L;
     const unsigned long long hc = *a.hit_count;
-    const uint32_t n_hits = (uint32_t)(hc < a.hit_cap ? hc : a.hit_cap);
+    // An overflowing pass is redone over fewer tiles: screening its
+    // truncated hits would be wasted work.
+    if (hc > a.hit_cap) return;
+    const uint32_t n_hits = (uint32_t)hc;
+    // Each warp claims hits in chunks (one atomic per chunk) and deals them
+    // to its idle lanes; chunks shrink for small launches so that every warp
+    // still gets work.
+    const uint32_t n_warps = gridDim.x * WARPS;
+    const uint32_t chunk = max(32u, min(256u, n_hits / max(1u, n_warps * 8u)));
+    uint32_t wcur = 0, wend = 0;   // this warp's claimed, not yet dealt hits
     uint32_t n_cols = 0;
     unsigned long long n_cols_all = 0;
     bool exhausted = false;
@@ -967,18 +966,23 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     for (;;) {
         // ---------------- assign ----------------
         const uint32_t im = __ballot_sync(kFull, !busy);
-        uint32_t base = 0, take = 0;
-        if (!exhausted && im) {
-            if (lane == 0) base = atomicAdd(a.hit_next, (uint32_t)__popc(im));
-            base = __shfl_sync(kFull, base, 0);
-            take = base < n_hits ? min((uint32_t)__popc(im), n_hits - base) : 0u;
-            if (base + (uint32_t)__popc(im) >= n_hits) exhausted = true;
+        const uint32_t need = __popc(im);
+        const uint32_t avail = wend - wcur;
+        uint32_t nb = 0, ncount = 0;
+        if (need > avail && !exhausted) {
+            if (lane == 0) nb = atomicAdd(a.hit_next, chunk);
+            nb = __shfl_sync(kFull, nb, 0);
+            ncount = nb < n_hits ? min(chunk, n_hits - nb) : 0u;
+            if (nb + chunk >= n_hits) exhausted = true;
         }
         bool fresh = false;
         if (!busy) {
             const uint32_t rk = __popc(im & lt);
-            if (rk < take) {
-                const Hit h = a.hits[base + rk];
+            uint32_t hidx = 0xffffffffu;
+            if (rk < avail) hidx = wcur + rk;
+            else if (rk - avail < ncount) hidx = nb + (rk - avail);
+            if (hidx != 0xffffffffu) {
+                const Hit h = load_hit(a.hits + hidx);
                 ht = h.t;
                 hq = h.q;
                 hu = h.unit;
@@ -992,8 +996,17 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
                 busy = true;
             }
         }
+        {
+            const uint32_t from_old = min(need, avail);
+            if (ncount) {
+                wcur = nb + min(need - from_old, ncount);
+                wend = nb + ncount;
+            } else {
+                wcur += from_old;
+            }
+        }
         if (!__any_sync(kFull, busy)) {
-            if (exhausted) break;
+            if (exhausted && wcur == wend) break;
             continue;
         }
 

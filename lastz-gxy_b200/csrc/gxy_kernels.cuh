@@ -91,7 +91,7 @@ struct ScreenArgs {
 };
 // Seed-hit enumeration: one warp per tile of 32 query windows; writes the
 // hits of every (window, variant) bucket to a.hits.
-void launch_enumerate(const ScreenArgs& a, int blocks, cudaStream_t st);
+void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st);
 // Capped lane-per-hit x-drop over a.hits; keeps the candidates.  grid = persistent.
 void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);
 

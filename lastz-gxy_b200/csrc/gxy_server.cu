@@ -67,6 +67,12 @@ struct gxy_server {
     uint64_t bytes_in_use = 0;
     uint64_t units_in_flight = 0;
     gxy_server_stats st{};
+    // Device free memory as last queried (cudaMemGetInfo costs tens of us):
+    // refreshed at most every 20 ms, and reduced meanwhile by what was
+    // admitted since the query.
+    size_t free_seen = 0;
+    uint64_t in_use_seen = 0;
+    std::chrono::steady_clock::time_point free_at{};
 };
 
 namespace {
@@ -168,8 +174,15 @@ void dispatcher(gxy_server* s) {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
             if (s->stop && s->pending.empty()) break;
-            size_t free_b = 0, total_b = 0;
-            cudaMemGetInfo(&free_b, &total_b);
+            const auto now = Clock::now();
+            if (s->free_at == Clock::time_point{} || now - s->free_at > std::chrono::milliseconds(20)) {
+                size_t total_b = 0;
+                cudaMemGetInfo(&s->free_seen, &total_b);
+                s->in_use_seen = s->bytes_in_use;
+                s->free_at = now;
+            }
+            const uint64_t grown = s->bytes_in_use > s->in_use_seen ? s->bytes_in_use - s->in_use_seen : 0;
+            size_t free_b = s->free_seen > grown ? s->free_seen - grown : 0;
             uint64_t batch_units = 0, batch_bases = 0;
             while (!s->pending.empty()) {
                 Request* q = s->pending.front();
