@@ -153,7 +153,7 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     if (e == cudaSuccess)
         e = w->prim_hist.ensure(((size_t)kRadixMax * std::max(w->ps.grid, w->ps.sort_grid_max) + 1) *
                                 sizeof(uint32_t));
-    if (e == cudaSuccess) e = w->counters.ensure(256);
+    if (e == cudaSuccess) e = w->counters.ensure(kCounterWords * 4);
     if (e == cudaSuccess) e = cudaMallocHost(&w->h_pinned, 1 << 16);
     if (e != cudaSuccess) {
         set_error(std::string("worker setup: ") + cudaGetErrorString(e));
@@ -272,7 +272,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         // worker's stream is idle here: every call ends synchronized).
         const size_t bu = nu * sizeof(UnitDev), bt = tsegs.size() * sizeof(SeqView),
                      bq = qsegs.size() * sizeof(SeqView);
-        const size_t off = 4096;
+        const size_t off = 32768;   // the counters come back into [0, kCounterWords * 4)
         if (off + bu + bt + bq <= W->h_pinned_bytes) {
             unsigned char* h = static_cast<unsigned char*>(W->h_pinned) + off;
             memcpy(h, ud.data(), bu);
@@ -310,11 +310,14 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     RadixPass passes[16];
     const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
 
-    // Device counters: u32 [0] tile, [1] candidates, [2] HSPs, [3] hit cursor;
-    // u64 at byte 32: [0] windows, [1] raw hits, [2] columns; u64 at byte 64: hits.
+    // Device counters (kCounterWords u32): the ones the kernels hit with
+    // atomics all the time sit 4 KB apart so that they fall in different L2
+    // slices.  u32 [kCTile] tile, [kCCand] candidates, [kCHsps] HSPs,
+    // [kCHitNext] screen hit cursor; u64 at [kCStats]: windows, raw hits,
+    // columns; u64 at [kCHits]: raw hits of the pass.
     uint32_t* cnt = W->counters.as<uint32_t>();
-    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + 8);
-    unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + 16);
+    unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + kCStats);
+    unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + kCHits);
     if (ctx->tuning.initial_candidates) W->cand_cap = ctx->tuning.initial_candidates;
     if (W->cand_cap == 0) W->cand_cap = 2u << 20;
     if (W->hit_cap == 0) W->hit_cap = 32ull << 20;
@@ -348,8 +351,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     bool single_pass_timing = false;
     bool in_capture = false;
     auto pass = [&](uint32_t t0, uint32_t t1) -> gxy_status {
-        GXY_CK(cudaMemsetAsync(cnt + 0, 0, 4, st));
-        GXY_CK(cudaMemsetAsync(cnt + 3, 0, 4, st));
+        GXY_CK(cudaMemsetAsync(cnt + kCTile, 0, 4, st));
+        GXY_CK(cudaMemsetAsync(cnt + kCHitNext, 0, 4, st));
         GXY_CK(cudaMemsetAsync(hitc, 0, 8, st));
         sa.tile_lo = t0;
         sa.tile_hi = t1;
@@ -389,9 +392,9 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(W->runit2.ensure((size_t)cap * 4));
         GXY_CK(W->perm.ensure((size_t)cap * 4));
         GXY_CK(W->perm2.ensure((size_t)cap * 4));
-        sa.tile_counter = cnt + 0;
-        sa.cand_count = cnt + 1;
-        sa.hit_next = cnt + 3;
+        sa.tile_counter = cnt + kCTile;
+        sa.cand_count = cnt + kCCand;
+        sa.hit_next = cnt + kCHitNext;
         sa.hit_count = hitc;
         sa.hits = W->hits.as<Hit>();
         sa.hit_cap = W->hit_cap;
@@ -418,29 +421,29 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         single_pass_timing = single;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t gexec = nullptr;
-        GXY_CK(cudaMemsetAsync(W->counters.p, 0, 256, st));
+        GXY_CK(cudaMemsetAsync(W->counters.p, 0, kCounterWords * 4, st));
         if (!single) {
             // Passes over window ranges, each checked for hit-buffer overflow.
             GXY_CK(cudaEventRecord(W->ev[0], st));
             for (uint32_t t0 = 0; t0 < tiles;) {
                 const uint32_t t1 = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)t0 + pass_tiles);
-                uint32_t before[24];   // counters before this pass, restored if it is redone
-                GXY_CK(cudaMemcpyAsync(before, cnt, sizeof(before), cudaMemcpyDeviceToHost, st));
+                // Counters before this pass, restored if it is redone.
+                std::vector<uint32_t> before(kCounterWords), after(kCounterWords);
+                GXY_CK(cudaMemcpyAsync(before.data(), cnt, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
                 GXY_CK(cudaStreamSynchronize(st));
                 API_TRY_ENGINE(pass(t0, t1));
-                uint32_t after[24];
-                GXY_CK(cudaMemcpyAsync(after, cnt, sizeof(after), cudaMemcpyDeviceToHost, st));
+                GXY_CK(cudaMemcpyAsync(after.data(), cnt, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
                 GXY_CK(cudaStreamSynchronize(st));
-                const unsigned long long nh = *reinterpret_cast<const unsigned long long*>(after + 16);
-                if (after[1] > cap && nh <= W->hit_cap) {
+                const unsigned long long nh = *reinterpret_cast<const unsigned long long*>(after.data() + kCHits);
+                if (after[kCCand] > cap && nh <= W->hit_cap) {
                     // Candidates overflowed in this pass: grow the candidate
                     // arrays keeping the earlier passes' entries, redo the pass.
-                    const uint64_t nc = (uint64_t)after[1] + after[1] / 2 + (1u << 20);
+                    const uint64_t nc = (uint64_t)after[kCCand] + after[kCCand] / 2 + (1u << 20);
                     if (nc >= (1ull << 31)) {
                         set_error("candidate count exceeds 2^31");
                         return GXY_EUNSUPPORTED;
                     }
-                    const size_t keep = before[1];
+                    const size_t keep = before[kCCand];
                     GXY_CK(grow_keep(W->ck0, nc * 8, keep * 8));
                     GXY_CK(grow_keep(W->cv0, nc * 4, keep * 4));
                     GXY_CK(grow_keep(W->cands, nc * sizeof(Cand), keep * sizeof(Cand)));
@@ -449,7 +452,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                     sa.cand_vals = W->cv0.as<uint32_t>();
                     sa.cands = W->cands.as<Cand>();
                     sa.cand_cap = cap;
-                    GXY_CK(cudaMemcpyAsync(cnt, before, sizeof(before), cudaMemcpyHostToDevice, st));
+                    GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
+                    GXY_CK(cudaStreamSynchronize(st));
                     continue;
                 }
                 if (nh > W->hit_cap) {
@@ -458,7 +462,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                         return GXY_ENOMEM;
                     }
                     // Undo this pass's candidates and counters; redo it over fewer tiles.
-                    GXY_CK(cudaMemcpyAsync(cnt, before, sizeof(before), cudaMemcpyHostToDevice, st));
+                    GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
+                    GXY_CK(cudaStreamSynchronize(st));
                     pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)(t1 - t0) * W->hit_cap / nh * 0.8));
                     continue;
                 }
@@ -490,13 +495,13 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                 GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
                 capture.active = true;
             }
-            GXY_CK(cudaMemsetAsync(W->counters.p, 0, 256, st));
+            GXY_CK(cudaMemsetAsync(W->counters.p, 0, kCounterWords * 4, st));
             if (!graph_now) GXY_CK(cudaEventRecord(W->ev[0], st));
             API_TRY_ENGINE(pass(0, (uint32_t)tiles));
             if (!graph_now) GXY_CK(cudaEventRecord(W->ev[1], st));
         }
         const int which = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
-                                         W->cv1.as<uint32_t>(), cnt + 1, 0, cap, passes, npass, W->ps, st);
+                                         W->cv1.as<uint32_t>(), cnt + kCCand, 0, cap, passes, npass, W->ps, st);
         const uint64_t* skeys = which ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
         const uint32_t* sidx = which ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
         GXY_CK(cudaMemsetAsync(W->flags.p, 0, cap, st));
@@ -505,7 +510,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         wa.keys = skeys;
         wa.idx = sidx;
         wa.cands = W->cands.as<Cand>();
-        wa.n_dev = cnt + 1;
+        wa.n_dev = cnt + kCCand;
         wa.n_cap = cap;
         wa.units = sa.units;
         wa.tsegs = sa.tsegs;
@@ -517,28 +522,29 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         wa.out_flag = W->flags.as<uint8_t>();
         wa.out_hsp = W->ohsp.as<Hsp>();
         launch_walk(wa, walk_warps, blocks_misc, st);
-        scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + 1, 0, cap, false, cnt + 2, W->ps, st);
+        scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCCand, 0, cap, false, cnt + kCHsps, W->ps,
+                st);
         launch_compact(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), W->ohsp.as<Hsp>(), sidx,
-                       W->cands.as<Cand>(), cnt + 1, cap, W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), blocks_misc, st);
+                       W->cands.as<Cand>(), cnt + kCCand, cap, W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), blocks_misc, st);
         Hsp* fin = W->rhsp.as<Hsp>();
         uint32_t* fin_unit = W->runit.as<uint32_t>();
         if (nu > 1) {
             // Group by unit, keeping each unit's (diagonal, t) order: stable sort.
             RadixPass up[4];
             const int nup = plan_radix(0, bits_for(nu - 1), 0, 0, up, 4);
-            launch_iota(W->perm.as<uint32_t>(), cnt + 2, cap, blocks_misc, st);
+            launch_iota(W->perm.as<uint32_t>(), cnt + kCHsps, cap, blocks_misc, st);
             GXY_CK(cudaMemcpyAsync(W->runit2.p, W->runit.p, (size_t)cap * 4, cudaMemcpyDeviceToDevice, st));
             const int w2 = radix_sort_u32(W->runit2.as<uint32_t>(), W->perm.as<uint32_t>(), W->offsets.as<uint32_t>(),
-                                          W->perm2.as<uint32_t>(), cnt + 2, 0, cap, up, nup, W->ps, st);
+                                          W->perm2.as<uint32_t>(), cnt + kCHsps, 0, cap, up, nup, W->ps, st);
             const uint32_t* perm = w2 ? W->perm2.as<uint32_t>() : W->perm.as<uint32_t>();
-            launch_gather_hsp(W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), perm, cnt + 2, cap, W->rhsp2.as<Hsp>(),
+            launch_gather_hsp(W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), perm, cnt + kCHsps, cap, W->rhsp2.as<Hsp>(),
                               W->runit2.as<uint32_t>(), blocks_misc, st);
             fin = W->rhsp2.as<Hsp>();
             fin_unit = W->runit2.as<uint32_t>();
         }
-        launch_fixup(fin, fin_unit, cnt + 2, cap, W->flags.as<uint8_t>(), blocks_misc, st);
+        launch_fixup(fin, fin_unit, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
         if (!graph_now) GXY_CK(cudaEventRecord(W->ev[2], st));
-        GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, 256, cudaMemcpyDeviceToHost, st));
+        GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
 
         if (graph_now) {
             capture.active = false;
@@ -563,9 +569,9 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(cudaGetLastError());
         GXY_CK(cudaStreamSynchronize(st));
         const uint32_t* hc = static_cast<const uint32_t*>(W->h_pinned);
-        const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + 8);
-        const unsigned long long nhits = *reinterpret_cast<const unsigned long long*>(hc + 16);
-        const uint32_t ncand = hc[1];
+        const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + kCStats);
+        const unsigned long long nhits = *reinterpret_cast<const unsigned long long*>(hc + kCHits);
+        const uint32_t ncand = hc[kCCand];
         if (single && nhits > W->hit_cap) {
             // Raw hits overflowed the hit buffer: grow it, or split into passes.
             if (nhits + nhits / 8 <= kMaxHitCap) {
@@ -588,7 +594,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             W->cand_cap = (uint32_t)nc;
             continue;
         }
-        const uint32_t nh = hc[2];
+        const uint32_t nh = hc[kCHsps];
         out.stats.windows = hs[0];
         out.stats.raw_hits = hs[1];
         out.stats.columns = hs[2];

@@ -67,6 +67,10 @@ struct UnitPlan {
     double avg_bucket;   // table positions / words: sizes the raw-hit buffer before the first pass
 };
 
+// Layout of a worker's device counters (u32 indices).
+constexpr uint32_t kCTile = 0, kCHsps = 2, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072;
+constexpr uint32_t kCounterWords = 4096;
+
 struct RunResult {
     std::vector<gxy_hsp> hsps;
     std::vector<uint32_t> unit;

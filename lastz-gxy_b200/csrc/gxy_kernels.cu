@@ -487,15 +487,22 @@ __device__ __forceinline__ void store_hit(Hit* p, uint32_t t, uint32_t q, uint32
 }
 __device__ __forceinline__ Hit load_hit(const Hit* p) { return *p; }
 
-__global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ ScreenArgs a) {
+// kRegVar: variants whose bucket bounds stay in registers between the two
+// passes (the rest are re-read): 1 without transitions, 13 for weight 12 with
+// one transition, else 16.
+template <uint32_t kRegVar>
+__global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ ScreenArgs a) {
     const int lane = threadIdx.x & 31;
     const uint32_t ntile = a.tile_hi - a.tile_lo;
     unsigned long long n_windows = 0, n_raw = 0;
+    // The next tile is claimed while the current one is processed, so the
+    // claim's round trip is off the critical path.
+    uint32_t next = 0;
+    if (lane == 0) next = atomicAdd(a.tile_counter, 1u);
     for (;;) {
-        uint32_t tile = 0;
-        if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
-        tile = __shfl_sync(kFull, tile, 0);
+        uint32_t tile = __shfl_sync(kFull, next, 0);
         if (tile >= ntile) break;
+        if (lane == 0) next = atomicAdd(a.tile_counter, 1u);
         tile += a.tile_lo;
         uint32_t lo = 0, hi = a.n_units;
         while (hi - lo > 1) {
@@ -513,7 +520,6 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
         n_windows += wv ? 1 : 0;
         // Pass 1: this lane's hit count over all variants.  The bucket
         // bounds of the first kRegVar variants stay in registers for pass 2.
-        constexpr uint32_t kRegVar = 16;
         uint32_t rb[kRegVar], rc[kRegVar];
         uint32_t tot = 0;
 #pragma unroll
@@ -543,24 +549,31 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
         if (wtot == 0) continue;
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.hit_count, (unsigned long long)wtot);
-        base = __shfl_sync(kFull, base, 0);
         n_raw += lane == 0 ? wtot : 0;
-        if (base + wtot > a.hit_cap) continue;   // overflow: the pass is redone with fewer tiles
         // Pass 2: write this lane's hits into its slots [dst, dst + tot).
         // Their order within the slots is free (candidates are sorted by a
         // unique (diagonal, t) key later), so the first position of every
-        // small bucket is loaded at once -- up to kRegVar loads in flight --
-        // before the rest.
+        // small bucket is loaded at once, before the rest; the first batch of
+        // those loads is in flight while the reservation comes back.
+        uint32_t first[8];
+#pragma unroll
+        for (uint32_t i = 0; i < 8; i++)
+            if (i < kRegVar) first[i] = (rc[i] != 0 && rc[i] <= 16) ? __ldg(U.positions + rb[i]) : 0u;
+        base = __shfl_sync(kFull, base, 0);
+        if (base + wtot > a.hit_cap) continue;   // overflow: the pass is redone with fewer tiles
         uint64_t dst = base + (incl - tot);
-        {
-            uint32_t first[kRegVar];
 #pragma unroll
-            for (uint32_t v = 0; v < kRegVar; v++)
-                first[v] = (rc[v] != 0 && rc[v] <= 16) ? __ldg(U.positions + rb[v]) : 0u;
+        for (uint32_t v0 = 0; v0 < kRegVar; v0 += 8) {
+            if (v0) {
 #pragma unroll
-            for (uint32_t v = 0; v < kRegVar; v++) {
-                if (rc[v] != 0 && rc[v] <= 16) store_hit(a.hits + dst++, first[v], q, u);
+                for (uint32_t i = 0; i < 8; i++)
+                    if (v0 + i < kRegVar)
+                        first[i] = (rc[v0 + i] != 0 && rc[v0 + i] <= 16) ? __ldg(U.positions + rb[v0 + i]) : 0u;
             }
+#pragma unroll
+            for (uint32_t i = 0; i < 8; i++)
+                if (v0 + i < kRegVar && rc[v0 + i] != 0 && rc[v0 + i] <= 16)
+                    store_hit(a.hits + dst++, first[i], q, u);
         }
         for (uint32_t v = 0; v < a.n_var; v++) {
             uint32_t b = 0, c = 0;
@@ -604,7 +617,9 @@ __global__ __launch_bounds__(256) void k_enumerate(const __grid_constant__ Scree
 
 void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st) {
     count_launch();
-    k_enumerate<<<sm_count * 8, 256, 0, st>>>(a);
+    if (a.n_var == 1) k_enumerate<1><<<sm_count * 8, 256, 0, st>>>(a);
+    else if (a.n_var == 13) k_enumerate<13><<<sm_count * 8, 256, 0, st>>>(a);
+    else k_enumerate<16><<<sm_count * 8, 256, 0, st>>>(a);
 }
 
 // ---------------------------------------------------------------------------

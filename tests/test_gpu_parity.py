@@ -114,6 +114,22 @@ def test_table_bucket_orders(gxy, ctx, pattern, step):
     assert int(np.diff(starts.astype(np.int64)).max()) > 4096
     want, _ = O.search(ot, O.pack_ascii(s), O.pack_ascii(q), orc_params(gxy.ScoringMatrix.hoxd70(), sp))
     assert as_tuples(got) == as_tuples(want) and len(want) > 0
+    # A query inside the tandem repeat: its windows hit buckets of hundreds
+    # of positions (the warp-cooperative copy in the enumeration).
+    q2 = s[43000 + 100:43000 + 400] + s[3000:3300]
+    got2 = gxy.search(tab, T, gxy.PackedSeq.from_ascii(q2), gxy.ScoringMatrix.hoxd70(), sp)
+    want2, _ = O.search(ot, O.pack_ascii(s), O.pack_ascii(q2), orc_params(gxy.ScoringMatrix.hoxd70(), sp))
+    assert as_tuples(got2) == as_tuples(want2) and len(want2) > 0
+
+
+def test_tiny_weight_tables(gxy, ctx):
+    # Weight 1 and 2 (4 and 16 words): every bucket is large.
+    rng = np.random.default_rng(5)
+    t, q = homologous_pair(rng, 3000, 0.9)
+    for pattern in ("1", "101", "11"):
+        sp = gxy.SearchParams(1, gxy.HspParams(910, 300), 0)
+        g, o = both(gxy, ctx, t, q, pattern, sp)
+        assert g == o, pattern
 
 
 def test_table_known_buckets(gxy, ctx):
