@@ -118,3 +118,35 @@ def test_chunked_batch_matches_driver_semantics(gxy, ctx, transitions, mwc):
         total += len(h)
         assert got[u].tobytes() == h.tobytes(), u
     assert total > 0
+
+
+def test_concurrent_searches_share_one_table(gxy, ctx):
+    # src/driver.rs:210-240 calls search() from rayon threads on one shared
+    # table; every concurrent call must give its sequential result.
+    import threading
+    rng = np.random.default_rng(34)
+    target = rand_ascii(rng, 150_000, b"ACGTACGTacgtN")
+    queries = make_queries(rng, target, 16, 1000, 20000)
+    T = gxy.PackedSeq.from_ascii(target)
+    tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    m, sp = gxy.ScoringMatrix.hoxd70(), gxy.SearchParams()
+    packed = [gxy.PackedSeq.from_ascii(q) for q in queries]
+    want = [gxy.search(tab, T, q, m, sp) for q in packed]
+    got = [None] * len(packed)
+    errors = []
+
+    def worker(k):
+        try:
+            for i in range(k, len(packed), 4):
+                got[i] = gxy.search(tab, T, packed[i], m, sp)
+        except Exception as e:   # surfaced below
+            errors.append(e)
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert g.tobytes() == w.tobytes(), i
+    assert sum(len(w) for w in want) > 0
