@@ -153,6 +153,27 @@ gxy_status gxy_dseq_download(const gxy_dseq* s, uint8_t* codes, uint8_t* valid, 
 uint64_t gxy_dseq_len(const gxy_dseq* s);
 gxy_status gxy_dseq_free(gxy_dseq* s);
 
+/* ---- input formats (src/sequences.rs:338-377, src/bit2.rs:73-163) -------- */
+/* Sequences parsed from a file's bytes straight into device sequences. */
+typedef struct {
+    uint64_t n;          /* sequences */
+    gxy_dseq** seqs;     /* device sequences; a caller that keeps one sets its slot to NULL */
+    char** names;        /* NUL-terminated names */
+} gxy_seq_set;
+/* parse_fasta (src/sequences.rs:338-377): records start at lines whose first
+ * byte is '>' (name = first whitespace-delimited token; an empty one is
+ * GXY_EINVAL), ASCII whitespace is skipped, bases before the first header
+ * join the first record, and each record is packed like
+ * PackedSeq::from_ascii.  Input below 4 GiB. */
+gxy_status gxy_parse_fasta(gxy_ctx* ctx, const uint8_t* bytes, uint64_t n, gxy_seq_set* out);
+/* parse_2bit (src/bit2.rs:73-163): UCSC 2bit, either byte order; N blocks
+ * become invalid bases (code 0), mask blocks soft-mask the valid ones.  Bad
+ * magic, version or a truncated file are GXY_EINVAL with the reason in
+ * gxy_last_error. */
+gxy_status gxy_parse_2bit(gxy_ctx* ctx, const uint8_t* bytes, uint64_t n, gxy_seq_set* out);
+/* Frees the names and every non-NULL device sequence of the set. */
+void gxy_seq_set_free(gxy_seq_set* set);
+
 /* ---- position table (src/pos_table.rs) --------------------------------- */
 /* PosTable::build(seq, pattern, step) followed, when max_word_count > 0, by
  * prune_hot_words(max_word_count) as the driver does (src/driver.rs:212-215).

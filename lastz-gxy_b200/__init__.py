@@ -26,7 +26,7 @@ from ._lib import GxyError, check, lib
 HSP_DTYPE = np.dtype([("t_start", "<u4"), ("q_start", "<u4"), ("length", "<u4"), ("score", "<i4")])
 
 __all__ = [
-    "GxyError", "HSP_DTYPE", "Context", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
+    "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
     "SearchParams", "PosTable", "search", "search_device", "batch_search", "chunk_target", "extend_hits",
     "Server", "build", "canonical_sort",
 ]
@@ -481,6 +481,38 @@ def batch_search(tables: Sequence[PosTable], queries: Sequence[DeviceSeq], units
         C.memmove(offs.ctypes.data, res.unit_offsets, (len(ul) + 1) * 8)
     lib().gxy_batch_result_free(C.byref(res))
     return [allh[int(offs[i]):int(offs[i + 1])] for i in range(len(ul))]
+
+
+def _take_seq_set(ctx: "Context", st: _lib.SeqSetC) -> list:
+    out = []
+    try:
+        for i in range(int(st.n)):
+            h = st.seqs[i]
+            name = st.names[i].decode()
+            n = int(lib().gxy_dseq_len(h))
+            out.append((name, DeviceSeq(ctx, C.c_void_p(h), n)))
+            st.seqs[i] = None   # ownership moves to the DeviceSeq
+    finally:
+        lib().gxy_seq_set_free(C.byref(st))
+    return out
+
+
+def parse_fasta(data: bytes, ctx: Optional[Context] = None) -> list:
+    """parse_fasta (src/sequences.rs:338-377) into device sequences: [(name, DeviceSeq)]."""
+    ctx = ctx or Context.default()
+    st = _lib.SeqSetC()
+    buf = C.create_string_buffer(bytes(data), len(data)) if len(data) else None
+    check(lib().gxy_parse_fasta(ctx.h, buf, len(data), C.byref(st)))
+    return _take_seq_set(ctx, st)
+
+
+def parse_2bit(data: bytes, ctx: Optional[Context] = None) -> list:
+    """parse_2bit (src/bit2.rs:73-163) into device sequences: [(name, DeviceSeq)]."""
+    ctx = ctx or Context.default()
+    st = _lib.SeqSetC()
+    buf = C.create_string_buffer(bytes(data), len(data)) if len(data) else None
+    check(lib().gxy_parse_2bit(ctx.h, buf, len(data), C.byref(st)))
+    return _take_seq_set(ctx, st)
 
 
 def chunk_target(target_len: int, primary_bp: int, halo_bp: int) -> list:

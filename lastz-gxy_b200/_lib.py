@@ -56,6 +56,10 @@ class StatsC(C.Structure):
                 ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reserved_", C.c_uint32)]
 
 
+class SeqSetC(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("seqs", C.POINTER(C.c_void_p)), ("names", C.POINTER(C.c_char_p))]
+
+
 class TuningC(C.Structure):
     _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
                 ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32), ("initial_candidates", C.c_uint32)]
@@ -128,6 +132,9 @@ SIGNATURES = {
     "gxy_server_wait": (C.c_int, [V, U64, U32, P(HspBufC), P(HspBufC), P(C.c_double)]),
     "gxy_server_get_stats": (C.c_int, [V, P(ServerStatsC)]),
     "gxy_server_destroy": (C.c_int, [V]),
+    "gxy_parse_fasta": (C.c_int, [V, V, U64, P(SeqSetC)]),
+    "gxy_parse_2bit": (C.c_int, [V, V, U64, P(SeqSetC)]),
+    "gxy_seq_set_free": (None, [P(SeqSetC)]),
 }
 
 _lib = None

@@ -285,3 +285,102 @@ class DiagHash:
             lib().orc_diag_free(self.h)
         except Exception:
             pass
+
+
+# ---- input formats: pure-Python restatements (small inputs only) -------------
+class InputError(ValueError):
+    """The reference's SeqError::EmptyHeader / Bit2Error variants."""
+
+
+_WS = b" \t\n\x0c\r"   # u8::is_ascii_whitespace
+
+
+def parse_fasta(data: bytes) -> list:
+    """parse_fasta (src/sequences.rs:338-377): [(name, ascii_bases)].
+
+    Lines split at LF; empty lines skipped; a line starting with '>' starts a
+    record named by its first whitespace-delimited token (none: error); every
+    other byte except ASCII whitespace is a base.  Bases before the first
+    header stay in the buffer and join the first record (:349-356)."""
+    seqs = []
+    cur_name = None
+    cur = bytearray()
+    for lineno, line in enumerate(data.split(b"\n")):
+        if not line:
+            continue
+        if line[:1] == b">":
+            if cur_name is not None:
+                seqs.append((cur_name, bytes(cur)))
+                cur = bytearray()
+            toks = line[1:].split()
+            if not toks:
+                raise InputError(f"empty header at line {lineno + 1}")
+            cur_name = toks[0].decode()
+        else:
+            cur.extend(b for b in line if b not in _WS)
+    if cur_name is not None:
+        seqs.append((cur_name, bytes(cur)))
+    return seqs
+
+
+def parse_2bit(data: bytes) -> list:
+    """parse_2bit (src/bit2.rs:73-163): [(name, ascii)] with N blocks as 'N'
+    and mask blocks lowercased (N stays N), the ASCII the reference feeds to
+    PackedSeq::from_ascii."""
+    import struct
+    if len(data) < 4:
+        raise InputError("truncated")
+    m = struct.unpack_from("<I", data, 0)[0]
+    if m == 0x1A412743:
+        e = "<"
+    elif m == 0x4327411A:
+        e = ">"
+    else:
+        raise InputError(f"bad magic 0x{m:08x}")
+
+    def u32(pos):
+        if pos + 4 > len(data):
+            raise InputError("truncated")
+        return struct.unpack_from(e + "I", data, pos)[0]
+    if u32(4) != 0:
+        raise InputError("bad version")
+    count = u32(8)
+    pos = 16
+    index = []
+    for _ in range(count):
+        if pos + 1 > len(data):
+            raise InputError("truncated")
+        ns = data[pos]
+        pos += 1
+        if pos + ns > len(data):
+            raise InputError("truncated")
+        name = data[pos:pos + ns].decode()
+        pos += ns
+        index.append((name, u32(pos)))
+        pos += 4
+    out = []
+    acgt = b"TCAG"
+    for name, off in index:
+        p = off
+        dna = u32(p); p += 4
+        blocks = []
+        for _ in range(2):
+            k = u32(p); p += 4
+            st = [u32(p + 4 * j) for j in range(k)]; p += 4 * k
+            sz = [u32(p + 4 * j) for j in range(k)]; p += 4 * k
+            blocks.append(list(zip(st, sz)))
+        p += 4
+        nb = (dna + 3) // 4
+        if p + nb > len(data):
+            raise InputError("truncated")
+        packed = data[p:p + nb]
+        asc = bytearray(acgt[(packed[i >> 2] >> (6 - (i & 3) * 2)) & 3] for i in range(dna))
+        for s, z in blocks[0]:
+            for i in range(min(s, dna), min(s + z, dna)):
+                asc[i] = ord("N")
+        for s, z in blocks[1]:
+            for i in range(min(s, dna), min(s + z, dna)):
+                if asc[i] != ord("N"):
+                    asc[i] = asc[i] | 0x20
+        out.append((name, bytes(asc)))
+    return out

@@ -190,3 +190,38 @@ def test_entropy():
     assert O.passes_entropy_gate(b, 0, 12, 1_000, 1_000) and not O.passes_entropy_gate(b, 0, 12, 999, 1_000)
     a = O.pack_ascii(b"ATATATATAT")
     assert not O.passes_entropy_gate(a, 0, 10, 1_000, 1_000) and O.passes_entropy_gate(a, 0, 10, 2_000, 1_000)
+
+
+# ---- input formats: src/sequences.rs:440-454, src/bit2.rs:321-449 -------------------
+from helpers import write_2bit  # noqa: E402
+
+
+def test_parse_fasta_blank_lines_and_case():
+    seqs = O.parse_fasta(b">a\n\nacgt\nACGT\n")                                      # sequences.rs:441-454
+    assert len(seqs) == 1 and seqs[0][0] == "a"
+    s = O.pack_ascii(seqs[0][1])
+    assert to_ascii(s) == b"ACGTACGT"
+    assert [masked(s, i) for i in range(8)] == [True] * 4 + [False] * 4
+
+
+def test_2bit_known_answers():
+    with pytest.raises(O.InputError):
+        O.parse_2bit(bytes(32))                                                        # bit2.rs:321-325
+    for be in (False, True):                                                           # :327-354
+        p = O.parse_2bit(write_2bit([("chr1", b"ACGTACGT")], big_endian=be))
+        assert p == [("chr1", b"ACGTACGT")]
+    assert O.parse_2bit(write_2bit([("chr1", b"ACGTACGTACGT")])) == [("chr1", b"ACGTACGTACGT")]   # :356-364
+    multi = [("chrA", b"ACGT"), ("chrB", b"TTTT"), ("chrC", b"GATTACACATG")]          # :366-382
+    assert O.parse_2bit(write_2bit(multi)) == multi
+    n = O.pack_ascii(O.parse_2bit(write_2bit([("chr1", b"ACGTNNNNACGT")]))[0][1])     # :384-393
+    assert to_ascii(n) == b"ACGTNNNNACGT"
+    assert not any((int(n.valid[i >> 3]) >> (i & 7)) & 1 for i in range(4, 8))
+    mk = O.pack_ascii(O.parse_2bit(write_2bit([("chr1", b"ACGTacgtACGT")]))[0][1])    # :395-412
+    assert to_ascii(mk) == b"ACGTACGTACGT"
+    assert [masked(mk, i) for i in range(12)] == [False] * 4 + [True] * 4 + [False] * 4
+    ov = O.pack_ascii(O.parse_2bit(write_2bit([("chr1", b"ACntACGT")]))[0][1])        # :414-424
+    assert not (int(ov.valid[0]) >> 2) & 1 and (int(ov.valid[0]) >> 3) & 1 and masked(ov, 3)
+    short = [("chr1", b"A"), ("chr2", b"AC"), ("chr3", b"ACG"), ("chr4", b"ACGT"), ("chr5", b"ACGTA")]
+    assert O.parse_2bit(write_2bit(short)) == short                                    # :426-439
+    with pytest.raises(O.InputError):                                                  # :441-447
+        O.parse_2bit(write_2bit([("chr1", b"ACGT")])[:-2])
