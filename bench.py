@@ -577,6 +577,57 @@ def run_chunked(args):
     return out
 
 
+def run_input(args):
+    """Input packing: one chromosome-style sequence of --length bp (default
+    100 Mbp) as FASTA (60-column lines) and as UCSC 2bit, parsed into device
+    sequences through the public API (host bytes in, device PackedSeq out,
+    copies included), against the oracle's host packing of the same bases
+    (PackedSeq::from_ascii restated in C; the reference also splits lines and
+    pushes byte by byte, so this CPU figure is a lower bound on its cost).
+    Result equality is checked on the downloaded sequences."""
+    import numpy as np
+    g = _pkg()
+    from lastz_gxy_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    L = args.length if args.length != 4_000_000 else 100_000_000
+    t0 = time.time()
+    seq = synth.c2(length=L).target.tobytes()
+    fasta = b">chr1 synthetic\n" + b"\n".join(seq[i:i + 60] for i in range(0, len(seq), 60)) + b"\n"
+    twobit = synth.to_2bit([("chr1", seq)])
+    gen_s = time.time() - t0
+    ctx = g.Context(0)
+    out = {"workload": f"input: one {L} bp chromosome-style sequence (45% soft-masked, N blocks)",
+           "fasta_bytes": len(fasta), "twobit_bytes": len(twobit), "generate_s": round(gen_s, 1)}
+    for name, fn, data in (("fasta", g.parse_fasta, fasta), ("2bit", g.parse_2bit, twobit)):
+        for _ in range(2):
+            r = fn(data, ctx)
+            del r
+        times = []
+        for _ in range(max(3, args.steps)):
+            t = time.perf_counter()
+            r = fn(data, ctx)
+            times.append(time.perf_counter() - t)
+            if len(times) < max(3, args.steps):
+                del r
+        best = statistics.median(times)
+        h = r[0][1].to_host()
+        o = O.pack_ascii(seq)
+        nb = (o.len + 3) // 4
+        same = bytes(h.codes[:nb]) == bytes(np.asarray(o.codes)[:nb]) and \
+            bytes(h.valid[:(o.len + 7) // 8]) == bytes(np.asarray(o.valid)[:(o.len + 7) // 8]) and \
+            bytes(h.mask[:(o.len + 7) // 8]) == bytes(np.asarray(o.mask)[:(o.len + 7) // 8])
+        out[name] = {"ms": round(best * 1e3, 2), "mbp_per_s": round(L / 1e6 / best, 1),
+                     "input_gb_per_s": round(len(data) / 1e9 / best, 2), "bit_identical": same}
+        del r
+    t = time.perf_counter()
+    O.pack_ascii(seq)
+    cpu = time.perf_counter() - t
+    out["cpu_pack"] = {"ms": round(cpu * 1e3, 2), "mbp_per_s": round(L / 1e6 / cpu, 1), "cores": 1,
+                       "kind": "port", "what": "oracle C PackedSeq::from_ascii of the bases (no line splitting)"}
+    return out
+
+
 def run_case(args):
     """One plus-strand search on the chromosome-style workload of --length bp
     (target and query both that long): the small case the ncu captures use."""
@@ -603,7 +654,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-bp", type=int, default=500_000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "chunked", "case"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "chunked", "case", "input"])
     ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
     ap.add_argument("--streams", type=int, default=2, help="served workload: dispatcher streams")
     ap.add_argument("--batch-units", type=int, default=64, help="served workload: units per batch at most")
@@ -630,6 +681,9 @@ def main():
         return
     if args.workload == "case":
         print(json.dumps(run_case(args)), flush=True)
+        return
+    if args.workload == "input":
+        print(json.dumps(run_input(args)), flush=True)
         return
     if world > 1:
         import datetime

@@ -501,8 +501,8 @@ def parse_fasta(data: bytes, ctx: Optional[Context] = None) -> list:
     """parse_fasta (src/sequences.rs:338-377) into device sequences: [(name, DeviceSeq)]."""
     ctx = ctx or Context.default()
     st = _lib.SeqSetC()
-    buf = C.create_string_buffer(bytes(data), len(data)) if len(data) else None
-    check(lib().gxy_parse_fasta(ctx.h, buf, len(data), C.byref(st)))
+    data = bytes(data)
+    check(lib().gxy_parse_fasta(ctx.h, C.cast(C.c_char_p(data), C.c_void_p), len(data), C.byref(st)))
     return _take_seq_set(ctx, st)
 
 
@@ -510,8 +510,8 @@ def parse_2bit(data: bytes, ctx: Optional[Context] = None) -> list:
     """parse_2bit (src/bit2.rs:73-163) into device sequences: [(name, DeviceSeq)]."""
     ctx = ctx or Context.default()
     st = _lib.SeqSetC()
-    buf = C.create_string_buffer(bytes(data), len(data)) if len(data) else None
-    check(lib().gxy_parse_2bit(ctx.h, buf, len(data), C.byref(st)))
+    data = bytes(data)
+    check(lib().gxy_parse_2bit(ctx.h, C.cast(C.c_char_p(data), C.c_void_p), len(data), C.byref(st)))
     return _take_seq_set(ctx, st)
 
 

@@ -257,3 +257,47 @@ def c5_requests(targets, n_requests: int, seed: int = 7, rate: float = 50.0, lo:
         ident = float(rng.uniform(0.60, 0.95))
         out.append(Request(t, ti, evolve(rng, targets[ti][s:s + L], ident, 0.005), ident))
     return out
+
+
+def to_2bit(seqs, big_endian: bool = False) -> bytes:
+    """A UCSC 2bit file of [(name, ascii)] (the format in src/bit2.rs:9-27):
+    N/n runs become N blocks, lowercase non-N runs mask blocks, and the packed
+    DNA holds T/C/A/G = 0/1/2/3, first base in the high bits (N as T)."""
+    import struct
+    e = ">" if big_endian else "<"
+    lut = np.zeros(256, np.uint8)
+    for ch, v in ((b"T", 0), (b"C", 1), (b"A", 2), (b"G", 3)):
+        lut[ch[0]] = v
+        lut[ch[0] | 0x20] = v
+
+    def runs(flags: np.ndarray):
+        f = np.concatenate([[False], flags, [False]]).astype(np.int8)
+        d = np.diff(f)
+        starts = np.flatnonzero(d == 1)
+        ends = np.flatnonzero(d == -1)
+        return starts, ends - starts
+
+    def arr(x):
+        return np.asarray(x, dtype=e + "u4").tobytes()
+    head = struct.pack(e + "IIII", 0x1A412743, 0, len(seqs), 0)
+    index_size = sum(1 + len(n) + 4 for n, _ in seqs)
+    body, index = [], b""
+    off = 16 + index_size
+    for name, asc in seqs:
+        a_ = np.frombuffer(bytes(asc), np.uint8)
+        up = a_ & 0xDF
+        is_n = up == ord("N")
+        is_low = (a_ >= 97) & (a_ <= 122) & ~is_n
+        ns, nz = runs(is_n)
+        ms, mz = runs(is_low)
+        rec = struct.pack(e + "II", len(a_), len(ns)) + arr(ns) + arr(nz)
+        rec += struct.pack(e + "I", len(ms)) + arr(ms) + arr(mz) + struct.pack(e + "I", 0)
+        c = lut[a_]
+        pad = (-len(c)) % 4
+        c = np.concatenate([c, np.zeros(pad, np.uint8)]).reshape(-1, 4)
+        pk = (c[:, 0] << 6) | (c[:, 1] << 4) | (c[:, 2] << 2) | c[:, 3]
+        rec += pk.astype(np.uint8).tobytes()
+        index += bytes([len(name)]) + name.encode() + struct.pack(e + "I", off)
+        body.append(rec)
+        off += len(rec)
+    return head + index + b"".join(body)

@@ -54,42 +54,8 @@ def oracle_search(target: bytes, query: bytes, pattern: str, matrix, sp, max_wor
     return h, st
 
 
-def write_2bit(seqs, big_endian: bool = False) -> bytes:
-    """A UCSC 2bit file of [(name, ascii)] (the format in src/bit2.rs:9-27):
-    N/n runs become N blocks, lowercase non-N runs mask blocks, and the packed
-    DNA holds T/C/A/G = 0/1/2/3, first base in the high bits (N as T)."""
-    import struct
-    e = ">" if big_endian else "<"
-    codes = {ord("T"): 0, ord("C"): 1, ord("A"): 2, ord("G"): 3}
 
-    def runs(flags):
-        out, start = [], None
-        for i, f in enumerate(flags + [False]):
-            if f and start is None:
-                start = i
-            elif not f and start is not None:
-                out.append((start, i - start))
-                start = None
-        return out
-    head = struct.pack(e + "IIII", 0x1A412743, 0, len(seqs), 0)
-    index_size = sum(1 + len(n) + 4 for n, _ in seqs)
-    body = b""
-    index = b""
-    off = 16 + index_size
-    for name, asc in seqs:
-        up = bytes(asc).upper()
-        nrun = runs([b == ord("N") for b in up])
-        mrun = runs([(97 <= b <= 122) and b not in (ord("n"),) for b in bytes(asc)])
-        rec = struct.pack(e + "II", len(asc), len(nrun))
-        rec += b"".join(struct.pack(e + "I", s) for s, _ in nrun) + b"".join(struct.pack(e + "I", z) for _, z in nrun)
-        rec += struct.pack(e + "I", len(mrun))
-        rec += b"".join(struct.pack(e + "I", s) for s, _ in mrun) + b"".join(struct.pack(e + "I", z) for _, z in mrun)
-        rec += struct.pack(e + "I", 0)
-        pk = bytearray((len(asc) + 3) // 4)
-        for i, b in enumerate(up):
-            pk[i >> 2] |= codes.get(b, 0) << (6 - (i & 3) * 2)
-        rec += bytes(pk)
-        index += bytes([len(name)]) + name.encode() + struct.pack(e + "I", off)
-        body += rec
-        off += len(rec)
-    return head + index + body
+def write_2bit(seqs, big_endian: bool = False) -> bytes:
+    """A UCSC 2bit file of [(name, ascii)] (lastz_gxy_b200.synth.to_2bit)."""
+    from lastz_gxy_b200 import synth
+    return synth.to_2bit(seqs, big_endian)
