@@ -495,15 +495,19 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
     const int lane = threadIdx.x & 31;
     const uint32_t ntile = a.tile_hi - a.tile_lo;
     unsigned long long n_windows = 0, n_raw = 0;
-    // The next tile is claimed while the current one is processed, so the
-    // claim's round trip is off the critical path.
+    // Tiles are claimed kClaim at a time, and the next claim is made while
+    // the current tiles are processed: one atomic per kClaim tiles (all warps
+    // hit that counter), its round trip off the critical path.
+    constexpr uint32_t kClaim = 4;
     uint32_t next = 0;
-    if (lane == 0) next = atomicAdd(a.tile_counter, 1u);
+    if (lane == 0) next = atomicAdd(a.tile_counter, kClaim);
     for (;;) {
-        uint32_t tile = __shfl_sync(kFull, next, 0);
-        if (tile >= ntile) break;
-        if (lane == 0) next = atomicAdd(a.tile_counter, 1u);
-        tile += a.tile_lo;
+      const uint32_t batch = __shfl_sync(kFull, next, 0);
+      if (batch >= ntile) break;
+      if (lane == 0) next = atomicAdd(a.tile_counter, kClaim);
+      const uint32_t batch_end = min(ntile, batch + kClaim);
+      for (uint32_t tl = batch; tl < batch_end; tl++) {
+        uint32_t tile = tl + a.tile_lo;
         uint32_t lo = 0, hi = a.n_units;
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -606,6 +610,7 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
             }
             if (big) dst += c;
         }
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n_windows += __shfl_xor_sync(kFull, n_windows, o);
