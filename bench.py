@@ -156,6 +156,20 @@ def enum_bytes(st: dict, lq: int, n_var: int) -> float:
     return 0.5 * lq + 8.0 * n_var * st["windows"] + 12.0 * st["raw_hits"]
 
 
+def table_roofline(ms_list, npos, lt: int, peak: float) -> dict:
+    """PosTable::build on the device (count, scan, bucket fill) against the
+    algorithmic bytes 0.5*Lt (codes, valid, mask read) + 4*N (positions
+    write) + 8*(4^w + 1) (starts written and read by the scan) + 4*N (count
+    atomics), N = positions; time = CUDA events around the whole build call."""
+    ms = statistics.median(ms_list)
+    n = npos if npos else lt
+    b = 0.5 * lt + 4 * n + 8 * ((1 << 24) + 1) + 4 * n
+    ach = b / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "table build (k_count_words + scan + k_fill_buckets)",
+            "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "build_ms": round(ms, 3), "algorithmic_bytes": int(b)}
+
+
 def run_ours(args, rank: int, world: int, device: int):
     import torch
     g = _pkg()
@@ -172,7 +186,11 @@ def run_ours(args, rank: int, world: int, device: int):
     flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device=f"cuda:{device}")
 
     def step_device(collect):
+        ctx.mark(2)
         tab = g.PosTable.build(dT, P12, 1, ctx=ctx)
+        ctx.mark(3)
+        if not table_npos:
+            table_npos.append(tab.total_positions())
         dQr = dQ.reverse_complement()
         for q in (dQ, dQr):
             st = {}
@@ -180,6 +198,7 @@ def run_ours(args, rank: int, world: int, device: int):
             collect.append((st, len(h)))
         dQr.free()
         tab.free()
+        table_ms.append(ctx.elapsed_ms(2, 3))   # read after the frees (which synchronise) so no extra wait
 
     def step_e2e(collect):
         tab = g.PosTable.build(T, P12, 1, ctx=ctx)          # host target -> device, PosTable::build
@@ -206,6 +225,7 @@ def run_ours(args, rank: int, world: int, device: int):
             times.append(ctx.elapsed_ms(0, 1))
         return times, col
 
+    table_ms, table_npos = [], []
     barrier = (lambda: torch.distributed.barrier()) if world > 1 else (lambda: None)
     for _ in range(args.warmup):
         step_device([])
@@ -267,6 +287,7 @@ def run_ours(args, rank: int, world: int, device: int):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                      else "fallback 6.65 TB/s",
                      "kernel_ms": round(scr_ms, 3), "algorithmic_bytes_per_launch": int(scr_bytes)},
+        "roofline_table": table_roofline(table_ms[-args.steps:], table_npos[-1], lt, peak),
         "roofline_enumerate": {"bound": "hbm", "kernel": "k_enumerate", "achieved": round(en_achieved, 1),
                                "peak": peak, "unit": "GB/s", "frac": round(en_achieved / peak, 4),
                                "kernel_ms": round(en_ms, 3), "algorithmic_bytes_per_launch": int(en_bytes),

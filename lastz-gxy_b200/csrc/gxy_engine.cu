@@ -149,7 +149,8 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
     w->ps.sort_grid_max = ctx->sm_count * 8;
-    if (e == cudaSuccess) e = w->prim_sums.ensure((w->ps.grid + 1) * sizeof(uint32_t));
+    if (e == cudaSuccess)
+        e = w->prim_sums.ensure(((size_t)std::max(w->ps.grid, w->ps.sort_grid_max) + 1) * sizeof(uint32_t));
     if (e == cudaSuccess)
         e = w->prim_hist.ensure(((size_t)kRadixMax * std::max(w->ps.grid, w->ps.sort_grid_max) + 1) *
                                 sizeof(uint32_t));

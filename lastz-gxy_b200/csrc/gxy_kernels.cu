@@ -162,10 +162,22 @@ void launch_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, 
     k_seed_words<<<blocks, 256, 0, st>>>(view, pat, step, nwin, sentinel, keys, vals, counts);
 }
 
+// Both table passes give each thread four windows at a time (stride apart,
+// so a warp's loads stay coalesced): four independent word loads, atomics and
+// stores in flight instead of one dependent chain per window.
 __global__ void k_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* counts) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nwin; k += gridDim.x * blockDim.x) {
-        uint32_t w;
-        if (word_at(view, pat, k * step, w)) atomicAdd(&counts[w], 1u);
+    const uint32_t S = gridDim.x * blockDim.x;
+    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nwin; k0 += 4 * S) {
+        uint32_t w[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint32_t k = k0 + u * S;
+            ok[u] = k < nwin && word_at(view, pat, k * step, w[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (ok[u]) atomicAdd(&counts[w[u]], 1u);
     }
 }
 
@@ -179,13 +191,25 @@ void launch_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin,
 
 __global__ void k_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, const uint32_t* starts,
                                uint32_t* fill, uint32_t* positions) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nwin; k += gridDim.x * blockDim.x) {
-        uint32_t w;
-        const uint32_t p = k * step;
-        if (word_at(view, pat, p, w)) {
-            const uint32_t r = atomicSub(&fill[w], 1u) - 1u;
-            positions[starts[w] + r] = p;
+    const uint32_t S = gridDim.x * blockDim.x;
+    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nwin; k0 += 4 * S) {
+        uint32_t w[4], r[4], b[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint32_t k = k0 + u * S;
+            ok[u] = k < nwin && word_at(view, pat, k * step, w[u]);
         }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (ok[u]) {
+                r[u] = atomicSub(&fill[w[u]], 1u) - 1u;
+                b[u] = __ldg(starts + w[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (ok[u]) positions[b[u] + r[u]] = (k0 + u * S) * step;
     }
 }
 

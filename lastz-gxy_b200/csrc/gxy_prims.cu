@@ -62,7 +62,18 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_reduce(const T* in, const
     uint64_t beg, end;
     block_range(n, (uint64_t)kScanThreads * kScanItems, beg, end);
     uint32_t s = 0;
-    for (uint64_t i = beg + threadIdx.x; i < end; i += kScanThreads) s += (uint32_t)in[i];
+    if (sizeof(T) == 4 && (reinterpret_cast<uintptr_t>(in) & 15u) == 0) {
+        // 16-byte loads: the block's range starts on a tile (4096 items) boundary.
+        const uint64_t nv = (end - beg) / 4;
+        const uint4* v4 = reinterpret_cast<const uint4*>(in + beg);
+        for (uint64_t i = threadIdx.x; i < nv; i += kScanThreads) {
+            const uint4 x = v4[i];
+            s += x.x + x.y + x.z + x.w;
+        }
+        for (uint64_t i = beg + nv * 4 + threadIdx.x; i < end; i += kScanThreads) s += (uint32_t)in[i];
+    } else {
+        for (uint64_t i = beg + threadIdx.x; i < end; i += kScanThreads) s += (uint32_t)in[i];
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
     __shared__ uint32_t s_w[kScanThreads / 32];
@@ -168,21 +179,45 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_total;
     uint32_t carry = block_sums[blockIdx.x];
+    static_assert(kScanItems == 8, "the 16-byte path moves 8 items per thread");
+    const bool vec = sizeof(T) == 4 && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
     for (uint64_t base = beg; base < end; base += (uint64_t)kScanThreads * kScanItems) {
-        // Each thread takes kScanItems consecutive items.
+        // Each thread takes kScanItems consecutive items (two 16-byte loads
+        // and stores when aligned and whole).
         const uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
+        const bool whole = vec && i0 + kScanItems <= end;
         uint32_t v[kScanItems];
         uint32_t s = 0;
+        if (whole) {
+            const uint4 x = *reinterpret_cast<const uint4*>(in + i0);
+            const uint4 y = *reinterpret_cast<const uint4*>(in + i0 + 4);
+            v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+            v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
 #pragma unroll
-        for (int k = 0; k < kScanItems; k++) {
-            v[k] = (i0 + k < end) ? (uint32_t)in[i0 + k] : 0u;
-            s += v[k];
+            for (int k = 0; k < kScanItems; k++) s += v[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < kScanItems; k++) {
+                v[k] = (i0 + k < end) ? (uint32_t)in[i0 + k] : 0u;
+                s += v[k];
+            }
         }
         uint32_t ex = block_excl_scan<kScanThreads>(s, s_warp, &s_total) + carry;
+        if (whole) {
+            uint32_t o[kScanItems];
 #pragma unroll
-        for (int k = 0; k < kScanItems; k++) {
-            if (i0 + k < end) out[i0 + k] = ex;
-            ex += v[k];
+            for (int k = 0; k < kScanItems; k++) {
+                o[k] = ex;
+                ex += v[k];
+            }
+            *reinterpret_cast<uint4*>(out + i0) = make_uint4(o[0], o[1], o[2], o[3]);
+            *reinterpret_cast<uint4*>(out + i0 + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kScanItems; k++) {
+                if (i0 + k < end) out[i0 + k] = ex;
+                ex += v[k];
+            }
         }
         carry += s_total;
     }
@@ -196,13 +231,19 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_
 template <typename T>
 void scan_impl(const T* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
                bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
+    // Blocks: enough for every block to own about two tiles at capacity, up
+    // to the larger of the scratch's two grids (its block_sums hold that many).
+    const uint64_t tile = (uint64_t)kScanThreads * kScanItems;
+    const int cap_grid = std::max(ps.grid, ps.sort_grid_max);
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n_cap + 2 * tile - 1) / (2 * tile),
+                                                                 (uint64_t)cap_grid));
     count_launch();
-    k_scan_reduce<T><<<ps.grid, kScanThreads, 0, st>>>(in, n_dev, n_host, n_cap, ps.block_sums);
+    k_scan_reduce<T><<<grid, kScanThreads, 0, st>>>(in, n_dev, n_host, n_cap, ps.block_sums);
     count_launch();
-    k_scan_small<<<1, 1024, 0, st>>>(ps.block_sums, ps.grid);
+    k_scan_small<<<1, 1024, 0, st>>>(ps.block_sums, grid);
     count_launch();
-    k_scan_down<T><<<ps.grid, kScanThreads, 0, st>>>(in, out, n_dev, n_host, n_cap, ps.block_sums,
-                                                      write_total_at_n ? 1 : 0, total);
+    k_scan_down<T><<<grid, kScanThreads, 0, st>>>(in, out, n_dev, n_host, n_cap, ps.block_sums,
+                                                   write_total_at_n ? 1 : 0, total);
 }
 
 // ---------------------------------------------------------------------------

@@ -23,9 +23,9 @@ constexpr int kRadixMax = 256;
 
 // Scratch a caller provides for the primitives (device memory).
 struct PrimScratch {
-    uint32_t* block_sums;   // >= grid entries (+1)
+    uint32_t* block_sums;   // >= max(grid, sort_grid_max) entries (+1)
     uint32_t* hist;         // >= kRadixMax * max(grid, sort_grid_max) entries (+1)
-    int grid;               // blocks of every scan launch
+    int grid;               // scan blocks (at most max(grid, sort_grid_max), sized by the capacity)
     int sort_grid_max;      // radix passes use min(this, one block per two tiles of n_cap) blocks
 };
 
