@@ -281,6 +281,20 @@ gxy_status gxy_extend_hits(gxy_ctx* ctx, const gxy_dseq* target, const gxy_dseq*
                            const uint32_t* q_pos, uint32_t seed_len, uint32_t mode,
                            gxy_hsp* out, uint8_t* ok);
 
+/* ---- consumers of the HSP list (src/anchor.rs, src/chain.rs) ------------- */
+/* choose_anchor (src/anchor.rs:25-69) for n HSPs of (target, query) on the
+ * device: t_pos[i], q_pos[i] = the midpoint of the highest-scoring window of
+ * min(max(window, 1), length) columns along HSP i (first window on ties).
+ * Scores from params->sub / ambig.  Empty or out-of-range HSPs: GXY_EINVAL. */
+gxy_status gxy_choose_anchors(gxy_ctx* ctx, const gxy_dseq* target, const gxy_dseq* query,
+                              const gxy_search_params* params, const gxy_hsp* hsps, uint64_t n, uint32_t window,
+                              uint32_t* t_pos, uint32_t* q_pos);
+/* best_chain (src/chain.rs:19-69): the highest-scoring chain of HSPs that is
+ * strictly increasing on both axes, in t_start order, with the reference's
+ * tie rules; out holds up to n HSPs, *out_n receives the chain length.  Host
+ * code, O(n log n) (the reference scans O(n^2)); empty HSPs: GXY_EINVAL. */
+gxy_status gxy_best_chain(const gxy_hsp* hsps, uint64_t n, gxy_hsp* out, uint64_t* out_n);
+
 /* ---- serving loop ---------------------------------------------------------- */
 /* Keeps the given tables resident, admits submitted queries while device
  * memory is below max_device_bytes and in-flight units below max_units, and

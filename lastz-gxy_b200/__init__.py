@@ -26,7 +26,7 @@ from ._lib import GxyError, check, lib
 HSP_DTYPE = np.dtype([("t_start", "<u4"), ("q_start", "<u4"), ("length", "<u4"), ("score", "<i4")])
 
 __all__ = [
-    "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
+    "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "choose_anchors", "best_chain", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
     "SearchParams", "PosTable", "search", "search_device", "batch_search", "chunk_target", "extend_hits",
     "Server", "build", "canonical_sort",
 ]
@@ -513,6 +513,30 @@ def parse_2bit(data: bytes, ctx: Optional[Context] = None) -> list:
     data = bytes(data)
     check(lib().gxy_parse_2bit(ctx.h, C.cast(C.c_char_p(data), C.c_void_p), len(data), C.byref(st)))
     return _take_seq_set(ctx, st)
+
+
+def choose_anchors(target: DeviceSeq, query: DeviceSeq, hsps: np.ndarray, matrix: ScoringMatrix,
+                   window: int, ctx: Optional[Context] = None) -> np.ndarray:
+    """choose_anchor (src/anchor.rs:25-69) for every HSP: an (n, 2) array of (t_pos, q_pos)."""
+    ctx = ctx or target.ctx
+    h = np.ascontiguousarray(np.asarray(hsps, HSP_DTYPE))
+    n = len(h)
+    t = np.zeros(n, np.uint32)
+    q = np.zeros(n, np.uint32)
+    p = _params_c(matrix, SearchParams())
+    check(lib().gxy_choose_anchors(ctx.h, target.h, query.h, C.byref(p), h.ctypes.data if n else None, n,
+                                   int(window), t.ctypes.data if n else None, q.ctypes.data if n else None))
+    return np.stack([t, q], axis=1)
+
+
+def best_chain(hsps: np.ndarray) -> np.ndarray:
+    """best_chain (src/chain.rs:19-69): the highest-scoring monotone chain, in t_start order."""
+    h = np.ascontiguousarray(np.asarray(hsps, HSP_DTYPE))
+    out = np.empty(len(h), HSP_DTYPE)
+    n = C.c_uint64()
+    check(lib().gxy_best_chain(h.ctypes.data if len(h) else None, len(h),
+                               out.ctypes.data if len(h) else None, C.byref(n)))
+    return out[:n.value].copy()
 
 
 def chunk_target(target_len: int, primary_bp: int, halo_bp: int) -> list:

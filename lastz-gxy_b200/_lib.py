@@ -132,6 +132,8 @@ SIGNATURES = {
     "gxy_server_wait": (C.c_int, [V, U64, U32, P(HspBufC), P(HspBufC), P(C.c_double)]),
     "gxy_server_get_stats": (C.c_int, [V, P(ServerStatsC)]),
     "gxy_server_destroy": (C.c_int, [V]),
+    "gxy_choose_anchors": (C.c_int, [V, V, V, P(SearchParamsC), V, U64, U32, V, V]),
+    "gxy_best_chain": (C.c_int, [V, U64, V, P(C.c_uint64)]),
     "gxy_parse_fasta": (C.c_int, [V, V, U64, P(SeqSetC)]),
     "gxy_parse_2bit": (C.c_int, [V, V, U64, P(SeqSetC)]),
     "gxy_seq_set_free": (None, [P(SeqSetC)]),

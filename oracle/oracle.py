@@ -384,3 +384,62 @@ def parse_2bit(data: bytes) -> list:
                     asc[i] = asc[i] | 0x20
         out.append((name, bytes(asc)))
     return out
+
+
+# ---- HSP consumers: pure-Python restatements ---------------------------------
+def choose_anchor(hsp, t: Seq, q: Seq, sub, ambig: int, window: int):
+    """choose_anchor (src/anchor.rs:25-69): (t_pos, q_pos) of the midpoint of
+    the first highest-scoring window of clamp(window, 1, length) columns."""
+    t0, q0, length = int(hsp[0]), int(hsp[1]), int(hsp[2])
+    assert length >= 1
+    w = min(max(window, 1), length)
+
+    def col(k):
+        ti, qi = t0 + k, q0 + k
+        tv = (int(t.valid[ti >> 3]) >> (ti & 7)) & 1
+        qv = (int(q.valid[qi >> 3]) >> (qi & 7)) & 1
+        if not (tv and qv):
+            return ambig
+        tc = (int(t.codes[ti >> 2]) >> ((ti & 3) * 2)) & 3
+        qc = (int(q.codes[qi >> 2]) >> ((qi & 3) * 2)) & 3
+        return sub[tc][qc]
+    cols = [col(k) for k in range(length)]
+    best_start, best = 0, sum(cols[:w])
+    cur = best
+    for start in range(1, length - w + 1):
+        cur = cur - cols[start - 1] + cols[start + w - 1]
+        if cur > best:
+            best, best_start = cur, start
+    mid = best_start + w // 2
+    return t0 + mid, q0 + mid
+
+
+def best_chain(hsps) -> list:
+    """best_chain (src/chain.rs:19-69), the reference's O(n^2) form: a list of
+    (t_start, q_start, length, score) tuples in chain order."""
+    hs = [tuple(int(x) for x in h) for h in hsps]
+    if not hs:
+        return []
+    srt = sorted(hs, key=lambda h: (h[0], h[1]))   # stable
+    n = len(srt)
+    best = [h[3] for h in srt]
+    parent = [-1] * n
+    for i in range(1, n):
+        bp, bi = 0, -1
+        ti, qi = srt[i][0], srt[i][1]
+        for j in range(i):
+            hj = srt[j]
+            if hj[0] + hj[2] <= ti and hj[1] + hj[2] <= qi and best[j] > bp:
+                bp, bi = best[j], j
+        best[i] = bp + srt[i][3]
+        parent[i] = bi
+    end = 0
+    for i in range(n):
+        if best[i] > best[end]:
+            end = i
+    out = []
+    c = end
+    while c >= 0:
+        out.append(srt[c])
+        c = parent[c]
+    return out[::-1]

@@ -4,6 +4,7 @@ import ctypes as C
 import os
 import re
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -97,3 +98,21 @@ def test_shard_units_partition():
         assert sorted(sum(parts, [])) == list(range(50))
         parts = [shard_units(50, r, world) for r in range(world)]
         assert sorted(sum(parts, [])) == list(range(50))
+
+
+def test_best_chain_matches_quadratic_reference(gxy):
+    # gxy_best_chain (host code, O(n log n)) against the reference's O(n^2)
+    # scan restated in the oracle: random HSP sets on a small grid so that
+    # equal starts, equal ends, equal scores and equal chain totals are common.
+    import oracle as O
+    rng = np.random.default_rng(17)
+    for trial in range(300):
+        n = int(rng.integers(0, 60))
+        span = int(rng.integers(5, 200))
+        h = np.zeros(n, gxy.HSP_DTYPE)
+        h["t_start"] = rng.integers(0, span, n)
+        h["q_start"] = rng.integers(0, span, n)
+        h["length"] = rng.integers(1, 12, n)
+        h["score"] = rng.choice([100, 200, 300, -50, 0], n) if trial % 3 else rng.integers(-100, 1000, n)
+        got = [tuple(int(x) for x in r) for r in gxy.best_chain(h)]
+        assert got == O.best_chain(h), trial

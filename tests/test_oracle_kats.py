@@ -225,3 +225,31 @@ def test_2bit_known_answers():
     assert O.parse_2bit(write_2bit(short)) == short                                    # :426-439
     with pytest.raises(O.InputError):                                                  # :441-447
         O.parse_2bit(write_2bit([("chr1", b"ACGT")])[:-2])
+
+
+# ---- HSP consumers: src/chain.rs:78-138, src/anchor.rs:79-126 --------------------------
+def test_best_chain_known_answers():
+    h = lambda t, q, l, s: (t, q, l, s)  # noqa: E731
+    assert O.best_chain([]) == []                                                         # chain.rs:79-82
+    assert O.best_chain([h(10, 20, 30, 1000)]) == [h(10, 20, 30, 1000)]                   # :84-88
+    a, b, c = h(0, 0, 20, 500), h(40, 40, 20, 500), h(80, 10, 20, 700)                    # :90-105
+    assert O.best_chain([a, b, c]) == [a, b]
+    a, b, c, d = h(0, 0, 10, 100), h(20, 20, 10, 100), h(40, 40, 10, 100), h(60, 60, 10, 500)
+    assert O.best_chain([a, b, c, d]) == [a, b, c, d]                                     # :107-117
+    a, b = h(0, 50, 10, 1000), h(20, 0, 10, 800)                                          # :119-128
+    assert O.best_chain([a, b]) == [a]
+    a, b = h(10, 10, 5, 100), h(0, 0, 5, 100)                                             # :130-137
+    assert O.best_chain([a, b]) == [b, a]
+
+
+def test_choose_anchor_known_answers():
+    sub = [row[:] for row in HOXD70_ROWS]
+    s = O.pack_ascii(b"ACGTACGTACGTACGT")                                                 # anchor.rs:79-88
+    assert O.choose_anchor((0, 0, 16, 0), s, s, sub, -100, 4) == (2, 2)
+    t, q = O.pack_ascii(b"AACCCCAA"), O.pack_ascii(b"TTCCCCTT")                           # :90-102
+    assert O.choose_anchor((0, 0, 8, 0), t, q, sub, -100, 4) == (4, 4)
+    a = O.pack_ascii(b"ACGT")                                                             # :104-110
+    assert O.choose_anchor((0, 0, 4, 0), a, a, sub, -100, 1000)[0] == 2
+
+
+HOXD70_ROWS = [[91, -114, -31, -123], [-114, 100, -125, -31], [-31, -125, 100, -114], [-123, -31, -114, 91]]
