@@ -168,8 +168,9 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
     e = cudaMemsetAsync(counts, 0, (nw + 1) * 4, st);
     const SeqView view = view_of(seq, lo, hi);
     launch_count_words(view, pat, step, nwin, counts, st);
-    scan_u32(counts, t->starts, nullptr, nw, nw, true, nullptr, W->ps, st);
-    launch_fill_buckets(view, pat, step, nwin, t->starts, counts, t->positions, st);
+    // The scan also leaves a copy of starts in counts: the fill's cursors.
+    scan_u32(counts, t->starts, nullptr, nw, nw, true, nullptr, W->ps, st, counts);
+    launch_fill_buckets(view, pat, step, nwin, counts, t->positions, st);
     uint32_t* total_h = static_cast<uint32_t*>(W->h_pinned);
     if (e == cudaSuccess) e = cudaMemcpyAsync(total_h, t->starts + nw, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

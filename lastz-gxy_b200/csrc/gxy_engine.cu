@@ -522,6 +522,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         wa.entropy_thr = p.entropy_thr;
         wa.out_flag = W->flags.as<uint8_t>();
         wa.out_hsp = W->ohsp.as<Hsp>();
+        wa.chunk_next = cnt + kCWalk;
+        GXY_CK(cudaMemsetAsync(cnt + kCWalk, 0, 4, st));
         launch_walk(wa, walk_warps, blocks_misc, st);
         scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCCand, 0, cap, false, cnt + kCHsps, W->ps,
                 st);

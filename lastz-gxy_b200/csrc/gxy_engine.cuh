@@ -68,7 +68,8 @@ struct UnitPlan {
 };
 
 // Layout of a worker's device counters (u32 indices).
-constexpr uint32_t kCTile = 0, kCHsps = 2, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072;
+constexpr uint32_t kCTile = 0, kCHsps = 2, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072,
+                   kCWalk = 3584;
 constexpr uint32_t kCounterWords = 4096;
 
 struct RunResult {

@@ -189,11 +189,11 @@ void launch_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin,
     k_count_words<<<blocks, 256, 0, st>>>(view, pat, step, nwin, counts);
 }
 
-__global__ void k_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, const uint32_t* starts,
-                               uint32_t* fill, uint32_t* positions) {
+__global__ void k_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* cursor,
+                               uint32_t* positions) {
     const uint32_t S = gridDim.x * blockDim.x;
     for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nwin; k0 += 4 * S) {
-        uint32_t w[4], r[4], b[4];
+        uint32_t w[4], slot[4];
         bool ok[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
@@ -201,24 +201,20 @@ __global__ void k_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_
             ok[u] = k < nwin && word_at(view, pat, k * step, w[u]);
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            if (ok[u]) {
-                r[u] = atomicSub(&fill[w[u]], 1u) - 1u;
-                b[u] = __ldg(starts + w[u]);
-            }
-        }
+        for (int u = 0; u < 4; u++)
+            if (ok[u]) slot[u] = atomicAdd(&cursor[w[u]], 1u);
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (ok[u]) positions[b[u] + r[u]] = (k0 + u * S) * step;
+            if (ok[u]) positions[slot[u]] = (k0 + u * S) * step;
     }
 }
 
-void launch_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, const uint32_t* starts,
-                         uint32_t* fill, uint32_t* positions, cudaStream_t st) {
+void launch_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* cursor,
+                         uint32_t* positions, cudaStream_t st) {
     if (!nwin) return;
     const int blocks = (int)umin64((nwin + 255) / 256, 148 * 16);
     count_launch();
-    k_fill_buckets<<<blocks, 256, 0, st>>>(view, pat, step, nwin, starts, fill, positions);
+    k_fill_buckets<<<blocks, 256, 0, st>>>(view, pat, step, nwin, cursor, positions);
 }
 
 __global__ void k_sort_small_buckets(const uint32_t* starts, uint64_t nw, uint32_t* pos, uint32_t* big,
@@ -1267,9 +1263,14 @@ __global__ __launch_bounds__(WARPS * 32) void k_walk(const __grid_constant__ Wal
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = min(*a.n_dev, a.n_cap);
-    const uint32_t gw = blockIdx.x * WARPS + w, nwarps = gridDim.x * WARPS;
     const uint32_t L = a.seed_len;
-    for (uint32_t r = gw; (uint64_t)r * 32 < n; r += nwarps) {
+    // Chunks of 32 sorted positions are claimed dynamically: a segment with
+    // long candidates (full re-extension) can take far longer than the rest.
+    for (;;) {
+        uint32_t r = 0;
+        if (lane == 0) r = atomicAdd(a.chunk_next, 1u);
+        r = __shfl_sync(kFull, r, 0);
+        if ((uint64_t)r * 32 >= n) break;
         const uint32_t i = r * 32 + lane;
         bool head = false;
         if (i < n) head = (i == 0) || ((a.keys[i] >> 32) != (a.keys[i - 1] >> 32));

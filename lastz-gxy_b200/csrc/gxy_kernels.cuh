@@ -34,11 +34,12 @@ void launch_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, 
 // counts[word]++ for every seedable window k*step of the view.
 void launch_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* counts,
                         cudaStream_t st);
-// Fills each bucket: positions[starts[w] + --fill[w]] = p for every seedable
-// window p (fill = the counts, left all zero).  The order of positions within
-// a bucket is arbitrary; launch_sort_buckets puts it in ascending order.
-void launch_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, const uint32_t* starts,
-                         uint32_t* fill, uint32_t* positions, cudaStream_t st);
+// Fills each bucket: positions[cursor[w]++] = p for every seedable window p
+// (cursor = a copy of starts, left at the bucket ends).  The order of
+// positions within a bucket is arbitrary; launch_sort_*_buckets puts it in
+// ascending order.
+void launch_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* cursor,
+                         uint32_t* positions, cudaStream_t st);
 // Sorts every bucket of at most 16 positions in place (one thread each) and
 // lists the larger ones as (first, size) pairs in big[0 .. 2 * *n_big)
 // (entries past big_cap are dropped; *n_big still counts them).
@@ -110,6 +111,7 @@ struct WalkArgs {
     int32_t entropy_thr;
     uint8_t* out_flag;         // per sorted position: 1 = emitted and kept
     Hsp* out_hsp;              // per sorted position
+    uint32_t* chunk_next;      // work counter: chunks of 32 sorted positions (zeroed by the caller)
 };
 // Diagonal suppression (src/diag_hash.rs:34-53 as used at
 // src/seed_search.rs:318-342) over the candidates sorted by (diagonal, t),

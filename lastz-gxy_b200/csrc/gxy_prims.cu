@@ -172,7 +172,8 @@ template <typename T>
 __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_t* out, const uint32_t* n_dev,
                                                              uint64_t n_host, uint64_t n_cap,
                                                              const uint32_t* block_sums,
-                                                             int write_total_at_n, uint32_t* total) {
+                                                             int write_total_at_n, uint32_t* total,
+                                                             uint32_t* out2) {
     const uint64_t n = read_n(n_dev, n_host, n_cap);
     uint64_t beg, end;
     block_range(n, (uint64_t)kScanThreads * kScanItems, beg, end);
@@ -180,7 +181,9 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_
     __shared__ uint32_t s_total;
     uint32_t carry = block_sums[blockIdx.x];
     static_assert(kScanItems == 8, "the 16-byte path moves 8 items per thread");
-    const bool vec = sizeof(T) == 4 && ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0;
+    const bool vec = sizeof(T) == 4 &&
+                     ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out) |
+                       reinterpret_cast<uintptr_t>(out2)) & 15u) == 0;
     for (uint64_t base = beg; base < end; base += (uint64_t)kScanThreads * kScanItems) {
         // Each thread takes kScanItems consecutive items (two 16-byte loads
         // and stores when aligned and whole).
@@ -212,10 +215,17 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_
             }
             *reinterpret_cast<uint4*>(out + i0) = make_uint4(o[0], o[1], o[2], o[3]);
             *reinterpret_cast<uint4*>(out + i0 + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+            if (out2) {
+                *reinterpret_cast<uint4*>(out2 + i0) = make_uint4(o[0], o[1], o[2], o[3]);
+                *reinterpret_cast<uint4*>(out2 + i0 + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+            }
         } else {
 #pragma unroll
             for (int k = 0; k < kScanItems; k++) {
-                if (i0 + k < end) out[i0 + k] = ex;
+                if (i0 + k < end) {
+                    out[i0 + k] = ex;
+                    if (out2) out2[i0 + k] = ex;
+                }
                 ex += v[k];
             }
         }
@@ -230,7 +240,8 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_down(const T* in, uint32_
 
 template <typename T>
 void scan_impl(const T* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
-               bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
+               bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st,
+               uint32_t* out2 = nullptr) {
     // Blocks: enough for every block to own about two tiles at capacity, up
     // to the larger of the scratch's two grids (its block_sums hold that many).
     const uint64_t tile = (uint64_t)kScanThreads * kScanItems;
@@ -243,7 +254,7 @@ void scan_impl(const T* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_hos
     k_scan_small<<<1, 1024, 0, st>>>(ps.block_sums, grid);
     count_launch();
     k_scan_down<T><<<grid, kScanThreads, 0, st>>>(in, out, n_dev, n_host, n_cap, ps.block_sums,
-                                                   write_total_at_n ? 1 : 0, total);
+                                                   write_total_at_n ? 1 : 0, total, out2);
 }
 
 // ---------------------------------------------------------------------------
@@ -407,8 +418,8 @@ void prims_init() {
 }
 
 void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
-              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {
-    scan_impl<uint32_t>(in, out, n_dev, n_host, n_cap, write_total_at_n, total, ps, st);
+              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st, uint32_t* out2) {
+    scan_impl<uint32_t>(in, out, n_dev, n_host, n_cap, write_total_at_n, total, ps, st, out2);
 }
 void scan_u8(const uint8_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st) {

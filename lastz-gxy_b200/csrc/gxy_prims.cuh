@@ -32,8 +32,10 @@ struct PrimScratch {
 // Exclusive scan of n u32 (or u8) values into out[0..n); out[n] and *total
 // (either may be null) receive the sum.  n is min(*n_dev, n_cap) when n_dev is
 // not null, else n_host.  The sum must fit in u32.
+// out2 (optional) receives a second copy of out[0..n); it may be `in` itself.
 void scan_u32(const uint32_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
-              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st);
+              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st,
+              uint32_t* out2 = nullptr);
 void scan_u8(const uint8_t* in, uint32_t* out, const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
              bool write_total_at_n, uint32_t* total, const PrimScratch& ps, cudaStream_t st);
 
