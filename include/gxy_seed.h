@@ -266,6 +266,46 @@ gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* co
                             gxy_batch_result* out, gxy_stats* stats);
 void gxy_batch_result_free(gxy_batch_result* r);
 
+/* ---- driver records: the batch's HSPs as the driver's ungapped records ---- */
+/* gxy_batch_search plus the driver's post-processing on the device
+ * (build_ungapped_record src/driver.rs:437-468; grouping, sort and dedup
+ * :370-391): every HSP of unit i becomes a record of group places[i].group
+ * with t_start + places[i].t_offset (the chunk's global start); records are
+ * ordered by (group, t_start, q_start, span) and repeats of those four fields
+ * are dropped, keeping the first (lowest unit).  Groups stand for the
+ * driver's (target, query, strand) triples in its output order; one group
+ * may collect the units of every chunk of its target (their primary regions
+ * are disjoint, so the order across chunks is the reference's chunk order).
+ * Records carry coordinates, span and score; names, lengths and the ASCII
+ * bases are the caller's, by group and coordinates. */
+typedef struct {
+    uint32_t group;      /* < 2^32 - 1 */
+    uint32_t t_offset;   /* added to t_start; t_offset + target length <= 2^32 */
+} gxy_unit_place;
+
+typedef struct {
+    uint32_t group;
+    uint32_t t_start;    /* global target coordinate */
+    uint32_t q_start;
+    uint32_t span;       /* t_span = q_span = the HSP length */
+    int32_t score;
+    uint32_t unit;       /* the unit that produced it */
+} gxy_record;
+
+typedef struct {
+    gxy_record* records;       /* group-major, each group by (t_start, q_start, span) */
+    uint64_t* group_offsets;   /* n_groups + 1 (n_groups = 1 + the largest group named) */
+    uint64_t n_records;
+    uint32_t n_groups;
+} gxy_record_result;
+
+gxy_status gxy_batch_records(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,
+                             uint32_t n_queries, const gxy_dseq* const* queries,
+                             uint32_t n_units, const gxy_unit* units, const gxy_unit_place* places,
+                             const gxy_search_params* params, const gxy_batch_opts* opts,
+                             gxy_record_result* out, gxy_stats* stats);
+void gxy_record_result_free(gxy_record_result* r);
+
 /* chunk_target (src/driver.rs:156-194): writes up to cap chunks as
  * (chunk_lo, chunk_hi, primary_lo_local, primary_hi_local) quadruples and
  * returns the count in *n (always set, even when cap is too small). */

@@ -24,10 +24,13 @@ from . import _lib
 from ._lib import GxyError, check, lib
 
 HSP_DTYPE = np.dtype([("t_start", "<u4"), ("q_start", "<u4"), ("length", "<u4"), ("score", "<i4")])
+RECORD_DTYPE = np.dtype([("group", "<u4"), ("t_start", "<u4"), ("q_start", "<u4"), ("span", "<u4"),
+                         ("score", "<i4"), ("unit", "<u4")])
 
 __all__ = [
     "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "choose_anchors", "best_chain", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
-    "SearchParams", "PosTable", "search", "search_device", "batch_search", "chunk_target", "extend_hits",
+    "SearchParams", "PosTable", "search", "search_device", "batch_search", "batch_records", "RECORD_DTYPE",
+    "chunk_target", "extend_hits",
     "Server", "build", "canonical_sort",
 ]
 
@@ -456,11 +459,7 @@ def batch_search(tables: Sequence[PosTable], queries: Sequence[DeviceSeq], units
     unit, each in canonical order."""
     ctx = ctx or tables[0].ctx
     ul = list(units)
-    uc = (_lib.UnitC * max(len(ul), 1))()
-    for i, u in enumerate(ul):
-        uc[i].table, uc[i].query, uc[i].strand = int(u[0]), int(u[1]), int(u[2])
-        if len(u) > 3:
-            uc[i].primary_lo, uc[i].primary_hi = int(u[3]), int(u[4])
+    uc = _units_c(ul)
     th = (C.c_void_p * max(len(tables), 1))(*[t.h for t in tables])
     qh = (C.c_void_p * max(len(queries), 1))(*[q.h for q in queries])
     p = _params_c(matrix, params)
@@ -481,6 +480,56 @@ def batch_search(tables: Sequence[PosTable], queries: Sequence[DeviceSeq], units
         C.memmove(offs.ctypes.data, res.unit_offsets, (len(ul) + 1) * 8)
     lib().gxy_batch_result_free(C.byref(res))
     return [allh[int(offs[i]):int(offs[i + 1])] for i in range(len(ul))]
+
+
+def _units_c(ul) -> "C.Array":
+    uc = (_lib.UnitC * max(len(ul), 1))()
+    for i, u in enumerate(ul):
+        uc[i].table, uc[i].query, uc[i].strand = int(u[0]), int(u[1]), int(u[2])
+        if len(u) > 3:
+            uc[i].primary_lo, uc[i].primary_hi = int(u[3]), int(u[4])
+    return uc
+
+
+def batch_records(tables: Sequence[PosTable], queries: Sequence[DeviceSeq], units, places, matrix: ScoringMatrix,
+                  params: SearchParams, use_graph: bool = False, stats: Optional[dict] = None,
+                  ctx: Optional[Context] = None):
+    """batch_search followed by the driver's record post-processing on the
+    device (src/driver.rs:370-391, :437-468).
+
+    units as for batch_search; places: one (group, t_offset) per unit -- the
+    output group (the driver's (target, query, strand) rank) and the chunk's
+    global start.  Returns (records, group_offsets): a RECORD_DTYPE array in
+    (group, t_start, q_start, span) order with repeats of those fields
+    dropped, and the n_groups + 1 offsets of each group in it."""
+    ctx = ctx or tables[0].ctx
+    ul = list(units)
+    pl = list(places)
+    if len(pl) != len(ul):
+        raise ValueError("one place per unit")
+    uc = _units_c(ul)
+    pc = (_lib.PlaceC * max(len(pl), 1))()
+    for i, (g, off) in enumerate(pl):
+        pc[i].group, pc[i].t_offset = int(g), int(off)
+    th = (C.c_void_p * max(len(tables), 1))(*[t.h for t in tables])
+    qh = (C.c_void_p * max(len(queries), 1))(*[q.h for q in queries])
+    p = _params_c(matrix, params)
+    opts = _lib.BatchOptsC()
+    opts.use_graph = 1 if use_graph else 0
+    res = _lib.RecordResultC()
+    st = _lib.StatsC()
+    check(lib().gxy_batch_records(ctx.h, len(tables), th, len(queries), qh, len(ul), uc, pc, C.byref(p),
+                                  C.byref(opts), C.byref(res), C.byref(st)))
+    if stats is not None:
+        stats.update(_stats(st))
+    n = int(res.n_records)
+    recs = np.empty(n, RECORD_DTYPE)
+    if n:
+        C.memmove(recs.ctypes.data, res.records, n * RECORD_DTYPE.itemsize)
+    offs = np.zeros(int(res.n_groups) + 1, np.uint64)
+    C.memmove(offs.ctypes.data, res.group_offsets, (int(res.n_groups) + 1) * 8)
+    lib().gxy_record_result_free(C.byref(res))
+    return recs, offs
 
 
 def _take_seq_set(ctx: "Context", st: _lib.SeqSetC) -> list:

@@ -75,6 +75,15 @@ class BatchResultC(C.Structure):
                 ("n_units", C.c_uint32)]
 
 
+class PlaceC(C.Structure):
+    _fields_ = [("group", C.c_uint32), ("t_offset", C.c_uint32)]
+
+
+class RecordResultC(C.Structure):
+    _fields_ = [("records", C.c_void_p), ("group_offsets", C.POINTER(C.c_uint64)), ("n_records", C.c_uint64),
+                ("n_groups", C.c_uint32)]
+
+
 class BatchOptsC(C.Structure):
     _fields_ = [("use_graph", C.c_uint32), ("reserved_", C.c_uint32 * 7)]
 
@@ -125,6 +134,9 @@ SIGNATURES = {
     "gxy_batch_search": (C.c_int, [V, U32, P(V), U32, P(V), U32, P(UnitC), P(SearchParamsC), P(BatchOptsC),
                                    P(BatchResultC), P(StatsC)]),
     "gxy_batch_result_free": (None, [P(BatchResultC)]),
+    "gxy_batch_records": (C.c_int, [V, U32, P(V), U32, P(V), U32, P(UnitC), P(PlaceC), P(SearchParamsC),
+                                    P(BatchOptsC), P(RecordResultC), P(StatsC)]),
+    "gxy_record_result_free": (None, [P(RecordResultC)]),
     "gxy_chunk_plan": (C.c_int, [U64, U32, U32, P(U64), U64, P(U64)]),
     "gxy_extend_hits": (C.c_int, [V, V, V, P(SearchParamsC), U64, V, V, U32, U32, V, V]),
     "gxy_server_create": (C.c_int, [V, U32, P(V), P(SearchParamsC), P(ServerOptsC), P(V)]),

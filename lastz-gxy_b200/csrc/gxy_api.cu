@@ -352,7 +352,8 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         cudaStreamSynchronize(w->st);
         DevBuf* bufs[] = {&w->prim_sums, &w->prim_hist, &w->counters, &w->d_units, &w->d_tsegs, &w->d_qsegs,
                           &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags, &w->offsets, &w->ohsp,
-                          &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2, &w->hits};
+                          &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2, &w->hits,
+                          &w->d_place, &w->rrec};
         for (DevBuf* b : bufs) b->release();
         dseq_destroy(w->qstage);
         dseq_destroy(w->tstage);
@@ -638,18 +639,12 @@ void gxy_hsp_buf_free(gxy_hsp_buf* buf) {
     buf->len = buf->cap = 0;
 }
 
-gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables, uint32_t n_queries,
+// The shared body of gxy_batch_search and gxy_batch_records: validates the
+// units, reverse-complements each query once per strand that needs it and
+// runs the engine (n_units > 0).
+static gxy_status batch_run(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables, uint32_t n_queries,
                             const gxy_dseq* const* queries, uint32_t n_units, const gxy_unit* units,
-                            const gxy_search_params* params, const gxy_batch_opts* opts, gxy_batch_result* out,
-                            gxy_stats* stats) {
-    if (!ctx || (!tables && n_tables) || (!queries && n_queries) || (!units && n_units) || !params || !out)
-        return GXY_EINVAL;
-    API_TRY(set_device(ctx));
-    memset(out, 0, sizeof(*out));
-    if (n_units == 0) {
-        out->unit_offsets = static_cast<uint64_t*>(calloc(1, sizeof(uint64_t)));
-        return GXY_OK;
-    }
+                            const gxy_search_params* params, const gxy_batch_opts* opts, RunResult& r) {
     const Pattern& pat = tables[units[0].table]->pat;
     uint64_t max_cols = 0;
     for (uint32_t i = 0; i < n_units; i++) {
@@ -705,8 +700,23 @@ gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* co
         plan[i].primary_hi = u.primary_hi;
         plan[i].avg_bucket = t->num_words ? (double)t->npos / (double)t->num_words : 0.0;
     }
+    return run_units(ctx, W, plan, tsegs, qsegs, pat, *params, opts && opts->use_graph, r);
+}
+
+gxy_status gxy_batch_search(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables, uint32_t n_queries,
+                            const gxy_dseq* const* queries, uint32_t n_units, const gxy_unit* units,
+                            const gxy_search_params* params, const gxy_batch_opts* opts, gxy_batch_result* out,
+                            gxy_stats* stats) {
+    if (!ctx || (!tables && n_tables) || (!queries && n_queries) || (!units && n_units) || !params || !out)
+        return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    memset(out, 0, sizeof(*out));
+    if (n_units == 0) {
+        out->unit_offsets = static_cast<uint64_t*>(calloc(1, sizeof(uint64_t)));
+        return GXY_OK;
+    }
     RunResult r;
-    API_TRY(run_units(ctx, W, plan, tsegs, qsegs, pat, *params, opts && opts->use_graph, r));
+    API_TRY(batch_run(ctx, n_tables, tables, n_queries, queries, n_units, units, params, opts, r));
     if (stats) *stats = r.stats;
     const uint64_t n = r.hsps.size();
     out->hsps = static_cast<gxy_hsp*>(malloc(std::max<uint64_t>(n, 1) * sizeof(gxy_hsp)));
@@ -728,6 +738,72 @@ void gxy_batch_result_free(gxy_batch_result* r) {
     if (!r) return;
     free(r->hsps);
     free(r->unit_offsets);
+    memset(r, 0, sizeof(*r));
+}
+
+gxy_status gxy_batch_records(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables, uint32_t n_queries,
+                             const gxy_dseq* const* queries, uint32_t n_units, const gxy_unit* units,
+                             const gxy_unit_place* places, const gxy_search_params* params,
+                             const gxy_batch_opts* opts, gxy_record_result* out, gxy_stats* stats) {
+    if (!ctx || (!tables && n_tables) || (!queries && n_queries) || (!units && n_units) || (!places && n_units) ||
+        !params || !out)
+        return GXY_EINVAL;
+    API_TRY(set_device(ctx));
+    memset(out, 0, sizeof(*out));
+    uint32_t n_groups = 0;
+    for (uint32_t i = 0; i < n_units; i++) {
+        if (units[i].table >= n_tables) {
+            set_error("unit references a missing table");
+            return GXY_EINVAL;
+        }
+        const gxy_table* t = tables[units[i].table];
+        // build_ungapped_record adds the chunk start in u32 (src/driver.rs:459).
+        if ((uint64_t)places[i].t_offset + (t->hi - t->lo) > (1ull << 32)) {
+            set_error("t_offset + target length exceeds 2^32");
+            return GXY_EINVAL;
+        }
+        if (places[i].group == UINT32_MAX) {
+            set_error("group index 2^32 - 1 is reserved");
+            return GXY_EINVAL;
+        }
+        n_groups = std::max(n_groups, places[i].group + 1);
+    }
+    out->group_offsets = static_cast<uint64_t*>(calloc((size_t)n_groups + 1, sizeof(uint64_t)));
+    if (!out->group_offsets) {
+        set_error("host allocation of the record result");
+        return GXY_ENOMEM;
+    }
+    out->n_groups = n_groups;
+    if (n_units == 0) return GXY_OK;
+    static_assert(sizeof(Place) == sizeof(gxy_unit_place), "device and ABI place layouts differ");
+    static_assert(sizeof(Record) == sizeof(gxy_record), "device and ABI record layouts differ");
+    RunResult r;
+    r.places = reinterpret_cast<const Place*>(places);
+    gxy_status e = batch_run(ctx, n_tables, tables, n_queries, queries, n_units, units, params, opts, r);
+    if (e != GXY_OK) {
+        gxy_record_result_free(out);
+        return e;
+    }
+    if (stats) *stats = r.stats;
+    const uint64_t n = r.records.size();
+    out->records = static_cast<gxy_record*>(malloc(std::max<uint64_t>(n, 1) * sizeof(gxy_record)));
+    if (!out->records) {
+        gxy_record_result_free(out);
+        set_error("host allocation of the record result");
+        return GXY_ENOMEM;
+    }
+    if (n) memcpy(out->records, r.records.data(), n * sizeof(gxy_record));
+    for (uint64_t i = 0; i < n; i++) out->group_offsets[out->records[i].group + 1]++;
+    for (uint32_t g = 0; g < n_groups; g++) out->group_offsets[g + 1] += out->group_offsets[g];
+    out->n_records = n;
+    out->n_groups = n_groups;
+    return GXY_OK;
+}
+
+void gxy_record_result_free(gxy_record_result* r) {
+    if (!r) return;
+    free(r->records);
+    free(r->group_offsets);
     memset(r, 0, sizeof(*r));
 }
 

@@ -229,6 +229,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     cudaStream_t st = W->st;
     out.hsps.clear();
     out.unit.clear();
+    out.records.clear();
     out.stats = gxy_stats{};
     const uint32_t nu = (uint32_t)units.size();
     // Key axes: every target and query segment gets a private key range.
@@ -268,26 +269,47 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     GXY_CK(W->d_units.ensure(nu * sizeof(UnitDev)));
     GXY_CK(W->d_tsegs.ensure(tsegs.size() * sizeof(SeqView)));
     GXY_CK(W->d_qsegs.ensure(qsegs.size() * sizeof(SeqView)));
+    const bool records = out.places != nullptr;
+    if (records) GXY_CK(W->d_place.ensure(nu * sizeof(Place)));
     {
         // Descriptors go through the pinned staging when they fit (the
         // worker's stream is idle here: every call ends synchronized).
         const size_t bu = nu * sizeof(UnitDev), bt = tsegs.size() * sizeof(SeqView),
-                     bq = qsegs.size() * sizeof(SeqView);
+                     bq = qsegs.size() * sizeof(SeqView), bp = records ? nu * sizeof(Place) : 0;
         const size_t off = 32768;   // the counters come back into [0, kCounterWords * 4)
-        if (off + bu + bt + bq <= W->h_pinned_bytes) {
+        if (off + bu + bt + bq + bp <= W->h_pinned_bytes) {
             unsigned char* h = static_cast<unsigned char*>(W->h_pinned) + off;
             memcpy(h, ud.data(), bu);
             memcpy(h + bu, tsegs.data(), bt);
             memcpy(h + bu + bt, qsegs.data(), bq);
+            if (bp) memcpy(h + bu + bt + bq, out.places, bp);
             GXY_CK(cudaMemcpyAsync(W->d_units.p, h, bu, cudaMemcpyHostToDevice, st));
             GXY_CK(cudaMemcpyAsync(W->d_tsegs.p, h + bu, bt, cudaMemcpyHostToDevice, st));
             GXY_CK(cudaMemcpyAsync(W->d_qsegs.p, h + bu + bt, bq, cudaMemcpyHostToDevice, st));
+            if (bp) GXY_CK(cudaMemcpyAsync(W->d_place.p, h + bu + bt + bq, bp, cudaMemcpyHostToDevice, st));
         } else {
             GXY_CK(cudaMemcpyAsync(W->d_units.p, ud.data(), bu, cudaMemcpyHostToDevice, st));
             GXY_CK(cudaMemcpyAsync(W->d_tsegs.p, tsegs.data(), bt, cudaMemcpyHostToDevice, st));
             GXY_CK(cudaMemcpyAsync(W->d_qsegs.p, qsegs.data(), bq, cudaMemcpyHostToDevice, st));
+            if (bp) GXY_CK(cudaMemcpyAsync(W->d_place.p, out.places, bp, cudaMemcpyHostToDevice, st));
             GXY_CK(cudaStreamSynchronize(st));   // the host vectors die with this call
         }
+    }
+    // Record key widths: group, global t, q, span (span <= min(target, query)).
+    int rb_g = 0, rb_t = 0, rb_q = 0, rb_l = 0;
+    if (records) {
+        uint64_t mg = 0, mt = 0, mq = 0, ml = 0;
+        for (uint32_t i = 0; i < nu; i++) {
+            const uint64_t tl = tsegs[units[i].tseg].len, ql = qsegs[units[i].qseg].len;
+            mg = std::max<uint64_t>(mg, out.places[i].group);
+            mt = std::max<uint64_t>(mt, out.places[i].t_offset + tl);
+            mq = std::max<uint64_t>(mq, ql);
+            ml = std::max<uint64_t>(ml, std::min(tl, ql));
+        }
+        rb_g = bits_for(mg);
+        rb_t = bits_for(mt ? mt - 1 : 0);
+        rb_q = bits_for(mq ? mq - 1 : 0);
+        rb_l = bits_for(ml);
     }
 
     ScreenArgs sa;
@@ -393,6 +415,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(W->runit2.ensure((size_t)cap * 4));
         GXY_CK(W->perm.ensure((size_t)cap * 4));
         GXY_CK(W->perm2.ensure((size_t)cap * 4));
+        if (records) GXY_CK(W->rrec.ensure((size_t)cap * sizeof(Record)));
         sa.tile_counter = cnt + kCTile;
         sa.cand_count = cnt + kCCand;
         sa.hit_next = cnt + kCHitNext;
@@ -489,6 +512,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             GXY_CK(W->runit2.ensure((size_t)cap * 4));
             GXY_CK(W->perm.ensure((size_t)cap * 4));
             GXY_CK(W->perm2.ensure((size_t)cap * 4));
+            if (records) GXY_CK(W->rrec.ensure((size_t)cap * sizeof(Record)));
         } else {
             // In graph mode the timing events sit around the graph launch.
             in_capture = graph_now;
@@ -546,6 +570,45 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             fin_unit = W->runit2.as<uint32_t>();
         }
         launch_fixup(fin, fin_unit, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
+        if (records) {
+            // Driver records (src/driver.rs:371-391): stable LSD sort by
+            // (group, global t, q, span) over the unit-major HSP order, then
+            // drop repeats of the same four fields, keeping the first.  One
+            // sort of a packed key when the fields fit 64 bits, else (q, span)
+            // first and (group, t) second.
+            const Place* pl = W->d_place.as<Place>();
+            RadixPass rp[16];
+            const uint32_t* perm;
+            if (rb_g + rb_t + rb_q + rb_l <= 64) {
+                const int sh_q = rb_l, sh_t = rb_l + rb_q, sh_g = rb_l + rb_q + rb_t;
+                launch_record_keys(fin, fin_unit, pl, nullptr, cnt + kCHsps, cap, 0, sh_g, sh_t, sh_q,
+                                   W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), blocks_misc, st);
+                const int np = plan_radix(0, rb_l + rb_q + rb_t + rb_g, 0, 0, rp, 16);
+                const int w = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
+                                             W->cv1.as<uint32_t>(), cnt + kCHsps, 0, cap, rp, np, W->ps, st);
+                perm = w ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
+            } else {
+                launch_record_keys(fin, fin_unit, pl, nullptr, cnt + kCHsps, cap, 1, 0, 0, 0, W->ck0.as<uint64_t>(),
+                                   W->cv0.as<uint32_t>(), blocks_misc, st);
+                int np = plan_radix(0, rb_l, 32, rb_q, rp, 16);
+                int w = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
+                                       W->cv1.as<uint32_t>(), cnt + kCHsps, 0, cap, rp, np, W->ps, st);
+                const uint32_t* p1 = w ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
+                uint64_t* k2 = w ? W->ck0.as<uint64_t>() : W->ck1.as<uint64_t>();
+                uint32_t* v2 = w ? W->cv0.as<uint32_t>() : W->cv1.as<uint32_t>();
+                uint64_t* k3 = w ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
+                uint32_t* v3 = w ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
+                launch_record_keys(fin, fin_unit, pl, p1, cnt + kCHsps, cap, 2, 0, 0, 0, k2, v2, blocks_misc, st);
+                np = plan_radix(0, rb_t, 32, rb_g, rp, 16);
+                w = radix_sort_u64(k2, v2, k3, v3, cnt + kCHsps, 0, cap, rp, np, W->ps, st);
+                perm = w ? v3 : v2;
+            }
+            launch_record_heads(fin, fin_unit, pl, perm, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
+            scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCHsps, 0, cap, false, cnt + kCRecs,
+                    W->ps, st);
+            launch_record_emit(fin, fin_unit, pl, perm, W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(),
+                               cnt + kCHsps, cap, W->rrec.as<Record>(), blocks_misc, st);
+        }
         if (!graph_now) GXY_CK(cudaEventRecord(W->ev[2], st));
         GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
 
@@ -613,6 +676,25 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.enum_ms = single ? ms_enum : 0.0;
         out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;
         out.stats.passes = single ? 1 : (uint32_t)((tiles + pass_tiles - 1) / pass_tiles);
+        if (records) {
+            const uint32_t nr = hc[kCRecs];
+            out.records.resize(nr);
+            if (nr) {
+                const size_t rb = (size_t)nr * sizeof(Record);
+                if (rb > W->h_res_bytes) {
+                    if (W->h_res) GXY_CK(cudaFreeHost(W->h_res));
+                    W->h_res = nullptr;
+                    W->h_res_bytes = 0;
+                    const size_t want = std::max<size_t>(1 << 20, rb + rb / 2);
+                    GXY_CK(cudaMallocHost(&W->h_res, want));
+                    W->h_res_bytes = want;
+                }
+                GXY_CK(cudaMemcpyAsync(W->h_res, W->rrec.p, rb, cudaMemcpyDeviceToHost, st));
+                GXY_CK(cudaStreamSynchronize(st));
+                memcpy(out.records.data(), W->h_res, rb);
+            }
+            return GXY_OK;
+        }
         // Results come back through the worker's pinned staging.
         const size_t hb = (size_t)nh * sizeof(Hsp), ub = nu > 1 ? (size_t)nh * 4 : 0;
         if (hb + ub > W->h_res_bytes) {

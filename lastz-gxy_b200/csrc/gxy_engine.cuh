@@ -41,6 +41,7 @@ struct Worker {
     DevBuf d_units, d_tsegs, d_qsegs;
     DevBuf ck0, ck1, cv0, cv1, cands, flags, offsets, ohsp;
     DevBuf rhsp, runit, rhsp2, runit2, perm, perm2;
+    DevBuf d_place, rrec;         // driver records: per-unit places, records
     DevBuf hits;                  // raw hits of one pass
     uint64_t hit_cap = 0;
     uint32_t cand_cap = 0;
@@ -68,7 +69,7 @@ struct UnitPlan {
 };
 
 // Layout of a worker's device counters (u32 indices).
-constexpr uint32_t kCTile = 0, kCHsps = 2, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072,
+constexpr uint32_t kCTile = 0, kCHsps = 2, kCRecs = 4, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072,
                    kCWalk = 3584;
 constexpr uint32_t kCounterWords = 4096;
 
@@ -82,6 +83,11 @@ struct RunResult {
     bool want_view = false;
     const gxy_hsp* view = nullptr;
     uint64_t n_view = 0;
+    // With places set (one per unit), the HSPs become driver records on the
+    // device instead (global t, per-group order, dedup): records is filled,
+    // hsps and unit stay empty.
+    const Place* places = nullptr;
+    std::vector<Record> records;
 };
 
 }  // namespace gxy

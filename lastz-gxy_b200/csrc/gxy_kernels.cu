@@ -1279,31 +1279,44 @@ __global__ __launch_bounds__(WARPS * 32) void k_walk(const __grid_constant__ Wal
             const uint32_t h = r * 32 + (uint32_t)(__ffs(hb) - 1);
             hb &= hb - 1;
             const uint32_t segkey = (uint32_t)(a.keys[h] >> 32);
+            // A segment (one diagonal key) can hold the candidates of several
+            // units that share a target segment, interleaved in t.  Each unit
+            // is walked by its own pass with its own cover: first the unit of
+            // the segment's first candidate (u0), then the other units in
+            // ascending order -- those above u0, then those below it.  Each
+            // pass finds the next unit as the smallest one above the current
+            // one (and below `ceil`); a segment of one unit takes one pass.
+            const uint32_t u0 = a.cands[a.idx[h]].unit;
+            uint32_t cur_unit = u0, ceil = 0xffffffffu, below = 0xffffffffu;
+            for (;;) {
             uint32_t j = h;
-            uint32_t cover = 0, cur_unit = 0xffffffffu;
+            uint32_t cover = 0;
+            uint32_t next = 0xffffffffu;
             for (;;) {
                 const uint32_t jj = j + lane;
                 const bool inseg = jj < n && (uint32_t)(a.keys[jj] >> 32) == segkey;
                 Cand c;
                 c.unit = 0xffffffffu; c.t = 0;
                 if (inseg) c = a.cands[a.idx[jj]];
-                const bool elig = inseg && (c.unit != cur_unit || c.t >= cover);
+                const bool elig = inseg && c.unit == cur_unit && c.t >= cover;
                 const uint32_t be = __ballot_sync(kFull, !inseg);
                 const uint32_t bc = __ballot_sync(kFull, elig);
                 const uint32_t stop = be ? (uint32_t)(__ffs(be) - 1) : 32u;
                 const uint32_t first = bc ? (uint32_t)(__ffs(bc) - 1) : 32u;
+                // Other units among the positions this step passes over.
+                const uint32_t upto = min(first, stop);
+                const bool seen = (uint32_t)lane <= upto && inseg;
+                next = min(next, __reduce_min_sync(kFull, (seen && c.unit > cur_unit && c.unit < ceil) ? c.unit
+                                                                                                  : 0xffffffffu));
+                below = min(below, __reduce_min_sync(kFull, (seen && c.unit < u0) ? c.unit : 0xffffffffu));
                 if (first < stop) {
-                    const uint32_t unit = __shfl_sync(kFull, c.unit, first);
+                    const uint32_t unit = cur_unit;
                     const uint32_t t = __shfl_sync(kFull, c.t, first);
                     const uint32_t q = __shfl_sync(kFull, c.q, first);
                     const uint32_t flags = __shfl_sync(kFull, c.flags, first);
                     int32_t score = __shfl_sync(kFull, c.score, first);
                     uint32_t lext = __shfl_sync(kFull, c.lext, first);
                     uint32_t rext = __shfl_sync(kFull, c.rext, first);
-                    if (unit != cur_unit) {
-                        cur_unit = unit;
-                        cover = 0;
-                    }
                     const UnitDev U = a.units[unit];
                     const SeqView T = a.tsegs[U.tseg];
                     if (flags & kCandLong) {
@@ -1333,6 +1346,15 @@ __global__ __launch_bounds__(WARPS * 32) void k_walk(const __grid_constant__ Wal
                 }
                 if (stop < 32) break;
                 j += 32;
+            }
+            if (next != 0xffffffffu) {
+                cur_unit = next;                      // the next unit above
+            } else if (ceil == 0xffffffffu && below != 0xffffffffu) {
+                cur_unit = below;                     // then the units below u0, ascending
+                ceil = u0;
+            } else {
+                break;
+            }
             }
         }
     }
@@ -1436,6 +1458,90 @@ __global__ void k_iota(uint32_t* v, const uint32_t* n_dev, uint32_t n_cap) {
 void launch_iota(uint32_t* v, const uint32_t* n_dev, uint32_t n_cap, int blocks, cudaStream_t st) {
     count_launch();
     k_iota<<<blocks, 256, 0, st>>>(v, n_dev, n_cap);
+}
+
+// ---------------------------------------------------------------------------
+// Driver records: global coordinates, per-group order and dedup
+// (build_ungapped_record src/driver.rs:437-468; sort and dedup_by :371-391).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t shl64(uint64_t x, int s) { return s >= 64 ? 0ull : x << s; }
+
+__global__ void k_record_keys(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                              const uint32_t* n_dev, uint32_t n_cap, int mode, int sh_g, int sh_t, int sh_q,
+                              uint64_t* key, uint32_t* val) {
+    const uint32_t n = min(*n_dev, n_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = perm ? perm[i] : i;
+        const Hsp h = hsp[p];
+        const Place pl = place[unit[p]];
+        const uint32_t t = h.t_start + pl.t_offset;
+        uint64_t k;
+        if (mode == 0)
+            k = shl64(pl.group, sh_g) | shl64(t, sh_t) | shl64(h.q_start, sh_q) | h.length;
+        else if (mode == 1)
+            k = ((uint64_t)h.q_start << 32) | h.length;
+        else
+            k = ((uint64_t)pl.group << 32) | t;
+        key[i] = k;
+        val[i] = p;
+    }
+}
+
+void launch_record_keys(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                        const uint32_t* n_dev, uint32_t n_cap, int mode, int sh_g, int sh_t, int sh_q, uint64_t* key,
+                        uint32_t* val, int blocks, cudaStream_t st) {
+    count_launch();
+    k_record_keys<<<blocks, 256, 0, st>>>(hsp, unit, place, perm, n_dev, n_cap, mode, sh_g, sh_t, sh_q, key, val);
+}
+
+__device__ __forceinline__ Record make_record(const Hsp* hsp, const uint32_t* unit, const Place* place,
+                                              uint32_t p) {
+    const Hsp h = hsp[p];
+    const uint32_t u = unit[p];
+    const Place pl = place[u];
+    Record r;
+    r.group = pl.group;
+    r.t_start = h.t_start + pl.t_offset;
+    r.q_start = h.q_start;
+    r.span = h.length;
+    r.score = h.score;
+    r.unit = u;
+    return r;
+}
+
+__global__ void k_record_heads(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                               const uint32_t* n_dev, uint32_t n_cap, uint8_t* flag) {
+    const uint32_t n = min(*n_dev, n_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint8_t head = 1;
+        if (i > 0) {
+            const Record a = make_record(hsp, unit, place, perm[i - 1]);
+            const Record b = make_record(hsp, unit, place, perm[i]);
+            head = (a.group != b.group || a.t_start != b.t_start || a.q_start != b.q_start || a.span != b.span);
+        }
+        flag[i] = head;
+    }
+}
+
+void launch_record_heads(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                         const uint32_t* n_dev, uint32_t n_cap, uint8_t* flag, int blocks, cudaStream_t st) {
+    count_launch();
+    k_record_heads<<<blocks, 256, 0, st>>>(hsp, unit, place, perm, n_dev, n_cap, flag);
+}
+
+__global__ void k_record_emit(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                              const uint8_t* flag, const uint32_t* offsets, const uint32_t* n_dev, uint32_t n_cap,
+                              Record* out) {
+    const uint32_t n = min(*n_dev, n_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flag[i]) out[offsets[i]] = make_record(hsp, unit, place, perm[i]);
+}
+
+void launch_record_emit(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                        const uint8_t* flag, const uint32_t* offsets, const uint32_t* n_dev, uint32_t n_cap,
+                        Record* out, int blocks, cudaStream_t st) {
+    count_launch();
+    k_record_emit<<<blocks, 256, 0, st>>>(hsp, unit, place, perm, flag, offsets, n_dev, n_cap, out);
 }
 
 // ---------------------------------------------------------------------------

@@ -130,6 +130,38 @@ void launch_gather_hsp(const Hsp* in, const uint32_t* in_unit, const uint32_t* p
                        uint32_t n_cap, Hsp* out, uint32_t* out_unit, int blocks, cudaStream_t st);
 void launch_iota(uint32_t* v, const uint32_t* n_dev, uint32_t n_cap, int blocks, cudaStream_t st);
 
+// --- driver records (src/driver.rs:371-391, :437-468) --------------------------
+// Where a unit's HSPs go: the output group (the driver's (target, query,
+// strand) rank) and the chunk's global start added to t_start.
+struct Place {
+    uint32_t group;
+    uint32_t t_offset;
+};
+// One ungapped record: t_span = q_span = span.  unit = the unit it came from.
+struct Record {
+    uint32_t group;
+    uint32_t t_start;
+    uint32_t q_start;
+    uint32_t span;
+    int32_t score;
+    uint32_t unit;
+};
+// Sort keys of the records.  mode 0: (group, t, q, span) packed into one u64
+// with the given shifts (span at bit 0); mode 1: (q << 32) | span; mode 2:
+// (group << 32) | t.  t = t_start + the unit's t_offset.  HSP i is
+// hsp[perm[i]] (perm may be null: the identity); val[i] = that index.
+void launch_record_keys(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                        const uint32_t* n_dev, uint32_t n_cap, int mode, int sh_g, int sh_t, int sh_q, uint64_t* key,
+                        uint32_t* val, int blocks, cudaStream_t st);
+// flag[i] = 1 when record perm[i] differs from record perm[i-1] in (group,
+// t, q, span) (dedup_by, src/driver.rs:381-387, keeps the first).
+void launch_record_heads(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                         const uint32_t* n_dev, uint32_t n_cap, uint8_t* flag, int blocks, cudaStream_t st);
+// out[offsets[i]] = the record of perm[i] for every flagged i.
+void launch_record_emit(const Hsp* hsp, const uint32_t* unit, const Place* place, const uint32_t* perm,
+                        const uint8_t* flag, const uint32_t* offsets, const uint32_t* n_dev, uint32_t n_cap,
+                        Record* out, int blocks, cudaStream_t st);
+
 // --- x-drop of given hits (test entry) ---------------------------------------
 void launch_extend_hits(SeqView T, SeqView Q, Score sc, const uint32_t* tpos, const uint32_t* qpos, uint64_t n,
                         uint32_t seed_len, uint32_t mode, Hsp* out, uint8_t* ok, cudaStream_t st);

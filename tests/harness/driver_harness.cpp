@@ -15,7 +15,12 @@
 // It stands in for the Rust -sys binding the reference would use (no Rust
 // toolchain here) and shows that the library is a drop-in for those calls.
 //
-// usage: driver_harness TARGET QUERY OUT PRIMARY_BP HALO_BP THREADS TRANSITIONS MAX_WORD_COUNT
+// MODE 1 makes the same records with one gxy_batch_records call instead:
+// the target and query stay on the device, every chunk's table is a view of
+// the target, and the filter, global coordinates, order and dedup all run
+// on the device.
+//
+// usage: driver_harness TARGET QUERY OUT PRIMARY_BP HALO_BP THREADS TRANSITIONS MAX_WORD_COUNT [MODE]
 //   TARGET / QUERY: files of raw ASCII bases.  OUT: binary records, see write_out().
 #include <algorithm>
 #include <atomic>
@@ -99,11 +104,73 @@ void write_out(const char* path, const std::vector<Record>& recs) {
     fclose(f);
 }
 
+gxy_search_params driver_params(uint32_t transitions) {
+    gxy_search_params p{};
+    const int32_t hoxd70[16] = {91, -114, -31, -123, -114, 100, -125, -31,
+                                -31, -125, 100, -114, -123, -31, -114, 91};   // src/scoring.rs:17-23
+    memcpy(p.sub, hoxd70, sizeof p.sub);
+    p.ambig = -100;
+    p.xdrop = 910;
+    p.hspthresh = 3000;
+    p.step = 1;
+    p.transitions = (uint8_t)transitions;
+    return p;
+}
+
+// MODE 1: the whole driver flow of one (target, query) pair in one batch.
+int batched(const std::string& target, const std::string& query, const char* out, uint32_t primary,
+            uint32_t halo, uint32_t transitions, uint32_t mwc, const char* pattern) {
+    gxy_ctx* ctx = nullptr;
+    gxy_status s = gxy_ctx_create(0, &ctx);
+    if (s != GXY_OK) die("gxy_ctx_create", s);
+    gxy_dseq *T = nullptr, *Q = nullptr;
+    s = gxy_dseq_from_ascii(ctx, reinterpret_cast<const uint8_t*>(target.data()), target.size(), &T);
+    if (s != GXY_OK) die("gxy_dseq_from_ascii", s);
+    s = gxy_dseq_from_ascii(ctx, reinterpret_cast<const uint8_t*>(query.data()), query.size(), &Q);
+    if (s != GXY_OK) die("gxy_dseq_from_ascii", s);
+    uint64_t nchunks = 0;
+    gxy_chunk_plan(target.size(), primary, halo, nullptr, 0, &nchunks);
+    std::vector<uint64_t> quads(4 * std::max<uint64_t>(nchunks, 1));
+    s = gxy_chunk_plan(target.size(), primary, halo, quads.data(), nchunks, &nchunks);
+    if (s != GXY_OK) die("gxy_chunk_plan", s);
+    std::vector<gxy_table*> tables(nchunks, nullptr);
+    std::vector<gxy_unit> units;
+    std::vector<gxy_unit_place> places;
+    for (uint64_t c = 0; c < nchunks; c++) {
+        s = gxy_table_build_view(ctx, T, quads[4 * c], quads[4 * c + 1], pattern, 1, mwc, &tables[c]);
+        if (s != GXY_OK) die("gxy_table_build_view", s);
+        for (uint32_t strand = 0; strand < 2; strand++) {
+            units.push_back(gxy_unit{(uint32_t)c, 0, strand, (uint32_t)quads[4 * c + 2], (uint32_t)quads[4 * c + 3]});
+            places.push_back(gxy_unit_place{strand, (uint32_t)quads[4 * c]});
+        }
+    }
+    const gxy_search_params p = driver_params(transitions);
+    const gxy_dseq* qs[1] = {Q};
+    gxy_record_result rr{};
+    s = gxy_batch_records(ctx, (uint32_t)nchunks, tables.data(), 1, qs, (uint32_t)units.size(), units.data(),
+                          places.data(), &p, nullptr, &rr, nullptr);
+    if (s != GXY_OK) die("gxy_batch_records", s);
+    std::vector<Record> recs;
+    recs.reserve(rr.n_records);
+    for (uint64_t i = 0; i < rr.n_records; i++) {
+        const gxy_record& r = rr.records[i];
+        recs.push_back(Record{0, r.group, r.t_start, r.q_start, r.span, r.score});
+    }
+    write_out(out, recs);
+    gxy_record_result_free(&rr);
+    for (gxy_table* t : tables) gxy_table_free(t);
+    gxy_dseq_free(T);
+    gxy_dseq_free(Q);
+    gxy_ctx_destroy(ctx);
+    printf("chunks %llu records %zu\n", (unsigned long long)nchunks, recs.size());
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
-    if (argc != 9) {
-        fprintf(stderr, "usage: %s TARGET QUERY OUT PRIMARY_BP HALO_BP THREADS TRANSITIONS MAX_WORD_COUNT\n",
+    if (argc != 9 && argc != 10) {
+        fprintf(stderr, "usage: %s TARGET QUERY OUT PRIMARY_BP HALO_BP THREADS TRANSITIONS MAX_WORD_COUNT [MODE]\n",
                 argv[0]);
         return 2;
     }
@@ -112,6 +179,8 @@ int main(int argc, char** argv) {
     const int threads = std::max(1, atoi(argv[6]));
     const uint32_t transitions = (uint32_t)atoi(argv[7]), mwc = (uint32_t)atoi(argv[8]);
     const char* pattern = "1110100110010101111";   // 12of19 (src/seeds.rs:56)
+    if (argc == 10 && atoi(argv[9]) == 1)
+        return batched(target, query, argv[3], primary, halo, transitions, mwc, pattern);
 
     gxy_ctx* ctx = nullptr;
     gxy_status s = gxy_ctx_create(0, &ctx);
@@ -147,15 +216,7 @@ int main(int argc, char** argv) {
 
     // search() per (chunk, query, strand); the pool interleaves the units so
     // that both strands of a chunk run at once on its shared table.
-    gxy_search_params p{};
-    const int32_t hoxd70[16] = {91, -114, -31, -123, -114, 100, -125, -31,
-                                -31, -125, 100, -114, -123, -31, -114, 91};   // src/scoring.rs:17-23
-    memcpy(p.sub, hoxd70, sizeof p.sub);
-    p.ambig = -100;
-    p.xdrop = 910;
-    p.hspthresh = 3000;
-    p.step = 1;
-    p.transitions = (uint8_t)transitions;
+    const gxy_search_params p = driver_params(transitions);
     std::vector<Record> recs;
     std::mutex mu;
     {

@@ -150,3 +150,30 @@ def test_concurrent_searches_share_one_table(gxy, ctx):
     for i, (g, w) in enumerate(zip(got, want)):
         assert g.tobytes() == w.tobytes(), i
     assert sum(len(w) for w in want) > 0
+
+
+def test_batch_repeated_and_split_units(gxy, ctx):
+    """Units that share (table, query, strand) -- the same unit twice, and one
+    chunk's primary range split over two units -- share one diagonal key range,
+    so their candidates interleave on each diagonal; each unit must still get
+    exactly its own search() result (its own diagonal cover)."""
+    rng = np.random.default_rng(33)
+    target, query = homologous_pair(rng, 120_000, 0.85)
+    T = gxy.PackedSeq.from_ascii(target)
+    tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    dq = [gxy.PackedSeq.from_ascii(query).to_device(ctx)]
+    cut = 50_000
+    units = [(0, 0, 0), (0, 0, 1), (0, 0, 0), (0, 0, 0, 0, cut), (0, 0, 0, cut, len(target)), (0, 0, 1)]
+    got = gxy.batch_search([tab], dq, units, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams())
+    want = oracle_units(target, [query], [(0, 0, 0), (0, 0, 1)])
+    plus, minus = want
+    assert len(plus) > 20
+    assert got[0].tobytes() == plus.tobytes()
+    assert got[1].tobytes() == minus.tobytes()
+    assert got[2].tobytes() == plus.tobytes()
+    lo = plus[plus["t_start"] < cut]
+    hi = plus[plus["t_start"] >= cut]
+    assert len(lo) > 0 and len(hi) > 0
+    assert got[3].tobytes() == lo.tobytes()
+    assert got[4].tobytes() == hi.tobytes()
+    assert got[5].tobytes() == minus.tobytes()
