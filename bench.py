@@ -372,6 +372,7 @@ def run_batched(args):
     contigs (~200 Mbp), both strands -- one batched launch per pass against the
     plain per-(query, strand) search() loop on the same GPU; results must match."""
     import torch
+    import numpy as np
     g = _pkg()
     from lastz_gxy_b200 import synth
     from lastz_gxy_b200.autotune import autotune
@@ -444,11 +445,14 @@ def replay_served(g, srv, reqs, packed):
     res = [None] * len(reqs)
     lat = [None] * len(reqs)
     done_t = [0.0] * len(reqs)
+    cv = threading.Condition()
 
     def waiter():
+        # Blocks (no polling) until request i is submitted, then on its result,
+        # as the serial arm's worker does.
         for i in range(len(reqs)):
-            while ids[i] is None:
-                time.sleep(0.0002)
+            with cv:
+                cv.wait_for(lambda: ids[i] is not None)
             p, mi, l = srv.wait(ids[i], timeout_ms=600_000)
             res[i], lat[i] = (p, mi), l
             done_t[i] = time.perf_counter()
@@ -459,7 +463,10 @@ def replay_served(g, srv, reqs, packed):
         d = start + r.arrival_s - reqs[0].arrival_s - time.perf_counter()
         if d > 0:
             time.sleep(d)
-        ids[i] = srv.submit(r.target, packed[i])
+        rid = srv.submit(r.target, packed[i])
+        with cv:
+            ids[i] = rid
+            cv.notify()
     w.join()
     return res, lat, max(done_t) - start
 
@@ -608,10 +615,35 @@ def run_chunked(args):
         dQr.free()
         ctx.mark(13)
         p_ms = ctx.elapsed_ms(12, 13)
+        # The driver's --nogapped records of the same units (global t, one
+        # group per strand, sorted, deduplicated) from one batch_records call.
+        places = [(strand, chunks[ci][0]) for ci, _, strand, _, _ in units]
+        ctx.mark(14)
+        recs, offs = g.batch_records(tabs, [dQ], units, places, m, sp, ctx=ctx)
+        ctx.mark(15)
+        r_ms = ctx.elapsed_ms(14, 15)
+        rdt = np.dtype([("t", "<u8"), ("q", "<u4"), ("l", "<u4"), ("s", "<i4")])
+        rec_same = len(offs) == 3
+        for strand in (0, 1):
+            parts = []
+            for u, (ci, _, sd, _, _) in enumerate(units):
+                if sd != strand:
+                    continue
+                a = np.empty(len(got[u]), rdt)
+                a["t"] = got[u]["t_start"].astype(np.uint64) + chunks[ci][0]
+                a["q"], a["l"], a["s"] = got[u]["q_start"], got[u]["length"], got[u]["score"]
+                parts.append(a)
+            w = np.unique(np.concatenate(parts)) if parts else np.empty(0, rdt)
+            r = recs[int(offs[strand]):int(offs[strand + 1])] if rec_same else recs[:0]
+            rec_same = rec_same and len(r) == len(w) and bool(
+                np.array_equal(r["t_start"].astype(np.uint64), w["t"]) and np.array_equal(r["q_start"], w["q"])
+                and np.array_equal(r["span"], w["l"]) and np.array_equal(r["score"], w["s"]))
         out[f"transitions_{tr}"] = {
             "batched": {"value": round(mbp2_total / (b_ms / 1e3), 2), "ms": round(b_ms, 1), "raw_hits": st["raw_hits"],
                         "candidates": st["candidates"], "hsps": st["hsps"], "passes": st["passes"]},
             "plain": {"value": round(mbp2_total / (p_ms / 1e3), 2), "ms": round(p_ms, 1)},
+            "records": {"value": round(mbp2_total / (r_ms / 1e3), 2), "ms": round(r_ms, 1), "n": int(len(recs)),
+                        "same_as_host_postprocessing": rec_same},
             "bit_identical": same, "autotune": tune["tuning"]}
     return out
 

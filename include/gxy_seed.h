@@ -348,6 +348,13 @@ typedef struct {
     /* Query bases (counted once per strand) one batch takes at most, so that
      * a batch stays short and requests behind it wait less; 0 = 16 Mbp. */
     uint64_t max_batch_bases;
+    /* Requests with at least big_bases query bases are "big": each runs in a
+     * batch of its own, at most max_big_inflight of them at a time, and
+     * while that many run, the smaller requests queued behind them are
+     * admitted ahead of them.  big_bases 0 = 1 Mbp; max_big_inflight 0 = 1. */
+    uint64_t big_bases;
+    uint32_t max_big_inflight;
+    uint32_t reserved_;
 } gxy_server_opts;
 
 gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,

@@ -91,7 +91,8 @@ class BatchOptsC(C.Structure):
 class ServerOptsC(C.Structure):
     _fields_ = [("max_device_bytes", C.c_uint64), ("max_units", C.c_uint32), ("max_streams", C.c_uint32),
                 ("max_batch_units", C.c_uint32), ("both_strands", C.c_uint32),
-                ("max_batch_bases", C.c_uint64)]
+                ("max_batch_bases", C.c_uint64), ("big_bases", C.c_uint64), ("max_big_inflight", C.c_uint32),
+                ("reserved_", C.c_uint32)]
 
 
 class ServerStatsC(C.Structure):

@@ -547,6 +547,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         wa.out_flag = W->flags.as<uint8_t>();
         wa.out_hsp = W->ohsp.as<Hsp>();
         wa.chunk_next = cnt + kCWalk;
+        wa.n_units = nu;
         GXY_CK(cudaMemsetAsync(cnt + kCWalk, 0, 4, st));
         launch_walk(wa, walk_warps, blocks_misc, st);
         scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCCand, 0, cap, false, cnt + kCHsps, W->ps,

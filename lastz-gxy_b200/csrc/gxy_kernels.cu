@@ -1304,11 +1304,13 @@ __global__ __launch_bounds__(WARPS * 32) void k_walk(const __grid_constant__ Wal
                 const uint32_t stop = be ? (uint32_t)(__ffs(be) - 1) : 32u;
                 const uint32_t first = bc ? (uint32_t)(__ffs(bc) - 1) : 32u;
                 // Other units among the positions this step passes over.
-                const uint32_t upto = min(first, stop);
-                const bool seen = (uint32_t)lane <= upto && inseg;
-                next = min(next, __reduce_min_sync(kFull, (seen && c.unit > cur_unit && c.unit < ceil) ? c.unit
-                                                                                                  : 0xffffffffu));
-                below = min(below, __reduce_min_sync(kFull, (seen && c.unit < u0) ? c.unit : 0xffffffffu));
+                if (a.n_units > 1) {
+                    const uint32_t upto = min(first, stop);
+                    const bool seen = (uint32_t)lane <= upto && inseg;
+                    next = min(next, __reduce_min_sync(kFull, (seen && c.unit > cur_unit && c.unit < ceil)
+                                                                  ? c.unit : 0xffffffffu));
+                    below = min(below, __reduce_min_sync(kFull, (seen && c.unit < u0) ? c.unit : 0xffffffffu));
+                }
                 if (first < stop) {
                     const uint32_t unit = cur_unit;
                     const uint32_t t = __shfl_sync(kFull, c.t, first);

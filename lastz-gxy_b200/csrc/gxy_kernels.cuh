@@ -112,6 +112,7 @@ struct WalkArgs {
     uint8_t* out_flag;         // per sorted position: 1 = emitted and kept
     Hsp* out_hsp;              // per sorted position
     uint32_t* chunk_next;      // work counter: chunks of 32 sorted positions (zeroed by the caller)
+    uint32_t n_units;          // units of the launch (one unit: every segment is walked in one pass)
 };
 // Diagonal suppression (src/diag_hash.rs:34-53 as used at
 // src/seed_search.rs:318-342) over the candidates sorted by (diagonal, t),

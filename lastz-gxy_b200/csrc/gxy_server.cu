@@ -66,6 +66,7 @@ struct gxy_server {
     uint64_t next_id = 1;
     uint64_t bytes_in_use = 0;
     uint64_t units_in_flight = 0;
+    uint32_t big_in_flight = 0;
     gxy_server_stats st{};
     // Device free memory as last queried (cudaMemGetInfo costs tens of us):
     // refreshed at most every 20 ms, and reduced meanwhile by what was
@@ -170,6 +171,7 @@ void dispatcher(gxy_server* s) {
     const uint32_t strands = s->opts.both_strands ? 2 : 1;
     for (;;) {
         std::vector<Request*> batch;
+        bool batch_big = false;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
@@ -184,8 +186,16 @@ void dispatcher(gxy_server* s) {
             const uint64_t grown = s->bytes_in_use > s->in_use_seen ? s->bytes_in_use - s->in_use_seen : 0;
             size_t free_b = s->free_seen > grown ? s->free_seen - grown : 0;
             uint64_t batch_units = 0, batch_bases = 0;
-            while (!s->pending.empty()) {
-                Request* q = s->pending.front();
+            // Arrival order, except that a big request waits in place (and
+            // the smaller ones behind it go ahead) while the big slots are
+            // taken; a big request always runs in a batch of its own.
+            for (auto it = s->pending.begin(); it != s->pending.end();) {
+                Request* q = *it;
+                const bool big = q->len >= s->opts.big_bases;
+                if (big && (!batch.empty() || s->big_in_flight >= s->opts.max_big_inflight)) {
+                    ++it;
+                    continue;
+                }
                 const bool fits_mem = s->bytes_in_use + q->bytes <= s->opts.max_device_bytes &&
                                       q->bytes + (64ull << 20) <= free_b;
                 const bool fits_units = s->units_in_flight + strands <= s->opts.max_units;
@@ -196,13 +206,18 @@ void dispatcher(gxy_server* s) {
                 // A request that could never fit alone is still run alone.
                 const bool alone = batch.empty() && s->units_in_flight == 0;
                 if (!(fits_mem && fits_units && fits_batch) && !alone) break;
-                s->pending.pop_front();
+                it = s->pending.erase(it);
                 batch.push_back(q);
                 s->bytes_in_use += q->bytes;
                 s->units_in_flight += strands;
                 batch_units += strands;
                 batch_bases += (uint64_t)q->len * strands;
                 if (free_b > q->bytes) free_b -= q->bytes;
+                if (big) {
+                    batch_big = true;
+                    s->big_in_flight++;
+                    break;
+                }
             }
             if (batch.empty()) {
                 // Budget taken by batches in flight: wait for one to finish.
@@ -217,6 +232,7 @@ void dispatcher(gxy_server* s) {
         {
             std::lock_guard<std::mutex> g(s->mu);
             const auto now = Clock::now();
+            if (batch_big) s->big_in_flight--;
             for (Request* q : batch) {
                 q->status = e;
                 q->done = true;
@@ -277,6 +293,8 @@ gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* c
     if (!o.max_streams) o.max_streams = 2;
     if (!o.max_batch_units) o.max_batch_units = 1024;
     if (!o.max_batch_bases) o.max_batch_bases = 16ull << 20;
+    if (!o.big_bases) o.big_bases = 1ull << 20;
+    if (!o.max_big_inflight) o.max_big_inflight = 1;
     s->opts = o;
     for (uint32_t i = 0; i < o.max_streams; i++) s->threads.emplace_back(dispatcher, s);
     *out = s;

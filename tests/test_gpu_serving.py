@@ -79,6 +79,23 @@ def test_admission_by_memory_budget(gxy, setup):
         assert ref[i][0].tobytes() == tight[i][0].tobytes() and ref[i][1].tobytes() == tight[i][1].tobytes()
 
 
+def test_big_requests_run_alone_and_small_ones_go_ahead(gxy, setup):
+    # With big_bases below most request sizes, the big requests each run in a
+    # batch of their own, one at a time; results do not change.
+    targets, tables, reqs = setup
+    ref, _ = run_server(gxy, tables, reqs, "alone")
+    lens = sorted(len(q) for _, q in reqs)
+    cut = lens[len(lens) // 3]
+    n_big = sum(1 for _, q in reqs if len(q) >= cut)
+    mix, st = run_server(gxy, tables, reqs, "mix", max_streams=2, max_batch_units=64, big_bases=cut,
+                         max_big_inflight=1)
+    assert st["completed"] == len(reqs)
+    # Every big request is a batch; the small ones share the others.
+    assert st["batches"] >= n_big + 1
+    for i in range(len(reqs)):
+        assert ref[i][0].tobytes() == mix[i][0].tobytes() and ref[i][1].tobytes() == mix[i][1].tobytes(), i
+
+
 def test_wait_timeout_and_unknown_id(gxy, setup):
     _, tables, reqs = setup
     srv = gxy.Server(tables, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams())
