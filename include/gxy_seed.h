@@ -106,7 +106,7 @@ typedef struct {
     uint64_t columns;      /* alignment columns the screen scanned on the two sides */
     double enum_ms;        /* CUDA-event time of the hit enumeration kernel (single pass) */
     uint32_t passes;       /* window-range passes the raw hits needed */
-    uint32_t reserved_;
+    uint32_t reruns;       /* pipeline runs repeated after a buffer had to grow */
 } gxy_stats;
 
 const char* gxy_status_string(gxy_status s);
@@ -355,6 +355,10 @@ typedef struct {
     uint64_t big_bases;
     uint32_t max_big_inflight;
     uint32_t reserved_;
+    /* When > 0, each dispatcher sizes its buffers at start for a query of
+     * this many bases against the largest resident table, so that requests up
+     * to that size never wait for a device allocation. */
+    uint64_t warm_bases;
 } gxy_server_opts;
 
 gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* const* tables,
@@ -373,6 +377,8 @@ typedef struct {
     uint64_t batches;
     uint64_t max_inflight_units;
     uint64_t bytes_in_use;
+    uint64_t reruns;        /* batches' pipeline runs repeated after a buffer had to grow */
+    double busy_ms;         /* summed device time of the batches */
 } gxy_server_stats;
 gxy_status gxy_server_get_stats(gxy_server* s, gxy_server_stats* st);
 gxy_status gxy_server_destroy(gxy_server* s);

@@ -408,7 +408,7 @@ class PosTable:
 def _stats(st: _lib.StatsC) -> dict:
     return {"windows": st.windows, "raw_hits": st.raw_hits, "candidates": st.candidates, "hsps": st.hsps,
             "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns, "enum_ms": st.enum_ms,
-            "passes": st.passes}
+            "passes": st.passes, "reruns": st.reruns}
 
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:

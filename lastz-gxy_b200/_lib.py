@@ -53,7 +53,7 @@ class HspBufC(C.Structure):
 class StatsC(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
                 ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double),
-                ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reserved_", C.c_uint32)]
+                ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reruns", C.c_uint32)]
 
 
 class SeqSetC(C.Structure):
@@ -92,12 +92,13 @@ class ServerOptsC(C.Structure):
     _fields_ = [("max_device_bytes", C.c_uint64), ("max_units", C.c_uint32), ("max_streams", C.c_uint32),
                 ("max_batch_units", C.c_uint32), ("both_strands", C.c_uint32),
                 ("max_batch_bases", C.c_uint64), ("big_bases", C.c_uint64), ("max_big_inflight", C.c_uint32),
-                ("reserved_", C.c_uint32)]
+                ("reserved_", C.c_uint32), ("warm_bases", C.c_uint64)]
 
 
 class ServerStatsC(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
-                ("max_inflight_units", C.c_uint64), ("bytes_in_use", C.c_uint64)]
+                ("max_inflight_units", C.c_uint64), ("bytes_in_use", C.c_uint64), ("reruns", C.c_uint64),
+                ("busy_ms", C.c_double)]
 
 
 V = C.c_void_p

@@ -223,6 +223,39 @@ static void build_variants(const Pattern& pat, uint32_t transitions, uint32_t* v
             for (uint32_t j = i + 1; j < w; j++) vx[nv++] = (2u << shifts[i]) ^ (2u << shifts[j]);
 }
 
+gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t hits, uint64_t candidates) {
+    const uint64_t max_hits = std::max<uint32_t>(4096, ctx->tuning.max_hits_per_pass);
+    hits = std::min(hits, max_hits);
+    candidates = std::min<uint64_t>(candidates, kMaxPresizedCandidates);
+    if (hits > W->hit_cap) {
+        W->hits.release();
+        W->hit_cap = hits;
+    }
+    if (candidates > W->cand_cap) W->cand_cap = (uint32_t)candidates;
+    const size_t cap = W->cand_cap;
+    GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
+    DevBuf* by8[] = {&W->ck0, &W->ck1};
+    for (DevBuf* b : by8) GXY_CK(b->ensure(cap * 8));
+    DevBuf* by4[] = {&W->cv0, &W->cv1, &W->runit, &W->runit2, &W->perm, &W->perm2};
+    for (DevBuf* b : by4) GXY_CK(b->ensure(cap * 4));
+    GXY_CK(W->cands.ensure(cap * sizeof(Cand)));
+    GXY_CK(W->flags.ensure(cap));
+    GXY_CK(W->offsets.ensure(cap * 4 + 4));
+    DevBuf* byh[] = {&W->ohsp, &W->rhsp, &W->rhsp2};
+    for (DevBuf* b : byh) GXY_CK(b->ensure(cap * sizeof(Hsp)));
+    // Pinned result staging for a tenth of the candidates as HSPs with units.
+    const size_t want = std::max<size_t>(1 << 20, cap / 10 * (sizeof(Hsp) + 4));
+    if (want > W->h_res_bytes) {
+        if (W->h_res) GXY_CK(cudaFreeHost(W->h_res));
+        W->h_res = nullptr;
+        W->h_res_bytes = 0;
+        GXY_CK(cudaMallocHost(&W->h_res, want));
+        W->h_res_bytes = want;
+    }
+    GXY_CK(cudaStreamSynchronize(W->st));
+    return GXY_OK;
+}
+
 gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units, std::vector<SeqView>& tsegs,
                      std::vector<SeqView>& qsegs, const Pattern& pat, const gxy_search_params& p, bool use_graph,
                      RunResult& out) {
@@ -355,6 +388,10 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     {
         double est = 1 << 20;
         for (const UnitPlan& u : units) est += 1.5 * (double)u.nwin * sa.n_var * u.avg_bucket;
+        // Candidates from the same estimate (a few percent of the raw hits
+        // pass the screen): an overflow would rerun the whole launch.
+        const uint64_t want_cand = std::min<uint64_t>((uint64_t)(est / kHitsPerCandidate), kMaxPresizedCandidates);
+        if (want_cand > W->cand_cap) W->cand_cap = (uint32_t)want_cand;
         if (est > (double)W->hit_cap) {
             if (est <= (double)kMaxHitCap) {
                 W->hits.release();
@@ -398,6 +435,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         return e;
     };
 
+    uint32_t reruns = 0;   // pipeline runs (or passes) repeated after a buffer grew
     for (int attempt = 0; attempt < 16; attempt++) {
         uint32_t cap = W->cand_cap;
         GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
@@ -478,6 +516,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                     sa.cand_cap = cap;
                     GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
                     GXY_CK(cudaStreamSynchronize(st));
+                    reruns++;
                     continue;
                 }
                 if (nh > W->hit_cap) {
@@ -489,6 +528,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                     GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
                     GXY_CK(cudaStreamSynchronize(st));
                     pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)(t1 - t0) * W->hit_cap / nh * 0.8));
+                    reruns++;
                     continue;
                 }
                 t0 = t1;
@@ -649,6 +689,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                 W->hit_cap = kMaxHitCap;
                 pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / nhits * 0.8));
             }
+            reruns++;
             continue;
         }
         if (ncand > cap) {
@@ -659,6 +700,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                 return GXY_EUNSUPPORTED;
             }
             W->cand_cap = (uint32_t)nc;
+            reruns++;
             continue;
         }
         const uint32_t nh = hc[kCHsps];
@@ -677,6 +719,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.enum_ms = single ? ms_enum : 0.0;
         out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;
         out.stats.passes = single ? 1 : (uint32_t)((tiles + pass_tiles - 1) / pass_tiles);
+        out.stats.reruns = reruns;
         if (records) {
             const uint32_t nr = hc[kCRecs];
             out.records.resize(nr);

@@ -72,6 +72,10 @@ struct UnitPlan {
 constexpr uint32_t kCTile = 0, kCHsps = 2, kCRecs = 4, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072,
                    kCWalk = 3584;
 constexpr uint32_t kCounterWords = 4096;
+// Candidate arrays are sized up front at one candidate per this many
+// estimated raw hits (the estimate carries a 1.5x margin), up to a bound.
+constexpr uint64_t kHitsPerCandidate = 16;
+constexpr uint64_t kMaxPresizedCandidates = 1ull << 24;
 
 struct RunResult {
     std::vector<gxy_hsp> hsps;
@@ -155,6 +159,10 @@ SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi);
 gxy_status check_params(const gxy_search_params* p, uint64_t max_cols);
 
 // Runs units through screen -> sort -> walk -> compaction on worker W.
+// Grows a worker's raw-hit and candidate buffers (and its pinned result
+// staging) to at least the given sizes now, so that no later call pays for
+// the allocation.
+gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t hits, uint64_t candidates);
 gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units, std::vector<SeqView>& tsegs,
                      std::vector<SeqView>& qsegs, const Pattern& pat, const gxy_search_params& p, bool use_graph,
                      RunResult& out);

@@ -67,6 +67,7 @@ struct gxy_server {
     uint64_t bytes_in_use = 0;
     uint64_t units_in_flight = 0;
     uint32_t big_in_flight = 0;
+    uint32_t started = 0;               // dispatchers past their start-up (worker and warm buffers)
     gxy_server_stats st{};
     // Device free memory as last queried (cudaMemGetInfo costs tens of us):
     // refreshed at most every 20 ms, and reduced meanwhile by what was
@@ -146,6 +147,11 @@ gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
     if (e == GXY_OK) e = run_units(s->ctx, W, plan, tsegs, qsegs, pat, s->params, false, res);
     cleanup();
     if (e != GXY_OK) return e;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->st.reruns += res.stats.reruns;
+        s->st.busy_ms += res.stats.device_ms;
+    }
     for (size_t i = 0; i < res.hsps.size(); i++) {
         const auto& o = unit_owner[res.unit[i]];
         (o.second ? batch[o.first]->minus : batch[o.first]->plus).push_back(res.hsps[i]);
@@ -165,10 +171,29 @@ void dispatcher(gxy_server* s) {
             q->done_at = Clock::now();
         }
         s->pending.clear();
+        s->started++;
         s->cv_done.notify_all();
         return;
     }
     const uint32_t strands = s->opts.both_strands ? 2 : 1;
+    if (s->opts.warm_bases) {
+        // The raw-hit estimate run_units makes for a query of warm_bases on
+        // the largest table (windows x variants x mean bucket, 1.5x margin).
+        const Pattern& pat = s->tables[0]->pat;
+        const uint32_t w = pat.weight;
+        const double n_var = 1.0 + (s->params.transitions >= 1 ? w : 0) +
+                             (s->params.transitions >= 2 ? w * (w - 1) / 2.0 : 0.0);
+        double avg = 0.0;
+        for (const gxy_table* t : s->tables)
+            if (t->num_words) avg = std::max(avg, (double)t->npos / (double)t->num_words);
+        const double est = (double)(1 << 20) + 1.5 * (double)s->opts.warm_bases * n_var * avg * strands;
+        reserve_worker(s->ctx, W, (uint64_t)est, (uint64_t)(est / kHitsPerCandidate));
+    }
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->started++;
+    }
+    s->cv_done.notify_all();
     for (;;) {
         std::vector<Request*> batch;
         bool batch_big = false;
@@ -297,6 +322,11 @@ gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* c
     if (!o.max_big_inflight) o.max_big_inflight = 1;
     s->opts = o;
     for (uint32_t i = 0; i < o.max_streams; i++) s->threads.emplace_back(dispatcher, s);
+    if (o.warm_bases) {
+        // Return once every dispatcher holds its warmed buffers.
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_done.wait(lk, [&] { return s->started >= o.max_streams; });
+    }
     *out = s;
     return GXY_OK;
 }

@@ -15,14 +15,15 @@ class Server:
 
     def __init__(self, tables: Sequence, matrix, params, max_device_bytes: int = 8 << 30, max_units: int = 4096,
                  max_streams: int = 2, max_batch_units: int = 256, both_strands: bool = True,
-                 max_batch_bases: int = 16 << 20, big_bases: int = 1 << 20, max_big_inflight: int = 1):
+                 max_batch_bases: int = 16 << 20, big_bases: int = 1 << 20, max_big_inflight: int = 1,
+                 warm_bases: int = 0):
         from . import _params_c
         self.ctx = tables[0].ctx
         self._tables = list(tables)
         th = (C.c_void_p * len(tables))(*[t.h for t in tables])
         p = _params_c(matrix, params)
         o = _lib.ServerOptsC(max_device_bytes, max_units, max_streams, max_batch_units, 1 if both_strands else 0,
-                              max_batch_bases, big_bases, max_big_inflight, 0)
+                              max_batch_bases, big_bases, max_big_inflight, 0, warm_bases)
         h = C.c_void_p()
         check(lib().gxy_server_create(self.ctx.h, len(tables), th, C.byref(p), C.byref(o), C.byref(h)))
         self.h = h
@@ -45,7 +46,8 @@ class Server:
         s = _lib.ServerStatsC()
         check(lib().gxy_server_get_stats(self.h, C.byref(s)))
         return {"submitted": s.submitted, "completed": s.completed, "batches": s.batches,
-                "max_inflight_units": s.max_inflight_units, "bytes_in_use": s.bytes_in_use}
+                "max_inflight_units": s.max_inflight_units, "bytes_in_use": s.bytes_in_use, "reruns": s.reruns,
+                "busy_ms": s.busy_ms}
 
     def close(self) -> None:
         if self.h:
