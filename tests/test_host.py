@@ -116,3 +116,44 @@ def test_best_chain_matches_quadratic_reference(gxy):
         h["score"] = rng.choice([100, 200, 300, -50, 0], n) if trial % 3 else rng.integers(-100, 1000, n)
         got = [tuple(int(x) for x in r) for r in gxy.best_chain(h)]
         assert got == O.best_chain(h), trial
+
+
+def test_ctypes_layouts_match_the_header(gxy, tmp_path):
+    """Every ctypes mirror of a C ABI struct has the size and field offsets
+    that a C compiler gives the struct in include/gxy_seed.h."""
+    import ctypes as C
+    import subprocess
+    from lastz_gxy_b200 import _lib
+    pairs = {"gxy_packed_seq": _lib.PackedSeqC, "gxy_search_params": _lib.SearchParamsC, "gxy_hsp": _lib.HspC,
+             "gxy_hsp_buf": _lib.HspBufC, "gxy_stats": _lib.StatsC, "gxy_seq_set": _lib.SeqSetC,
+             "gxy_tuning": _lib.TuningC, "gxy_unit": _lib.UnitC, "gxy_batch_result": _lib.BatchResultC,
+             "gxy_unit_place": _lib.PlaceC, "gxy_record_result": _lib.RecordResultC,
+             "gxy_batch_opts": _lib.BatchOptsC, "gxy_server_opts": _lib.ServerOptsC,
+             "gxy_server_stats": _lib.ServerStatsC}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gxy_seed.h"', 'int main(void) {']
+    for cname, py in pairs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    for cname, dt in (("gxy_hsp", gxy.HSP_DTYPE), ("gxy_record", gxy.RECORD_DTYPE)):
+        lines.append(f'printf("{cname} npsize %zu\\n", sizeof({cname}));')
+        for fname in dt.names:
+            lines.append(f'printf("{cname} np_{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        a, b, v = line.split()
+        got[(a, b)] = int(v)
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+    for cname, dt in (("gxy_hsp", gxy.HSP_DTYPE), ("gxy_record", gxy.RECORD_DTYPE)):
+        assert got[(cname, "npsize")] == dt.itemsize, cname
+        for fname in dt.names:
+            assert got[(cname, "np_" + fname)] == dt.fields[fname][1], (cname, fname)
