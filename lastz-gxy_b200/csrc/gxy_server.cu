@@ -213,11 +213,14 @@ void dispatcher(gxy_server* s) {
             uint64_t batch_units = 0, batch_bases = 0;
             // Arrival order, except that a big request waits in place (and
             // the smaller ones behind it go ahead) while the big slots are
-            // taken; a big request always runs in a batch of its own.
+            // taken; a big request always runs in a batch of its own.  A
+            // batch holds requests of one table only: the table's bucket
+            // bounds then stay in L2 for the whole launch.
             for (auto it = s->pending.begin(); it != s->pending.end();) {
                 Request* q = *it;
                 const bool big = q->len >= s->opts.big_bases;
-                if (big && (!batch.empty() || s->big_in_flight >= s->opts.max_big_inflight)) {
+                if ((big && (!batch.empty() || s->big_in_flight >= s->opts.max_big_inflight)) ||
+                    (!batch.empty() && q->table != batch[0]->table)) {
                     ++it;
                     continue;
                 }
