@@ -69,12 +69,13 @@ struct gxy_server {
     uint32_t big_in_flight = 0;
     uint32_t started = 0;               // dispatchers past their start-up (worker and warm buffers)
     gxy_server_stats st{};
-    // Device free memory as last queried (cudaMemGetInfo costs tens of us):
-    // refreshed at most every 20 ms, and reduced meanwhile by what was
-    // admitted since the query.
-    size_t free_seen = 0;
-    uint64_t in_use_seen = 0;
-    std::chrono::steady_clock::time_point free_at{};
+    // Free device memory: cudaMemGetInfo once at creation (it can take tens
+    // of milliseconds while the device works, so it stays off the dispatch
+    // path), then less whatever the allocation pool has reserved since --
+    // a host-side counter.
+    size_t free_at_create = 0;
+    uint64_t pool_at_create = 0;
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -201,15 +202,13 @@ void dispatcher(gxy_server* s) {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
             if (s->stop && s->pending.empty()) break;
-            const auto now = Clock::now();
-            if (s->free_at == Clock::time_point{} || now - s->free_at > std::chrono::milliseconds(20)) {
-                size_t total_b = 0;
-                cudaMemGetInfo(&s->free_seen, &total_b);
-                s->in_use_seen = s->bytes_in_use;
-                s->free_at = now;
-            }
-            const uint64_t grown = s->bytes_in_use > s->in_use_seen ? s->bytes_in_use - s->in_use_seen : 0;
-            size_t free_b = s->free_seen > grown ? s->free_seen - grown : 0;
+            // Free memory now: what was free at creation, less the pool's
+            // growth since, less the estimates of the requests in flight
+            // (their buffers may not be allocated yet).
+            uint64_t reserved = 0;
+            if (s->pool) cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+            const uint64_t grown = (reserved > s->pool_at_create ? reserved - s->pool_at_create : 0) + s->bytes_in_use;
+            size_t free_b = s->free_at_create > grown ? s->free_at_create - grown : 0;
             uint64_t batch_units = 0, batch_bases = 0;
             // Arrival order, except that a big request waits in place (and
             // the smaller ones behind it go ahead) while the big slots are
@@ -313,6 +312,14 @@ gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* c
     }
     gxy_server* s = new gxy_server();
     s->ctx = ctx;
+    {
+        cudaSetDevice(ctx->device);
+        size_t total_b = 0;
+        if (cudaMemGetInfo(&s->free_at_create, &total_b) != cudaSuccess) s->free_at_create = SIZE_MAX;
+        if (cudaDeviceGetDefaultMemPool(&s->pool, ctx->device) != cudaSuccess) s->pool = nullptr;
+        if (s->pool) cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &s->pool_at_create);
+        cudaGetLastError();
+    }
     s->tables.assign(tables, tables + n_tables);
     s->params = *params;
     gxy_server_opts o = opts ? *opts : gxy_server_opts{};
