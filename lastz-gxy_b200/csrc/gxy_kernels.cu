@@ -905,6 +905,30 @@ __device__ __forceinline__ void pk_step(PkSide& S, int32_t T, const int32_t* plu
     S.b = max(S.b, S.p);
 }
 
+// Column k of a side that cannot break yet (no x-drop test).
+template <int k>
+__device__ __forceinline__ void pk_step_free(PkSide& S, const int32_t* plut) {
+    const uint32_t idx = (uint32_t)(((k & 1) ? S.o : S.e) >> (4 * (k >> 1))) & 15u;
+    S.p += plut[idx];
+    S.b = max(S.b, S.p);
+}
+
+// The fast path with side B fresh: its first kFree columns cannot reach the
+// x-drop (each column lowers p by at most 256 * |min score| + 1), so they skip
+// the test.  A dead B (no columns) is updated too, but its result is unused.
+template <int kFree>
+__device__ __forceinline__ void pk_scan_pair_bfresh(PkSide& A, PkSide& B, int32_t T, const int32_t* plut,
+                                                    int32_t pamb) {
+#define GXY_PKF(k)                                                         \
+    pk_step<false, k>(A, T, plut, pamb);                                   \
+    if (k < kFree) pk_step_free<k>(B, plut); else pk_step<false, k>(B, T, plut, pamb);
+    GXY_PKF(0) GXY_PKF(1) GXY_PKF(2) GXY_PKF(3) GXY_PKF(4) GXY_PKF(5) GXY_PKF(6) GXY_PKF(7)
+    GXY_PKF(8) GXY_PKF(9) GXY_PKF(10) GXY_PKF(11) GXY_PKF(12) GXY_PKF(13) GXY_PKF(14) GXY_PKF(15)
+    GXY_PKF(16) GXY_PKF(17) GXY_PKF(18) GXY_PKF(19) GXY_PKF(20) GXY_PKF(21) GXY_PKF(22) GXY_PKF(23)
+    GXY_PKF(24) GXY_PKF(25) GXY_PKF(26) GXY_PKF(27) GXY_PKF(28) GXY_PKF(29) GXY_PKF(30) GXY_PKF(31)
+#undef GXY_PKF
+}
+
 // Both sides column by column in lockstep: two independent serial chains.
 template <bool kSlow>
 __device__ __forceinline__ void pk_scan_pair(PkSide& A, PkSide& B, int32_t T, const int32_t* plut, int32_t pamb) {
@@ -976,6 +1000,11 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     const int32_t ambig = a.sc.ambig, thresh = a.sc.hspthresh;
     const int32_t pamb = ambig * 256 - 1;
     const int32_t T = (a.sc.xdrop + 1) * 256;
+    // Columns a fresh side scans before its first possible break.
+    int32_t worst = a.sc.ambig;
+    for (int i = 0; i < 16; i++) worst = min(worst, a.sc.sub[i]);
+    const int32_t per_col = worst < 0 ? 256 * (-worst) + 1 : 1;
+    const int free_cols = (int)min(8, (T - 1) / per_col);
     const uint32_t seed_mask = L >= 32 ? 0xffffffffu : ((1u << L) - 1u);
     // No seed footprint scores above this: a hit whose two sides' bests stay
     // below thresh - seed_ub can never pass, whatever its seed scores.
@@ -1097,6 +1126,7 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
             const bool slow = (an != 0 && (an < 32 || avv != 0xffffffffu)) ||
                               (bn != 0 && (bn < 32 || bvv != 0xffffffffu));
             if (__any_sync(kFull, slow)) pk_scan_pair<true>(A, B, T, s_plut, pamb);
+            else if (free_cols >= 7) pk_scan_pair_bfresh<7>(A, B, T, s_plut, pamb);
             else pk_scan_pair<false>(A, B, T, s_plut, pamb);
             if (an) {
                 const uint32_t used = ((uint32_t)a0 & 255u) - ((uint32_t)A.p & 255u);
