@@ -73,9 +73,11 @@ constexpr uint32_t kCTile = 0, kCHsps = 2, kCRecs = 4, kCStats = 8, kCCand = 102
                    kCWalk = 3584;
 constexpr uint32_t kCounterWords = 4096;
 // Candidate arrays are sized up front at one candidate per this many
-// estimated raw hits (the estimate carries a 1.5x margin), up to a bound.
-constexpr uint64_t kHitsPerCandidate = 16;
-constexpr uint64_t kMaxPresizedCandidates = 1ull << 24;
+// estimated raw hits (the estimate carries a 1.5x margin; about 3 % of raw
+// hits become candidates), up to a bound.  Larger arrays also widen the
+// capacity-sized sort and scan grids of every later launch on the worker.
+constexpr uint64_t kHitsPerCandidate = 32;
+constexpr uint64_t kMaxPresizedCandidates = 1ull << 22;
 
 struct RunResult {
     std::vector<gxy_hsp> hsps;
