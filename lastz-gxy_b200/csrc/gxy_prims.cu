@@ -87,7 +87,7 @@ __global__ __launch_bounds__(kScanThreads) void k_scan_reduce(const T* in, const
 }
 
 // Single-block exclusive scan of a short array in place (the block sums of a
-// scan, or the digit-major histograms of a radix pass); a[n] = total.  Each
+// scan); a[n] = total.  Each
 // warp owns a contiguous run of 256-element chunks; a lane holds 8
 // consecutive elements (two 16-byte loads when a is 16-byte aligned), so
 // every warp access is one contiguous kilobyte.
@@ -284,6 +284,25 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_hist(const K* keys, cons
     }
 }
 
+// One block per digit d: exclusive scan, in place, of the digit's per-block
+// counts hist[d * grid .. + grid), and totals[d] = their sum.  The scatter
+// adds the digits' exclusive prefix over totals (radix entries) itself, so
+// no single block has to scan the whole radix x grid histogram.
+__global__ __launch_bounds__(256) void k_radix_digit_scan(uint32_t* hist, int grid, uint32_t* totals) {
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_total;
+    uint32_t* h = hist + (uint64_t)blockIdx.x * grid;
+    uint32_t carry = 0;
+    for (int base = 0; base < grid; base += 256) {
+        const int i = base + (int)threadIdx.x;
+        const uint32_t v = i < grid ? h[i] : 0u;
+        const uint32_t ex = block_excl_scan<256>(v, s_warp, &s_total);
+        if (i < grid) h[i] = carry + ex;
+        carry += s_total;
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
 template <typename K>
 struct SortSmem {
     K keys[kSortTile];
@@ -300,7 +319,8 @@ template <typename K>
 __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                                  K* __restrict__ kout, uint32_t* __restrict__ vout,
                                                                  const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
-                                                                 int shift, int bits, const uint32_t* hist) {
+                                                                 int shift, int bits, const uint32_t* hist,
+                                                                 const uint32_t* totals) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
     const uint64_t n = read_n(n_dev, n_host, n_cap);
@@ -310,8 +330,15 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(const K* __restr
     const uint32_t lt = lanemask_lt();
     uint64_t beg, end;
     block_range(n, kSortTile, beg, end);
-    for (int d = threadIdx.x; d < kRadixMax; d += kSortThreads)
-        S.off[d] = d < radix ? hist[(uint64_t)d * gridDim.x + blockIdx.x] : 0u;
+    {
+        // Output offset of digit d for this block: all smaller digits' totals
+        // plus digit d's count in the blocks before this one.
+        static_assert(kSortThreads == kRadixMax, "one thread per digit");
+        const int d = threadIdx.x;
+        const uint32_t t = d < radix ? totals[d] : 0u;
+        const uint32_t g = block_excl_scan<kSortThreads>(t, S.warp_tmp, &S.total);
+        S.off[d] = d < radix ? g + hist[(uint64_t)d * gridDim.x + blockIdx.x] : 0u;
+    }
     for (uint64_t tb = beg; tb < end; tb += kSortTile) {
         for (int i = threadIdx.x; i < kSortWarps * kRadixMax; i += kSortThreads) (&S.wcnt[0][0])[i] = 0;
         __syncthreads();
@@ -385,8 +412,8 @@ int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, 
                const RadixPass* passes, int npass, const PrimScratch& ps, cudaStream_t st) {
     const size_t smem = sizeof(SortSmem<K>);
     // Blocks: enough for every block to own about two tiles at capacity, so
-    // that large sorts fill the GPU and small ones keep their digit-major
-    // histogram (radix x grid entries, scanned by one block) short.
+    // that large sorts fill the GPU and small ones keep their per-digit
+    // histogram scans (grid entries each) short.
     const uint64_t want = (n_cap + 2 * (uint64_t)kSortTile - 1) / (2 * (uint64_t)kSortTile);
     const int cap_grid = ps.sort_grid_max > 0 ? ps.sort_grid_max : ps.grid;
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)cap_grid));
@@ -400,10 +427,11 @@ int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, 
         k_radix_hist<K><<<grid, kSortThreads, 0, st>>>(kin, n_dev, n_host, n_cap, passes[p].shift,
                                                        passes[p].bits, ps.hist);
         count_launch();
-        k_scan_small<<<1, 1024, 0, st>>>(ps.hist, radix * grid);
+        k_radix_digit_scan<<<radix, 256, 0, st>>>(ps.hist, grid, ps.block_sums);
         count_launch();
         k_radix_scatter<K><<<grid, kSortThreads, smem, st>>>(kin, vin, kout, vout, n_dev, n_host, n_cap,
-                                                             passes[p].shift, passes[p].bits, ps.hist);
+                                                             passes[p].shift, passes[p].bits, ps.hist,
+                                                             ps.block_sums);
         K* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }

@@ -4,8 +4,9 @@
 // so a pipeline whose sizes are only known on the device (the candidate count
 // after the screen) needs no host round trip and can be captured in a graph.
 // Every block owns one contiguous range of the input; the radix sort's
-// per-block digit histograms are scanned digit-major, and each block ranks its
-// tiles with warp match-any so equal digits keep their input order (stable).
+// per-block digit histograms are scanned one digit per block, and each block
+// ranks its tiles with warp match-any so equal digits keep their input order
+// (stable).
 #pragma once
 
 #include <cstdint>
@@ -23,7 +24,7 @@ constexpr int kRadixMax = 256;
 
 // Scratch a caller provides for the primitives (device memory).
 struct PrimScratch {
-    uint32_t* block_sums;   // >= max(grid, sort_grid_max) entries (+1)
+    uint32_t* block_sums;   // >= max(grid, sort_grid_max, kRadixMax) entries (+1)
     uint32_t* hist;         // >= kRadixMax * max(grid, sort_grid_max) entries (+1)
     int grid;               // scan blocks (at most max(grid, sort_grid_max), sized by the capacity)
     int sort_grid_max;      // radix passes use min(this, one block per two tiles of n_cap) blocks
