@@ -1304,8 +1304,35 @@ __global__ __launch_bounds__(WARPS * 32) void k_walk(const __grid_constant__ Wal
         if ((uint64_t)r * 32 >= n) break;
         const uint32_t i = r * 32 + lane;
         bool head = false;
-        if (i < n) head = (i == 0) || ((a.keys[i] >> 32) != (a.keys[i - 1] >> 32));
-        uint32_t hb = __ballot_sync(kFull, head);
+        uint32_t key_hi = 0;
+        if (i < n) {
+            key_hi = (uint32_t)(a.keys[i] >> 32);
+            head = (i == 0) || (key_hi != (uint32_t)(a.keys[i - 1] >> 32));
+        }
+        // A diagonal segment of one candidate needs no walk: nothing can
+        // cover it, so it is kept when it passes.  Its own lane settles it
+        // when its extension is already exact (not a long candidate, and no
+        // entropy gate, which takes the whole warp).
+        bool alone = false;
+        if (head && !a.has_entropy) {
+            const bool tail = (i + 1 >= n) || (key_hi != (uint32_t)(a.keys[i + 1] >> 32));
+            if (tail) {
+                const Cand c = a.cands[a.idx[i]];
+                if (!(c.flags & kCandLong)) {
+                    alone = true;
+                    if (c.score >= a.sc.hspthresh) {
+                        const UnitDev U = a.units[c.unit];
+                        const uint32_t ts = c.t - c.lext, len = a.seed_len + c.lext + c.rext;
+                        Hsp o;
+                        o.t_start = ts; o.q_start = c.q - c.lext; o.length = len; o.score = c.score;
+                        a.out_hsp[i] = o;
+                        a.out_flag[i] = (U.primary_hi <= U.primary_lo || (ts >= U.primary_lo && ts < U.primary_hi))
+                                            ? 1 : 0;
+                    }
+                }
+            }
+        }
+        uint32_t hb = __ballot_sync(kFull, head && !alone);
         while (hb) {
             const uint32_t h = r * 32 + (uint32_t)(__ffs(hb) - 1);
             hb &= hb - 1;

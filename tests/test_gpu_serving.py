@@ -96,6 +96,17 @@ def test_big_requests_run_alone_and_small_ones_go_ahead(gxy, setup):
         assert ref[i][0].tobytes() == mix[i][0].tobytes() and ref[i][1].tobytes() == mix[i][1].tobytes(), i
 
 
+def test_warm_buffers_and_stats(gxy, setup):
+    # warm_bases sizes every dispatcher's buffers at creation; results do not
+    # change, and no batch has to rerun after a buffer grew.
+    targets, tables, reqs = setup
+    ref, _ = run_server(gxy, tables, reqs[:8], "alone")
+    warm, st = run_server(gxy, tables, reqs[:8], "mix", max_streams=2, warm_bases=max(len(q) for _, q in reqs))
+    assert st["completed"] == 8 and st["reruns"] == 0 and st["busy_ms"] > 0
+    for i in range(8):
+        assert ref[i][0].tobytes() == warm[i][0].tobytes() and ref[i][1].tobytes() == warm[i][1].tobytes()
+
+
 def test_wait_timeout_and_unknown_id(gxy, setup):
     _, tables, reqs = setup
     srv = gxy.Server(tables, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams())
