@@ -609,7 +609,7 @@ def run_chunked(args):
     for tr in (1, 0):
         sp = g.SearchParams(transitions=tr)
         tune = autotune(ctx, tabs, [dQ], units, m, sp, workload="chunked", sample_units=4, reps=1, use_cache=False,
-                        space={"screen_blocks_per_sm": [4, 3], "screen_cap": [128, 64]})
+                        space={"screen_blocks_per_sm": [4, 3], "screen_cap": [192, 128]})
         st = {}
         ctx.mark(10)
         got = g.batch_search(tabs, [dQ], units, m, sp, stats=st, ctx=ctx)

@@ -19,7 +19,7 @@ from typing import Optional
 DEFAULT_SPACE = {
     "screen_warps": [8, 16],
     "screen_blocks_per_sm": [4, 3],
-    "screen_cap": [128, 64, 192],
+    "screen_cap": [192, 128, 64],
     "walk_warps": [8, 4],
 }
 
