@@ -13,7 +13,8 @@ value: device-resident inputs, CUDA-event time of each step on the library's
 primary stream, L2 flushed between steps (the step's working set, ~100 MB,
 fits in the 126 MB L2).  e2e: the same step through the public C ABI from host
 buffers (target and query PackedSeq copied in from pinned host memory each
-step, HSPs copied out).  The two strands' search() calls run concurrently
+step, the query from a second host thread while the table builds; HSPs
+copied out).  The two strands' search() calls run concurrently
 from two host threads, each on its own stream, as the reference's driver
 runs its (chunk, query, strand) units in parallel on a shared table.
 
@@ -241,8 +242,9 @@ def run_ours(args, rank: int, world: int, device: int):
         table_ms.append(ctx.elapsed_ms(2, 3))   # read after the frees (which synchronise) so no extra wait
 
     def step_e2e(collect):
+        fq = pool.submit(Q.to_device, ctx)                    # host query -> device (second thread)
         tab = g.PosTable.build(T, P12, 1, ctx=ctx)          # host target -> device, PosTable::build
-        dq = Q.to_device(ctx)                                 # host query -> device
+        dq = fq.result()
         dqr = dq.reverse_complement()
         n = 0
         for _, h in both_strands(tab, (dq, dqr)):             # HSPs come back to host
