@@ -191,13 +191,13 @@ __device__ __forceinline__ LaneExt extend_lane(const SeqView& T, const SeqView& 
 }
 
 // ---------------------------------------------------------------------------
-// Warp-cooperative x-drop: one warp per hit, 32 columns per step, the x-drop
-// cut found with shuffle scans.  Column k of a step breaks the reference's
+// Warp-cooperative x-drop: one warp per hit, 64 columns per step (two per
+// lane), the x-drop cut found with shuffle scans.  Column k of a step breaks the reference's
 // loop iff run_k <= PM_{k-1} and PM_{k-1} - run_k > xdrop, where
 // PM_{k-1} = max(best, run_0..run_{k-1}); the best extent is the first column
 // whose running score equals the step's maximum (the reference updates only
 // on a strict increase).  Sequence bytes are staged through shared memory in
-// 16-byte vector loads, kStageCols columns per refill.
+// 16-byte vector loads: kStageSpan positions per refill.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kStageCols = 1024;
 constexpr uint32_t kStageSpan = kStageCols + 128;          // positions staged per refill
@@ -233,46 +233,56 @@ template <bool kForward>
 __device__ void side_warp(const SeqView& T, const SeqView& Q, uint32_t t0, uint32_t q0,
                           uint32_t maxext, int32_t xdrop, const int32_t* lut, int32_t ambig,
                           WarpStage* st, int32_t& best_out, uint32_t& bext_out) {
+    // 64 columns per step: lane l scores columns 2l and 2l+1.  A refill
+    // stages 1,152 positions, enough for 15 steps (960 columns) with every
+    // lane's 32-position funnel read inside the stage.
+    constexpr uint32_t kSteps = 960;
     const int lane = threadIdx.x & 31;
     int32_t run = 0, best = 0;
     uint32_t bext = 0, ext = 0;
     uint64_t ta = 0, qa = 0;   // staged windows' first global positions
     uint32_t staged = 0;       // columns left in the current stage
+    const uint32_t c0 = 2u * (uint32_t)lane, c1 = c0 + 1;
     while (ext < maxext) {
-        const uint64_t tg = kForward ? T.base + t0 + ext : T.base + t0 - ext - 31;
-        const uint64_t qg = kForward ? Q.base + q0 + ext : Q.base + q0 - ext - 31;
-        if (staged < 32) {
-            // Refill so that the next kStageCols columns lie inside the stage.
+        // The step's 64 positions: [tg, tg + 64).
+        const uint64_t tg = kForward ? T.base + t0 + ext : T.base + t0 - ext - 63;
+        const uint64_t qg = kForward ? Q.base + q0 + ext : Q.base + q0 - ext - 63;
+        if (staged < 64) {
             __syncwarp();
             if (kForward) {
                 ta = tg & ~127ull;
                 qa = qg & ~127ull;
             } else {
-                const uint64_t tl = tg + 31 >= kStageCols ? tg + 31 - (kStageCols - 1) : 0;
-                const uint64_t ql = qg + 31 >= kStageCols ? qg + 31 - (kStageCols - 1) : 0;
+                const uint64_t tl = tg + 63 >= kSteps ? tg + 63 - (kSteps - 1) : 0;
+                const uint64_t ql = qg + 63 >= kSteps ? qg + 63 - (kSteps - 1) : 0;
                 ta = tl & ~127ull;
                 qa = ql & ~127ull;
             }
             stage_fill(T.codes, T.valid, ta, st->tcodes, st->tvalid, lane);
             stage_fill(Q.codes, Q.valid, qa, st->qcodes, st->qvalid, lane);
             __syncwarp();
-            staged = kStageCols;
+            staged = kSteps;
         }
-        const uint32_t to = (uint32_t)(tg - ta), qo = (uint32_t)(qg - qa);
+        // This lane's two columns sit at window offsets c0, c1 (forward) or
+        // 63 - c0, 63 - c1 (backward): one funnel read from the lower one.
+        const uint32_t lo = kForward ? c0 : 62u - c0;
+        const uint32_t to = (uint32_t)(tg - ta) + lo, qo = (uint32_t)(qg - qa) + lo;
         const uint64_t tc = stage_codes32(st->tcodes, to);
         const uint64_t qc = stage_codes32(st->qcodes, qo);
         const uint32_t vv = stage_bits32(st->tvalid, to) & stage_bits32(st->qvalid, qo);
-        const uint32_t n = min(32u, maxext - ext);
-        const int sh = kForward ? lane : 31 - lane;
-        const bool act = (uint32_t)lane < n;
-        int32_t x = act ? col_score(tc, qc, vv, sh, lut, ambig) : 0;
+        const uint32_t n = min(64u, maxext - ext);
+        const bool a0 = c0 < n, a1 = c1 < n;
+        const int32_t x0 = a0 ? col_score(tc, qc, vv, kForward ? 0 : 1, lut, ambig) : 0;
+        const int32_t x1 = a1 ? col_score(tc, qc, vv, kForward ? 1 : 0, lut, ambig) : 0;
+        int32_t x = x0 + x1;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int32_t y = __shfl_up_sync(kFull, x, o);
             if (lane >= o) x += y;
         }
-        const int32_t r = run + x;
-        int32_t m = act ? r : INT32_MIN;
+        const int32_t r1 = run + x;      // running score after column c1
+        const int32_t r0 = r1 - x1;      // after column c0
+        int32_t m = a0 ? (a1 ? max(r0, r1) : r0) : INT32_MIN;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int32_t y = __shfl_up_sync(kFull, m, o);
@@ -280,22 +290,36 @@ __device__ void side_warp(const SeqView& T, const SeqView& Q, uint32_t t0, uint3
         }
         int32_t pm = __shfl_up_sync(kFull, m, 1);
         if (lane == 0) pm = INT32_MIN;
-        pm = max(pm, best);
-        const bool brk = act && r <= pm && (pm - r > xdrop);
-        const uint32_t bm = __ballot_sync(kFull, brk);
-        const uint32_t nproc = bm ? (uint32_t)(__ffs(bm) - 1) : n;
-        int32_t c = ((uint32_t)lane < nproc) ? r : INT32_MIN;
+        pm = max(pm, best);              // prefix maximum before column c0
+        const bool brk0 = a0 && r0 <= pm && (pm - r0 > xdrop);
+        const int32_t pm1 = max(pm, r0); // before column c1
+        const bool brk1 = a1 && r1 <= pm1 && (pm1 - r1 > xdrop);
+        const uint32_t bm = __ballot_sync(kFull, brk0 || brk1);
+        uint32_t nproc = n;              // columns before the break column
+        if (bm) {
+            const int bl = __ffs(bm) - 1;
+            const bool b0 = __shfl_sync(kFull, brk0, bl);
+            nproc = 2u * (uint32_t)bl + (b0 ? 0u : 1u);
+        }
+        int32_t c = INT32_MIN;
+        if (c0 < nproc) c = r0;
+        if (c1 < nproc) c = max(c, r1);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(kFull, c, o));
         if (c > best) {
-            const uint32_t eq = __ballot_sync(kFull, (uint32_t)lane < nproc && r == c);
-            bext = ext + (uint32_t)__ffs(eq);
+            // The first column that reaches the step's maximum.
+            const bool e0 = c0 < nproc && r0 == c;
+            const bool e1 = c1 < nproc && r1 == c;
+            const uint32_t eq = __ballot_sync(kFull, e0 || e1);
+            const int el = __ffs(eq) - 1;
+            const bool f0 = __shfl_sync(kFull, e0, el);
+            bext = ext + 2u * (uint32_t)el + (f0 ? 1u : 2u);
             best = c;
         }
         if (bm) break;
-        run = __shfl_sync(kFull, r, 31);
+        run = __shfl_sync(kFull, r1, 31);
         ext += n;
-        staged -= 32;
+        staged -= 64;
     }
     best_out = best;
     bext_out = bext;
