@@ -443,3 +443,40 @@ def best_chain(hsps) -> list:
         out.append(srt[c])
         c = parent[c]
     return out[::-1]
+
+
+def driver_records(entries) -> list:
+    """The driver's --nogapped post-processing of search() results.
+
+    entries: (target_index, query_index, strand, chunk_start, primary_lo,
+    primary_hi, hsps) per (chunk, query, strand) unit, in the order the units
+    completed.  Per unit: keep HSPs whose chunk-local t_start lies in
+    [primary_lo, primary_hi) (src/driver.rs:250-256) and build ungapped
+    records with t_start + chunk_start and t_span = q_span = length
+    (build_ungapped_record, src/driver.rs:437-468).  Units with records are
+    then ordered by (target, query, strand), stably (src/driver.rs:370-371),
+    and each unit's records are sorted by (t_start, q_start, t_span, q_span)
+    and consecutive duplicates of those fields (and the strand) dropped,
+    keeping the first (src/driver.rs:373-389), before the units' lists are
+    concatenated.  Returns (target, query, strand, t_start, q_start, span,
+    score) tuples."""
+    grouped = []
+    for ti, qi, strand, chunk_start, plo, phi, hsps in entries:
+        recs = []
+        for h in hsps:
+            t, q, length, score = (int(x) for x in h)
+            if plo <= t < phi:
+                recs.append(((t + chunk_start) & 0xFFFFFFFF, q, length, length, score))
+        if recs:
+            grouped.append((ti, qi, strand, recs))
+    grouped.sort(key=lambda g: (g[0], g[1], g[2]))   # stable, like sort_by_key
+    out = []
+    for ti, qi, strand, recs in grouped:
+        recs.sort(key=lambda r: r[:4])                # stable, like sort_by_key
+        kept = []
+        for r in recs:
+            if kept and kept[-1][:4] == r[:4]:
+                continue
+            kept.append(r)
+        out.extend((ti, qi, strand, r[0], r[1], r[2], r[4]) for r in kept)
+    return out

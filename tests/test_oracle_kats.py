@@ -253,3 +253,65 @@ def test_choose_anchor_known_answers():
 
 
 HOXD70_ROWS = [[91, -114, -31, -123], [-114, 100, -125, -31], [-31, -125, 100, -114], [-123, -31, -114, 91]]
+
+
+def test_driver_records_order_dedup_and_filter():
+    """The driver's record post-processing (src/driver.rs:250-256, :370-391,
+    :437-468): primary filter, global t, per-unit sort by (t, q, t_span,
+    q_span) and keep-first dedup, units in (target, query, strand) order."""
+    import oracle as O
+    entries = [
+        # (ti, qi, strand, chunk_start, plo, phi, hsps (t, q, len, score))
+        (0, 0, 1, 0, 0, 100, [(5, 7, 20, 3100)]),
+        (0, 0, 0, 100, 10, 60, [(30, 2, 20, 3200), (10, 1, 20, 3000), (9, 0, 20, 9999), (60, 0, 20, 9999),
+                                 (10, 1, 20, 3000), (10, 1, 21, 3050)]),
+        (0, 0, 0, 0, 0, 50, [(40, 3, 20, 3300)]),
+        (1, 0, 0, 0, 0, 100, []),
+    ]
+    got = O.driver_records(entries)
+    assert got == [
+        # (0,0,0): the chunk at 100 first (it completed first), then the chunk at 0
+        (0, 0, 0, 110, 1, 20, 3000), (0, 0, 0, 110, 1, 21, 3050), (0, 0, 0, 130, 2, 20, 3200),
+        (0, 0, 0, 40, 3, 20, 3300),
+        (0, 0, 1, 5, 7, 20, 3100),
+    ]
+
+
+def test_driver_records_chunk_order_equals_one_sort_per_group():
+    """With chunks completing in target order, the reference's per-unit sort
+    and concatenation equals one sort of each (target, query, strand) group:
+    primary regions are disjoint and ascending, so no record crosses a chunk
+    boundary.  This is the order gxy_batch_records produces."""
+    import random
+    import oracle as O
+    rng = random.Random(5)
+    primary, halo, tlen = 1000, 150, 4500
+    chunks = []
+    ps = 0
+    while ps < tlen:
+        pe = min(ps + primary, tlen)
+        lo, hi = max(ps - halo, 0), min(pe + halo, tlen)
+        chunks.append((lo, hi, ps - lo, pe - lo))
+        ps = pe
+    entries = []
+    for lo, hi, plo, phi in chunks:
+        for strand in (0, 1):
+            # Equal coordinates carry equal scores, as extensions of the same columns do.
+            hs = []
+            for _ in range(40):
+                t, q, ln = rng.randrange(0, hi - lo), rng.randrange(0, 3000), rng.randrange(19, 60)
+                hs.append((t, q, ln, 3000 + (t * 7 + q * 3 + ln) % 6000))
+            hs += hs[:5]   # repeats
+            entries.append((0, 0, strand, lo, plo, phi, hs))
+    got = O.driver_records(entries)
+    want = []
+    for strand in (0, 1):
+        recs = set()
+        for ti, qi, sd, lo, plo, phi, hs in entries:
+            if sd != strand:
+                continue
+            for t, q, ln, sc in hs:
+                if plo <= t < phi:
+                    recs.add((t + lo, q, ln, sc))
+        want.extend((0, 0, strand, t, q, ln, sc) for t, q, ln, sc in sorted(recs))
+    assert got == want
