@@ -157,3 +157,13 @@ def test_ctypes_layouts_match_the_header(gxy, tmp_path):
         assert got[(cname, "npsize")] == dt.itemsize, cname
         for fname in dt.names:
             assert got[(cname, "np_" + fname)] == dt.fields[fname][1], (cname, fname)
+
+
+def test_driver_harness_compiles_against_the_header(gxy, tmp_path):
+    """The C++ caller that mirrors the reference's driver builds against
+    include/gxy_seed.h and links the library (running it needs a GPU)."""
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    out = str(tmp_path / "driver_harness")
+    subprocess.run(["make", "-s", "-C", os.path.join(here, "harness"), f"OUT={out}"], check=True)
+    assert os.path.exists(out)
