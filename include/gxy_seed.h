@@ -4,7 +4,7 @@
  * The stage replaces, bit for bit, what the reference computes in
  *   PosTable::build            src/pos_table.rs:35-83
  *   PosTable::prune_hot_words  src/pos_table.rs:113-136
- *   seed_search::search        src/seed_search.rs:271-351
+ *   seed_search::search        src/seed_search.rs:45-125
  *     (DiagHash src/diag_hash.rs:34-53, extend_hit src/hsp.rs:66-211,
  *      extend_hit_avx2 src/hsp_simd.rs:27-243, entropy gate src/entropy.rs:27-67)
  * and is called where the reference's driver calls them (src/driver.rs:212-240,
@@ -69,7 +69,7 @@ typedef struct {
     int32_t xdrop;
     int32_t hspthresh;
     uint32_t step;
-    uint8_t transitions;   /* 0, 1, >=2 (treated as 2), src/seed_search.rs:295-316 */
+    uint8_t transitions;   /* 0, 1, >=2 (treated as 2), src/seed_search.rs:69-90 */
     uint8_t has_entropy;   /* entropy_threshold.is_some() */
     uint8_t pad_[2];
     int32_t entropy_thr;
@@ -88,7 +88,7 @@ typedef struct {
  * entries; when too small the call returns GXY_EOVERFLOW and len holds the
  * number needed.  HSPs come back in canonical order: by diagonal
  * (t_start - q_start), then t_start, length, score -- the reference sorts by
- * (diagonal, t_start) and dedups (src/seed_search.rs:348-349). */
+ * (diagonal, t_start) and dedups (src/seed_search.rs:122-123). */
 typedef struct {
     gxy_hsp* hsps;
     uint64_t len;
@@ -107,6 +107,9 @@ typedef struct {
     double enum_ms;        /* CUDA-event time of the hit enumeration kernel (single pass) */
     uint32_t passes;       /* window-range passes the raw hits needed */
     uint32_t reruns;       /* pipeline runs repeated after a buffer had to grow */
+    uint64_t survivors;    /* raw hits the upper-bound filter passed on to the exact screen
+                              (equal to raw_hits when the filter does not apply) */
+    uint64_t filter_columns; /* alignment columns the upper-bound filter scanned on the two sides */
 } gxy_stats;
 
 const char* gxy_status_string(gxy_status s);
@@ -119,8 +122,8 @@ uint64_t gxy_kernel_launches(void);
 gxy_status gxy_ctx_create(int device, gxy_ctx** out);
 gxy_status gxy_ctx_destroy(gxy_ctx* ctx);
 /* Tunables (screen kernel warps per block, column cap per side, screen blocks
- * per SM, walk warps per block, raw hits per pass).  Zero leaves a field
- * unchanged. */
+ * per SM, walk warps per block, raw hits per pass, the upper-bound filter's
+ * column cap and round size).  Zero leaves a field unchanged. */
 typedef struct {
     uint32_t screen_warps;
     uint32_t screen_cap;
@@ -129,6 +132,10 @@ typedef struct {
     uint32_t max_hits_per_pass;   /* raw-hit buffer bound; larger searches run in window passes */
     uint32_t initial_candidates;  /* candidate capacity every search starts from (grown on demand);
                                      0 in the context = keep what each stream's buffers grew to */
+    uint32_t filter_cap;          /* upper-bound filter: columns per side after which a hit is
+                                     passed on unexamined (a multiple of 32, 32..256) */
+    uint32_t filter_flush;        /* upper-bound filter: queued hits per warp that start a filter
+                                     round (32..512) */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
@@ -177,7 +184,7 @@ void gxy_seq_set_free(gxy_seq_set* set);
 /* ---- position table (src/pos_table.rs) --------------------------------- */
 /* PosTable::build(seq, pattern, step) followed, when max_word_count > 0, by
  * prune_hot_words(max_word_count) as the driver does (src/driver.rs:212-215).
- * pattern01 is the 0/1 seed pattern (src/seeds.rs:113-126), at most 32
+ * pattern01 is the 0/1 seed pattern (src/seeds.rs:38-51), at most 32
  * positions; weight <= 15 (2^30 buckets) is supported. */
 gxy_status gxy_table_build(gxy_ctx* ctx, const gxy_packed_seq* target, const char* pattern01,
                            uint32_t step, uint32_t max_word_count, gxy_table** out);
@@ -218,7 +225,7 @@ gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_p
 gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions);
 gxy_status gxy_table_free(gxy_table* t);
 
-/* ---- the drop-in search (src/seed_search.rs:271-351) --------------------- */
+/* ---- the drop-in search (src/seed_search.rs:45-125) --------------------- */
 /* seed_search::search(&table, &target, &query, &matrix, &params).  The
  * target must be the sequence the table was built from (the reference's
  * driver and tweener always pass the same one); it is re-read from host only

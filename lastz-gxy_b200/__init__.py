@@ -4,8 +4,8 @@ The names, argument meanings and error behaviour follow the reference's Rust
 API for this path:
 
     PosTable::build / prune_hot_words   src/pos_table.rs:35-136
-    seed_search::search                 src/seed_search.rs:271-351
-    SeedPattern                         src/seeds.rs:20-173
+    seed_search::search                 src/seed_search.rs:45-125
+    SeedPattern                         src/seeds.rs:20-162
     ScoringMatrix::hoxd70               src/scoring.rs:17-58
     HspParams / SearchParams            src/hsp.rs:46-59, src/seed_search.rs:19-41
     PackedSeq                           src/sequences.rs:53-318
@@ -61,9 +61,9 @@ class Context:
         return cls._default[device]
 
     def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0,
-                   max_hits_per_pass=0, initial_candidates=0) -> None:
+                   max_hits_per_pass=0, initial_candidates=0, filter_cap=0, filter_flush=0) -> None:
         t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass,
-                         initial_candidates)
+                         initial_candidates, filter_cap, filter_flush)
         check(lib().gxy_ctx_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -71,7 +71,8 @@ class Context:
         check(lib().gxy_ctx_get_tuning(self.h, C.byref(t)))
         return {"screen_warps": t.screen_warps, "screen_cap": t.screen_cap,
                 "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps,
-                "max_hits_per_pass": t.max_hits_per_pass, "initial_candidates": t.initial_candidates}
+                "max_hits_per_pass": t.max_hits_per_pass, "initial_candidates": t.initial_candidates,
+                "filter_cap": t.filter_cap, "filter_flush": t.filter_flush}
 
     def mark(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's primary stream."""
@@ -225,7 +226,7 @@ class DeviceSeq:
 # Seed pattern, scoring, parameters
 # ---------------------------------------------------------------------------
 class SeedPattern:
-    """Spaced seed (src/seeds.rs:20-173): '1' care, '0' don't care, <= 32 positions."""
+    """Spaced seed (src/seeds.rs:20-162): '1' care, '0' don't care, <= 32 positions."""
 
     def __init__(self, name: str, mask: Sequence[bool]):
         if len(mask) == 0:
@@ -408,7 +409,7 @@ class PosTable:
 def _stats(st: _lib.StatsC) -> dict:
     return {"windows": st.windows, "raw_hits": st.raw_hits, "candidates": st.candidates, "hsps": st.hsps,
             "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns, "enum_ms": st.enum_ms,
-            "passes": st.passes, "reruns": st.reruns}
+            "passes": st.passes, "reruns": st.reruns, "survivors": st.survivors, "filter_columns": st.filter_columns}
 
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:
@@ -422,7 +423,7 @@ def _take_buf(buf: _lib.HspBufC) -> np.ndarray:
 
 def search(table: PosTable, target: PackedSeq, query: PackedSeq, matrix: ScoringMatrix, params: SearchParams,
            stats: Optional[dict] = None) -> np.ndarray:
-    """seed_search::search (src/seed_search.rs:271-351) on the GPU.
+    """seed_search::search (src/seed_search.rs:45-125) on the GPU.
 
     Returns the HSPs as a structured array (t_start, q_start, length, score) in
     canonical (diagonal, t_start, length, score) order."""

@@ -53,7 +53,8 @@ class HspBufC(C.Structure):
 class StatsC(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
                 ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double),
-                ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reruns", C.c_uint32)]
+                ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reruns", C.c_uint32),
+                ("survivors", C.c_uint64), ("filter_columns", C.c_uint64)]
 
 
 class SeqSetC(C.Structure):
@@ -62,7 +63,8 @@ class SeqSetC(C.Structure):
 
 class TuningC(C.Structure):
     _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
-                ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32), ("initial_candidates", C.c_uint32)]
+                ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32), ("initial_candidates", C.c_uint32),
+                ("filter_cap", C.c_uint32), ("filter_flush", C.c_uint32)]
 
 
 class UnitC(C.Structure):

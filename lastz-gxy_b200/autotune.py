@@ -1,25 +1,40 @@
 """Autotuner for the batched seed->HSP launch.
 
-The tunables are the screen kernel's block shape (warps per block) and
-occupancy (blocks per SM, which also sets its register budget), the column cap
-per side after which the lane screen hands a still-extending hit to the warp
-extender, and the walk kernel's block shape.  The tuner times a sample of the
-caller's units under each setting with the library's own CUDA-event counters,
-keeps the fastest, applies it to the context and caches it in a JSON file
-keyed by device, seed weight, transition count and workload class -- so the
-one-transition and no-transition searches are tuned separately.
+The tunables:
+
+* filter_flush -- hits per warp that the fused enumerate + upper-bound filter
+  kernel queues in shared memory before a filter round (the hits-per-warp
+  batch: larger rounds leave fewer lanes idle at a round's end, smaller ones
+  keep the queue's hits closer to the query windows that produced them);
+* filter_cap -- columns per side after which the filter passes a hit on to
+  the exact screen unexamined;
+* screen_cap -- columns per side after which the exact lane screen hands a
+  still-extending hit to the warp extender of the diagonal walk;
+* screen_warps / screen_blocks_per_sm -- the exact screen's block shape and
+  occupancy (blocks per SM also sets its register budget);
+* walk_warps -- the diagonal walk's block shape.
+
+The tuner times a sample of the caller's units with the library's own
+CUDA-event counters, one parameter at a time (coordinate descent from the
+context's current setting, `sweeps` passes over the parameters), keeps the
+fastest, applies it to the context and caches it in a JSON file keyed by
+device, seed weight, transition count and workload class -- so the
+one-transition and no-transition searches are tuned separately.  Every
+setting must give the same HSPs as the first one timed; a setting that does
+not is refused and the tuner raises.
 """
 from __future__ import annotations
 
-import itertools
 import json
 import os
 from typing import Optional
 
 DEFAULT_SPACE = {
+    "filter_flush": [256, 128, 512],
+    "filter_cap": [96, 64, 160],
+    "screen_cap": [192, 128],
     "screen_warps": [8, 16],
     "screen_blocks_per_sm": [4, 3],
-    "screen_cap": [192, 128, 64],
     "walk_warps": [8, 4],
 }
 
@@ -45,7 +60,8 @@ def tuning_key(ctx, pattern: str, transitions: int, workload: str) -> str:
 
 
 def autotune(ctx, tables, queries, units, matrix, params, workload: str = "batch", space: Optional[dict] = None,
-             sample_units: int = 512, reps: int = 2, cache: Optional[str] = None, use_cache: bool = True) -> dict:
+             sample_units: int = 512, reps: int = 2, cache: Optional[str] = None, use_cache: bool = True,
+             sweeps: int = 1) -> dict:
     """Picks the fastest tuning for batch_search on (a sample of) these units and applies it."""
     from . import batch_search
     path = _cache_path(cache)
@@ -65,14 +81,20 @@ def autotune(ctx, tables, queries, units, matrix, params, workload: str = "batch
     ul = list(units)
     step = max(1, len(ul) // max(1, sample_units))
     sample = ul[::step][:sample_units]
-    names = list(sp)
-    results = []
+    cur = ctx.tuning()
+    cfg = {n: cur[n] for n in sp}
+    timed = {}
     ref = None
-    for combo in itertools.product(*[sp[n] for n in names]):
-        cfg = dict(zip(names, combo))
-        ctx.set_tuning(**cfg)
+
+    def run(c: dict) -> float:
+        nonlocal ref
+        k = tuple(sorted(c.items()))
+        if k in timed:
+            return timed[k]
+        ctx.set_tuning(**c)
         best = None
-        for _ in range(reps):
+        out = None
+        for _ in range(max(1, reps)):
             st = {}
             out = batch_search(tables, queries, sample, matrix, params, stats=st, ctx=ctx)
             best = st["device_ms"] if best is None else min(best, st["device_ms"])
@@ -80,13 +102,21 @@ def autotune(ctx, tables, queries, units, matrix, params, workload: str = "batch
         if ref is None:
             ref = sig
         elif sig != ref:
-            raise RuntimeError(f"tuning {cfg} changed the HSPs; refusing to tune")
-        results.append((best, cfg))
-    results.sort(key=lambda x: x[0])
-    best_ms, best_cfg = results[0]
-    ctx.set_tuning(**best_cfg)
-    entry = {"tuning": best_cfg, "device_ms": best_ms, "sample_units": len(sample),
-             "tried": [{"ms": round(ms, 4), **cfg} for ms, cfg in results]}
+            raise RuntimeError(f"tuning {c} changed the HSPs; refusing to tune")
+        timed[k] = best
+        return best
+
+    best_ms = run(cfg)
+    for _ in range(max(1, sweeps)):
+        for name in sp:
+            for v in sp[name]:
+                trial = dict(cfg, **{name: v})
+                ms = run(trial)
+                if ms < best_ms:
+                    best_ms, cfg = ms, trial
+    ctx.set_tuning(**cfg)
+    entry = {"tuning": cfg, "device_ms": best_ms, "sample_units": len(sample),
+             "tried": [{"ms": round(ms, 4), **dict(k)} for k, ms in sorted(timed.items(), key=lambda x: x[1])]}
     store[key] = entry
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)

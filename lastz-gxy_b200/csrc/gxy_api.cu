@@ -47,44 +47,8 @@ gxy_status set_device(gxy_ctx* ctx) {
     return GXY_OK;
 }
 
-// SeedPattern::parse (src/seeds.rs:113-126) with the engine's limits.
-gxy_status parse_pattern(const char* s, Pattern& pat) {
-    if (!s) {
-        set_error("pattern is null");
-        return GXY_EINVAL;
-    }
-    memset(&pat, 0, sizeof(pat));
-    uint32_t len = 0, w = 0;
-    for (const char* c = s; *c; c++) {
-        if (*c != '0' && *c != '1') {
-            set_error(std::string("seed pattern character '") + *c + "' is not '0' or '1'");
-            return GXY_EINVAL;
-        }
-        if (len >= 32) {
-            set_error("seed pattern exceeds the 32-position limit (src/seeds.rs:103-107)");
-            return GXY_EINVAL;
-        }
-        if (*c == '1') {
-            if (w >= (uint32_t)kMaxWeight) {
-                set_error("seed weight > 15 needs more than 2^30 buckets; unsupported");
-                return GXY_EUNSUPPORTED;
-            }
-            pat.care[w++] = (uint8_t)len;
-            pat.care_mask |= 1u << len;
-        }
-        len++;
-    }
-    if (len == 0) {
-        set_error("seed pattern is empty");
-        return GXY_EINVAL;
-    }
-    pat.len = len;
-    pat.weight = w;
-    return GXY_OK;
-}
-
 uint32_t n_windows(uint64_t len, uint32_t L, uint32_t step) {
-    // iter_with_stride (src/seeds.rs:226-236): 0, step, ... <= len - L.
+    // iter_with_stride (src/seeds.rs:151-161): 0, step, ... <= len - L.
     if (len < L) return 0;
     return (uint32_t)((len - L) / step + 1);
 }
@@ -150,6 +114,7 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
     auto fail = [&](gxy_status s) {
         dev_free(t->starts);
         dev_free(t->positions);
+        dev_free(t->occ);
         delete t;
         return s;
     };
@@ -185,6 +150,10 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
         const gxy_status ps = prune_table(t, mwc, W);
         if (ps != GXY_OK) return fail(ps);
     }
+    // The searches test a bucket's occupancy bit before reading its bounds.
+    if (e == cudaSuccess) e = dev_alloc((void**)&t->occ, (size_t)((nw + 31) / 32) * 4, st);
+    if (e == cudaSuccess) launch_occupancy(t->starts, nw, t->occ, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("table finish: ") + cudaGetErrorString(e));
@@ -273,6 +242,7 @@ gxy_status search_impl(gxy_ctx* ctx, Worker* W, const gxy_table* table, const Se
     units[0].qseg = 0;
     units[0].starts = table->starts;
     units[0].positions = table->positions;
+    units[0].occ = table->occ;
     units[0].nwin = n_windows(Q.len, table->pat.len, p->step);
     units[0].primary_lo = units[0].primary_hi = 0;
     units[0].avg_bucket = table->num_words ? (double)table->npos / (double)table->num_words : 0.0;
@@ -302,7 +272,7 @@ const char* gxy_status_string(gxy_status s) {
 }
 
 const char* gxy_last_error(void) { return last_error(); }
-uint32_t gxy_abi_version(void) { return 1; }
+uint32_t gxy_abi_version(void) { return 2; }
 uint64_t gxy_kernel_launches(void) { return launches(); }
 
 gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
@@ -405,6 +375,8 @@ gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
     if (t->walk_warps) ctx->tuning.walk_warps = t->walk_warps == 4 ? 4 : 8;
     if (t->max_hits_per_pass) ctx->tuning.max_hits_per_pass = std::max<uint32_t>(4096, t->max_hits_per_pass);
     if (t->initial_candidates) ctx->tuning.initial_candidates = std::max<uint32_t>(1024, t->initial_candidates);
+    if (t->filter_cap) ctx->tuning.filter_cap = std::min<uint32_t>(256, std::max<uint32_t>(32, t->filter_cap & ~31u));
+    if (t->filter_flush) ctx->tuning.filter_flush = std::min<uint32_t>(512, std::max<uint32_t>(32, t->filter_flush));
     return GXY_OK;
 }
 
@@ -582,6 +554,7 @@ gxy_status gxy_table_free(gxy_table* t) {
     cudaSetDevice(t->ctx->device);
     dev_free(t->starts);
     dev_free(t->positions);
+    dev_free(t->occ);
     dseq_destroy(t->owned);
     delete t;
     return GXY_OK;
@@ -695,6 +668,7 @@ static gxy_status batch_run(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* co
         plan[i].qseg = (uint32_t)qseg_of[qi];
         plan[i].starts = t->starts;
         plan[i].positions = t->positions;
+        plan[i].occ = t->occ;
         plan[i].nwin = n_windows(queries[u.query]->len, pat.len, params->step);
         plan[i].primary_lo = u.primary_lo;
         plan[i].primary_hi = u.primary_hi;

@@ -36,12 +36,13 @@ struct SeqView {
 };
 
 // One reference search() call: a (target segment, query segment) pair with
-// the target's position table (src/seed_search.rs:271-277).
+// the target's position table (src/seed_search.rs:45-51).
 struct UnitDev {
     uint32_t tseg;
     uint32_t qseg;
     const uint32_t* starts;
     const uint32_t* positions;
+    const uint32_t* occ;  // bucket occupancy bitmap (bit w & 31 of occ[w >> 5])
     uint32_t nwin;        // query windows 0, step, ... <= len - L
     uint32_t tile_base;   // first screen tile of this unit
     uint32_t primary_lo;  // driver primary-region filter, src/driver.rs:250-256
@@ -97,6 +98,24 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+// Each set bit of x becomes a set 2-bit pair (bit k -> bits 2k, 2k+1).
+__device__ __forceinline__ uint64_t spread_bits_to_pairs(uint32_t x) {
+    uint64_t v = x;
+    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    v = (v | (v << 2)) & 0x3333333333333333ull;
+    v = (v | (v << 1)) & 0x5555555555555555ull;
+    return v * 3;   // each set bit -> a set 2-bit pair
+}
+
+// Reverses the order of the 32 two-bit codes of a word (a left-side chunk
+// read upwards becomes column 0 = the position next to the seed).
+__device__ __forceinline__ uint64_t rev_pairs64(uint64_t c) {
+    c = __brevll(c);
+    return ((c >> 1) & 0x5555555555555555ull) | ((c & 0x5555555555555555ull) << 1);
 }
 
 // Column score (src/hsp.rs:198-211): ambig when either base is invalid.

@@ -177,6 +177,42 @@ void checkin(gxy_ctx* ctx, Worker* w) {
     ctx->free_workers.push_back(w);
 }
 
+// SeedPattern::parse (src/seeds.rs:38-51) with the engine's limits.
+gxy_status parse_pattern(const char* s, Pattern& pat) {
+    if (!s) {
+        set_error("pattern is null");
+        return GXY_EINVAL;
+    }
+    memset(&pat, 0, sizeof(pat));
+    uint32_t len = 0, w = 0;
+    for (const char* c = s; *c; c++) {
+        if (*c != '0' && *c != '1') {
+            set_error(std::string("seed pattern character '") + *c + "' is not '0' or '1'");
+            return GXY_EINVAL;
+        }
+        if (len >= 32) {
+            set_error("seed pattern exceeds the 32-position limit (src/seeds.rs:28-32)");
+            return GXY_EINVAL;
+        }
+        if (*c == '1') {
+            if (w >= (uint32_t)kMaxWeight) {
+                set_error("seed weight > 15 needs more than 2^30 buckets; unsupported");
+                return GXY_EUNSUPPORTED;
+            }
+            pat.care[w++] = (uint8_t)len;
+            pat.care_mask |= 1u << len;
+        }
+        len++;
+    }
+    if (len == 0) {
+        set_error("seed pattern is empty");
+        return GXY_EINVAL;
+    }
+    pat.len = len;
+    pat.weight = w;
+    return GXY_OK;
+}
+
 gxy_status check_params(const gxy_search_params* p, uint64_t max_cols) {
     if (!p) {
         set_error("params is null");
@@ -210,7 +246,7 @@ static int bits_for(uint64_t x) {
 }
 
 static void build_variants(const Pattern& pat, uint32_t transitions, uint32_t* vx, uint32_t& nv) {
-    // src/seed_search.rs:289, :303-316.
+    // src/seed_search.rs:63, :303-316.
     const uint32_t w = pat.weight;
     uint32_t shifts[16];
     for (uint32_t i = 0; i < w; i++) shifts[i] = 2 * (w - 1 - i);
@@ -287,6 +323,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         ud[i].qseg = u.qseg;
         ud[i].starts = u.starts;
         ud[i].positions = u.positions;
+        ud[i].occ = u.occ;
         ud[i].nwin = u.nwin;
         ud[i].tile_base = (uint32_t)tiles;
         ud[i].primary_lo = u.primary_lo;
@@ -362,6 +399,13 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     sa.sc.hspthresh = p.hspthresh;
     sa.cap = std::max<uint32_t>(32, ctx->tuning.screen_cap);
     sa.qkey_total = (uint32_t)qk;
+    // Enumeration fused with the upper-bound filter when the scores admit
+    // class bounds (they do for every matrix with a non-positive class);
+    // otherwise every raw hit goes to the exact screen.
+    sa.f_cap = std::max<uint32_t>(32, ctx->tuning.filter_cap);
+    sa.f_flush = std::max<uint32_t>(32, ctx->tuning.filter_flush);
+    bool use_filter = filter_bounds(sa);
+    for (const UnitPlan& u : units) use_filter = use_filter && u.occ != nullptr;
 
     RadixPass passes[16];
     const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
@@ -388,18 +432,21 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     {
         double est = 1 << 20;
         for (const UnitPlan& u : units) est += 1.5 * (double)u.nwin * sa.n_var * u.avg_bucket;
+        // The hit buffer holds the filter's survivors only (a few percent of
+        // the raw hits); the candidate estimate stays on raw hits.
+        const double est_buf = use_filter ? (1 << 20) + est / kRawPerSurvivorSlot : est;
         // Candidates from the same estimate (a few percent of the raw hits
         // pass the screen): an overflow would rerun the whole launch.
         const uint64_t want_cand = std::min<uint64_t>((uint64_t)(est / kHitsPerCandidate), kMaxPresizedCandidates);
         if (want_cand > W->cand_cap) W->cand_cap = (uint32_t)want_cand;
-        if (est > (double)W->hit_cap) {
-            if (est <= (double)kMaxHitCap) {
+        if (est_buf > (double)W->hit_cap) {
+            if (est_buf <= (double)kMaxHitCap) {
                 W->hits.release();
-                W->hit_cap = (uint64_t)est;
+                W->hit_cap = (uint64_t)est_buf;
             } else {
                 W->hits.release();
                 W->hit_cap = kMaxHitCap;
-                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / est));
+                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / est_buf));
             }
         }
     }
@@ -416,7 +463,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(cudaMemsetAsync(hitc, 0, 8, st));
         sa.tile_lo = t0;
         sa.tile_hi = t1;
-        launch_enumerate(sa, ctx->sm_count, st);
+        if (use_filter) launch_seed_filter(sa, ctx->sm_count, 16, st);
+        else launch_enumerate(sa, ctx->sm_count, st);
         if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
         launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
         return GXY_OK;
@@ -438,6 +486,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     uint32_t reruns = 0;   // pipeline runs (or passes) repeated after a buffer grew
     for (int attempt = 0; attempt < 16; attempt++) {
         uint32_t cap = W->cand_cap;
+        uint64_t survivors = 0;   // hits the passes wrote to the hit buffer
         GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
         GXY_CK(W->ck0.ensure((size_t)cap * 8));
         GXY_CK(W->ck1.ensure((size_t)cap * 8));
@@ -532,6 +581,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                     continue;
                 }
                 t0 = t1;
+                survivors += nh;
                 // Hit density varies along the query (repeats): grow the
                 // window range again after a sparse pass, up to twice.
                 if ((double)nh < 0.5 * (double)W->hit_cap) {
@@ -679,6 +729,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + kCStats);
         const unsigned long long nhits = *reinterpret_cast<const unsigned long long*>(hc + kCHits);
         const uint32_t ncand = hc[kCCand];
+        if (single) survivors = nhits;
         if (single && nhits > W->hit_cap) {
             // Raw hits overflowed the hit buffer: grow it, or split into passes.
             if (nhits + nhits / 8 <= kMaxHitCap) {
@@ -707,6 +758,8 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.windows = hs[0];
         out.stats.raw_hits = hs[1];
         out.stats.columns = hs[2];
+        out.stats.filter_columns = hs[3];
+        out.stats.survivors = use_filter ? survivors : hs[1];
         out.stats.candidates = ncand;
         out.stats.hsps = nh;
         float ms = 0.f, ms_enum = 0.f, ms_screen = 0.f;

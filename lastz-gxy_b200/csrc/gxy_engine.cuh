@@ -62,6 +62,7 @@ struct UnitPlan {
     uint32_t qseg;
     const uint32_t* starts;
     const uint32_t* positions;
+    const uint32_t* occ;   // the table's bucket occupancy bitmap
     uint32_t nwin;
     uint32_t primary_lo;
     uint32_t primary_hi;
@@ -77,6 +78,9 @@ constexpr uint32_t kCounterWords = 4096;
 // hits become candidates), up to a bound.  Larger arrays also widen the
 // capacity-sized sort and scan grids of every later launch on the worker.
 constexpr uint64_t kHitsPerCandidate = 32;
+// With the upper-bound filter the hit buffer is sized at one slot per this
+// many estimated raw hits (survivors are a few percent of the raw hits).
+constexpr double kRawPerSurvivorSlot = 8.0;
 constexpr uint64_t kMaxPresizedCandidates = 1ull << 22;
 
 struct RunResult {
@@ -117,6 +121,7 @@ struct gxy_table {
     uint64_t lo = 0, hi = 0;
     uint32_t* starts = nullptr;
     uint32_t* positions = nullptr;
+    uint32_t* occ = nullptr;   // bit (w & 31) of occ[w >> 5]: bucket w is non-empty
     uint64_t num_words = 0;
     uint64_t npos = 0;
     // Positions within a bucket are in ascending order (the reference's
@@ -139,7 +144,7 @@ struct gxy_ctx {
     // Screen column cap 192 (the packed screen's limit): on the 10 Mbp plain
     // launch, longer screening leaves fewer candidates for the walk to
     // re-extend (two searches 4.27 ms, against 4.31 ms at 128 and 4.51 at 64).
-    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0};
+    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 256};
     cudaEvent_t marks[16] = {};
 };
 
@@ -158,6 +163,10 @@ void dseq_destroy(gxy_dseq* s);
 void dseq_destroy_async(gxy_dseq* s, cudaStream_t st);
 gxy_status dseq_fill_host(gxy_dseq* d, const gxy_packed_seq* h, cudaStream_t st);
 SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi);
+
+// SeedPattern::parse (src/seeds.rs:38-51) with the engine's limits: at most
+// 32 positions (src/seeds.rs:28-32), weight at most kMaxWeight.
+gxy_status parse_pattern(const char* s, Pattern& pat);
 
 // Validates params and the i32 envelope for a search over sequences whose
 // diagonal spans are at most max_cols columns.

@@ -66,15 +66,6 @@ void launch_pack_ascii(const uint8_t* ascii, uint64_t n, uint64_t* codes, uint32
 // base becomes its complement (3 - c), an invalid one code 0 and unmasked,
 // and the mask bit moves with the base (src/sequences.rs:303-318).  One thread
 // per 32 output positions; the 32 input positions are one unaligned load.
-__device__ __forceinline__ uint64_t spread_bits_to_pairs(uint32_t x) {
-    uint64_t v = x;
-    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
-    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
-    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
-    v = (v | (v << 2)) & 0x3333333333333333ull;
-    v = (v | (v << 1)) & 0x5555555555555555ull;
-    return v * 3;   // each set bit -> a set 2-bit pair
-}
 
 __global__ void k_reverse_complement(const uint64_t* __restrict__ ic, const uint32_t* __restrict__ iv,
                                      const uint32_t* __restrict__ im, uint64_t n, uint64_t* oc, uint32_t* ov,
@@ -120,24 +111,6 @@ void launch_reverse_complement(const uint64_t* icodes, const uint32_t* ivalid, c
 // ---------------------------------------------------------------------------
 // Seed words and the table build
 // ---------------------------------------------------------------------------
-
-// SeedExtractor::word_at (src/seeds.rs:208-222) at view-local position p
-// (the caller guarantees p + L <= len): seedable iff every care position is
-// valid and unmasked; the leftmost care position lands in the top bits.
-__device__ __forceinline__ bool word_at(const SeqView& S, const Pattern& pat, uint32_t p, uint32_t& word) {
-    const uint64_t gp = S.base + p;
-    const uint32_t ok = load_bits32(S.valid, gp) & ~load_bits32(S.mask, gp);
-    if ((ok & pat.care_mask) != pat.care_mask) return false;
-    const uint64_t c = load_codes32(S.codes, gp);
-    uint32_t w = 0;
-#pragma unroll
-    for (int i = 0; i < kMaxWeight; i++) {
-        if ((uint32_t)i >= pat.weight) break;
-        w = (w << 2) | ((uint32_t)(c >> (2 * pat.care[i])) & 3u);
-    }
-    word = w;
-    return true;
-}
 
 __global__ void k_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t sentinel,
                              uint32_t* keys, uint32_t* vals, uint32_t* counts) {
@@ -315,32 +288,11 @@ void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64
 }
 
 // ---------------------------------------------------------------------------
-// Screen: fused hit enumeration + capped lane-per-hit x-drop.
-//
-// Each warp runs a producer and 32 consumers over a shared-memory queue of
-// hits (t, q, unit).
-//  - Producer (warp-cooperative): takes tiles of 32 consecutive query windows
-//    of one unit from a global work counter, forms each window's seed word
-//    and its transition variants (src/seed_search.rs:303-316), and pushes the
-//    hits of each variant's bucket (src/pos_table.rs:102-108) into the queue.
-//  - Consumers (one lane per hit): an idle lane takes the next queued hit and
-//    loads one 128-position window of the target and of the query around it;
-//    from those registers it scores the seed footprint and the first 32
-//    columns of both sides of extend_hit (src/hsp.rs:98-195) -- the sides are
-//    independent.  A side still running after 32 columns continues one chunk
-//    per iteration with fresh loads, while the other lanes take new hits.
-// A hit is extended up to `cap` columns per side:
-//  - ended below hspthresh: dropped.  Such a hit can never change the output:
-//    search() only records diagonal cover for a hit whose HSP passes
-//    (src/seed_search.rs:321-340), so whether it was admitted is irrelevant.
-//  - ended at or above hspthresh, or still running at the cap: kept as a
-//    candidate for the walk, which applies the diagonal rule in order.
+// Scan helpers of the exact lane-per-hit screens below (k_screen_wide and
+// the packed k_screen).  The screens read hits from a global array written
+// either by k_enumerate (every raw hit) or by k_seed_filter in gxy_filter.cu
+// (only the hits whose upper-bound x-drop might reach hspthresh).
 // ---------------------------------------------------------------------------
-
-__device__ __forceinline__ uint64_t rev_pairs64(uint64_t c) {
-    c = __brevll(c);
-    return ((c >> 1) & 0x5555555555555555ull) | ((c & 0x5555555555555555ull) << 1);
-}
 
 // 32 positions starting at offset o of a 4-word window (o <= 96).
 __device__ __forceinline__ uint64_t win_codes(const uint64_t (&w)[4], uint32_t o) {
@@ -495,7 +447,7 @@ __device__ __forceinline__ void scan_pair_any(SideScan& A, SideScan& B, uint32_t
 // ---------------------------------------------------------------------------
 // Enumeration: one warp per tile of 32 consecutive query windows of one unit.
 // Each lane forms its window's seed word and transition variants
-// (src/seed_search.rs:303-316); the warp reserves room for all hits of the
+// (src/seed_search.rs:76-90); the warp reserves room for all hits of the
 // tile with one atomic and writes (t, q, unit) for every position of every
 // variant's bucket (src/pos_table.rs:102-108).  Large buckets are copied by
 // the whole warp.
@@ -660,7 +612,7 @@ void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st) {
 // hits.  A hit is extended up to `cap` columns per side:
 //  - ended below hspthresh: dropped.  Such a hit can never change the output:
 //    search() only records diagonal cover for a hit whose HSP passes
-//    (src/seed_search.rs:321-340), so whether it was admitted is irrelevant.
+//    (src/seed_search.rs:95-114), so whether it was admitted is irrelevant.
 //  - ended at or above hspthresh, or still running at the cap: kept as a
 //    candidate for the walk, which applies the diagonal rule in order.
 // ---------------------------------------------------------------------------

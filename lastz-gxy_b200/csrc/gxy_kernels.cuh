@@ -16,6 +16,24 @@ struct Pattern {
     uint8_t care[16];     // care offsets, leftmost first
 };
 
+// SeedExtractor::word_at (src/seeds.rs:133-147) at view-local position p
+// (the caller guarantees p + L <= len): seedable iff every care position is
+// valid and unmasked; the leftmost care position lands in the top bits.
+__device__ __forceinline__ bool word_at(const SeqView& S, const Pattern& pat, uint32_t p, uint32_t& word) {
+    const uint64_t gp = S.base + p;
+    const uint32_t ok = load_bits32(S.valid, gp) & ~load_bits32(S.mask, gp);
+    if ((ok & pat.care_mask) != pat.care_mask) return false;
+    const uint64_t c = load_codes32(S.codes, gp);
+    uint32_t w = 0;
+#pragma unroll
+    for (int i = 0; i < kMaxWeight; i++) {
+        if ((uint32_t)i >= pat.weight) break;
+        w = (w << 2) | ((uint32_t)(c >> (2 * pat.care[i])) & 3u);
+    }
+    word = w;
+    return true;
+}
+
 // --- packing -----------------------------------------------------------------
 // PackedSeq::from_ascii (src/sequences.rs:89-131): n ASCII bytes -> a device
 // sequence laid out as gxy_device.cuh describes.
@@ -88,13 +106,30 @@ struct ScreenArgs {
     Cand* cands;
     uint32_t cand_cap;
     uint32_t* cand_count;
-    unsigned long long* stats;   // [0] windows, [1] raw hits, [2] columns examined
+    unsigned long long* stats;   // [0] windows, [1] raw hits, [2] columns examined, [3] filter columns
+    // Upper-bound filter of k_seed_filter (FilterBounds in gxy_filter.cu).
+    int32_t fub[4];        // per class x = t_code ^ q_code: the largest score of that class
+    uint64_t f_inv;        // class word given to the columns where either base is invalid
+    uint64_t f_end;        // class word given to the columns past a side's end
+    int32_t f_seed_max;    // seed length x the largest class bound
+    uint32_t f_cap;        // columns per side after which a hit survives unexamined
+    uint32_t f_flush;      // queued hits per warp that start a filter round
 };
 // Seed-hit enumeration: one warp per tile of 32 query windows; writes the
 // hits of every (window, variant) bucket to a.hits.
 void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st);
 // Capped lane-per-hit x-drop over a.hits; keeps the candidates.  grid = persistent.
 void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);
+// Seed-hit enumeration fused with an upper-bound x-drop filter: writes to
+// a.hits only the hits that might reach hspthresh (gxy_filter.cu).
+// filter_bounds fills a's fub/f_inv/f_end/f_seed_max from a.sc and a.pat and
+// returns false when the scoring admits no such bound (then the caller runs
+// launch_enumerate + launch_screen over every raw hit).
+bool filter_bounds(ScreenArgs& a);
+void launch_seed_filter(const ScreenArgs& a, int sm_count, int warps_per_block, cudaStream_t st);
+// Bucket occupancy bitmap of a table: bit (w & 31) of occ[w >> 5] is set iff
+// bucket w holds a position.
+void launch_occupancy(const uint32_t* starts, uint64_t num_words, uint32_t* occ, cudaStream_t st);
 
 struct WalkArgs {
     const uint64_t* keys;      // candidate keys in sorted order
@@ -115,7 +150,7 @@ struct WalkArgs {
     uint32_t n_units;          // units of the launch (one unit: every segment is walked in one pass)
 };
 // Diagonal suppression (src/diag_hash.rs:34-53 as used at
-// src/seed_search.rs:318-342) over the candidates sorted by (diagonal, t),
+// src/seed_search.rs:92-116) over the candidates sorted by (diagonal, t),
 // one warp per diagonal segment.
 void launch_walk(const WalkArgs& a, int warps_per_block, int blocks, cudaStream_t st);
 

@@ -12,8 +12,8 @@
 // The array is part of this library's device code: every GPU that loads the
 // library holds its kStaticScratchBytes until the process exits.  Host code
 // must not pass the array's name to a kernel (on the host it is only a
-// stand-in symbol); the device address comes from cudaGetSymbolAddress, once
-// per device, on the first call made with that device current.
+// stand-in symbol); the device address comes from cudaGetSymbolAddress on
+// each call, made with the caller's device current.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -55,9 +55,12 @@ gxy_status fail(gxy_status s, const std::string& m) {
     return s;
 }
 
-// The device address of the scratch array for the current device.
+// The device address of the scratch array on the current device.  It is
+// looked up on every call (a cheap host call) rather than cached, so a
+// device reset between calls, which reloads the module and moves the array,
+// cannot leave a stale address behind; the primitives' kernel attributes are
+// set again for the same reason.
 gxy_status scratch_address(int dev, DeviceSlot& slot) {
-    if (slot.ptr) return GXY_OK;
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p)
@@ -68,27 +71,6 @@ gxy_status scratch_address(int dev, DeviceSlot& slot) {
     prims_init();
     slot.sm_count = sms;
     slot.ptr = static_cast<unsigned char*>(p);
-    return GXY_OK;
-}
-
-// SeedPattern::parse (src/seeds.rs:113-126) with this library's limits.
-gxy_status pattern_of(const char* s, Pattern& pat) {
-    if (!s) return fail(GXY_EINVAL, "pattern is null");
-    memset(&pat, 0, sizeof(pat));
-    uint32_t len = 0, w = 0;
-    for (const char* c = s; *c; c++) {
-        if (*c != '0' && *c != '1') return fail(GXY_EINVAL, "seed pattern characters must be '0' or '1'");
-        if (len >= 32) return fail(GXY_EINVAL, "seed pattern exceeds the 32-position limit");
-        if (*c == '1') {
-            if (w >= (uint32_t)kMaxWeight) return fail(GXY_EUNSUPPORTED, "seed weight > 15 is unsupported");
-            pat.care[w++] = (uint8_t)len;
-            pat.care_mask |= 1u << len;
-        }
-        len++;
-    }
-    if (len == 0) return fail(GXY_EINVAL, "seed pattern is empty");
-    pat.len = len;
-    pat.weight = w;
     return GXY_OK;
 }
 
@@ -107,7 +89,7 @@ extern "C" gxy_status gxy_table_build_static(const gxy_packed_seq* target, const
         return fail(GXY_EINVAL, "target longer than " + std::to_string(kStaticMaxLen) +
                                     " bp: too large for the allocation-free table build");
     Pattern pat;
-    gxy_status s = pattern_of(pattern01, pat);
+    gxy_status s = parse_pattern(pattern01, pat);
     if (s != GXY_OK) return s;
     const uint64_t nw = 1ull << (2 * pat.weight);
     if (starts_cap < nw + 1) return fail(GXY_EINVAL, "starts_out holds fewer than num_words + 1 entries");
@@ -170,6 +152,10 @@ extern "C" gxy_status gxy_table_build_static(const gxy_packed_seq* target, const
     const int np = plan_radix(0, bits, 0, 0, passes, 8);
     const int which = radix_sort_u32(k0, v0, k1, v1, nullptr, nwin, nwin, passes, np, ps, st);
     const uint32_t* sorted_pos = which ? v1 : v0;
+    // A failed launch above leaves the array unwritten: report it before
+    // anything is read back or copied out.
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(GXY_ECUDA, std::string("static table build: ") + cudaGetErrorString(e));
     uint32_t total = 0;
     e = cudaMemcpyAsync(&total, starts_out + nw, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

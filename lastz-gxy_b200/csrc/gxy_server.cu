@@ -136,6 +136,7 @@ gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
             qsegs.push_back(view_of(qs, 0, qs->len));
             u.starts = t->starts;
             u.positions = t->positions;
+            u.occ = t->occ;
             u.nwin = windows_of(q->len, pat.len, s->params.step);
             u.primary_lo = u.primary_hi = 0;
             u.avg_bucket = t->num_words ? (double)t->npos / (double)t->num_words : 0.0;

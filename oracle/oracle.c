@@ -109,7 +109,7 @@ void orc_slice(const orc_seq* in, uint64_t start, uint64_t end, uint8_t* codes, 
 /* Seeds (src/seeds.rs).                                                    */
 /* ------------------------------------------------------------------------ */
 
-/* SeedPattern::parse + SeedPattern::new (src/seeds.rs:101-126), and
+/* SeedPattern::parse + SeedPattern::new (src/seeds.rs:26-51), and
  * SeedExtractor::new's care-offset list (:187-195). */
 int orc_pattern_parse(const char* pattern01, uint8_t* care, uint32_t* weight) {
     int len = 0;
@@ -125,7 +125,7 @@ int orc_pattern_parse(const char* pattern01, uint8_t* care, uint32_t* weight) {
     return len;
 }
 
-/* SeedExtractor::word_at, src/seeds.rs:208-222: None when the window runs past
+/* SeedExtractor::word_at, src/seeds.rs:133-147: None when the window runs past
  * the end or any care position is invalid or soft-masked; the leftmost care
  * position lands in the most significant bits. */
 static inline int word_at(const orc_seq* s, const uint8_t* care, uint32_t weight, uint32_t plen,
@@ -154,7 +154,7 @@ int orc_word_at(const orc_seq* s, const char* pattern01, uint64_t pos, uint64_t*
 /* ------------------------------------------------------------------------ */
 
 /* PosTable::build, src/pos_table.rs:35-83.  Windows come from
- * iter_with_stride (src/seeds.rs:226-236): pos = 0, step, ... <= len-L (with
+ * iter_with_stride (src/seeds.rs:151-161): pos = 0, step, ... <= len-L (with
  * len-L saturating at 0).  Count per word, exclusive prefix into starts,
  * then scatter in ascending position order. */
 int orc_table_build(const orc_seq* s, const char* pattern01, uint32_t step, orc_table* out) {
@@ -525,7 +525,7 @@ static inline int dh_mark_covered(diag_hash* h, uint32_t t_end, uint32_t q_end) 
 }
 
 /* ------------------------------------------------------------------------ */
-/* search (src/seed_search.rs:271-351).                                     */
+/* search (src/seed_search.rs:45-125).                                     */
 /* ------------------------------------------------------------------------ */
 static int hsp_cmp(const void* a, const void* b) {
     const orc_hsp* x = (const orc_hsp*)a;
@@ -546,10 +546,10 @@ int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* que
     orc_stats st = {0, 0, 0, 0};
     *out = NULL;
     *n_out = 0;
-    /* shifts, src/seed_search.rs:289. */
+    /* shifts, src/seed_search.rs:63. */
     uint32_t shifts[32];
     for (uint32_t i = 0; i < w; i++) shifts[i] = 2 * (w - 1 - i);
-    /* variants capacity, src/seed_search.rs:295-299. */
+    /* variants capacity, src/seed_search.rs:69-73. */
     uint32_t vcap = p->transitions == 0 ? 1 : (p->transitions == 1 ? 1 + w : 1 + w + w * (w ? w - 1 : 0) / 2);
     uint64_t* variants = (uint64_t*)malloc(vcap * sizeof(uint64_t));
     uint32_t bounds[2 * (1 + 15 + 105)];
@@ -564,7 +564,7 @@ int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* que
         uint64_t word;
         if (!word_at(query, table->care, w, L, qpos, &word)) continue;
         st.windows++;
-        /* variant order, src/seed_search.rs:303-316. */
+        /* variant order, src/seed_search.rs:76-90. */
         uint32_t nv = 0;
         variants[nv++] = word;
         if (p->transitions >= 1)
@@ -573,7 +573,7 @@ int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* que
             for (uint32_t i = 0; i < w; i++)
                 for (uint32_t j = i + 1; j < w; j++)
                     variants[nv++] = word ^ (2ull << shifts[i]) ^ (2ull << shifts[j]);
-        /* src/seed_search.rs:318-342.  The bucket bounds of all variants are
+        /* src/seed_search.rs:92-116.  The bucket bounds of all variants are
          * read first (independent loads the CPU can overlap); the hits are
          * then visited in the reference's order. */
         for (uint32_t v = 0; v < nv; v++) {
@@ -608,7 +608,7 @@ int orc_search(const orc_table* table, const orc_seq* target, const orc_seq* que
             }
         }
     }
-    /* sort by (diagonal, t_start) + dedup, src/seed_search.rs:348-349; the
+    /* sort by (diagonal, t_start) + dedup, src/seed_search.rs:122-123; the
      * oracle breaks key ties by (length, score) so its order is canonical. */
     qsort(res, n, sizeof(orc_hsp), hsp_cmp);
     {

@@ -78,7 +78,7 @@ void orc_reverse_complement(const orc_seq* in, uint8_t* codes, uint8_t* valid, u
 void orc_slice(const orc_seq* in, uint64_t start, uint64_t end, uint8_t* codes, uint8_t* valid,
                uint8_t* mask);
 
-/* ---- seeds (src/seeds.rs:113-126, :208-236) ---- */
+/* ---- seeds (src/seeds.rs:38-51, :208-236) ---- */
 /* Parses a 0/1 pattern; returns the pattern length, or -1 on a bad char, empty
  * or longer than 32 positions. */
 int orc_pattern_parse(const char* pattern01, uint8_t* care, uint32_t* weight);
@@ -106,7 +106,7 @@ double orc_shannon_entropy(const orc_seq* s, uint64_t start, uint64_t end);
 int orc_passes_entropy_gate(const orc_seq* s, uint32_t t_start, uint32_t t_end, int32_t score,
                             int32_t threshold);
 
-/* ---- search (src/seed_search.rs:271-351 with src/diag_hash.rs:34-53) ---- */
+/* ---- search (src/seed_search.rs:45-125 with src/diag_hash.rs:34-53) ---- */
 /* use_avx2 selects extend_hit_avx2 (the reference's dispatch on x86 with an
  * i8-safe matrix, src/hsp.rs:66-87) instead of extend_hit_scalar.  Output is
  * malloc'd, sorted canonically by (diagonal, t_start, length, score) and

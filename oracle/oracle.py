@@ -232,7 +232,7 @@ def _to_array(ptr, n: int) -> np.ndarray:
 
 
 def search(table: Table, target: Seq, query: Seq, p: OrcParams, avx2: bool = False):
-    """seed_search::search (src/seed_search.rs:271-351).  Returns (hsps, stats)."""
+    """seed_search::search (src/seed_search.rs:45-125).  Returns (hsps, stats)."""
     out = C.POINTER(OrcHsp)()
     n = C.c_uint64(0)
     st = OrcStats()
@@ -479,4 +479,25 @@ def driver_records(entries) -> list:
                 continue
             kept.append(r)
         out.extend((ti, qi, strand, r[0], r[1], r[2], r[4]) for r in kept)
+    return out
+
+
+def chunk_target(target_len: int, primary_bp: int, halo_bp: int) -> list:
+    """chunk_target (src/driver.rs:156-194): [(chunk_lo, chunk_hi,
+    primary_start_local, primary_end_local)].  One chunk covering the whole
+    target when chunking is off or the target is at most primary + halo long
+    (src/driver.rs:162); otherwise primaries of primary_bp bases, each widened
+    by halo_bp on both sides and clamped to the target."""
+    if primary_bp == 0 or target_len <= primary_bp + halo_bp:
+        return [(0, target_len, 0, target_len)]
+    out = []
+    ps = 0
+    while ps < target_len:
+        pe = min(ps + primary_bp, target_len)
+        lo = max(ps - halo_bp, 0)
+        hi = min(pe + halo_bp, target_len)
+        out.append((lo, hi, ps - lo, pe - lo))
+        if pe == target_len:
+            break
+        ps = pe
     return out

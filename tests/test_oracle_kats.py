@@ -61,7 +61,7 @@ def test_soft_mask_and_slice():
     assert masked(rc, 2) and masked(rc, 3) and not any(masked(rc, i) for i in (0, 1, 4, 5))
 
 
-# ---- src/seeds.rs:260-356 -----------------------------------------------------------
+# ---- src/seeds.rs:185-281 -----------------------------------------------------------
 def test_seed_words():
     assert O.word_at(O.pack_ascii(b"ACGT"), "1111", 0) == 0x1B                  # :291-299
     assert O.word_at(O.pack_ascii(b"ACGT"), "1001", 0) == 0b0011                # :301-309
@@ -152,7 +152,7 @@ def test_avx2_matches_scalar(seed):
         assert O.extend_hit(T, Q, p, tp, qp, L) == O.extend_hit(T, Q, p, tp, qp, L, avx2=True)
 
 
-# ---- src/seed_search.rs:362-506 -----------------------------------------------------
+# ---- src/seed_search.rs:136-280 -----------------------------------------------------
 def search(t, q, pattern, xdrop, thresh, transitions):
     T, Q = O.pack_ascii(t), O.pack_ascii(q)
     h, _ = O.search(O.Table(T, pattern, 1), T, Q, HOX(xdrop=xdrop, hspthresh=thresh, transitions=transitions))

@@ -35,6 +35,22 @@ def static_build(gxy, seq, pattern: str, step: int):
     return st, ps
 
 
+def check_against_both(gxy, s: bytes, pattern: str, step: int):
+    """The static build equals gxy_table_build's table and the oracle's
+    PosTable::build (src/pos_table.rs:35-83), bucket order included."""
+    import oracle as O
+    T = gxy.PackedSeq.from_ascii(s)
+    got_starts, got_pos = static_build(gxy, T, pattern, step)
+    ref = gxy.PosTable.build(T, pattern, step)
+    ref_starts, ref_pos = ref.arrays()
+    assert np.array_equal(got_starts, ref_starts)
+    assert np.array_equal(got_pos, ref_pos)
+    ref.free()
+    orc = O.Table(O.pack_ascii(s), pattern, step)
+    assert np.array_equal(got_starts, orc.starts())
+    assert np.array_equal(got_pos, orc.positions())
+
+
 @pytest.mark.parametrize("pattern,step", [("1110100110010101111", 1), ("11111111", 2)])
 def test_static_build_matches_table_build(gxy, pattern, step):
     import torch
@@ -42,13 +58,20 @@ def test_static_build_matches_table_build(gxy, pattern, step):
     rng = np.random.default_rng(7 + step)
     seqs = [rand_ascii(rng, 300_000, b"ACGTACGTacgtN"), rand_ascii(rng, 170_001, b"ACGTacgN")]
     for s in seqs:   # two calls in a row through the shared static array
-        T = gxy.PackedSeq.from_ascii(s)
-        got_starts, got_pos = static_build(gxy, T, pattern, step)
-        ref = gxy.PosTable.build(T, pattern, step)
-        ref_starts, ref_pos = ref.arrays()
-        assert np.array_equal(got_starts, ref_starts)
-        assert np.array_equal(got_pos, ref_pos)
-        ref.free()
+        check_against_both(gxy, s, pattern, step)
+
+
+def test_static_build_edges(gxy):
+    # A target shorter than the pattern (no windows: the sort runs on zero
+    # keys and every bucket is empty), then one of exactly the size limit
+    # (the array's layout at its bound), then a short one again, whose result
+    # must not see the large one's leftovers.
+    import torch
+    torch.cuda.init()
+    rng = np.random.default_rng(11)
+    check_against_both(gxy, b"ACGTACGTACGTACGTAC", "1110100110010101111", 1)
+    check_against_both(gxy, rand_ascii(rng, 1 << 20, b"ACGTACGTacgtN"), "1110100110010101111", 1)
+    check_against_both(gxy, rand_ascii(rng, 5_000, b"ACGTacgt"), "1110100110010101111", 1)
 
 
 def test_static_build_rejects_oversize(gxy):
