@@ -42,7 +42,8 @@ typedef enum {
     GXY_ETIMEDOUT = 4,      /* a bounded device or host wait ran out */
     GXY_ECUDA = 5,          /* CUDA runtime error */
     GXY_ENOTREADY = 6,      /* serving: request not finished yet */
-    GXY_EOVERFLOW = 7       /* a caller-provided buffer is too small; *needed is set */
+    GXY_EOVERFLOW = 7,      /* a caller-provided buffer is too small; *needed is set */
+    GXY_ECANCELED = 8       /* serving: the request was cancelled before its results were kept */
 } gxy_status;
 
 typedef struct gxy_ctx gxy_ctx;       /* one device, its streams and memory pool */
@@ -134,8 +135,8 @@ typedef struct {
                                      0 in the context = keep what each stream's buffers grew to */
     uint32_t filter_cap;          /* upper-bound filter: columns per side after which a hit is
                                      passed on unexamined (a multiple of 32, 32..256) */
-    uint32_t filter_flush;        /* upper-bound filter: queued hits per warp that start a filter
-                                     round (32..512) */
+    uint32_t filter_claim;        /* upper-bound filter: raw hits a warp claims at a time (32..4096;
+                                     1 = sized from each launch's hit count, the default) */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
@@ -386,8 +387,27 @@ typedef struct {
     uint64_t bytes_in_use;
     uint64_t reruns;        /* batches' pipeline runs repeated after a buffer had to grow */
     double busy_ms;         /* summed device time of the batches */
+    uint64_t failed;        /* requests that completed with an error status */
+    uint64_t canceled;      /* requests cancelled before their results were kept */
+    uint64_t isolated;      /* failed batches whose requests were rerun one by one */
+    uint64_t mem_refreshes; /* free-device-memory queries since creation */
 } gxy_server_stats;
 gxy_status gxy_server_get_stats(gxy_server* s, gxy_server_stats* st);
+/* Cancels a request.  A queued request leaves the queue at once; one already
+ * in a running batch finishes on the device but its results are dropped.
+ * Either way gxy_server_wait then returns GXY_ECANCELED for it.  A request
+ * that has already completed keeps its results (the call still returns
+ * GXY_OK); an unknown id (never submitted, or already waited for) is
+ * GXY_EINVAL. */
+gxy_status gxy_server_cancel(gxy_server* s, uint64_t request_id);
+/* Test hook (fault injection on the host): every batch that holds
+ * request_id fails with `status` before any device work, as a failed device
+ * allocation would.  A failed batch of several requests is rerun one request
+ * at a time, so only the faulty request completes with that status.
+ * status GXY_OK clears the fault.  Ids are handed out in submission order
+ * starting at 1, so a fault can be set for an id not yet submitted (it then
+ * holds from the moment that request is queued). */
+gxy_status gxy_server_inject_fault(gxy_server* s, uint64_t request_id, gxy_status status);
 gxy_status gxy_server_destroy(gxy_server* s);
 
 #if defined(__GNUC__)

@@ -61,9 +61,9 @@ class Context:
         return cls._default[device]
 
     def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0,
-                   max_hits_per_pass=0, initial_candidates=0, filter_cap=0, filter_flush=0) -> None:
+                   max_hits_per_pass=0, initial_candidates=0, filter_cap=0, filter_claim=0) -> None:
         t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass,
-                         initial_candidates, filter_cap, filter_flush)
+                         initial_candidates, filter_cap, filter_claim)
         check(lib().gxy_ctx_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -72,7 +72,7 @@ class Context:
         return {"screen_warps": t.screen_warps, "screen_cap": t.screen_cap,
                 "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps,
                 "max_hits_per_pass": t.max_hits_per_pass, "initial_candidates": t.initial_candidates,
-                "filter_cap": t.filter_cap, "filter_flush": t.filter_flush}
+                "filter_cap": t.filter_cap, "filter_claim": t.filter_claim}
 
     def mark(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's primary stream."""

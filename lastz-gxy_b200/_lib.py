@@ -13,7 +13,8 @@ import subprocess
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgxyseed.so")
 
-GXY_OK, GXY_EINVAL, GXY_ENOMEM, GXY_EUNSUPPORTED, GXY_ETIMEDOUT, GXY_ECUDA, GXY_ENOTREADY, GXY_EOVERFLOW = range(8)
+(GXY_OK, GXY_EINVAL, GXY_ENOMEM, GXY_EUNSUPPORTED, GXY_ETIMEDOUT, GXY_ECUDA, GXY_ENOTREADY, GXY_EOVERFLOW,
+ GXY_ECANCELED) = range(9)
 
 
 class GxyError(RuntimeError):
@@ -64,7 +65,7 @@ class SeqSetC(C.Structure):
 class TuningC(C.Structure):
     _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
                 ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32), ("initial_candidates", C.c_uint32),
-                ("filter_cap", C.c_uint32), ("filter_flush", C.c_uint32)]
+                ("filter_cap", C.c_uint32), ("filter_claim", C.c_uint32)]
 
 
 class UnitC(C.Structure):
@@ -100,7 +101,8 @@ class ServerOptsC(C.Structure):
 class ServerStatsC(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("max_inflight_units", C.c_uint64), ("bytes_in_use", C.c_uint64), ("reruns", C.c_uint64),
-                ("busy_ms", C.c_double)]
+                ("busy_ms", C.c_double), ("failed", C.c_uint64), ("canceled", C.c_uint64),
+                ("isolated", C.c_uint64), ("mem_refreshes", C.c_uint64)]
 
 
 V = C.c_void_p
@@ -148,6 +150,8 @@ SIGNATURES = {
     "gxy_server_wait": (C.c_int, [V, U64, U32, P(HspBufC), P(HspBufC), P(C.c_double)]),
     "gxy_server_get_stats": (C.c_int, [V, P(ServerStatsC)]),
     "gxy_server_destroy": (C.c_int, [V]),
+    "gxy_server_cancel": (C.c_int, [V, U64]),
+    "gxy_server_inject_fault": (C.c_int, [V, U64, C.c_int]),
     "gxy_choose_anchors": (C.c_int, [V, V, V, P(SearchParamsC), V, U64, U32, V, V]),
     "gxy_best_chain": (C.c_int, [V, U64, V, P(C.c_uint64)]),
     "gxy_parse_fasta": (C.c_int, [V, V, U64, P(SeqSetC)]),

@@ -2,10 +2,10 @@
 
 The tunables:
 
-* filter_flush -- hits per warp that the fused enumerate + upper-bound filter
-  kernel queues in shared memory before a filter round (the hits-per-warp
-  batch: larger rounds leave fewer lanes idle at a round's end, smaller ones
-  keep the queue's hits closer to the query windows that produced them);
+* filter_claim -- raw hits a warp of the upper-bound filter claims at a time
+  (the hits-per-warp batch: larger claims cost fewer atomics, smaller ones
+  balance the warps better at the end of a launch; 1 sizes it from each
+  launch's hit count);
 * filter_cap -- columns per side after which the filter passes a hit on to
   the exact screen unexamined;
 * screen_cap -- columns per side after which the exact lane screen hands a
@@ -30,7 +30,7 @@ import os
 from typing import Optional
 
 DEFAULT_SPACE = {
-    "filter_flush": [256, 128, 512],
+    "filter_claim": [1, 128, 512],
     "filter_cap": [96, 64, 160],
     "screen_cap": [192, 128],
     "screen_warps": [8, 16],

@@ -267,6 +267,7 @@ const char* gxy_status_string(gxy_status s) {
         case GXY_ECUDA: return "CUDA error";
         case GXY_ENOTREADY: return "not ready";
         case GXY_EOVERFLOW: return "buffer too small";
+        case GXY_ECANCELED: return "cancelled";
     }
     return "unknown status";
 }
@@ -376,7 +377,8 @@ gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
     if (t->max_hits_per_pass) ctx->tuning.max_hits_per_pass = std::max<uint32_t>(4096, t->max_hits_per_pass);
     if (t->initial_candidates) ctx->tuning.initial_candidates = std::max<uint32_t>(1024, t->initial_candidates);
     if (t->filter_cap) ctx->tuning.filter_cap = std::min<uint32_t>(256, std::max<uint32_t>(32, t->filter_cap & ~31u));
-    if (t->filter_flush) ctx->tuning.filter_flush = std::min<uint32_t>(512, std::max<uint32_t>(32, t->filter_flush));
+    if (t->filter_claim)
+        ctx->tuning.filter_claim = t->filter_claim == 1 ? 1u : std::min<uint32_t>(4096, std::max<uint32_t>(32, t->filter_claim));
     return GXY_OK;
 }
 

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 
 namespace gxy {
@@ -144,7 +145,7 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     for (DevBuf* b : {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->prim_sums, &w->prim_hist, &w->counters, &w->d_units,
                       &w->d_tsegs, &w->d_qsegs, &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags,
                       &w->offsets, &w->ohsp, &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2,
-                      &w->hits})
+                      &w->hits, &w->surv})
         b->st = w->st;
     for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
@@ -399,13 +400,12 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     sa.sc.hspthresh = p.hspthresh;
     sa.cap = std::max<uint32_t>(32, ctx->tuning.screen_cap);
     sa.qkey_total = (uint32_t)qk;
-    // Enumeration fused with the upper-bound filter when the scores admit
-    // class bounds (they do for every matrix with a non-positive class);
-    // otherwise every raw hit goes to the exact screen.
+    // The upper-bound filter runs between enumeration and the exact screen
+    // when the scores admit class bounds (every matrix with a class whose
+    // scores are all <= 0); otherwise the exact screen takes every raw hit.
     sa.f_cap = std::max<uint32_t>(32, ctx->tuning.filter_cap);
-    sa.f_flush = std::max<uint32_t>(32, ctx->tuning.filter_flush);
-    bool use_filter = filter_bounds(sa);
-    for (const UnitPlan& u : units) use_filter = use_filter && u.occ != nullptr;
+    sa.f_claim = ctx->tuning.filter_claim > 1 ? ctx->tuning.filter_claim : 0u;
+    const bool use_filter = filter_bounds(sa);
 
     RadixPass passes[16];
     const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
@@ -418,6 +418,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     uint32_t* cnt = W->counters.as<uint32_t>();
     unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + kCStats);
     unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + kCHits);
+    unsigned long long* survc = reinterpret_cast<unsigned long long*>(cnt + kCSurv);
     if (ctx->tuning.initial_candidates) W->cand_cap = ctx->tuning.initial_candidates;
     if (W->cand_cap == 0) W->cand_cap = 2u << 20;
     if (W->hit_cap == 0) W->hit_cap = 32ull << 20;
@@ -432,9 +433,15 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     {
         double est = 1 << 20;
         for (const UnitPlan& u : units) est += 1.5 * (double)u.nwin * sa.n_var * u.avg_bucket;
-        // The hit buffer holds the filter's survivors only (a few percent of
-        // the raw hits); the candidate estimate stays on raw hits.
-        const double est_buf = use_filter ? (1 << 20) + est / kRawPerSurvivorSlot : est;
+        // The survivor buffer holds a few percent of the raw hits.
+        const double est_buf = est;
+        if (use_filter) {
+            const uint64_t want_s = (uint64_t)std::min<double>((double)kMaxHitCap, (1 << 20) + est / kRawPerSurvivorSlot);
+            if (want_s > W->surv_cap) {
+                W->surv.release();
+                W->surv_cap = want_s;
+            }
+        }
         // Candidates from the same estimate (a few percent of the raw hits
         // pass the screen): an overflow would rerun the whole launch.
         const uint64_t want_cand = std::min<uint64_t>((uint64_t)(est / kHitsPerCandidate), kMaxPresizedCandidates);
@@ -463,8 +470,22 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(cudaMemsetAsync(hitc, 0, 8, st));
         sa.tile_lo = t0;
         sa.tile_hi = t1;
-        if (use_filter) launch_seed_filter(sa, ctx->sm_count, 16, st);
-        else launch_enumerate(sa, ctx->sm_count, st);
+        if (use_filter) {
+            // Raw hits -> the bounded filter -> survivors -> the exact screen.
+            GXY_CK(cudaMemsetAsync(survc, 0, 8, st));
+            GXY_CK(cudaMemsetAsync(cnt + kCFiltNext, 0, 4, st));
+            launch_enumerate(sa, ctx->sm_count, st);
+            ScreenArgs sv = sa;
+            sv.hits = W->surv.as<Hit>();
+            sv.hit_cap = W->surv_cap;
+            sv.hit_count = survc;
+            FilterIO io{sa.hits, hitc, sa.hit_cap, cnt + kCFiltNext};
+            launch_filter_hits(sv, io, ctx->sm_count, st);
+            if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
+            launch_screen(sv, (int)ctx->tuning.screen_warps, blocks_screen, st);
+            return GXY_OK;
+        }
+        launch_enumerate(sa, ctx->sm_count, st);
         if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
         launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
         return GXY_OK;
@@ -486,8 +507,9 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     uint32_t reruns = 0;   // pipeline runs (or passes) repeated after a buffer grew
     for (int attempt = 0; attempt < 16; attempt++) {
         uint32_t cap = W->cand_cap;
-        uint64_t survivors = 0;   // hits the passes wrote to the hit buffer
+        uint64_t survivors = 0;   // hits the passes passed on to the exact screen
         GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
+        if (use_filter) GXY_CK(W->surv.ensure((size_t)W->surv_cap * sizeof(Hit)));
         GXY_CK(W->ck0.ensure((size_t)cap * 8));
         GXY_CK(W->ck1.ensure((size_t)cap * 8));
         GXY_CK(W->cv0.ensure((size_t)cap * 4));
@@ -546,6 +568,24 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                 GXY_CK(cudaMemcpyAsync(after.data(), cnt, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
                 GXY_CK(cudaStreamSynchronize(st));
                 const unsigned long long nh = *reinterpret_cast<const unsigned long long*>(after.data() + kCHits);
+                const unsigned long long ns = *reinterpret_cast<const unsigned long long*>(after.data() + kCSurv);
+                if (use_filter && nh <= W->hit_cap && ns > W->surv_cap) {
+                    // Survivors overflowed (the screen skipped the pass): grow, redo the pass.
+                    W->surv.release();
+                    const uint64_t want = ns + ns / 2 + (1u << 20);
+                    if (want > kMaxHitCap) {
+                        // Too many for one buffer: fewer tiles per pass instead.
+                        W->surv_cap = kMaxHitCap;
+                        pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)(t1 - t0) * kMaxHitCap / ns * 0.8));
+                    } else {
+                        W->surv_cap = want;
+                    }
+                    GXY_CK(W->surv.ensure((size_t)W->surv_cap * sizeof(Hit)));
+                    GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
+                    GXY_CK(cudaStreamSynchronize(st));
+                    reruns++;
+                    continue;
+                }
                 if (after[kCCand] > cap && nh <= W->hit_cap) {
                     // Candidates overflowed in this pass: grow the candidate
                     // arrays keeping the earlier passes' entries, redo the pass.
@@ -581,7 +621,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
                     continue;
                 }
                 t0 = t1;
-                survivors += nh;
+                survivors += use_filter ? ns : nh;
                 // Hit density varies along the query (repeats): grow the
                 // window range again after a sparse pass, up to twice.
                 if ((double)nh < 0.5 * (double)W->hit_cap) {
@@ -729,7 +769,20 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + kCStats);
         const unsigned long long nhits = *reinterpret_cast<const unsigned long long*>(hc + kCHits);
         const uint32_t ncand = hc[kCCand];
-        if (single) survivors = nhits;
+        const unsigned long long nsurv = *reinterpret_cast<const unsigned long long*>(hc + kCSurv);
+        if (single) survivors = use_filter ? nsurv : nhits;
+        if (single && use_filter && nhits <= W->hit_cap && nsurv > W->surv_cap) {
+            W->surv.release();
+            const uint64_t want = nsurv + nsurv / 4 + (1u << 20);
+            if (want > kMaxHitCap) {
+                W->surv_cap = kMaxHitCap;
+                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / nsurv * 0.8));
+            } else {
+                W->surv_cap = want;
+            }
+            reruns++;
+            continue;
+        }
         if (single && nhits > W->hit_cap) {
             // Raw hits overflowed the hit buffer: grow it, or split into passes.
             if (nhits + nhits / 8 <= kMaxHitCap) {

@@ -44,6 +44,8 @@ struct Worker {
     DevBuf d_place, rrec;         // driver records: per-unit places, records
     DevBuf hits;                  // raw hits of one pass
     uint64_t hit_cap = 0;
+    DevBuf surv;                  // hits of one pass that pass the upper-bound filter
+    uint64_t surv_cap = 0;
     uint32_t cand_cap = 0;
     uint32_t res_cap = 0;
     void* h_pinned = nullptr;     // small host staging: counters, unit and segment descriptors
@@ -71,7 +73,7 @@ struct UnitPlan {
 
 // Layout of a worker's device counters (u32 indices).
 constexpr uint32_t kCTile = 0, kCHsps = 2, kCRecs = 4, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072,
-                   kCWalk = 3584;
+                   kCSurv = 3328, kCWalk = 3584, kCFiltNext = 3840;
 constexpr uint32_t kCounterWords = 4096;
 // Candidate arrays are sized up front at one candidate per this many
 // estimated raw hits (the estimate carries a 1.5x margin; about 3 % of raw
@@ -144,7 +146,7 @@ struct gxy_ctx {
     // Screen column cap 192 (the packed screen's limit): on the 10 Mbp plain
     // launch, longer screening leaves fewer candidates for the walk to
     // re-extend (two searches 4.27 ms, against 4.31 ms at 128 and 4.51 at 64).
-    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 256};
+    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 1};
     cudaEvent_t marks[16] = {};
 };
 

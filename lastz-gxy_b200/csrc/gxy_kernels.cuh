@@ -107,26 +107,34 @@ struct ScreenArgs {
     uint32_t cand_cap;
     uint32_t* cand_count;
     unsigned long long* stats;   // [0] windows, [1] raw hits, [2] columns examined, [3] filter columns
-    // Upper-bound filter of k_seed_filter (FilterBounds in gxy_filter.cu).
+    // The upper-bound filter (gxy_filter.cu, filter_bounds).
     int32_t fub[4];        // per class x = t_code ^ q_code: the largest score of that class
     uint64_t f_inv;        // class word given to the columns where either base is invalid
     uint64_t f_end;        // class word given to the columns past a side's end
     int32_t f_seed_max;    // seed length x the largest class bound
     uint32_t f_cap;        // columns per side after which a hit survives unexamined
-    uint32_t f_flush;      // queued hits per warp that start a filter round
+    uint32_t f_claim;      // raw hits a filter warp claims at a time (0: sized from the hit count)
 };
 // Seed-hit enumeration: one warp per tile of 32 query windows; writes the
 // hits of every (window, variant) bucket to a.hits.
 void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st);
 // Capped lane-per-hit x-drop over a.hits; keeps the candidates.  grid = persistent.
 void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);
-// Seed-hit enumeration fused with an upper-bound x-drop filter: writes to
-// a.hits only the hits that might reach hspthresh (gxy_filter.cu).
-// filter_bounds fills a's fub/f_inv/f_end/f_seed_max from a.sc and a.pat and
-// returns false when the scoring admits no such bound (then the caller runs
-// launch_enumerate + launch_screen over every raw hit).
+// The upper-bound x-drop filter between enumeration and the exact screen
+// (gxy_filter.cu).  filter_bounds fills a's fub/f_inv/f_end/f_seed_max from
+// a.sc and a.pat and returns false when the scoring admits no such bound
+// (then the exact screen takes every raw hit).
 bool filter_bounds(ScreenArgs& a);
-void launch_seed_filter(const ScreenArgs& a, int sm_count, int warps_per_block, cudaStream_t st);
+// The bounded x-drop over a raw-hit array: reads
+// io.raw[0, *io.raw_count) (nothing when that count exceeds io.raw_cap) and
+// writes the survivors to a.hits / a.hit_count / a.hit_cap.
+struct FilterIO {
+    const Hit* raw;
+    const unsigned long long* raw_count;
+    uint64_t raw_cap;
+    uint32_t* cursor;      // zeroed by the caller
+};
+void launch_filter_hits(const ScreenArgs& a, const FilterIO& io, int sm_count, cudaStream_t st);
 // Bucket occupancy bitmap of a table: bit (w & 31) of occ[w >> 5] is set iff
 // bucket w holds a position.
 void launch_occupancy(const uint32_t* starts, uint64_t num_words, uint32_t* occ, cudaStream_t st);

@@ -38,7 +38,9 @@ struct Request {
     Clock::time_point submitted;
     Clock::time_point done_at;
     bool done = false;
+    bool canceled = false;
     gxy_status status = GXY_OK;
+    gxy_status fault = GXY_OK;          // injected failure (test hook), GXY_OK when none
     std::vector<gxy_hsp> plus, minus;
 };
 
@@ -76,13 +78,30 @@ struct gxy_server {
     size_t free_at_create = 0;
     uint64_t pool_at_create = 0;
     cudaMemPool_t pool = nullptr;
+    // Other processes on a shared GPU allocate too, which the pool counter
+    // cannot see: a monitor thread re-reads the free memory every
+    // kMemRefreshMs, off the dispatch path, so the estimate's drift is
+    // bounded by what others allocate within that interval.
+    std::thread monitor;
+    std::condition_variable cv_stop;
+    std::map<uint64_t, gxy_status> future_faults;   // injected faults of ids not yet submitted
 };
+
+static constexpr int kMemRefreshMs = 500;
 
 namespace {
 
 // Runs one batch of requests on worker W.  Called without the server lock.
 gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
     cudaStream_t stream = W->st;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        for (Request* q : batch)
+            if (q->fault != GXY_OK) {
+                set_error("injected fault");
+                return q->fault;
+            }
+    }
     const Pattern& pat = s->tables[0]->pat;
     std::vector<gxy_dseq*> owned;
     auto cleanup = [&]() {
@@ -256,13 +275,35 @@ void dispatcher(gxy_server* s) {
             s->st.max_inflight_units = std::max<uint64_t>(s->st.max_inflight_units, s->units_in_flight);
             s->st.bytes_in_use = s->bytes_in_use;
         }
-        const gxy_status e = run_batch(s, W, batch);
+        std::vector<gxy_status> status(batch.size(), run_batch(s, W, batch));
+        if (status[0] != GXY_OK && batch.size() > 1) {
+            // One request's failure (an allocation, an input outside the
+            // exact envelope) must not fail its batch-mates: rerun the
+            // requests one at a time, each with its own status.
+            {
+                std::lock_guard<std::mutex> g(s->mu);
+                s->st.isolated++;
+            }
+            for (size_t i = 0; i < batch.size(); i++) {
+                std::vector<Request*> one{batch[i]};
+                batch[i]->plus.clear();
+                batch[i]->minus.clear();
+                status[i] = run_batch(s, W, one);
+            }
+        }
         {
             std::lock_guard<std::mutex> g(s->mu);
             const auto now = Clock::now();
             if (batch_big) s->big_in_flight--;
-            for (Request* q : batch) {
-                q->status = e;
+            for (size_t i = 0; i < batch.size(); i++) {
+                Request* q = batch[i];
+                q->status = q->canceled ? GXY_ECANCELED : status[i];
+                if (q->status != GXY_OK) {
+                    q->plus.clear();
+                    q->minus.clear();
+                    if (q->canceled) s->st.canceled++;
+                    else s->st.failed++;
+                }
                 q->done = true;
                 q->done_at = now;
                 q->codes.clear();
@@ -281,6 +322,31 @@ void dispatcher(gxy_server* s) {
         s->cv_work.notify_all();
     }
     checkin(s->ctx, W);
+}
+
+// Re-reads the device's free memory every kMemRefreshMs (cudaMemGetInfo
+// can take tens of milliseconds on a busy device, so only this thread calls
+// it) and re-bases the admission estimate on it.
+void memory_monitor(gxy_server* s) {
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stop) {
+        s->cv_stop.wait_for(lk, std::chrono::milliseconds(kMemRefreshMs), [&] { return s->stop; });
+        if (s->stop) break;
+        lk.unlock();
+        size_t free_b = 0, total_b = 0;
+        uint64_t reserved = 0;
+        const bool ok = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
+        if (ok && s->pool) cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaGetLastError();
+        lk.lock();
+        if (ok) {
+            // Free memory now already excludes the pool's current reservation.
+            s->free_at_create = free_b;
+            s->pool_at_create = reserved;
+            s->st.mem_refreshes++;
+        }
+    }
 }
 
 gxy_status copy_out(const std::vector<gxy_hsp>& v, gxy_hsp_buf* out) {
@@ -333,6 +399,7 @@ gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* c
     if (!o.max_big_inflight) o.max_big_inflight = 1;
     s->opts = o;
     for (uint32_t i = 0; i < o.max_streams; i++) s->threads.emplace_back(dispatcher, s);
+    s->monitor = std::thread(memory_monitor, s);
     if (o.warm_bases) {
         // Return once every dispatcher holds its warmed buffers.
         std::unique_lock<std::mutex> lk(s->mu);
@@ -364,6 +431,11 @@ gxy_status gxy_server_submit(gxy_server* s, uint32_t table, const gxy_packed_seq
             return GXY_EINVAL;
         }
         q->id = s->next_id++;
+        auto f = s->future_faults.find(q->id);
+        if (f != s->future_faults.end()) {
+            q->fault = f->second;
+            s->future_faults.erase(f);
+        }
         s->requests[q->id] = q;
         s->pending.push_back(q);
         s->st.submitted++;
@@ -404,6 +476,51 @@ gxy_status gxy_server_get_stats(gxy_server* s, gxy_server_stats* st) {
     return GXY_OK;
 }
 
+gxy_status gxy_server_cancel(gxy_server* s, uint64_t request_id) {
+    if (!s) return GXY_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) {
+        set_error("unknown request id");
+        return GXY_EINVAL;
+    }
+    Request* q = it->second;
+    if (q->done) return GXY_OK;
+    q->canceled = true;
+    auto p = std::find(s->pending.begin(), s->pending.end(), q);
+    if (p != s->pending.end()) {
+        // Still queued: it never reaches the device.
+        s->pending.erase(p);
+        q->status = GXY_ECANCELED;
+        q->done = true;
+        q->done_at = Clock::now();
+        q->codes.clear();
+        q->valid.clear();
+        q->mask.clear();
+        s->st.canceled++;
+        s->st.completed++;
+        s->cv_done.notify_all();
+    }
+    return GXY_OK;
+}
+
+gxy_status gxy_server_inject_fault(gxy_server* s, uint64_t request_id, gxy_status status) {
+    if (!s) return GXY_EINVAL;
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) {
+        if (request_id >= s->next_id) {
+            // Ids are handed out in submission order: the fault waits for it.
+            s->future_faults[request_id] = status;
+            return GXY_OK;
+        }
+        set_error("unknown request id");
+        return GXY_EINVAL;
+    }
+    it->second->fault = status;
+    return GXY_OK;
+}
+
 gxy_status gxy_server_destroy(gxy_server* s) {
     if (!s) return GXY_OK;
     {
@@ -411,6 +528,8 @@ gxy_status gxy_server_destroy(gxy_server* s) {
         s->stop = true;
     }
     s->cv_work.notify_all();
+    s->cv_stop.notify_all();
+    if (s->monitor.joinable()) s->monitor.join();
     for (auto& t : s->threads) t.join();
     for (auto& kv : s->requests) delete kv.second;
     delete s;

@@ -42,12 +42,31 @@ class Server:
         check(lib().gxy_server_wait(self.h, request_id, timeout_ms, C.byref(plus), C.byref(minus), C.byref(lat)))
         return _take_buf(plus), _take_buf(minus), lat.value
 
+    def wait_status(self, request_id: int, timeout_ms: int = 600000):
+        """Like wait(), but returns (status, plus, minus, latency_ms) instead of
+        raising when the request completed with an error status."""
+        from . import _take_buf
+        plus, minus = _lib.HspBufC(), _lib.HspBufC()
+        lat = C.c_double()
+        st = lib().gxy_server_wait(self.h, request_id, timeout_ms, C.byref(plus), C.byref(minus), C.byref(lat))
+        if st != _lib.GXY_OK:
+            return st, None, None, lat.value
+        return st, _take_buf(plus), _take_buf(minus), lat.value
+
+    def cancel(self, request_id: int) -> None:
+        check(lib().gxy_server_cancel(self.h, request_id))
+
+    def inject_fault(self, request_id: int, status: int) -> None:
+        """Test hook: batches holding this request fail with `status` before any device work."""
+        check(lib().gxy_server_inject_fault(self.h, request_id, status))
+
     def stats(self) -> dict:
         s = _lib.ServerStatsC()
         check(lib().gxy_server_get_stats(self.h, C.byref(s)))
         return {"submitted": s.submitted, "completed": s.completed, "batches": s.batches,
                 "max_inflight_units": s.max_inflight_units, "bytes_in_use": s.bytes_in_use, "reruns": s.reruns,
-                "busy_ms": s.busy_ms}
+                "busy_ms": s.busy_ms, "failed": s.failed, "canceled": s.canceled, "isolated": s.isolated,
+                "mem_refreshes": s.mem_refreshes}
 
     def close(self) -> None:
         if self.h:

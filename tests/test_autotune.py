@@ -19,7 +19,7 @@ class FakeCtx:
 
     def __init__(self):
         self.t = {"screen_warps": 8, "screen_cap": 192, "screen_blocks_per_sm": 4, "walk_warps": 8,
-                  "max_hits_per_pass": 1 << 28, "initial_candidates": 0, "filter_cap": 96, "filter_flush": 256}
+                  "max_hits_per_pass": 1 << 28, "initial_candidates": 0, "filter_cap": 96, "filter_claim": 256}
         self.applied = []
 
     def tuning(self):
@@ -57,16 +57,16 @@ def fake_batch(ctx, cost, bad=None):
 def test_picks_fastest_and_caches(gxy, tmp_path, monkeypatch):
     from lastz_gxy_b200 import autotune as at
     ctx = FakeCtx()
-    # Fastest at filter_flush 512, filter_cap 64, walk_warps 4.
-    cost = lambda t: (10.0 - (t["filter_flush"] == 512) * 2 - (t["filter_cap"] == 64) - (t["walk_warps"] == 4) * 0.5)
+    # Fastest at filter_claim 512, filter_cap 64, walk_warps 4.
+    cost = lambda t: (10.0 - (t["filter_claim"] == 512) * 2 - (t["filter_cap"] == 64) - (t["walk_warps"] == 4) * 0.5)
     fn, calls = fake_batch(ctx, cost)
     monkeypatch.setattr(gxy, "batch_search", fn)
     cache = str(tmp_path / "tune.json")
     units = [(0, i, s) for i in range(40) for s in (0, 1)]
     e = at.autotune(ctx, [FakeTable()], [None], units, None, Params(1), workload="w", sample_units=16, reps=1,
                     cache=cache)
-    assert e["tuning"]["filter_flush"] == 512 and e["tuning"]["filter_cap"] == 64 and e["tuning"]["walk_warps"] == 4
-    assert ctx.t["filter_flush"] == 512 and ctx.t["filter_cap"] == 64
+    assert e["tuning"]["filter_claim"] == 512 and e["tuning"]["filter_cap"] == 64 and e["tuning"]["walk_warps"] == 4
+    assert ctx.t["filter_claim"] == 512 and ctx.t["filter_cap"] == 64
     assert e["sample_units"] == 16
     store = json.load(open(cache))
     key = at.tuning_key(ctx, P12, 1, "w")
@@ -75,7 +75,7 @@ def test_picks_fastest_and_caches(gxy, tmp_path, monkeypatch):
     n = len(calls)
     ctx2 = FakeCtx()
     e2 = at.autotune(ctx2, [FakeTable()], [None], units, None, Params(1), workload="w", cache=cache)
-    assert len(calls) == n and e2["tuning"] == e["tuning"] and ctx2.t["filter_flush"] == 512
+    assert len(calls) == n and e2["tuning"] == e["tuning"] and ctx2.t["filter_claim"] == 512
     # Zero transitions is a different key: tuned afresh.
     at.autotune(FakeCtx(), [FakeTable()], [None], units, None, Params(0), workload="w", sample_units=16, reps=1,
                 cache=cache)
