@@ -63,9 +63,9 @@ def peaks() -> tuple[float, str]:
 
 
 def profiled_traffic():
-    """DRAM bytes of the screen and enumerate kernels from one committed ncu
-    capture (profiles/kernel_traffic.json), with the raw hits of that launch;
-    None when the file is absent."""
+    """DRAM read + write bytes per launch of the search kernels, measured by
+    ncu on the plain workload's plus-strand search (profiles/kernel_traffic.json,
+    with the command that made it); None when the file is absent."""
     p = os.path.join(ROOT, "profiles", "kernel_traffic.json")
     try:
         with open(p) as f:
@@ -74,14 +74,17 @@ def profiled_traffic():
         return None
 
 
-def scaled_traffic(tr, kernel: str, raw_hits: float):
-    """Per-launch DRAM traffic of `kernel` at this launch's raw hits: the
-    captured read + write bytes scaled by raw hits (both kernels' traffic
-    grows with the hits they enumerate or screen)."""
-    if not tr or kernel not in tr:
-        return None
-    k = tr[kernel]
-    return int((k["dram_read_bytes"] + k["dram_write_bytes"]) * raw_hits / k["raw_hits"])
+def measured_traffic(tr, kernel: str, raw_hits: float):
+    """(bytes, source) of `kernel` for a launch with raw_hits raw hits: the
+    measured bytes when the capture is of this workload (same raw hits), else
+    the measurement scaled by raw hits and labelled an estimate."""
+    if not tr or kernel not in tr.get("kernels", {}):
+        return None, None
+    k = tr["kernels"][kernel]
+    b = k["dram_read_bytes"] + k["dram_write_bytes"]
+    if tr.get("raw_hits") == int(round(raw_hits)):
+        return int(b), f"measured: ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch ({tr['workload']})"
+    return int(b * raw_hits / tr["raw_hits"]), "ESTIMATE: the ncu capture in profiles/kernel_traffic.json scaled by raw hits"
 
 
 class ClockSampler:
@@ -144,20 +147,27 @@ def mbp2(lt: int, lq: int, strands: int = 2) -> float:
 
 
 def screen_bytes(st: dict, seed_len: int) -> float:
-    """Algorithmic bytes of one x-drop screen launch: 8 B per raw hit read
-    (t, q), 3/8 B x 2 per examined column -- codes + valid bits of both
-    sequences over the seed footprint and the columns both sides scanned,
-    break columns included -- and 44 B per candidate written (record, key,
-    index)."""
-    cols = st["columns"] + seed_len * st["raw_hits"]
-    return 8.0 * st["raw_hits"] + 0.75 * cols + 44.0 * st["candidates"]
+    """Algorithmic bytes of one exact-screen launch: 12 B per surviving hit
+    read (t, q, unit), 3/8 B x 2 per examined column -- codes + valid bits of
+    both sequences over the seed footprint and the columns both sides
+    scanned, break columns included -- and 44 B per candidate written
+    (record, key, index)."""
+    cols = st["columns"] + seed_len * st["survivors"]
+    return 12.0 * st["survivors"] + 0.75 * cols + 44.0 * st["candidates"]
+
+
+def filter_bytes(st: dict) -> float:
+    """Algorithmic bytes of one upper-bound filter launch: 12 B per raw hit
+    read, 3/8 B x 2 per column it scanned on the two sides (codes + valid bits
+    of both sequences), 12 B per survivor written."""
+    return 12.0 * st["raw_hits"] + 0.75 * st["filter_columns"] + 12.0 * st["survivors"]
 
 
 def enum_bytes(st: dict, lq: int, n_var: int) -> float:
     """Algorithmic bytes of one enumeration launch: 0.5 B/bp of query read,
     8 B of starts per (seedable window, variant), 4 B of positions per raw hit,
-    8 B per raw hit written."""
-    return 0.5 * lq + 8.0 * n_var * st["windows"] + 12.0 * st["raw_hits"]
+    12 B per raw hit written."""
+    return 0.5 * lq + 8.0 * n_var * st["windows"] + 16.0 * st["raw_hits"]
 
 
 def table_roofline(ms_list, npos, lt: int, peak: float) -> dict:
@@ -294,20 +304,34 @@ def run_ours(args, rank: int, world: int, device: int):
     per_step = mbp2(lt, lq)
     value = world * per_step * args.steps / (total_ms / 1e3)
     e2e_value = world * per_step * args.steps / (e2e_ms / 1e3)
-    # Roofline of the dominant kernel (the screen), from the timed steps.
+    # Rooflines of the three search kernels from the timed steps (the two
+    # strands share the device there) and alone (one launch at a time, after
+    # the timed steps); the dominant kernel is the one with the most time alone.
     stats = [s for s, _ in dev_col]
-    scr_ms = statistics.mean(s["screen_ms"] for s in stats)
-    scr_bytes = statistics.mean(screen_bytes(s, 19) for s in stats)
-    en_ms = statistics.mean(s["enum_ms"] for s in stats)
-    en_bytes = statistics.mean(enum_bytes(s, lq, n_var) for s in stats)
-    peak, peak_kind = peaks()
-    achieved = scr_bytes / (scr_ms / 1e3) / 1e9
-    en_achieved = en_bytes / (en_ms / 1e3) / 1e9
-    tr = profiled_traffic()
     ser = [s for s, _ in ser_col]
-    ser_scr_ms = statistics.mean(s["screen_ms"] for s in ser)
-    ser_en_ms = statistics.mean(s["enum_ms"] for s in ser)
+    peak, peak_kind = peaks()
+    tr = profiled_traffic()
     raw = statistics.mean(s["raw_hits"] for s in stats)
+    kern = {}
+    for name, key, fb in (("k_enumerate", "enum_ms", lambda s: enum_bytes(s, lq, n_var)),
+                          ("k_filter_hits", "filter_ms", filter_bytes),
+                          ("k_screen", "screen_ms", lambda s: screen_bytes(s, 19))):
+        ms = statistics.mean(s[key] for s in stats)
+        ms_alone = statistics.mean(s[key] for s in ser)
+        byt = statistics.mean(fb(s) for s in stats)
+        traffic, tsrc = measured_traffic(tr, name, raw)
+        kern[name] = {"bound": "hbm", "kernel": name, "achieved": round(byt / (ms / 1e3) / 1e9, 1),
+                      "peak": peak, "unit": "GB/s", "frac": round(byt / (ms / 1e3) / 1e9 / peak, 4),
+                      "traffic": traffic, "traffic_source": tsrc,
+                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                      else "fallback 6.65 TB/s",
+                      "kernel_ms": round(ms, 3), "algorithmic_bytes_per_launch": int(byt),
+                      "timing": "CUDA events around each launch on its stream in the timed steps, where the other "
+                                "strand's search shares the device",
+                      "alone": {"kernel_ms": round(ms_alone, 3), "achieved": round(byt / (ms_alone / 1e3) / 1e9, 1),
+                                "frac": round(byt / (ms_alone / 1e3) / 1e9 / peak, 4),
+                                "timing": "the same launches one at a time after the timed steps"}}
+    dominant = max(kern, key=lambda k: kern[k]["kernel_ms"])
     nh = sum(n for _, n in dev_col) / args.steps
     h2d = (T.codes.nbytes + T.valid.nbytes + T.mask.nbytes) + (Q.codes.nbytes + Q.valid.nbytes + Q.mask.nbytes)
     d2h = int(sum(e2e_col) / args.steps) * 16
@@ -328,28 +352,11 @@ def run_ours(args, rank: int, world: int, device: int):
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms / args.steps, 3),
                 "host_buffers": "pinned PackedSeq arrays in, HSP arrays out"},
         "gpu_launches": int(launches * args.steps),
-        "roofline": {"bound": "hbm", "kernel": "k_screen", "achieved": round(achieved, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": scaled_traffic(tr, "k_screen", raw),
-                     "traffic_source": "ESTIMATE: ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                       "k_screen launch on the 4 Mbp case (profiles/kernel_traffic.json), scaled "
-                                       "to this launch by raw hits",
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                     else "fallback 6.65 TB/s",
-                     "kernel_ms": round(scr_ms, 3), "algorithmic_bytes_per_launch": int(scr_bytes),
-                     "timing": "CUDA events around each launch in the timed steps, where the other strand's "
-                               "search shares the device; alone: the same launches one at a time after the timed steps",
-                     "alone": {"kernel_ms": round(ser_scr_ms, 3),
-                               "achieved": round(scr_bytes / (ser_scr_ms / 1e3) / 1e9, 1),
-                               "frac": round(scr_bytes / (ser_scr_ms / 1e3) / 1e9 / peak, 4)}},
+        "roofline": kern[dominant],
+        "roofline_kernels": kern,
         "roofline_table": table_roofline(table_ms[-args.steps:], table_npos[-1], lt, peak),
-        "roofline_enumerate": {"bound": "hbm", "kernel": "k_enumerate", "achieved": round(en_achieved, 1),
-                               "peak": peak, "unit": "GB/s", "frac": round(en_achieved / peak, 4),
-                               "kernel_ms": round(en_ms, 3), "algorithmic_bytes_per_launch": int(en_bytes),
-                               "traffic": scaled_traffic(tr, "k_enumerate", raw),
-                               "alone": {"kernel_ms": round(ser_en_ms, 3),
-                                         "achieved": round(en_bytes / (ser_en_ms / 1e3) / 1e9, 1),
-                                         "frac": round(en_bytes / (ser_en_ms / 1e3) / 1e9 / peak, 4)}},
+        "filter": {"survivors_per_raw_hit": round(statistics.mean(s["survivors"] / max(1, s["raw_hits"]) for s in stats), 5),
+                   "candidates_per_survivor": round(statistics.mean(s["candidates"] / max(1, s["survivors"]) for s in stats), 4)},
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu:

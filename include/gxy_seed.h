@@ -103,7 +103,8 @@ typedef struct {
     uint64_t candidates;   /* hits that pass or run past the screen's column cap */
     uint64_t hsps;         /* HSPs returned */
     double device_ms;      /* CUDA-event time of the call's device work */
-    double screen_ms;      /* CUDA-event time of the x-drop screen kernel (with enumeration when passes > 1) */
+    double screen_ms;      /* CUDA-event time of the exact x-drop screen kernel (with enumeration and
+                              the filter when passes > 1) */
     uint64_t columns;      /* alignment columns the screen scanned on the two sides */
     double enum_ms;        /* CUDA-event time of the hit enumeration kernel (single pass) */
     uint32_t passes;       /* window-range passes the raw hits needed */
@@ -111,6 +112,7 @@ typedef struct {
     uint64_t survivors;    /* raw hits the upper-bound filter passed on to the exact screen
                               (equal to raw_hits when the filter does not apply) */
     uint64_t filter_columns; /* alignment columns the upper-bound filter scanned on the two sides */
+    double filter_ms;      /* CUDA-event time of the upper-bound filter kernel (single pass) */
 } gxy_stats;
 
 const char* gxy_status_string(gxy_status s);

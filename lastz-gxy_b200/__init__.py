@@ -409,7 +409,8 @@ class PosTable:
 def _stats(st: _lib.StatsC) -> dict:
     return {"windows": st.windows, "raw_hits": st.raw_hits, "candidates": st.candidates, "hsps": st.hsps,
             "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns, "enum_ms": st.enum_ms,
-            "passes": st.passes, "reruns": st.reruns, "survivors": st.survivors, "filter_columns": st.filter_columns}
+            "passes": st.passes, "reruns": st.reruns, "survivors": st.survivors, "filter_columns": st.filter_columns,
+            "filter_ms": st.filter_ms}
 
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:

@@ -55,7 +55,7 @@ class StatsC(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
                 ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double),
                 ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reruns", C.c_uint32),
-                ("survivors", C.c_uint64), ("filter_columns", C.c_uint64)]
+                ("survivors", C.c_uint64), ("filter_columns", C.c_uint64), ("filter_ms", C.c_double)]
 
 
 class SeqSetC(C.Structure):

@@ -147,7 +147,7 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
                       &w->offsets, &w->ohsp, &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2,
                       &w->hits, &w->surv})
         b->st = w->st;
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
+    for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
     w->ps.sort_grid_max = ctx->sm_count * 8;
     if (e == cudaSuccess)
@@ -475,6 +475,7 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             GXY_CK(cudaMemsetAsync(survc, 0, 8, st));
             GXY_CK(cudaMemsetAsync(cnt + kCFiltNext, 0, 4, st));
             launch_enumerate(sa, ctx->sm_count, st);
+            if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[4], st));
             ScreenArgs sv = sa;
             sv.hits = W->surv.as<Hit>();
             sv.hit_cap = W->surv_cap;
@@ -486,7 +487,10 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             return GXY_OK;
         }
         launch_enumerate(sa, ctx->sm_count, st);
-        if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
+        if (single_pass_timing && !in_capture) {
+            GXY_CK(cudaEventRecord(W->ev[4], st));
+            GXY_CK(cudaEventRecord(W->ev[3], st));
+        }
         launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
         return GXY_OK;
     };
@@ -815,14 +819,20 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         out.stats.survivors = use_filter ? survivors : hs[1];
         out.stats.candidates = ncand;
         out.stats.hsps = nh;
-        float ms = 0.f, ms_enum = 0.f, ms_screen = 0.f;
+        float ms = 0.f, ms_enum = 0.f, ms_filter = 0.f, ms_screen = 0.f;
         GXY_CK(cudaEventElapsedTime(&ms, W->ev[0], W->ev[2]));
         if (!graph_now) {
-            GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[3]));
+            if (single) {
+                GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[4]));
+                GXY_CK(cudaEventElapsedTime(&ms_filter, W->ev[4], W->ev[3]));
+            } else {
+                GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[3]));
+            }
             GXY_CK(cudaEventElapsedTime(&ms_screen, W->ev[3], W->ev[1]));
         }
         out.stats.device_ms = ms;
         out.stats.enum_ms = single ? ms_enum : 0.0;
+        out.stats.filter_ms = single ? ms_filter : 0.0;
         out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;
         out.stats.passes = single ? 1 : (uint32_t)((tiles + pass_tiles - 1) / pass_tiles);
         out.stats.reruns = reruns;

@@ -34,7 +34,7 @@ struct DevBuf {
 struct Worker {
     cudaStream_t st = nullptr;
     DevBuf tk0, tv0, tk1, tv1;    // table-build temporaries
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // start, screen end, end, filter end, enumerate end
     PrimScratch ps{};
     DevBuf prim_sums, prim_hist;
     DevBuf counters;              // u32[8] + u64[4]
