@@ -318,6 +318,8 @@ def run_ours(args, rank: int, world: int, device: int):
                           ("k_screen", "screen_ms", lambda s: screen_bytes(s, 19))):
         ms = statistics.mean(s[key] for s in stats)
         ms_alone = statistics.mean(s[key] for s in ser)
+        if ms <= 0 or ms_alone <= 0:
+            continue   # not timed (a multi-pass launch)
         byt = statistics.mean(fb(s) for s in stats)
         traffic, tsrc = measured_traffic(tr, name, raw)
         kern[name] = {"bound": "hbm", "kernel": name, "achieved": round(byt / (ms / 1e3) / 1e9, 1),

@@ -113,6 +113,8 @@ typedef struct {
                               (equal to raw_hits when the filter does not apply) */
     uint64_t filter_columns; /* alignment columns the upper-bound filter scanned on the two sides */
     double filter_ms;      /* CUDA-event time of the upper-bound filter kernel (single pass) */
+    uint32_t rounds;       /* host rounds of passes (each ends with the epilogue and one counter copy) */
+    uint32_t graph_updates; /* rounds launched by updating the worker's kept CUDA graph in place */
 } gxy_stats;
 
 const char* gxy_status_string(gxy_status s);
@@ -161,6 +163,7 @@ gxy_status gxy_dseq_reverse_complement(gxy_ctx* ctx, const gxy_dseq* in, gxy_dse
  * ceil(len/8) bytes; any pointer may be NULL. */
 gxy_status gxy_dseq_download(const gxy_dseq* s, uint8_t* codes, uint8_t* valid, uint8_t* mask);
 uint64_t gxy_dseq_len(const gxy_dseq* s);
+/* Frees a device sequence; valid before or after its context is destroyed. */
 gxy_status gxy_dseq_free(gxy_dseq* s);
 
 /* ---- input formats (src/sequences.rs:338-377, src/bit2.rs:73-163) -------- */
@@ -226,6 +229,7 @@ gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_p
 /* Copies starts (num_words + 1 entries) and positions to host buffers; either
  * may be NULL. */
 gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions);
+/* Frees a table; valid before or after its context is destroyed. */
 gxy_status gxy_table_free(gxy_table* t);
 
 /* ---- the drop-in search (src/seed_search.rs:45-125) --------------------- */
@@ -344,6 +348,16 @@ gxy_status gxy_choose_anchors(gxy_ctx* ctx, const gxy_dseq* target, const gxy_ds
  * tie rules; out holds up to n HSPs, *out_n receives the chain length.  Host
  * code, O(n log n) (the reference scans O(n^2)); empty HSPs: GXY_EINVAL. */
 gxy_status gxy_best_chain(const gxy_hsp* hsps, uint64_t n, gxy_hsp* out, uint64_t* out_n);
+/* best_chain (src/chain.rs:19-69) for n_groups groups at once on the device
+ * (the driver's --chain applies it per (target, query, strand) group,
+ * src/driver.rs).  Group g is hsps[group_offsets[g] .. group_offsets[g+1]);
+ * group_offsets has n_groups + 1 entries, starts at 0 and does not decrease.
+ * Group g's chain goes to out[group_offsets[g] ..] in t_start order (the rest
+ * of its range is zeroed) and its length to chain_len[g].  The reference's
+ * O(n^2) scan, one block per group, with its tie rules; any HSP length is
+ * accepted.  Host buffers; fewer than 2^31 HSPs in all. */
+gxy_status gxy_best_chain_groups(gxy_ctx* ctx, const gxy_hsp* hsps, const uint64_t* group_offsets,
+                                 uint32_t n_groups, gxy_hsp* out, uint64_t* chain_len);
 
 /* ---- serving loop ---------------------------------------------------------- */
 /* Keeps the given tables resident, admits submitted queries while device

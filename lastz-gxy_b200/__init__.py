@@ -28,7 +28,7 @@ RECORD_DTYPE = np.dtype([("group", "<u4"), ("t_start", "<u4"), ("q_start", "<u4"
                          ("score", "<i4"), ("unit", "<u4")])
 
 __all__ = [
-    "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "choose_anchors", "best_chain", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
+    "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "choose_anchors", "best_chain", "best_chain_groups", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
     "SearchParams", "PosTable", "search", "search_device", "batch_search", "batch_records", "RECORD_DTYPE",
     "chunk_target", "extend_hits",
     "Server", "build", "canonical_sort",
@@ -410,7 +410,7 @@ def _stats(st: _lib.StatsC) -> dict:
     return {"windows": st.windows, "raw_hits": st.raw_hits, "candidates": st.candidates, "hsps": st.hsps,
             "device_ms": st.device_ms, "screen_ms": st.screen_ms, "columns": st.columns, "enum_ms": st.enum_ms,
             "passes": st.passes, "reruns": st.reruns, "survivors": st.survivors, "filter_columns": st.filter_columns,
-            "filter_ms": st.filter_ms}
+            "filter_ms": st.filter_ms, "rounds": st.rounds, "graph_updates": st.graph_updates}
 
 
 def _take_buf(buf: _lib.HspBufC) -> np.ndarray:
@@ -588,6 +588,22 @@ def best_chain(hsps: np.ndarray) -> np.ndarray:
     check(lib().gxy_best_chain(h.ctypes.data if len(h) else None, len(h),
                                out.ctypes.data if len(h) else None, C.byref(n)))
     return out[:n.value].copy()
+
+
+def best_chain_groups(groups, ctx: Optional[Context] = None) -> list:
+    """best_chain (src/chain.rs:19-69) for every HSP array of `groups` at once
+    on the device: one chain (an HSP array in t_start order) per group."""
+    ctx = ctx or Context.default()
+    arrs = [np.ascontiguousarray(np.asarray(g, HSP_DTYPE)) for g in groups]
+    off = np.zeros(len(arrs) + 1, np.uint64)
+    if arrs:
+        off[1:] = np.cumsum([len(a) for a in arrs])
+    h = np.concatenate(arrs) if arrs else np.empty(0, HSP_DTYPE)
+    out = np.empty(len(h), HSP_DTYPE)
+    ln = np.zeros(max(len(arrs), 1), np.uint64)
+    check(lib().gxy_best_chain_groups(ctx.h, h.ctypes.data if len(h) else None, off.ctypes.data, len(arrs),
+                                      out.ctypes.data if len(h) else None, ln.ctypes.data))
+    return [out[int(off[g]):int(off[g]) + int(ln[g])].copy() for g in range(len(arrs))]
 
 
 def chunk_target(target_len: int, primary_bp: int, halo_bp: int) -> list:

@@ -55,7 +55,8 @@ class StatsC(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("candidates", C.c_uint64),
                 ("hsps", C.c_uint64), ("device_ms", C.c_double), ("screen_ms", C.c_double),
                 ("columns", C.c_uint64), ("enum_ms", C.c_double), ("passes", C.c_uint32), ("reruns", C.c_uint32),
-                ("survivors", C.c_uint64), ("filter_columns", C.c_uint64), ("filter_ms", C.c_double)]
+                ("survivors", C.c_uint64), ("filter_columns", C.c_uint64), ("filter_ms", C.c_double),
+                ("rounds", C.c_uint32), ("graph_updates", C.c_uint32)]
 
 
 class SeqSetC(C.Structure):
@@ -154,6 +155,7 @@ SIGNATURES = {
     "gxy_server_inject_fault": (C.c_int, [V, U64, C.c_int]),
     "gxy_choose_anchors": (C.c_int, [V, V, V, P(SearchParamsC), V, U64, U32, V, V]),
     "gxy_best_chain": (C.c_int, [V, U64, V, P(C.c_uint64)]),
+    "gxy_best_chain_groups": (C.c_int, [V, V, V, U32, V, V]),
     "gxy_parse_fasta": (C.c_int, [V, V, U64, P(SeqSetC)]),
     "gxy_parse_2bit": (C.c_int, [V, V, U64, P(SeqSetC)]),
     "gxy_seq_set_free": (None, [P(SeqSetC)]),

@@ -104,6 +104,7 @@ gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t 
     const uint32_t nwin = n_windows(hi - lo, pat.len, step);
     gxy_table* t = new gxy_table();
     t->ctx = ctx;
+    t->device = ctx->device;
     t->seq = seq;
     t->lo = lo;
     t->hi = hi;
@@ -273,7 +274,7 @@ const char* gxy_status_string(gxy_status s) {
 }
 
 const char* gxy_last_error(void) { return last_error(); }
-uint32_t gxy_abi_version(void) { return 2; }
+uint32_t gxy_abi_version(void) { return 3; }
 uint64_t gxy_kernel_launches(void) { return launches(); }
 
 gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
@@ -301,6 +302,7 @@ gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
     uint64_t thr = ~0ull;
     API_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     prims_init();
+    filter_init();
     gxy_ctx* c = new gxy_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
@@ -324,14 +326,15 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         DevBuf* bufs[] = {&w->prim_sums, &w->prim_hist, &w->counters, &w->d_units, &w->d_tsegs, &w->d_qsegs,
                           &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags, &w->offsets, &w->ohsp,
                           &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2, &w->hits,
-                          &w->d_place, &w->rrec};
+                          &w->d_place, &w->rrec, &w->surv, &w->redo, &w->rk0, &w->rk1, &w->rv0, &w->rv1};
         for (DevBuf* b : bufs) b->release();
+        if (w->gexec) cudaGraphExecDestroy(w->gexec);
         dseq_destroy(w->qstage);
         dseq_destroy(w->tstage);
         for (gxy_dseq* d : w->rc_tmp) dseq_destroy(d);
         DevBuf* tb[] = {&w->tk0, &w->tv0, &w->tk1, &w->tv1};
         for (DevBuf* b : tb) b->release();
-        for (int i = 0; i < 4; i++)
+        for (int i = 0; i < 5; i++)
             if (w->ev[i]) cudaEventDestroy(w->ev[i]);
         if (w->h_pinned) cudaFreeHost(w->h_pinned);
         if (w->h_res) cudaFreeHost(w->h_res);
@@ -474,7 +477,7 @@ uint64_t gxy_dseq_len(const gxy_dseq* s) { return s ? s->len : 0; }
 
 gxy_status gxy_dseq_free(gxy_dseq* s) {
     if (!s) return GXY_OK;
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     dseq_destroy(s);
     return GXY_OK;
 }
@@ -553,7 +556,7 @@ gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* po
 
 gxy_status gxy_table_free(gxy_table* t) {
     if (!t) return GXY_OK;
-    cudaSetDevice(t->ctx->device);
+    cudaSetDevice(t->device);
     dev_free(t->starts);
     dev_free(t->positions);
     dev_free(t->occ);

@@ -3,6 +3,7 @@
 #include "gxy_engine.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdlib>
 #include <cstring>
@@ -64,6 +65,7 @@ void dev_free(void* p) {
 gxy_status dseq_alloc(gxy_ctx* ctx, uint64_t len, gxy_dseq** out, cudaStream_t st) {
     gxy_dseq* d = new gxy_dseq();
     d->ctx = ctx;
+    d->device = ctx->device;
     d->len = len;
     uint64_t nw = (kPad + len + kTailPad + 31) / 32;
     nw = (nw + 3) & ~3ull;   // each array a multiple of 16 bytes
@@ -145,7 +147,7 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     for (DevBuf* b : {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->prim_sums, &w->prim_hist, &w->counters, &w->d_units,
                       &w->d_tsegs, &w->d_qsegs, &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags,
                       &w->offsets, &w->ohsp, &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2,
-                      &w->hits, &w->surv})
+                      &w->hits, &w->surv, &w->redo, &w->rk0, &w->rk1, &w->rv0, &w->rv1})
         b->st = w->st;
     for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
@@ -293,6 +295,47 @@ gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t hits, uint64_t candi
     return GXY_OK;
 }
 
+// Captures what `issue` launches on the worker's stream into a CUDA graph and
+// launches it.  The instantiated graph stays with the worker: a later call
+// with the same shape (the same kernels in the same order; launch arguments
+// may differ) updates it in place instead of instantiating anew.
+template <typename F>
+static gxy_status run_graph(Worker* W, F&& issue) {
+    cudaStream_t st = W->st;
+    GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const gxy_status is = issue();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (is != GXY_OK || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (is != GXY_OK) return is;
+        set_error(std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+        return GXY_ECUDA;
+    }
+    bool updated = false;
+    if (W->gexec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(W->gexec, g, &info) == cudaSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(W->gexec);
+            W->gexec = nullptr;
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (!updated) e = cudaGraphInstantiate(&W->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        W->gexec = nullptr;
+        set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
+    W->graph_updates += updated ? 1 : 0;
+    GXY_CK(cudaGraphLaunch(W->gexec, st));
+    return GXY_OK;
+}
+
 gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units, std::vector<SeqView>& tsegs,
                      std::vector<SeqView>& qsegs, const Pattern& pat, const gxy_search_params& p, bool use_graph,
                      RunResult& out) {
@@ -410,11 +453,6 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
     RadixPass passes[16];
     const int npass = plan_radix(0, bits_for(tk ? tk - 1 : 0), 32, bits_for(tk + qk), passes, 16);
 
-    // Device counters (kCounterWords u32): the ones the kernels hit with
-    // atomics all the time sit 4 KB apart so that they fall in different L2
-    // slices.  u32 [kCTile] tile, [kCCand] candidates, [kCHsps] HSPs,
-    // [kCHitNext] screen hit cursor; u64 at [kCStats]: windows, raw hits,
-    // columns; u64 at [kCHits]: raw hits of the pass.
     uint32_t* cnt = W->counters.as<uint32_t>();
     unsigned long long* st64 = reinterpret_cast<unsigned long long*>(cnt + kCStats);
     unsigned long long* hitc = reinterpret_cast<unsigned long long*>(cnt + kCHits);
@@ -427,14 +465,14 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         W->hits.release();
         W->hit_cap = kMaxHitCap;
     }
-    uint32_t pass_tiles = (uint32_t)tiles;
-    // Size the raw-hit buffer from the expected hits (windows x variants x mean
-    // bucket, with margin) so that large searches do not run twice.
+    // Size the raw-hit buffer from the expected hits (windows x variants x
+    // mean bucket, with margin); a launch with more raw hits than the buffer
+    // holds runs as several passes, each taking tiles until the buffer is
+    // full and handing the tile that did not fit to the next pass, all on
+    // the device.
+    double est = 1 << 20;
+    for (const UnitPlan& u : units) est += 1.5 * (double)u.nwin * sa.n_var * u.avg_bucket;
     {
-        double est = 1 << 20;
-        for (const UnitPlan& u : units) est += 1.5 * (double)u.nwin * sa.n_var * u.avg_bucket;
-        // The survivor buffer holds a few percent of the raw hits.
-        const double est_buf = est;
         if (use_filter) {
             const uint64_t want_s = (uint64_t)std::min<double>((double)kMaxHitCap, (1 << 20) + est / kRawPerSurvivorSlot);
             if (want_s > W->surv_cap) {
@@ -446,72 +484,148 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         // pass the screen): an overflow would rerun the whole launch.
         const uint64_t want_cand = std::min<uint64_t>((uint64_t)(est / kHitsPerCandidate), kMaxPresizedCandidates);
         if (want_cand > W->cand_cap) W->cand_cap = (uint32_t)want_cand;
-        if (est_buf > (double)W->hit_cap) {
-            if (est_buf <= (double)kMaxHitCap) {
-                W->hits.release();
-                W->hit_cap = (uint64_t)est_buf;
-            } else {
-                W->hits.release();
-                W->hit_cap = kMaxHitCap;
-                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / est_buf));
-            }
+        const uint64_t want_hits = std::min<uint64_t>(kMaxHitCap, (uint64_t)est);
+        if (want_hits > W->hit_cap) {
+            W->hits.release();
+            W->hit_cap = want_hits;
         }
     }
     const int blocks_screen = ctx->sm_count * (int)std::max<uint32_t>(1, ctx->tuning.screen_blocks_per_sm);
     const int blocks_misc = ctx->sm_count * 4;
     const int walk_warps = ctx->tuning.walk_warps == 4 ? 4 : 8;
+    GXY_CK(W->redo.ensure((size_t)2 * kRedoCap * 4));
 
-    // One pass: enumerate tiles [t0, t1) into the hit buffer, then screen them.
-    bool single_pass_timing = false;
-    bool in_capture = false;
-    auto pass = [&](uint32_t t0, uint32_t t1) -> gxy_status {
-        GXY_CK(cudaMemsetAsync(cnt + kCTile, 0, 4, st));
-        GXY_CK(cudaMemsetAsync(cnt + kCHitNext, 0, 4, st));
-        GXY_CK(cudaMemsetAsync(hitc, 0, 8, st));
-        sa.tile_lo = t0;
-        sa.tile_hi = t1;
+    // One pass: start it (k_pass_reset), enumerate into the hit buffer, filter
+    // and screen.  With timing (a one-pass launch outside a graph) the kernels
+    // are bracketed by events 0 / 4 / 3 / 1.
+    auto pass = [&](bool timing) {
+        launch_pass_reset(cnt, use_filter ? W->surv_cap : ~0ull, st);
+        if (timing) cudaEventRecord(W->ev[0], st);
+        launch_enumerate(sa, ctx->sm_count, st);
+        if (timing) cudaEventRecord(W->ev[4], st);
         if (use_filter) {
             // Raw hits -> the bounded filter -> survivors -> the exact screen.
-            GXY_CK(cudaMemsetAsync(survc, 0, 8, st));
-            GXY_CK(cudaMemsetAsync(cnt + kCFiltNext, 0, 4, st));
-            launch_enumerate(sa, ctx->sm_count, st);
-            if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[4], st));
             ScreenArgs sv = sa;
             sv.hits = W->surv.as<Hit>();
             sv.hit_cap = W->surv_cap;
             sv.hit_count = survc;
             FilterIO io{sa.hits, hitc, sa.hit_cap, cnt + kCFiltNext};
             launch_filter_hits(sv, io, ctx->sm_count, st);
-            if (single_pass_timing && !in_capture) GXY_CK(cudaEventRecord(W->ev[3], st));
+            if (timing) cudaEventRecord(W->ev[3], st);
             launch_screen(sv, (int)ctx->tuning.screen_warps, blocks_screen, st);
-            return GXY_OK;
+        } else {
+            if (timing) cudaEventRecord(W->ev[3], st);
+            launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
         }
-        launch_enumerate(sa, ctx->sm_count, st);
-        if (single_pass_timing && !in_capture) {
-            GXY_CK(cudaEventRecord(W->ev[4], st));
-            GXY_CK(cudaEventRecord(W->ev[3], st));
-        }
-        launch_screen(sa, (int)ctx->tuning.screen_warps, blocks_screen, st);
+        if (timing) cudaEventRecord(W->ev[1], st);
+    };
+
+    // After the passes: sort the candidates by (diagonal, t), walk the
+    // diagonals, compact, group by unit, order each run, and (with places)
+    // make the driver's records; then the counters come back to the host.
+    Hsp* fin = nullptr;
+    uint32_t* fin_unit = nullptr;
+    uint32_t cap = W->cand_cap;
+    auto epilogue = [&]() -> gxy_status {
+        const int which = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
+                                             W->cv1.as<uint32_t>(), cnt + kCCand, 0, cap, passes, npass, W->ps, st);
+            const uint64_t* skeys = which ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
+            const uint32_t* sidx = which ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
+            GXY_CK(cudaMemsetAsync(W->flags.p, 0, cap, st));
+            WalkArgs wa;
+            memset(&wa, 0, sizeof(wa));
+            wa.keys = skeys;
+            wa.idx = sidx;
+            wa.cands = W->cands.as<Cand>();
+            wa.n_dev = cnt + kCCand;
+            wa.n_cap = cap;
+            wa.units = sa.units;
+            wa.tsegs = sa.tsegs;
+            wa.qsegs = sa.qsegs;
+            wa.seed_len = pat.len;
+            wa.sc = sa.sc;
+            wa.has_entropy = p.has_entropy;
+            wa.entropy_thr = p.entropy_thr;
+            wa.out_flag = W->flags.as<uint8_t>();
+            wa.out_hsp = W->ohsp.as<Hsp>();
+            wa.chunk_next = cnt + kCWalk;
+            wa.n_units = nu;
+            GXY_CK(cudaMemsetAsync(cnt + kCWalk, 0, 4, st));
+            launch_walk(wa, walk_warps, blocks_misc, st);
+            scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCCand, 0, cap, false, cnt + kCHsps, W->ps,
+                    st);
+            launch_compact(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), W->ohsp.as<Hsp>(), sidx,
+                           W->cands.as<Cand>(), cnt + kCCand, cap, W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), blocks_misc, st);
+            fin = W->rhsp.as<Hsp>();
+            fin_unit = W->runit.as<uint32_t>();
+            if (nu > 1) {
+                // Group by unit, keeping each unit's (diagonal, t) order: stable sort.
+                RadixPass up[4];
+                const int nup = plan_radix(0, bits_for(nu - 1), 0, 0, up, 4);
+                launch_iota(W->perm.as<uint32_t>(), cnt + kCHsps, cap, blocks_misc, st);
+                GXY_CK(cudaMemcpyAsync(W->runit2.p, W->runit.p, (size_t)cap * 4, cudaMemcpyDeviceToDevice, st));
+                const int w2 = radix_sort_u32(W->runit2.as<uint32_t>(), W->perm.as<uint32_t>(), W->offsets.as<uint32_t>(),
+                                              W->perm2.as<uint32_t>(), cnt + kCHsps, 0, cap, up, nup, W->ps, st);
+                const uint32_t* perm = w2 ? W->perm2.as<uint32_t>() : W->perm.as<uint32_t>();
+                launch_gather_hsp(W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), perm, cnt + kCHsps, cap, W->rhsp2.as<Hsp>(),
+                                  W->runit2.as<uint32_t>(), blocks_misc, st);
+                fin = W->rhsp2.as<Hsp>();
+                fin_unit = W->runit2.as<uint32_t>();
+            }
+            launch_fixup(fin, fin_unit, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
+            if (records) {
+                // Driver records (src/driver.rs:371-391): stable LSD sort by
+                // (group, global t, q, span) over the unit-major HSP order, then
+                // drop repeats of the same four fields, keeping the first.  One
+                // sort of a packed key when the fields fit 64 bits, else (q, span)
+                // first and (group, t) second.
+                const Place* pl = W->d_place.as<Place>();
+                RadixPass rp[16];
+                const uint32_t* perm;
+                if (rb_g + rb_t + rb_q + rb_l <= 64) {
+                    const int sh_q = rb_l, sh_t = rb_l + rb_q, sh_g = rb_l + rb_q + rb_t;
+                    launch_record_keys(fin, fin_unit, pl, nullptr, cnt + kCHsps, cap, 0, sh_g, sh_t, sh_q,
+                                       W->rk0.as<uint64_t>(), W->rv0.as<uint32_t>(), blocks_misc, st);
+                    const int np = plan_radix(0, rb_l + rb_q + rb_t + rb_g, 0, 0, rp, 16);
+                    const int w = radix_sort_u64(W->rk0.as<uint64_t>(), W->rv0.as<uint32_t>(), W->rk1.as<uint64_t>(),
+                                                 W->rv1.as<uint32_t>(), cnt + kCHsps, 0, cap, rp, np, W->ps, st);
+                    perm = w ? W->rv1.as<uint32_t>() : W->rv0.as<uint32_t>();
+                } else {
+                    launch_record_keys(fin, fin_unit, pl, nullptr, cnt + kCHsps, cap, 1, 0, 0, 0, W->rk0.as<uint64_t>(),
+                                       W->rv0.as<uint32_t>(), blocks_misc, st);
+                    int np = plan_radix(0, rb_l, 32, rb_q, rp, 16);
+                    int w = radix_sort_u64(W->rk0.as<uint64_t>(), W->rv0.as<uint32_t>(), W->rk1.as<uint64_t>(),
+                                           W->rv1.as<uint32_t>(), cnt + kCHsps, 0, cap, rp, np, W->ps, st);
+                    const uint32_t* p1 = w ? W->rv1.as<uint32_t>() : W->rv0.as<uint32_t>();
+                    uint64_t* k2 = w ? W->rk0.as<uint64_t>() : W->rk1.as<uint64_t>();
+                    uint32_t* v2 = w ? W->rv0.as<uint32_t>() : W->rv1.as<uint32_t>();
+                    uint64_t* k3 = w ? W->rk1.as<uint64_t>() : W->rk0.as<uint64_t>();
+                    uint32_t* v3 = w ? W->rv1.as<uint32_t>() : W->rv0.as<uint32_t>();
+                    launch_record_keys(fin, fin_unit, pl, p1, cnt + kCHsps, cap, 2, 0, 0, 0, k2, v2, blocks_misc, st);
+                    np = plan_radix(0, rb_t, 32, rb_g, rp, 16);
+                    w = radix_sort_u64(k2, v2, k3, v3, cnt + kCHsps, 0, cap, rp, np, W->ps, st);
+                    perm = w ? v3 : v2;
+                }
+                launch_record_heads(fin, fin_unit, pl, perm, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
+                scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCHsps, 0, cap, false, cnt + kCRecs,
+                        W->ps, st);
+                launch_record_emit(fin, fin_unit, pl, perm, W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(),
+                                   cnt + kCHsps, cap, W->rrec.as<Record>(), blocks_misc, st);
+            }
+            GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
         return GXY_OK;
     };
 
-    // Grows a buffer to `bytes`, keeping its first `keep` bytes.
-    auto grow_keep = [&](DevBuf& b, size_t bytes, size_t keep) -> cudaError_t {
-        if (bytes <= b.bytes && b.p) return cudaSuccess;
-        void* np = nullptr;
-        cudaError_t e = cudaMallocAsync(&np, bytes, b.st);
-        if (e != cudaSuccess) return e;
-        if (b.p && keep) e = cudaMemcpyAsync(np, b.p, keep, cudaMemcpyDeviceToDevice, b.st);
-        if (b.p) cudaFreeAsync(b.p, b.st);
-        b.p = np;
-        b.bytes = bytes;
-        return e;
-    };
-
-    uint32_t reruns = 0;   // pipeline runs (or passes) repeated after a buffer grew
+    // Passes in the first round: the estimate's share of the buffer, with
+    // room to spare (a pass with nothing left to do returns at once).
+    const uint64_t est_hits = (uint64_t)est;
+    const uint64_t first_round = std::min<uint64_t>(
+        256, std::max<uint64_t>(1, (est_hits + W->hit_cap - 1) / std::max<uint64_t>(1, W->hit_cap)));
+    uint32_t reruns = 0;   // launches repeated after a buffer had to grow
+    const uint64_t graph_updates0 = W->graph_updates;
+    uint32_t rounds = 0;
     for (int attempt = 0; attempt < 16; attempt++) {
-        uint32_t cap = W->cand_cap;
-        uint64_t survivors = 0;   // hits the passes passed on to the exact screen
+        cap = W->cand_cap;
         GXY_CK(W->hits.ensure((size_t)W->hit_cap * sizeof(Hit)));
         if (use_filter) GXY_CK(W->surv.ensure((size_t)W->surv_cap * sizeof(Hit)));
         GXY_CK(W->ck0.ensure((size_t)cap * 8));
@@ -528,7 +642,13 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         GXY_CK(W->runit2.ensure((size_t)cap * 4));
         GXY_CK(W->perm.ensure((size_t)cap * 4));
         GXY_CK(W->perm2.ensure((size_t)cap * 4));
-        if (records) GXY_CK(W->rrec.ensure((size_t)cap * sizeof(Record)));
+        if (records) {
+            GXY_CK(W->rrec.ensure((size_t)cap * sizeof(Record)));
+            GXY_CK(W->rk0.ensure((size_t)cap * 8));
+            GXY_CK(W->rk1.ensure((size_t)cap * 8));
+            GXY_CK(W->rv0.ensure((size_t)cap * 4));
+            GXY_CK(W->rv1.ensure((size_t)cap * 4));
+        }
         sa.tile_counter = cnt + kCTile;
         sa.cand_count = cnt + kCCand;
         sa.hit_next = cnt + kCHitNext;
@@ -540,263 +660,78 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
         sa.cand_vals = W->cv0.as<uint32_t>();
         sa.cands = W->cands.as<Cand>();
         sa.cand_cap = cap;
+        sa.ctl = cnt;
+        sa.redo = W->redo.as<uint32_t>();
 
-        const bool single = pass_tiles >= tiles;
-        const bool graph_now = use_graph && single;
-        // Ends an open capture if this attempt leaves early with an error.
-        struct CaptureGuard {
-            cudaStream_t st;
-            bool active = false;
-            ~CaptureGuard() {
-                if (!active) return;
-                cudaGraph_t g = nullptr;
-                cudaStreamEndCapture(st, &g);
-                if (g) cudaGraphDestroy(g);
-                cudaGetLastError();
-            }
-        } capture{st};
-        single_pass_timing = single;
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t gexec = nullptr;
+        // Round one: counters cleared, the passes, the epilogue and the
+        // counters' copy back -- one CUDA graph (kept across calls and
+        // updated in place) when use_graph, else plain launches.
+        const uint32_t n_round = (uint32_t)first_round;
+        const bool timing = !use_graph && n_round == 1;
         GXY_CK(cudaMemsetAsync(W->counters.p, 0, kCounterWords * 4, st));
-        if (!single) {
-            // Passes over window ranges, each checked for hit-buffer overflow.
+        if (use_graph) {
             GXY_CK(cudaEventRecord(W->ev[0], st));
-            for (uint32_t t0 = 0; t0 < tiles;) {
-                const uint32_t t1 = (uint32_t)std::min<uint64_t>(tiles, (uint64_t)t0 + pass_tiles);
-                // Counters before this pass, restored if it is redone.
-                std::vector<uint32_t> before(kCounterWords), after(kCounterWords);
-                GXY_CK(cudaMemcpyAsync(before.data(), cnt, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
-                GXY_CK(cudaStreamSynchronize(st));
-                API_TRY_ENGINE(pass(t0, t1));
-                GXY_CK(cudaMemcpyAsync(after.data(), cnt, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
-                GXY_CK(cudaStreamSynchronize(st));
-                const unsigned long long nh = *reinterpret_cast<const unsigned long long*>(after.data() + kCHits);
-                const unsigned long long ns = *reinterpret_cast<const unsigned long long*>(after.data() + kCSurv);
-                if (use_filter && nh <= W->hit_cap && ns > W->surv_cap) {
-                    // Survivors overflowed (the screen skipped the pass): grow, redo the pass.
-                    W->surv.release();
-                    const uint64_t want = ns + ns / 2 + (1u << 20);
-                    if (want > kMaxHitCap) {
-                        // Too many for one buffer: fewer tiles per pass instead.
-                        W->surv_cap = kMaxHitCap;
-                        pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)(t1 - t0) * kMaxHitCap / ns * 0.8));
-                    } else {
-                        W->surv_cap = want;
-                    }
-                    GXY_CK(W->surv.ensure((size_t)W->surv_cap * sizeof(Hit)));
-                    GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
-                    GXY_CK(cudaStreamSynchronize(st));
-                    reruns++;
-                    continue;
-                }
-                if (after[kCCand] > cap && nh <= W->hit_cap) {
-                    // Candidates overflowed in this pass: grow the candidate
-                    // arrays keeping the earlier passes' entries, redo the pass.
-                    const uint64_t nc = (uint64_t)after[kCCand] + after[kCCand] / 2 + (1u << 20);
-                    if (nc >= (1ull << 31)) {
-                        set_error("candidate count exceeds 2^31");
-                        return GXY_EUNSUPPORTED;
-                    }
-                    const size_t keep = before[kCCand];
-                    GXY_CK(grow_keep(W->ck0, nc * 8, keep * 8));
-                    GXY_CK(grow_keep(W->cv0, nc * 4, keep * 4));
-                    GXY_CK(grow_keep(W->cands, nc * sizeof(Cand), keep * sizeof(Cand)));
-                    W->cand_cap = cap = (uint32_t)nc;
-                    sa.cand_keys = W->ck0.as<uint64_t>();
-                    sa.cand_vals = W->cv0.as<uint32_t>();
-                    sa.cands = W->cands.as<Cand>();
-                    sa.cand_cap = cap;
-                    GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
-                    GXY_CK(cudaStreamSynchronize(st));
-                    reruns++;
-                    continue;
-                }
-                if (nh > W->hit_cap) {
-                    if (t1 - t0 == 1) {
+            API_TRY_ENGINE(run_graph(W, [&]() -> gxy_status {
+                for (uint32_t i = 0; i < n_round; i++) pass(false);
+                return epilogue();
+            }));
+        } else {
+            if (!timing) GXY_CK(cudaEventRecord(W->ev[0], st));
+            for (uint32_t i = 0; i < n_round; i++) pass(timing);
+            API_TRY_ENGINE(epilogue());
+        }
+        GXY_CK(cudaEventRecord(W->ev[2], st));
+        GXY_CK(cudaGetLastError());
+        GXY_CK(cudaStreamSynchronize(st));
+        rounds = 1;
+        const uint32_t* hc = static_cast<const uint32_t*>(W->h_pinned);
+        // Further rounds while tiles remain (the estimate was short): more
+        // passes, then the epilogue again over all candidates so far.
+        bool multi = n_round > 1;
+        uint64_t last_tile = ~0ull, last_redo = ~0ull;
+        for (int round = 0;; round++) {
+            if (round > 4096) {
+                set_error("the passes made no progress");
+                return GXY_ECUDA;
+            }
+            const uint32_t np = hc[kCPass];
+            const uint64_t tile_at = hc[kCTile], redo_left = hc[kCRedoN + (np & 1u)];
+            if (hc[kCRedoOver]) {
+                set_error("more tiles than the hit buffer's passes can carry over");
+                return GXY_ENOMEM;
+            }
+            if (tile_at < tiles || redo_left) {
+                if (tile_at == last_tile && redo_left == last_redo) {
+                    const unsigned long long mf = *reinterpret_cast<const unsigned long long*>(hc + kCMaxFail);
+                    if (mf > W->hit_cap) {
                         set_error("one tile of 32 query windows has more raw hits than the hit buffer holds");
                         return GXY_ENOMEM;
                     }
-                    // Undo this pass's candidates and counters; redo it over fewer tiles.
-                    GXY_CK(cudaMemcpyAsync(cnt, before.data(), kCounterWords * 4, cudaMemcpyHostToDevice, st));
-                    GXY_CK(cudaStreamSynchronize(st));
-                    pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)(t1 - t0) * W->hit_cap / nh * 0.8));
-                    reruns++;
-                    continue;
                 }
-                t0 = t1;
-                survivors += use_filter ? ns : nh;
-                // Hit density varies along the query (repeats): grow the
-                // window range again after a sparse pass, up to twice.
-                if ((double)nh < 0.5 * (double)W->hit_cap) {
-                    const double f = std::min(2.0, 0.8 * (double)W->hit_cap / std::max<double>(1.0, (double)nh));
-                    pass_tiles = (uint32_t)std::min<double>((double)tiles, std::max(1.0, (double)pass_tiles * f));
-                }
+                last_tile = tile_at;
+                last_redo = redo_left;
+                multi = true;
+                const uint64_t more = std::min<uint64_t>(
+                    256, (uint64_t)((double)(tiles - std::min<uint64_t>(tile_at, tiles)) / tiles * first_round) + 2);
+                for (uint64_t i = 0; i < more; i++) pass(false);
+                API_TRY_ENGINE(epilogue());
+                rounds++;
+                GXY_CK(cudaEventRecord(W->ev[2], st));
+                GXY_CK(cudaGetLastError());
+                GXY_CK(cudaStreamSynchronize(st));
+                continue;
             }
-            GXY_CK(cudaEventRecord(W->ev[3], st));
-            GXY_CK(cudaEventRecord(W->ev[1], st));
-            GXY_CK(W->ck1.ensure((size_t)cap * 8));
-            GXY_CK(W->cv1.ensure((size_t)cap * 4));
-            GXY_CK(W->flags.ensure((size_t)cap));
-            GXY_CK(W->offsets.ensure((size_t)cap * 4 + 4));
-            GXY_CK(W->ohsp.ensure((size_t)cap * sizeof(Hsp)));
-            GXY_CK(W->rhsp.ensure((size_t)cap * sizeof(Hsp)));
-            GXY_CK(W->runit.ensure((size_t)cap * 4));
-            GXY_CK(W->rhsp2.ensure((size_t)cap * sizeof(Hsp)));
-            GXY_CK(W->runit2.ensure((size_t)cap * 4));
-            GXY_CK(W->perm.ensure((size_t)cap * 4));
-            GXY_CK(W->perm2.ensure((size_t)cap * 4));
-            if (records) GXY_CK(W->rrec.ensure((size_t)cap * sizeof(Record)));
-        } else {
-            // In graph mode the timing events sit around the graph launch.
-            in_capture = graph_now;
-            if (graph_now) {
-                GXY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                capture.active = true;
-            }
-            GXY_CK(cudaMemsetAsync(W->counters.p, 0, kCounterWords * 4, st));
-            if (!graph_now) GXY_CK(cudaEventRecord(W->ev[0], st));
-            API_TRY_ENGINE(pass(0, (uint32_t)tiles));
-            if (!graph_now) GXY_CK(cudaEventRecord(W->ev[1], st));
+            break;
         }
-        const int which = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
-                                         W->cv1.as<uint32_t>(), cnt + kCCand, 0, cap, passes, npass, W->ps, st);
-        const uint64_t* skeys = which ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
-        const uint32_t* sidx = which ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
-        GXY_CK(cudaMemsetAsync(W->flags.p, 0, cap, st));
-        WalkArgs wa;
-        memset(&wa, 0, sizeof(wa));
-        wa.keys = skeys;
-        wa.idx = sidx;
-        wa.cands = W->cands.as<Cand>();
-        wa.n_dev = cnt + kCCand;
-        wa.n_cap = cap;
-        wa.units = sa.units;
-        wa.tsegs = sa.tsegs;
-        wa.qsegs = sa.qsegs;
-        wa.seed_len = pat.len;
-        wa.sc = sa.sc;
-        wa.has_entropy = p.has_entropy;
-        wa.entropy_thr = p.entropy_thr;
-        wa.out_flag = W->flags.as<uint8_t>();
-        wa.out_hsp = W->ohsp.as<Hsp>();
-        wa.chunk_next = cnt + kCWalk;
-        wa.n_units = nu;
-        GXY_CK(cudaMemsetAsync(cnt + kCWalk, 0, 4, st));
-        launch_walk(wa, walk_warps, blocks_misc, st);
-        scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCCand, 0, cap, false, cnt + kCHsps, W->ps,
-                st);
-        launch_compact(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), W->ohsp.as<Hsp>(), sidx,
-                       W->cands.as<Cand>(), cnt + kCCand, cap, W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), blocks_misc, st);
-        Hsp* fin = W->rhsp.as<Hsp>();
-        uint32_t* fin_unit = W->runit.as<uint32_t>();
-        if (nu > 1) {
-            // Group by unit, keeping each unit's (diagonal, t) order: stable sort.
-            RadixPass up[4];
-            const int nup = plan_radix(0, bits_for(nu - 1), 0, 0, up, 4);
-            launch_iota(W->perm.as<uint32_t>(), cnt + kCHsps, cap, blocks_misc, st);
-            GXY_CK(cudaMemcpyAsync(W->runit2.p, W->runit.p, (size_t)cap * 4, cudaMemcpyDeviceToDevice, st));
-            const int w2 = radix_sort_u32(W->runit2.as<uint32_t>(), W->perm.as<uint32_t>(), W->offsets.as<uint32_t>(),
-                                          W->perm2.as<uint32_t>(), cnt + kCHsps, 0, cap, up, nup, W->ps, st);
-            const uint32_t* perm = w2 ? W->perm2.as<uint32_t>() : W->perm.as<uint32_t>();
-            launch_gather_hsp(W->rhsp.as<Hsp>(), W->runit.as<uint32_t>(), perm, cnt + kCHsps, cap, W->rhsp2.as<Hsp>(),
-                              W->runit2.as<uint32_t>(), blocks_misc, st);
-            fin = W->rhsp2.as<Hsp>();
-            fin_unit = W->runit2.as<uint32_t>();
-        }
-        launch_fixup(fin, fin_unit, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
-        if (records) {
-            // Driver records (src/driver.rs:371-391): stable LSD sort by
-            // (group, global t, q, span) over the unit-major HSP order, then
-            // drop repeats of the same four fields, keeping the first.  One
-            // sort of a packed key when the fields fit 64 bits, else (q, span)
-            // first and (group, t) second.
-            const Place* pl = W->d_place.as<Place>();
-            RadixPass rp[16];
-            const uint32_t* perm;
-            if (rb_g + rb_t + rb_q + rb_l <= 64) {
-                const int sh_q = rb_l, sh_t = rb_l + rb_q, sh_g = rb_l + rb_q + rb_t;
-                launch_record_keys(fin, fin_unit, pl, nullptr, cnt + kCHsps, cap, 0, sh_g, sh_t, sh_q,
-                                   W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), blocks_misc, st);
-                const int np = plan_radix(0, rb_l + rb_q + rb_t + rb_g, 0, 0, rp, 16);
-                const int w = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
-                                             W->cv1.as<uint32_t>(), cnt + kCHsps, 0, cap, rp, np, W->ps, st);
-                perm = w ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
-            } else {
-                launch_record_keys(fin, fin_unit, pl, nullptr, cnt + kCHsps, cap, 1, 0, 0, 0, W->ck0.as<uint64_t>(),
-                                   W->cv0.as<uint32_t>(), blocks_misc, st);
-                int np = plan_radix(0, rb_l, 32, rb_q, rp, 16);
-                int w = radix_sort_u64(W->ck0.as<uint64_t>(), W->cv0.as<uint32_t>(), W->ck1.as<uint64_t>(),
-                                       W->cv1.as<uint32_t>(), cnt + kCHsps, 0, cap, rp, np, W->ps, st);
-                const uint32_t* p1 = w ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
-                uint64_t* k2 = w ? W->ck0.as<uint64_t>() : W->ck1.as<uint64_t>();
-                uint32_t* v2 = w ? W->cv0.as<uint32_t>() : W->cv1.as<uint32_t>();
-                uint64_t* k3 = w ? W->ck1.as<uint64_t>() : W->ck0.as<uint64_t>();
-                uint32_t* v3 = w ? W->cv1.as<uint32_t>() : W->cv0.as<uint32_t>();
-                launch_record_keys(fin, fin_unit, pl, p1, cnt + kCHsps, cap, 2, 0, 0, 0, k2, v2, blocks_misc, st);
-                np = plan_radix(0, rb_t, 32, rb_g, rp, 16);
-                w = radix_sort_u64(k2, v2, k3, v3, cnt + kCHsps, 0, cap, rp, np, W->ps, st);
-                perm = w ? v3 : v2;
-            }
-            launch_record_heads(fin, fin_unit, pl, perm, cnt + kCHsps, cap, W->flags.as<uint8_t>(), blocks_misc, st);
-            scan_u8(W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(), cnt + kCHsps, 0, cap, false, cnt + kCRecs,
-                    W->ps, st);
-            launch_record_emit(fin, fin_unit, pl, perm, W->flags.as<uint8_t>(), W->offsets.as<uint32_t>(),
-                               cnt + kCHsps, cap, W->rrec.as<Record>(), blocks_misc, st);
-        }
-        if (!graph_now) GXY_CK(cudaEventRecord(W->ev[2], st));
-        GXY_CK(cudaMemcpyAsync(W->h_pinned, W->counters.p, kCounterWords * 4, cudaMemcpyDeviceToHost, st));
-
-        if (graph_now) {
-            capture.active = false;
-            GXY_CK(cudaStreamEndCapture(st, &graph));
-            cudaError_t e = cudaGraphInstantiate(&gexec, graph, 0);
-            if (e != cudaSuccess) {
-                cudaGraphDestroy(graph);
-                set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-                return GXY_ECUDA;
-            }
-            in_capture = false;
-            e = cudaEventRecord(W->ev[0], st);
-            if (e == cudaSuccess) e = cudaGraphLaunch(gexec, st);
-            if (e == cudaSuccess) e = cudaEventRecord(W->ev[2], st);
-            cudaGraphExecDestroy(gexec);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) {
-                set_error(std::string("cudaGraphLaunch: ") + cudaGetErrorString(e));
-                return GXY_ECUDA;
-            }
-        }
-        GXY_CK(cudaGetLastError());
-        GXY_CK(cudaStreamSynchronize(st));
-        const uint32_t* hc = static_cast<const uint32_t*>(W->h_pinned);
         const unsigned long long* hs = reinterpret_cast<const unsigned long long*>(hc + kCStats);
-        const unsigned long long nhits = *reinterpret_cast<const unsigned long long*>(hc + kCHits);
+        const unsigned long long nhits_last = *reinterpret_cast<const unsigned long long*>(hc + kCHits);
+        const unsigned long long nsurv_last = *reinterpret_cast<const unsigned long long*>(hc + kCSurv);
         const uint32_t ncand = hc[kCCand];
-        const unsigned long long nsurv = *reinterpret_cast<const unsigned long long*>(hc + kCSurv);
-        if (single) survivors = use_filter ? nsurv : nhits;
-        if (single && use_filter && nhits <= W->hit_cap && nsurv > W->surv_cap) {
+        if (use_filter && (hc[kCSurvOver] || nsurv_last > W->surv_cap)) {
+            // A pass had more survivors than the survivor buffer holds: grow
+            // it to the raw-hit buffer's size (survivors <= raw hits).
             W->surv.release();
-            const uint64_t want = nsurv + nsurv / 4 + (1u << 20);
-            if (want > kMaxHitCap) {
-                W->surv_cap = kMaxHitCap;
-                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / nsurv * 0.8));
-            } else {
-                W->surv_cap = want;
-            }
-            reruns++;
-            continue;
-        }
-        if (single && nhits > W->hit_cap) {
-            // Raw hits overflowed the hit buffer: grow it, or split into passes.
-            if (nhits + nhits / 8 <= kMaxHitCap) {
-                W->hits.release();
-                W->hit_cap = nhits + nhits / 8 + 1024;
-            } else {
-                W->hits.release();
-                W->hit_cap = kMaxHitCap;
-                pass_tiles = std::max<uint32_t>(1, (uint32_t)((double)tiles * kMaxHitCap / nhits * 0.8));
-            }
+            W->surv_cap = std::max<uint64_t>(W->surv_cap * 2, std::min<uint64_t>(W->hit_cap, W->surv_cap * 8));
             reruns++;
             continue;
         }
@@ -811,31 +746,30 @@ gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units
             reruns++;
             continue;
         }
-        const uint32_t nh = hc[kCHsps];
+        const uint32_t work_passes = hc[kCWorkPasses] + (nhits_last ? 1u : 0u);
         out.stats.windows = hs[0];
         out.stats.raw_hits = hs[1];
         out.stats.columns = hs[2];
         out.stats.filter_columns = hs[3];
-        out.stats.survivors = use_filter ? survivors : hs[1];
         out.stats.candidates = ncand;
-        out.stats.hsps = nh;
         float ms = 0.f, ms_enum = 0.f, ms_filter = 0.f, ms_screen = 0.f;
         GXY_CK(cudaEventElapsedTime(&ms, W->ev[0], W->ev[2]));
-        if (!graph_now) {
-            if (single) {
-                GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[4]));
-                GXY_CK(cudaEventElapsedTime(&ms_filter, W->ev[4], W->ev[3]));
-            } else {
-                GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[3]));
-            }
+        if (timing && !multi) {
+            GXY_CK(cudaEventElapsedTime(&ms_enum, W->ev[0], W->ev[4]));
+            GXY_CK(cudaEventElapsedTime(&ms_filter, W->ev[4], W->ev[3]));
             GXY_CK(cudaEventElapsedTime(&ms_screen, W->ev[3], W->ev[1]));
         }
         out.stats.device_ms = ms;
-        out.stats.enum_ms = single ? ms_enum : 0.0;
-        out.stats.filter_ms = single ? ms_filter : 0.0;
-        out.stats.screen_ms = single ? ms_screen : ms_enum + ms_screen;
-        out.stats.passes = single ? 1 : (uint32_t)((tiles + pass_tiles - 1) / pass_tiles);
+        out.stats.enum_ms = ms_enum;
+        out.stats.filter_ms = ms_filter;
+        out.stats.screen_ms = ms_screen;
+        out.stats.passes = std::max<uint32_t>(1, work_passes);
         out.stats.reruns = reruns;
+        out.stats.rounds = rounds;
+        out.stats.graph_updates = (uint32_t)(W->graph_updates - graph_updates0);
+        out.stats.survivors = use_filter ? hs[4] + nsurv_last : hs[1];
+        const uint32_t nh = hc[kCHsps];
+        out.stats.hsps = nh;
         if (records) {
             const uint32_t nr = hc[kCRecs];
             out.records.resize(nr);

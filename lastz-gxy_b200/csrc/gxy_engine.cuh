@@ -42,10 +42,15 @@ struct Worker {
     DevBuf ck0, ck1, cv0, cv1, cands, flags, offsets, ohsp;
     DevBuf rhsp, runit, rhsp2, runit2, perm, perm2;
     DevBuf d_place, rrec;         // driver records: per-unit places, records
+    DevBuf rk0, rk1, rv0, rv1;    // driver records: sort keys and values (the candidates' arrays
+                                  // stay intact, so a later round of passes can add to them)
     DevBuf hits;                  // raw hits of one pass
     uint64_t hit_cap = 0;
     DevBuf surv;                  // hits of one pass that pass the upper-bound filter
     uint64_t surv_cap = 0;
+    DevBuf redo;                  // the two lists of tiles a pass hands to the next one
+    cudaGraphExec_t gexec = nullptr;   // the last batched launch's graph, updated in place when it fits
+    uint64_t graph_updates = 0;
     uint32_t cand_cap = 0;
     uint32_t res_cap = 0;
     void* h_pinned = nullptr;     // small host staging: counters, unit and segment descriptors
@@ -71,10 +76,6 @@ struct UnitPlan {
     double avg_bucket;   // table positions / words: sizes the raw-hit buffer before the first pass
 };
 
-// Layout of a worker's device counters (u32 indices).
-constexpr uint32_t kCTile = 0, kCHsps = 2, kCRecs = 4, kCStats = 8, kCCand = 1024, kCHitNext = 2048, kCHits = 3072,
-                   kCSurv = 3328, kCWalk = 3584, kCFiltNext = 3840;
-constexpr uint32_t kCounterWords = 4096;
 // Candidate arrays are sized up front at one candidate per this many
 // estimated raw hits (the estimate carries a 1.5x margin; about 3 % of raw
 // hits become candidates), up to a bound.  Larger arrays also widen the
@@ -83,7 +84,7 @@ constexpr uint64_t kHitsPerCandidate = 32;
 // With the upper-bound filter the hit buffer is sized at one slot per this
 // many estimated raw hits (survivors are a few percent of the raw hits).
 constexpr double kRawPerSurvivorSlot = 8.0;
-constexpr uint64_t kMaxPresizedCandidates = 1ull << 22;
+constexpr uint64_t kMaxPresizedCandidates = 1ull << 25;
 
 struct RunResult {
     std::vector<gxy_hsp> hsps;
@@ -106,6 +107,7 @@ struct RunResult {
 
 struct gxy_dseq {
     gxy_ctx* ctx = nullptr;
+    int device = 0;   // the context's device, kept so that the sequence can be freed after its context
     void* alloc = nullptr;
     size_t bytes = 0;
     uint64_t* codes = nullptr;
@@ -118,6 +120,7 @@ struct gxy_dseq {
 
 struct gxy_table {
     gxy_ctx* ctx = nullptr;
+    int device = 0;   // as gxy_dseq::device
     gxy_dseq* owned = nullptr;
     const gxy_dseq* seq = nullptr;
     uint64_t lo = 0, hi = 0;

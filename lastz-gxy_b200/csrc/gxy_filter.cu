@@ -31,8 +31,6 @@
 #include "gxy_kernels.cuh"
 
 #include <algorithm>
-#include <atomic>
-#include <cstdlib>
 
 namespace gxy {
 
@@ -126,9 +124,9 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
     unsigned char* lut = smem;
     lut_fill(lut, a.fub);
     __syncthreads();
-    const unsigned long long rc = *io.raw_count;
-    if (rc > io.raw_cap) return;   // the pass is redone over fewer tiles
-    const uint32_t n_hits = (uint32_t)rc;
+    // Past the buffer's end the pass did not write (those tiles went to the
+    // next pass).
+    const uint32_t n_hits = (uint32_t)min(*io.raw_count, (unsigned long long)io.raw_cap);
     const int lane = threadIdx.x & 31;
     const uint32_t lane8 = (uint32_t)lane * 8u, lt = lanemask_lt();
     const uint32_t L = a.pat.len;
@@ -167,19 +165,21 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
                 ht = h.t;
                 hq = h.q;
                 hu = h.unit;
-                if (hu != cur_unit) {
+                if (hu != kNoUnit && hu != cur_unit) {
                     cur_unit = hu;
                     const UnitDev U = a.units[hu];
                     T = a.tsegs[U.tseg];
                     Q = a.qsegs[U.qseg];
                 }
-                busy = true;
-                rrem = min(T.len - ht - L, Q.len - hq - L);
-                lrem = min(ht, hq);
-                rrun = rbest = lrun = lbest = 0;
-                rext = lext = 0;
-                ralive = rrem > 0;
-                lalive = lrem > 0;
+                busy = hu != kNoUnit;   // else an unused slot of a failed reservation
+                if (busy) {
+                    rrem = min(T.len - ht - L, Q.len - hq - L);
+                    lrem = min(ht, hq);
+                    rrun = rbest = lrun = lbest = 0;
+                    rext = lext = 0;
+                    ralive = rrem > 0;
+                    lalive = lrem > 0;
+                }
             }
         }
         {
@@ -254,7 +254,10 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
                 }
             }
         }
-        if (done) busy = false;
+        if (done) {
+            busy = false;
+            ralive = lalive = false;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n_cols += __shfl_xor_sync(kFull, n_cols, o);
@@ -311,19 +314,13 @@ bool filter_bounds(ScreenArgs& a) {
     return true;
 }
 
+void filter_init() {
+    cudaFuncSetAttribute(k_filter_hits<kFilterWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLutBytes);
+}
+
 void launch_filter_hits(const ScreenArgs& a, const FilterIO& io, int sm_count, cudaStream_t st) {
-    constexpr int kNW = kFilterWarps;
-    // The attribute is set once per device (it belongs to the device's context).
-    static std::atomic<uint64_t> ready{0};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    const uint64_t bit = 1ull << (dev & 63);
-    if (!(ready.load(std::memory_order_acquire) & bit)) {
-        cudaFuncSetAttribute(k_filter_hits<kNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, kLutBytes);
-        ready.fetch_or(bit, std::memory_order_acq_rel);
-    }
     count_launch();
-    k_filter_hits<kNW><<<sm_count * 2, kNW * 32, kLutBytes, st>>>(a, io);
+    k_filter_hits<kFilterWarps><<<sm_count * 2, kFilterWarps * 32, kLutBytes, st>>>(a, io);
 }
 
 void launch_occupancy(const uint32_t* starts, uint64_t num_words, uint32_t* occ, cudaStream_t st) {

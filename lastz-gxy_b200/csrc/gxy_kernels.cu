@@ -467,18 +467,62 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
     const int lane = threadIdx.x & 31;
     const uint32_t ntile = a.tile_hi - a.tile_lo;
     unsigned long long n_windows = 0, n_raw = 0;
-    // Tiles are claimed kClaim at a time, and the next claim is made while
-    // the current tiles are processed: one atomic per kClaim tiles (all warps
-    // hit that counter), its round trip off the critical path.  (Measured on
-    // the 10 Mbp plain launch: 2 beats 4 by 2 % and 8 is slower.)
+    uint32_t* const ctl = a.ctl;
+    unsigned long long* const max_fail = reinterpret_cast<unsigned long long*>(ctl + kCMaxFail);
+    // This pass takes the tiles the previous pass could not fit first (its
+    // redo list), then fresh tiles until the hit buffer is full.
+    const uint32_t pass = ctl[kCPass];
+    const uint32_t* redo_in = a.redo + ((pass - 1) & 1u) * kRedoCap;
+    uint32_t* redo_out = a.redo + (pass & 1u) * kRedoCap;
+    const uint32_t n_redo = ctl[kCRedoN + ((pass - 1) & 1u)];
+    uint32_t* const n_redo_out = ctl + kCRedoN + (pass & 1u);
+    // A tile that did not fit this pass goes to the next pass's list.
+    auto defer = [&](uint32_t tl, unsigned long long wtot) {
+        atomicExch(ctl + kCStop, 1u);
+        const uint32_t i = atomicAdd(n_redo_out, 1u);
+        if (i < kRedoCap) redo_out[i] = tl;
+        else atomicExch(ctl + kCRedoOver, 1u);
+        atomicMax(max_fail, wtot);
+    };
+    bool redo_done = false;
+    // Fresh tiles are claimed kClaim at a time, and the next claim is made
+    // while the current tiles are processed: one atomic per kClaim tiles
+    // (all warps hit that counter), its round trip off the critical path.
+    // (Measured on the 10 Mbp plain launch: 2 beats 4 by 2 % and 8 is slower.)
     constexpr uint32_t kClaim = 2;
-    uint32_t next = 0;
-    if (lane == 0) next = atomicAdd(a.tile_counter, kClaim);
+    uint32_t next = 0xffffffffu;   // a claimed batch not yet started (warp-uniform)
     for (;;) {
-      const uint32_t batch = __shfl_sync(kFull, next, 0);
-      if (batch >= ntile) break;
-      if (lane == 0) next = atomicAdd(a.tile_counter, kClaim);
-      const uint32_t batch_end = min(ntile, batch + kClaim);
+      uint32_t batch, batch_end;
+      if (!redo_done) {
+          uint32_t i = 0;
+          if (lane == 0) i = atomicAdd(ctl + kCRedoTake, 1u);
+          i = __shfl_sync(kFull, i, 0);
+          if (i < n_redo) {
+              batch = redo_in[i];
+              batch_end = batch + 1;
+          } else {
+              redo_done = true;
+              continue;
+          }
+      } else {
+          if (next == 0xffffffffu) {
+              // Stop claiming once the buffer is full; the tiles not claimed
+              // yet wait for the next pass behind the tile cursor.
+              if (*reinterpret_cast<volatile uint32_t*>(ctl + kCStop)) break;
+              uint32_t c = 0;
+              if (lane == 0) c = atomicAdd(a.tile_counter, kClaim);
+              next = __shfl_sync(kFull, c, 0);
+          }
+          batch = next;
+          if (batch >= ntile) break;
+          next = 0xffffffffu;
+          if (!*reinterpret_cast<volatile uint32_t*>(ctl + kCStop)) {
+              uint32_t c = 0;
+              if (lane == 0) c = atomicAdd(a.tile_counter, kClaim);
+              next = __shfl_sync(kFull, c, 0);
+          }
+          batch_end = min(ntile, batch + kClaim);
+      }
       for (uint32_t tl = batch; tl < batch_end; tl++) {
         uint32_t tile = tl + a.tile_lo;
         uint32_t lo = 0, hi = a.n_units;
@@ -494,7 +538,6 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
         uint32_t word = 0;
         bool wv = false;
         if (k < U.nwin) wv = word_at(a.qsegs[U.qseg], a.pat, q, word);
-        n_windows += wv ? 1 : 0;
         // Pass 1: this lane's hit count over all variants.  The bucket
         // bounds of the first kRegVar variants stay in registers for pass 2.
         uint32_t rb[kRegVar], rc[kRegVar];
@@ -530,10 +573,12 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
             if (lane >= o) incl += y;
         }
         const uint32_t wtot = __shfl_sync(kFull, incl, 31);
-        if (wtot == 0) continue;
+        if (wtot == 0) {
+            n_windows += wv ? 1 : 0;
+            continue;
+        }
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.hit_count, (unsigned long long)wtot);
-        n_raw += lane == 0 ? wtot : 0;
         // Pass 2: write this lane's hits into its slots [dst, dst + tot).
         // Their order within the slots is free (candidates are sorted by a
         // unique (diagonal, t) key later), so the first position of every
@@ -544,7 +589,16 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
         for (uint32_t i = 0; i < 8; i++)
             if (i < kRegVar) first[i] = (rc[i] != 0 && rc[i] <= 16) ? __ldg(U.positions + rb[i]) : 0u;
         base = __shfl_sync(kFull, base, 0);
-        if (base + wtot > a.hit_cap) continue;   // overflow: the pass is redone with fewer tiles
+        if (base + wtot > a.hit_cap) {
+            // The buffer is full: this tile goes to the next pass, and the
+            // part of its reservation inside the buffer is marked unused.
+            if (lane == 0) defer(tl, wtot);
+            for (uint64_t j = base + lane; j < min((unsigned long long)a.hit_cap, base + wtot); j += 32)
+                a.hits[j].unit = kNoUnit;
+            continue;
+        }
+        n_windows += wv ? 1 : 0;
+        n_raw += lane == 0 ? wtot : 0;
         uint64_t dst = base + (incl - tot);
 #pragma unroll
         for (uint32_t v0 = 0; v0 < kRegVar; v0 += 8) {
@@ -592,12 +646,38 @@ __global__ __launch_bounds__(256, 4) void k_enumerate(const __grid_constant__ Sc
         }
       }
     }
+    // A batch claimed ahead but not started: the next pass takes it.
+    if (next != 0xffffffffu && lane == 0)
+        for (uint32_t tl = next; tl < min(ntile, next + kClaim); tl++) defer(tl, 0);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n_windows += __shfl_xor_sync(kFull, n_windows, o);
     if (lane == 0) {
         atomicAdd(&a.stats[0], n_windows);
         atomicAdd(&a.stats[1], n_raw);
     }
+}
+
+__global__ void k_pass_reset(uint32_t* ctl, uint64_t surv_cap) {
+    if (threadIdx.x != 0) return;
+    unsigned long long* hits = reinterpret_cast<unsigned long long*>(ctl + kCHits);
+    unsigned long long* surv = reinterpret_cast<unsigned long long*>(ctl + kCSurv);
+    if (*surv > surv_cap) ctl[kCSurvOver] = 1u;   // the previous pass lost survivors
+    if (*hits) ctl[kCWorkPasses]++;
+    reinterpret_cast<unsigned long long*>(ctl + kCStats)[4] += *surv;   // survivors of the launch
+    const uint32_t p = ctl[kCPass] + 1;
+    ctl[kCPass] = p;
+    ctl[kCRedoN + (p & 1u)] = 0;
+    ctl[kCRedoTake] = 0;
+    ctl[kCStop] = 0;
+    ctl[kCHitNext] = 0;
+    ctl[kCFiltNext] = 0;
+    *hits = 0;
+    *surv = 0;
+}
+
+void launch_pass_reset(uint32_t* ctl, uint64_t surv_cap, cudaStream_t st) {
+    count_launch();
+    k_pass_reset<<<1, 32, 0, st>>>(ctl, surv_cap);
 }
 
 void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st) {
@@ -632,9 +712,9 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen_wide(const __grid_c
     const uint32_t lt = lanemask_lt();
     const uint32_t L = a.pat.len;
     const int32_t ambig = a.sc.ambig, xdrop = a.sc.xdrop, thresh = a.sc.hspthresh;
-    const unsigned long long hc = *a.hit_count;
-    if (hc > a.hit_cap) return;   // the pass is redone over fewer tiles
-    const uint32_t n_hits = (uint32_t)hc;
+    // Past the buffer's end the pass did not write (those tiles went to the
+    // next pass).
+    const uint32_t n_hits = (uint32_t)min(*a.hit_count, (unsigned long long)a.hit_cap);
     unsigned long long n_cols = 0;
     bool exhausted = false;
 
@@ -664,14 +744,14 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen_wide(const __grid_c
                 ht = h.t;
                 hq = h.q;
                 hu = h.unit;
-                if (hu != cur_unit) {
+                if (hu != kNoUnit && hu != cur_unit) {
                     cur_unit = hu;
                     const UnitDev U = a.units[hu];
                     T = a.tsegs[U.tseg];
                     Q = a.qsegs[U.qseg];
                 }
-                fresh = true;
-                busy = true;
+                fresh = hu != kNoUnit;   // an unused slot of a failed reservation
+                busy = fresh;
             }
         }
         if (!__any_sync(kFull, busy)) {
@@ -970,11 +1050,9 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
     int32_t top = ambig;
     for (int i = 0; i < 16; i++) top = max(top, a.sc.sub[i]);
     const int32_t seed_ub = top * (int32_t)L;
-    const unsigned long long hc = *a.hit_count;
-    // An overflowing pass is redone over fewer tiles: screening its
-    // truncated hits would be wasted work.
-    if (hc > a.hit_cap) return;
-    const uint32_t n_hits = (uint32_t)hc;
+    // Past the buffer's end the pass did not write (those hits went to the
+    // next pass, or were lost with a survivor overflow, which reruns the launch).
+    const uint32_t n_hits = (uint32_t)min(*a.hit_count, (unsigned long long)a.hit_cap);
     // Each warp claims hits in chunks (one atomic per chunk) and deals them
     // to its idle lanes; chunks shrink for small launches so that every warp
     // still gets work.
@@ -1015,14 +1093,14 @@ __global__ __launch_bounds__(WARPS * 32, MINB) void k_screen(const __grid_consta
                 ht = h.t;
                 hq = h.q;
                 hu = h.unit;
-                if (hu != cur_unit) {
+                if (hu != kNoUnit && hu != cur_unit) {
                     cur_unit = hu;
                     const UnitDev U = a.units[hu];
                     T_ = a.tsegs[U.tseg];
                     Q_ = a.qsegs[U.qseg];
                 }
-                fresh = true;
-                busy = true;
+                fresh = hu != kNoUnit;   // an unused slot of a failed reservation
+                busy = fresh;
             }
         }
         {

@@ -75,12 +75,33 @@ void launch_prune_copy(const uint32_t* positions, const uint32_t* starts, uint64
                        const uint32_t* new_starts, uint32_t limit, uint32_t* new_positions, cudaStream_t st);
 
 // --- search ------------------------------------------------------------------
-// A raw seed hit: target position t, query window q, unit.
+// A raw seed hit: target position t, query window q, unit.  unit kNoUnit
+// marks a slot of a hit-buffer reservation that failed (skipped by readers).
 struct Hit {
     uint32_t t;
     uint32_t q;
     uint32_t unit;
 };
+constexpr uint32_t kNoUnit = 0xffffffffu;
+
+// Layout of a worker's device counters (u32 indices).  The ones every warp
+// hits with atomics sit 1-4 KB apart so that they fall in different L2
+// slices.
+//  - per launch: [kCTile] tile cursor, [kCPass] passes run, [kCCand]
+//    candidates, [kCHsps] HSPs, [kCRecs] records, u64 [kCStats] statistics,
+//    [kCRedoN + 0/1] redo-list lengths, u64 [kCMaxFail] largest tile that
+//    did not fit the hit buffer, flags [kCSurvOver] and [kCRedoOver],
+//    [kCWorkPasses] passes that found raw hits, [kCWalk] walk cursor;
+//  - per pass (reset by k_pass_reset): u64 [kCHits] raw hits, u64 [kCSurv]
+//    survivors, [kCHitNext] screen cursor, [kCFiltNext] filter cursor,
+//    [kCRedoTake] redo-list cursor, [kCStop] the hit buffer is full.
+constexpr uint32_t kCTile = 0, kCHsps = 2, kCRecs = 4, kCStats = 8, kCPass = 128, kCStop = 160, kCRedoN = 192,
+                   kCMaxFail = 224, kCSurvOver = 256, kCRedoOver = 288, kCWorkPasses = 320, kCCand = 1024,
+                   kCHitNext = 2048, kCRedoTake = 2560, kCHits = 3072, kCSurv = 3328, kCWalk = 3584,
+                   kCFiltNext = 3840;
+constexpr uint32_t kCounterWords = 4096;
+// Tiles a pass can hand to the next one (two lists of this many).
+constexpr uint32_t kRedoCap = 1u << 16;
 
 struct ScreenArgs {
     const UnitDev* units;
@@ -114,10 +135,20 @@ struct ScreenArgs {
     int32_t f_seed_max;    // seed length x the largest class bound
     uint32_t f_cap;        // columns per side after which a hit survives unexamined
     uint32_t f_claim;      // raw hits a filter warp claims at a time (0: sized from the hit count)
+    // Passes that resume on the device: the worker's counters (layout
+    // above) and the two redo lists of tiles that did not fit the hit buffer.
+    uint32_t* ctl;
+    uint32_t* redo;
 };
 // Seed-hit enumeration: one warp per tile of 32 query windows; writes the
-// hits of every (window, variant) bucket to a.hits.
+// hits of every (window, variant) bucket to a.hits.  A pass takes the tiles
+// the previous pass could not fit first, then fresh tiles from a.tile_counter
+// until the hit buffer is full; a tile that does not fit goes to the next
+// pass's list.
 void launch_enumerate(const ScreenArgs& a, int sm_count, cudaStream_t st);
+// Starts a pass: flags survivor overflow of the previous pass (its count above
+// surv_cap), advances the pass counter and resets the per-pass counters.
+void launch_pass_reset(uint32_t* ctl, uint64_t surv_cap, cudaStream_t st);
 // Capped lane-per-hit x-drop over a.hits; keeps the candidates.  grid = persistent.
 void launch_screen(const ScreenArgs& a, int warps_per_block, int blocks, cudaStream_t st);
 // The upper-bound x-drop filter between enumeration and the exact screen
@@ -135,6 +166,9 @@ struct FilterIO {
     uint32_t* cursor;      // zeroed by the caller
 };
 void launch_filter_hits(const ScreenArgs& a, const FilterIO& io, int sm_count, cudaStream_t st);
+// Per-device kernel attributes of the filter (its shared-memory table); call
+// once with the device current, before any stream capture.
+void filter_init();
 // Bucket occupancy bitmap of a table: bit (w & 31) of occ[w >> 5] is set iff
 // bucket w holds a position.
 void launch_occupancy(const uint32_t* starts, uint64_t num_words, uint32_t* occ, cudaStream_t st);

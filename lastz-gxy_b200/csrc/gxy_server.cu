@@ -79,9 +79,8 @@ struct gxy_server {
     uint64_t pool_at_create = 0;
     cudaMemPool_t pool = nullptr;
     // Other processes on a shared GPU allocate too, which the pool counter
-    // cannot see: a monitor thread re-reads the free memory every
-    // kMemRefreshMs, off the dispatch path, so the estimate's drift is
-    // bounded by what others allocate within that interval.
+    // cannot see: a monitor thread re-reads the free memory whenever the
+    // server has been idle for kMemRefreshMs, off the dispatch path.
     std::thread monitor;
     std::condition_variable cv_stop;
     std::map<uint64_t, gxy_status> future_faults;   // injected faults of ids not yet submitted
@@ -324,15 +323,18 @@ void dispatcher(gxy_server* s) {
     checkin(s->ctx, W);
 }
 
-// Re-reads the device's free memory every kMemRefreshMs (cudaMemGetInfo
-// can take tens of milliseconds on a busy device, so only this thread calls
-// it) and re-bases the admission estimate on it.
+// Re-reads the device's free memory at most every kMemRefreshMs, and only
+// while the server is idle (no request queued or in flight): cudaMemGetInfo
+// can take tens of milliseconds on a busy device and holds up the other
+// threads' CUDA calls meanwhile, so it never runs under a batch.  The
+// admission estimate is re-based on what it returns.
 void memory_monitor(gxy_server* s) {
     cudaSetDevice(s->ctx->device);
     std::unique_lock<std::mutex> lk(s->mu);
     while (!s->stop) {
         s->cv_stop.wait_for(lk, std::chrono::milliseconds(kMemRefreshMs), [&] { return s->stop; });
         if (s->stop) break;
+        if (s->units_in_flight || !s->pending.empty()) continue;
         lk.unlock();
         size_t free_b = 0, total_b = 0;
         uint64_t reserved = 0;

@@ -700,3 +700,54 @@ void orc_diag_free(void* h) {
 }
 
 void orc_free(void* ptr) { free(ptr); }
+
+/* ------------------------------------------------------------------------ */
+/* best_chain (src/chain.rs:19-69): stable sort by (t_start, q_start)       */
+/* (:28-29), weighted longest-increasing-chain DP with the first            */
+/* predecessor of the largest best (strict >, :37-46), the first terminal   */
+/* of the largest best (:49-56), traceback (:58-66).                        */
+/* ------------------------------------------------------------------------ */
+static int chain_cmp(const void* a, const void* b) {
+    const orc_hsp* x = *(const orc_hsp* const*)a;
+    const orc_hsp* y = *(const orc_hsp* const*)b;
+    if (x->t_start != y->t_start) return x->t_start < y->t_start ? -1 : 1;
+    if (x->q_start != y->q_start) return x->q_start < y->q_start ? -1 : 1;
+    return x < y ? -1 : (x > y);   /* input order: a stable sort */
+}
+
+uint64_t orc_best_chain(const orc_hsp* hsps, uint64_t n, orc_hsp* out) {
+    if (n == 0) return 0;
+    const orc_hsp** srt = (const orc_hsp**)malloc(n * sizeof(*srt));
+    int64_t* best = (int64_t*)malloc(n * sizeof(int64_t));
+    int64_t* parent = (int64_t*)malloc(n * sizeof(int64_t));
+    for (uint64_t i = 0; i < n; i++) srt[i] = &hsps[i];
+    qsort(srt, n, sizeof(*srt), chain_cmp);
+    for (uint64_t i = 0; i < n; i++) {
+        best[i] = srt[i]->score;
+        parent[i] = -1;
+    }
+    for (uint64_t i = 1; i < n; i++) {
+        int64_t bp = 0, bi = -1;
+        const uint32_t ti = srt[i]->t_start, qi = srt[i]->q_start;
+        for (uint64_t j = 0; j < i; j++) {
+            const orc_hsp* h = srt[j];
+            if (h->t_start + h->length <= ti && h->q_start + h->length <= qi && best[j] > bp) {
+                bp = best[j];
+                bi = (int64_t)j;
+            }
+        }
+        best[i] = bp + srt[i]->score;
+        parent[i] = bi;
+    }
+    uint64_t end = 0;
+    for (uint64_t i = 1; i < n; i++)
+        if (best[i] > best[end]) end = i;
+    uint64_t len = 0;
+    for (int64_t c = (int64_t)end; c >= 0; c = parent[c]) len++;
+    uint64_t k = len;
+    for (int64_t c = (int64_t)end; c >= 0; c = parent[c]) out[--k] = *srt[c];
+    free(srt);
+    free(best);
+    free(parent);
+    return len;
+}

@@ -128,6 +128,10 @@ int orc_diag_admit(void* h, uint32_t t_pos, uint32_t q_pos);
 void orc_diag_mark_covered(void* h, uint32_t t_end, uint32_t q_end);
 void orc_diag_free(void* h);
 
+/* best_chain (src/chain.rs:19-69) in the reference's O(n^2) form: the chain
+ * into out (up to n HSPs) in t_start order; returns its length. */
+uint64_t orc_best_chain(const orc_hsp* hsps, uint64_t n, orc_hsp* out);
+
 void orc_free(void* p);
 
 #ifdef __cplusplus

@@ -96,6 +96,8 @@ def lib():
         L.orc_search_units.argtypes = [C.c_int, P(P(OrcTable)), P(OrcSeq), P(OrcSeq), P(OrcParams), C.c_int,
                                        C.c_int, P(P(OrcHsp)), P(C.c_uint64), P(OrcStats)]
         L.orc_search_units.restype = C.c_int
+        L.orc_best_chain.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
+        L.orc_best_chain.restype = C.c_uint64
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_diag_new.restype = C.c_void_p
         L.orc_diag_admit.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
@@ -412,6 +414,15 @@ def choose_anchor(hsp, t: Seq, q: Seq, sub, ambig: int, window: int):
             best, best_start = cur, start
     mid = best_start + w // 2
     return t0 + mid, q0 + mid
+
+
+def best_chain_c(hsps: np.ndarray) -> np.ndarray:
+    """best_chain (src/chain.rs:19-69) through liboracle's O(n^2) C form, for
+    groups too large for the Python loop below: an HSP record array."""
+    h = np.ascontiguousarray(hsps)
+    out = np.empty(len(h), h.dtype)
+    n = lib().orc_best_chain(h.ctypes.data if len(h) else None, len(h), out.ctypes.data if len(h) else None)
+    return out[:n].copy()
 
 
 def best_chain(hsps) -> list:

@@ -177,3 +177,56 @@ def test_batch_repeated_and_split_units(gxy, ctx):
     assert got[3].tobytes() == lo.tobytes()
     assert got[4].tobytes() == hi.tobytes()
     assert got[5].tobytes() == minus.tobytes()
+
+
+def test_graph_multi_pass_and_kept_graph(gxy):
+    # A raw-hit buffer far smaller than the launch's hits: the passes resume
+    # on the device (tiles that do not fit go to the next pass) inside one
+    # CUDA graph, with further rounds when the graph's passes fall short.
+    # The graph stays with the worker across calls: the same shape is
+    # updated in place, another shape (more passes, other units) is
+    # instantiated anew.  Every result must equal the oracle's.
+    rng = np.random.default_rng(33)
+    target = rand_ascii(rng, 150_000, b"ACGT" * 12 + b"aN")   # 33k raw hits, 27k in the first 9 units
+    queries = make_queries(rng, target, 8, 3000, 30000)
+    c2 = gxy.Context(0)
+    try:
+        tab = gxy.PosTable.build(gxy.PackedSeq.from_ascii(target), P12, 1, ctx=c2)
+        dq = [gxy.PackedSeq.from_ascii(q).to_device(c2) for q in queries]
+        m, sp = gxy.ScoringMatrix.hoxd70(), gxy.SearchParams()
+        units = [(0, qi, s) for qi in range(len(queries)) for s in (0, 1)]
+        want = oracle_units(target, queries, units)
+        assert sum(len(w) for w in want) > 0
+        c2.set_tuning(max_hits_per_pass=4096)
+        for k, sub in enumerate((units, units, units[:9], units)):
+            st = {}
+            got = gxy.batch_search([tab], dq, sub, m, sp, use_graph=True, stats=st, ctx=c2)
+            assert st["raw_hits"] > 3 * 4096 and st["passes"] > 1
+            if k == 1:
+                # the same shape again: the kept graph is updated in place
+                assert st["graph_updates"] >= 1, st
+            for u, g in zip(sub, got):
+                assert g.tobytes() == want[units.index(u)].tobytes(), u
+        for d in dq:
+            d.free()
+        tab.free()
+    finally:
+        c2.close()
+
+
+def test_objects_freed_after_their_context(gxy, ctx):
+    # Device sequences and tables keep their device ordinal, so freeing them
+    # after their context was destroyed touches no freed host memory; the
+    # default context keeps working afterwards.
+    c2 = gxy.Context(0)
+    t = gxy.PackedSeq.from_ascii(b"ACGTTGCAAC" * 3000)
+    dq = t.to_device(c2)
+    tab = gxy.PosTable.build(t, P12, 1, ctx=c2)
+    c2.close()
+    dq.free()
+    tab.free()
+    T = gxy.PackedSeq.from_ascii(b"ACGTACGGTCAGTTACGATC" * 2000)
+    tab2 = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    h = gxy.search(tab2, T, T, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams())
+    assert len(h) > 0
+    tab2.free()

@@ -48,3 +48,86 @@ def test_anchor_rejects_bad_hsps(gxy, ctx):
     for bad in ([(0, 0, 0, 5)], [(4, 0, 8, 5)]):
         with pytest.raises(gxy.GxyError):
             gxy.choose_anchors(dT, dT, np.array(bad, gxy.HSP_DTYPE), gxy.ScoringMatrix.hoxd70(), 4, ctx)
+
+
+# ---------------------------------------------------------------------------
+# best_chain (src/chain.rs:19-69) for many groups on the device.
+# ---------------------------------------------------------------------------
+def _rows(a):
+    return [tuple(int(x) for x in r) for r in a]
+
+
+def test_chain_groups_known_answers(gxy, ctx):
+    # The reference's own cases (src/chain.rs:78-138), one group each, in one launch.
+    h = lambda t, q, n, s: (t, q, n, s)  # noqa: E731
+    cases = [([], []),                                                                     # chain.rs:79-82
+             ([h(10, 20, 30, 1000)], [h(10, 20, 30, 1000)])]                               # :84-88
+    a, b, c = h(0, 0, 20, 500), h(40, 40, 20, 500), h(80, 10, 20, 700)                    # :90-105
+    cases.append(([a, b, c], [a, b]))
+    a, b, c, d = h(0, 0, 10, 100), h(20, 20, 10, 100), h(40, 40, 10, 100), h(60, 60, 10, 500)
+    cases.append(([a, b, c, d], [a, b, c, d]))                                             # :107-117
+    a, b = h(0, 50, 10, 1000), h(20, 0, 10, 800)                                          # :119-128
+    cases.append(([a, b], [a]))
+    a, b = h(10, 10, 5, 100), h(0, 0, 5, 100)                                             # :130-137
+    cases.append(([a, b], [b, a]))
+    arrs = [np.array(g, gxy.HSP_DTYPE).reshape(-1) for g, _ in cases]
+    got = gxy.best_chain_groups(arrs, ctx)
+    for g, (_, want) in zip(got, cases):
+        assert _rows(g) == want
+
+
+def _random_group(rng, gxy, n, span, ties):
+    g = np.zeros(n, gxy.HSP_DTYPE)
+    g["t_start"] = rng.integers(0, span, n)
+    g["q_start"] = rng.integers(0, span, n)
+    g["length"] = rng.integers(0, 40, n)
+    g["score"] = rng.integers(-20, 400, n)
+    if ties and n > 4:
+        # duplicate (t_start, q_start) pairs and equal scores: the tie rules
+        k = n // 4
+        g[:k]["t_start"] = g[k:2 * k]["t_start"]
+        g[:k]["q_start"] = g[k:2 * k]["q_start"]
+        g["score"][::3] = 100
+    return g
+
+
+def test_chain_groups_random_vs_oracle(gxy, ctx):
+    rng = np.random.default_rng(71)
+    sizes = [0, 1, 2, 3, 7, 31, 32, 33, 255, 256, 257, 1000, 4095, 4096, 4097, 6000] + \
+        [int(x) for x in rng.integers(0, 200, 300)]
+    groups = [_random_group(rng, gxy, n, max(64, n * 8), ties=i % 2 == 0) for i, n in enumerate(sizes)]
+    got = gxy.best_chain_groups(groups, ctx)
+    assert len(got) == len(groups)
+    for i, (g, arr) in enumerate(zip(got, groups)):
+        want = O.best_chain_c(arr)
+        assert g.tobytes() == want.tobytes(), (i, len(arr))
+
+
+def test_chain_groups_on_search_hsps(gxy, ctx):
+    # Chains of the HSPs of real searches: one group per (target, strand),
+    # against the oracle's O(n^2) form and the host's O(n log n) form.
+    rng = np.random.default_rng(72)
+    groups = []
+    for k in range(6):
+        t, q = homologous_pair(rng, 40000 + 10000 * k, 0.75 + 0.02 * k, lower=0.1, nfrac=0.01)
+        T, Q = gxy.PackedSeq.from_ascii(t), gxy.PackedSeq.from_ascii(q)
+        tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+        for QQ in (Q, Q.reverse_complement()):
+            groups.append(gxy.search(tab, T, QQ, gxy.ScoringMatrix.hoxd70(),
+                                     gxy.SearchParams(1, gxy.HspParams(910, 1000), 1)))
+    assert sum(len(g) for g in groups) > 100
+    got = gxy.best_chain_groups(groups, ctx)
+    for g, arr in zip(got, groups):
+        assert g.tobytes() == O.best_chain_c(arr).tobytes()
+        assert g.tobytes() == gxy.best_chain(arr).tobytes()
+
+
+def test_chain_groups_rejects_bad_offsets(gxy, ctx):
+    from lastz_gxy_b200._lib import lib
+    h = np.zeros(4, gxy.HSP_DTYPE)
+    out = np.zeros(4, gxy.HSP_DTYPE)
+    ln = np.zeros(2, np.uint64)
+    for off in ([0, 3, 2], [1, 2, 4]):
+        o = np.array(off, np.uint64)
+        assert lib().gxy_best_chain_groups(ctx.h, h.ctypes.data, o.ctypes.data, 2, out.ctypes.data,
+                                           ln.ctypes.data) != 0

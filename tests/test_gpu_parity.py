@@ -332,3 +332,39 @@ def test_window_passes_match_single_pass(gxy):
         tab.free()
     finally:
         c2.close()
+
+
+@pytest.mark.parametrize("case", ["hoxd70", "ambig_high", "no_negative_class", "asymmetric"])
+def test_filter_bounds_cases(gxy, ctx, case):
+    # The upper-bound filter between enumeration and the exact screen takes
+    # each class x = t ^ q at its largest score (at least the ambiguous one);
+    # it is off when no class is <= 0 (a bounded side would never break).
+    # Whatever the matrix, the output must equal the oracle's: a matrix with
+    # the ambiguous score above the transversions (invalid columns in every
+    # class), one with no non-positive class (filter off: every raw hit goes
+    # to the exact screen), and an asymmetric one (sub[t][q] != sub[q][t]).
+    rng = np.random.default_rng(41)
+    t, q = homologous_pair(rng, 40000, 0.8, lower=0.05, nfrac=0.01)
+    base = gxy.ScoringMatrix.hoxd70()
+    sp = gxy.SearchParams(1, gxy.HspParams(910, 3000), 1)
+    if case == "hoxd70":
+        m = base
+    elif case == "ambig_high":
+        m = gxy.ScoringMatrix(sub=[row[:] for row in base.sub], ambig_score=-20)
+    elif case == "no_negative_class":
+        # Transitions score +5: every class has a positive member.
+        sub = [row[:] for row in base.sub]
+        for a, b in ((0, 2), (2, 0), (1, 3), (3, 1), (0, 1), (1, 0), (2, 3), (3, 2), (0, 3), (3, 0), (1, 2), (2, 1)):
+            sub[a][b] = 5 if (a ^ b) == 2 else sub[a][b]
+        sub[0][1] = 1   # class 1 gets a positive member
+        sub[0][3] = 1   # class 3 too
+        m = gxy.ScoringMatrix(sub=sub, ambig_score=-100)
+        sp = gxy.SearchParams(1, gxy.HspParams(910, 6000), 1)
+    else:
+        sub = [row[:] for row in base.sub]
+        sub[0][2], sub[2][0] = -20, -60
+        sub[1][0], sub[0][1] = -90, -130
+        m = gxy.ScoringMatrix(sub=sub, ambig_score=-100)
+    g, o = both(gxy, ctx, t, q, P12, sp, matrix=m)
+    assert g == o
+    assert len(o) > 0

@@ -216,7 +216,7 @@ def test_cancel(gxy, setup):
 
 def test_free_memory_is_refreshed(gxy, setup):
     # The admission estimate is re-based on the device's free memory at a low
-    # rate by the server's monitor thread.
+    # rate, while the server is idle, by the server's monitor thread.
     import time
     _, tables, _ = setup
     srv = gxy.Server(tables, gxy.ScoringMatrix.hoxd70(), gxy.SearchParams())
