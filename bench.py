@@ -170,18 +170,30 @@ def enum_bytes(st: dict, lq: int, n_var: int) -> float:
     return 0.5 * lq + 8.0 * n_var * st["windows"] + 16.0 * st["raw_hits"]
 
 
-def table_roofline(ms_list, npos, lt: int, peak: float) -> dict:
-    """PosTable::build on the device (count, scan, bucket fill) against the
-    algorithmic bytes 0.5*Lt (codes, valid, mask read) + 4*N (positions
-    write) + 8*(4^w + 1) (starts written and read by the scan) + 4*N (count
-    atomics), N = positions; time = CUDA events around the whole build call."""
+def table_bytes(npos: int, lt: int, weight: int = 12) -> float:
+    """Algorithmic bytes of PosTable::build over lt bases: the sequence read
+    once (2-bit codes + valid + mask bits = 0.5 B/bp), the positions written
+    (4 B each) and the bucket starts written (4 B x (4^w + 1)) with the
+    occupancy bitmap (4^w / 8 B) -- what any build must move."""
+    nw = 1 << (2 * weight)
+    return 0.5 * lt + 4.0 * npos + 4.0 * (nw + 1) + nw / 8.0
+
+
+def table_roofline(ms_list, npos, lt: int, peak: float, views: int = 1, workload: str = "") -> dict:
+    """PosTable::build on the device (a stable radix sort of the seedable
+    windows by word, then the bucket starts) against table_bytes; time = CUDA
+    events around the whole build call (allocation and the host sync
+    included).  For a multi-view build npos is a list of (positions, bp)."""
     ms = statistics.median(ms_list)
-    n = npos if npos else lt
-    b = 0.5 * lt + 4 * n + 8 * ((1 << 24) + 1) + 4 * n
+    b = sum(table_bytes(n, l) for n, l in npos) if views > 1 else table_bytes(npos if npos else lt, lt)
     ach = b / (ms / 1e3) / 1e9
-    return {"bound": "hbm", "kernel": "table build (k_count_words + scan + k_fill_buckets)",
-            "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
-            "build_ms": round(ms, 3), "algorithmic_bytes": int(b)}
+    out = {"bound": "hbm", "kernel": "table build (k_radix_hist/k_radix_scatter over the seed words, "
+                                     "k_tbl_first + k_tbl_starts + k_tbl_gaps)",
+           "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+           "build_ms": round(ms, 3), "algorithmic_bytes": int(b)}
+    if workload:
+        out["workload"] = workload
+    return out
 
 
 def run_ours(args, rank: int, world: int, device: int):
@@ -707,15 +719,36 @@ def run_chunked(args):
     dT = g.PackedSeq.from_ascii(pr.target.tobytes()).to_device(ctx)
     dQ = g.PackedSeq.from_ascii(pr.query.tobytes()).to_device(ctx)
     chunks = g.chunk_target(len(pr.target), 10_000_000, 50_000)
+    # One chunk's table alone (timed three times), then every chunk's table
+    # from one sort.
+    mid = chunks[len(chunks) // 2]
+    one_ms = []
+    for _ in range(3):
+        ctx.mark(8)
+        t1 = g.PosTable.build_view(dT, mid[0], mid[1], P12, 1, ctx=ctx)
+        ctx.mark(9)
+        one_ms.append(ctx.elapsed_ms(8, 9))
+        one_npos = t1.total_positions()
+        t1.free()
     ctx.mark(8)
-    tabs = [g.PosTable.build_view(dT, lo, hi, P12, 1, ctx=ctx) for lo, hi, _, _ in chunks]
+    tabs = g.PosTable.build_views(dT, [(lo, hi) for lo, hi, _, _ in chunks], P12, 1, ctx=ctx)
     ctx.mark(9)
     table_ms = ctx.elapsed_ms(8, 9)
+    pk = peaks()[0]
+    tab_roof = {"one_chunk": table_roofline(one_ms, one_npos, mid[1] - mid[0], pk,
+                                            workload="chunk %d..%d (%d bp)" % (mid[0], mid[1], mid[1] - mid[0])),
+                "all_chunks": table_roofline([table_ms], [(t.total_positions(), hi - lo) for t, (lo, hi, _, _) in
+                                                          zip(tabs, chunks)], 0, pk, views=len(chunks),
+                                             workload="%d chunk tables from one sort" % len(chunks))}
     units = [(ci, 0, st, chunks[ci][2], chunks[ci][3]) for ci in range(len(chunks)) for st in (0, 1)]
     mbp2_total = sum(mbp2(c[3] - c[2], len(pr.query), 1) for c in chunks) * 2
     out = {"workload": "chunked: %d bp target x %d bp query, %d chunks x 2 strands" % (
         len(pr.target), len(pr.query), len(chunks)), "mbp2": round(mbp2_total, 2), "table_build_ms": round(table_ms, 2),
+        "roofline_table": tab_roof,
         "generate_s": round(gen_s, 1)}
+    if args.max_hits_per_pass:
+        ctx.set_tuning(max_hits_per_pass=args.max_hits_per_pass)
+        out["max_hits_per_pass"] = args.max_hits_per_pass
     for tr in (1, 0):
         sp = g.SearchParams(transitions=tr)
         tune = autotune(ctx, tabs, [dQ], units, m, sp, workload="chunked", sample_units=4, reps=1, use_cache=False,
@@ -854,6 +887,8 @@ def main():
                     help="served workload: query bases (per strand) per batch at most")
     ap.add_argument("--length", type=int, default=4_000_000, help="case workload length (bp)")
     ap.add_argument("--scale", type=float, default=1.0, help="batched workload size factor")
+    ap.add_argument("--max-hits-per-pass", type=int, default=0,
+                    help="chunked workload: raw-hit buffer of the batched launches (0: the library default)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -200,6 +200,15 @@ gxy_status gxy_table_build(gxy_ctx* ctx, const gxy_packed_seq* target, const cha
 gxy_status gxy_table_build_view(gxy_ctx* ctx, const gxy_dseq* target, uint64_t lo, uint64_t hi,
                                 const char* pattern01, uint32_t step, uint32_t max_word_count,
                                 gxy_table** out);
+/* gxy_table_build_view for n views [lo[i], hi[i]) of one device sequence at
+ * once -- every chunk table of the driver (src/driver.rs:156-215) -- by one
+ * sort over all the views' windows.  out[i] (n entries) receives view i's
+ * table, equal to gxy_table_build_view of that view.  The tables share their
+ * device arrays, which go when the last of them is freed; each is freed with
+ * gxy_table_free as usual. */
+gxy_status gxy_table_build_views(gxy_ctx* ctx, const gxy_dseq* target, uint32_t n, const uint64_t* lo,
+                                 const uint64_t* hi, const char* pattern01, uint32_t step,
+                                 uint32_t max_word_count, gxy_table** out);
 /* PosTable::prune_hot_words(limit) (src/pos_table.rs:113-136) on a built
  * table: drops every bucket with more than limit positions. */
 gxy_status gxy_table_prune_hot_words(gxy_table* t, uint32_t limit);
@@ -229,7 +238,8 @@ gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_p
 /* Copies starts (num_words + 1 entries) and positions to host buffers; either
  * may be NULL. */
 gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions);
-/* Frees a table; valid before or after its context is destroyed. */
+/* Frees a table; valid before or after its context is destroyed, and for
+ * the tables of one gxy_table_build_views call in any order. */
 gxy_status gxy_table_free(gxy_table* t);
 
 /* ---- the drop-in search (src/seed_search.rs:45-125) --------------------- */

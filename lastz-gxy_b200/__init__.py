@@ -363,6 +363,28 @@ class PosTable:
         t.view = (lo, hi)
         return t
 
+    @classmethod
+    def build_views(cls, dseq: DeviceSeq, ranges, pattern, step: int, max_word_count: int = 0,
+                    ctx: Optional[Context] = None) -> list:
+        """One table per (lo, hi) view of dseq, built by one sort over all the
+        views' windows (the driver's chunk tables, src/driver.rs:156-210);
+        each equals build_view of its range."""
+        ctx = ctx or dseq.ctx
+        n = len(ranges)
+        if n == 0:
+            return []
+        lo = np.array([r[0] for r in ranges], np.uint64)
+        hi = np.array([r[1] for r in ranges], np.uint64)
+        hs = (C.c_void_p * n)()
+        check(lib().gxy_table_build_views(ctx.h, dseq.h, n, lo.ctypes.data, hi.ctypes.data, _pattern_str(pattern),
+                                          step, max_word_count, hs))
+        out = []
+        for i in range(n):
+            t = cls(ctx, C.c_void_p(hs[i]), pattern, dseq)
+            t.view = (int(lo[i]), int(hi[i]))
+            out.append(t)
+        return out
+
     def prune_hot_words(self, limit: int) -> None:
         """PosTable::prune_hot_words(limit) (src/pos_table.rs:113-136)."""
         check(lib().gxy_table_prune_hot_words(self.h, limit))

@@ -130,6 +130,7 @@ SIGNATURES = {
     "gxy_dseq_free": (C.c_int, [V]),
     "gxy_table_build": (C.c_int, [V, P(PackedSeqC), C.c_char_p, U32, U32, P(V)]),
     "gxy_table_build_view": (C.c_int, [V, V, U64, U64, C.c_char_p, U32, U32, P(V)]),
+    "gxy_table_build_views": (C.c_int, [V, V, U32, V, V, C.c_char_p, U32, U32, V]),
     "gxy_table_prune_hot_words": (C.c_int, [V, U32]),
     "gxy_table_build_static": (C.c_int, [P(PackedSeqC), C.c_char_p, U32, V, U64, V, U64, P(U64)]),
     "gxy_table_info": (C.c_int, [V, P(U64), P(U64), P(U32), P(U32)]),

@@ -47,12 +47,6 @@ gxy_status set_device(gxy_ctx* ctx) {
     return GXY_OK;
 }
 
-uint32_t n_windows(uint64_t len, uint32_t L, uint32_t step) {
-    // iter_with_stride (src/seeds.rs:151-161): 0, step, ... <= len - L.
-    if (len < L) return 0;
-    return (uint32_t)((len - L) / step + 1);
-}
-
 bool same_host_seq(const gxy_table* t, const gxy_packed_seq* s) {
     return s->codes == t->hc && s->valid == t->hv && s->mask == t->hm && s->len == t->hlen;
 }
@@ -86,134 +80,109 @@ gxy_status prune_table(gxy_table* t, uint32_t limit, Worker* W) {
         set_error(std::string("table prune: ") + cudaGetErrorString(e));
         return GXY_ECUDA;
     }
-    dev_free(t->starts);
-    dev_free(t->positions);
+    if (t->own_arrays) {
+        dev_free(t->starts);
+        dev_free(t->positions);
+    }
     t->starts = new_starts;
     t->positions = newpos;
+    t->own_arrays = true;
     t->npos = total2;
+    // Pruned buckets are empty now: their occupancy bits go.
+    launch_occupancy(t->starts, nw, t->occ, st);
+    e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(std::string("table prune: ") + cudaGetErrorString(e));
+        return GXY_ECUDA;
+    }
     return GXY_OK;
 }
 
-gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t hi, const Pattern& pat,
-                       uint32_t step, uint32_t mwc, gxy_table** out) {
+}  // namespace
+
+TableMem::~TableMem() {
+    cudaSetDevice(device);
+    dev_free(starts);
+    dev_free(positions);
+    dev_free(occ);
+}
+
+namespace {
+
+// PosTable::build for n views [lo[v], hi[v]) of seq, as one sort; out[v] is
+// view v's table.  The tables share one TableMem.
+gxy_status build_tables(gxy_ctx* ctx, const gxy_dseq* seq, uint32_t n, const uint64_t* lo, const uint64_t* hi,
+                        const Pattern& pat, uint32_t step, uint32_t mwc, gxy_table** out) {
     WorkerLease L(ctx);
     if (!L.w) return L.err;
     Worker* W = L.w;
     cudaStream_t st = W->st;
     const uint64_t nw = 1ull << (2 * pat.weight);
-    const uint32_t nwin = n_windows(hi - lo, pat.len, step);
-    gxy_table* t = new gxy_table();
-    t->ctx = ctx;
-    t->device = ctx->device;
-    t->seq = seq;
-    t->lo = lo;
-    t->hi = hi;
-    t->num_words = nw;
-    t->pat = pat;
-    t->step = step;
-    DevBuf& counts_buf = W->tk0;
-    auto fail = [&](gxy_status s) {
-        dev_free(t->starts);
-        dev_free(t->positions);
-        dev_free(t->occ);
-        delete t;
-        return s;
-    };
-    // counts[word] -> exclusive scan -> starts (src/pos_table.rs:42-58); then
-    // each window drops its position into its bucket (src/pos_table.rs:69-75)
-    // through an atomic cursor, so bucket order is arbitrary until the table
-    // is made canonical (on download).
-    cudaError_t e = dev_alloc((void**)&t->starts, (nw + 1) * 4, st);
-    if (e == cudaSuccess) e = dev_alloc((void**)&t->positions, (size_t)std::max<uint32_t>(nwin, 1) * 4, st);
-    if (e == cudaSuccess) e = counts_buf.ensure((size_t)(nw + 1) * 4);
+    const uint64_t occ_words = (nw + 31) / 32;
+    uint64_t total = 0;
+    for (uint32_t v = 0; v < n; v++) total += n_windows(hi[v] - lo[v], pat.len, step);
+    auto mem = std::make_shared<TableMem>();
+    mem->device = ctx->device;
+    // A stable sort of the seedable windows by (view, word)
+    // (src/pos_table.rs:42-75), which also fills starts and the occupancy
+    // bitmaps the searches test before they read a bucket's bounds.
+    cudaError_t e = dev_alloc((void**)&mem->starts, (size_t)n * (nw + 1) * 4, st);
+    if (e == cudaSuccess) e = dev_alloc((void**)&mem->positions, (size_t)std::max<uint64_t>(total, 1) * 4, st);
+    if (e == cudaSuccess) e = dev_alloc((void**)&mem->occ, (size_t)n * occ_words * 4, st);
     if (e != cudaSuccess) {
         set_error(std::string("table allocation: ") + cudaGetErrorString(e));
-        return fail(GXY_ENOMEM);
+        return GXY_ENOMEM;
     }
-    uint32_t* counts = counts_buf.as<uint32_t>();
-    e = cudaMemsetAsync(counts, 0, (nw + 1) * 4, st);
-    const SeqView view = view_of(seq, lo, hi);
-    launch_count_words(view, pat, step, nwin, counts, st);
-    // The scan also leaves a copy of starts in counts: the fill's cursors.
-    scan_u32(counts, t->starts, nullptr, nw, nw, true, nullptr, W->ps, st, counts);
-    launch_fill_buckets(view, pat, step, nwin, counts, t->positions, st);
-    uint32_t* total_h = static_cast<uint32_t*>(W->h_pinned);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(total_h, t->starts + nw, 4, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    std::vector<uint32_t> first((size_t)n + 1);
+    API_TRY(sort_build_views(seq, n, lo, hi, pat, step, mem->starts, mem->positions, mem->occ, first.data(), W));
+    std::vector<gxy_table*> made;
+    auto fail = [&](gxy_status s) {
+        for (gxy_table* t : made) {
+            if (t->own_arrays) {
+                dev_free(t->starts);
+                dev_free(t->positions);
+            }
+            delete t;
+        }
+        return s;
+    };
+    for (uint32_t v = 0; v < n; v++) {
+        gxy_table* t = new gxy_table();
+        made.push_back(t);
+        t->ctx = ctx;
+        t->device = ctx->device;
+        t->seq = seq;
+        t->lo = lo[v];
+        t->hi = hi[v];
+        t->num_words = nw;
+        t->pat = pat;
+        t->step = step;
+        t->mem = mem;
+        t->starts = mem->starts + (size_t)v * (nw + 1);
+        t->positions = mem->positions + first[v];
+        t->occ = mem->occ + (size_t)v * occ_words;
+        t->npos = first[v + 1] - first[v];
+        if (mwc > 0) {
+            const gxy_status ps = prune_table(t, mwc, W);
+            if (ps != GXY_OK) return fail(ps);
+        }
+    }
+    e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error(std::string("table build: ") + cudaGetErrorString(e));
         return fail(GXY_ECUDA);
     }
-    t->npos = *total_h;
-    t->canonical = t->npos == 0;
-    if (e == cudaSuccess && mwc > 0) {
-        const gxy_status ps = prune_table(t, mwc, W);
-        if (ps != GXY_OK) return fail(ps);
-    }
-    // The searches test a bucket's occupancy bit before reading its bounds.
-    if (e == cudaSuccess) e = dev_alloc((void**)&t->occ, (size_t)((nw + 31) / 32) * 4, st);
-    if (e == cudaSuccess) launch_occupancy(t->starts, nw, t->occ, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        set_error(std::string("table finish: ") + cudaGetErrorString(e));
-        return fail(GXY_ECUDA);
-    }
-    *out = t;
+    for (uint32_t v = 0; v < n; v++) out[v] = made[v];
     return GXY_OK;
 }
 
-// Puts every bucket in ascending position order, the order of the
-// reference's stable scatter (src/pos_table.rs:69-75): buckets of <= 16 by
-// one thread each, <= kBlockBucket by one block each, larger ones by the
-// radix sort, one bucket at a time.
-gxy_status canonicalize(gxy_table* t, Worker* W) {
-    if (t->canonical) return GXY_OK;
-    cudaStream_t st = W->st;
-    uint32_t cap = 1u << 16;
-    uint32_t* hn = static_cast<uint32_t*>(W->h_pinned);
-    for (;;) {
-        API_CK(W->tk1.ensure(((size_t)cap * 2 + 1) * 4));
-        uint32_t* nbig = W->tk1.as<uint32_t>();
-        API_CK(cudaMemsetAsync(nbig, 0, 4, st));
-        launch_sort_small_buckets(t->starts, t->num_words, t->positions, nbig + 1, nbig, cap, st);
-        API_CK(cudaMemcpyAsync(hn, nbig, 4, cudaMemcpyDeviceToHost, st));
-        API_CK(cudaStreamSynchronize(st));
-        if (*hn > cap) {
-            cap = *hn;   // re-sorting the sorted small buckets is harmless
-            continue;
-        }
-        break;
-    }
-    const uint32_t n_big = *hn;
-    uint32_t* big = W->tk1.as<uint32_t>() + 1;
-    launch_sort_block_buckets(big, n_big, t->positions, st);
-    if (n_big) {
-        std::vector<uint32_t> hb((size_t)n_big * 2);
-        API_CK(cudaMemcpyAsync(hb.data(), big, hb.size() * 4, cudaMemcpyDeviceToHost, st));
-        API_CK(cudaStreamSynchronize(st));
-        int bits = 0;
-        while (bits < 32 && (1ull << bits) < t->hi - t->lo) bits++;
-        RadixPass passes[8];
-        const int np = plan_radix(0, std::max(bits, 1), 0, 0, passes, 8);
-        for (uint32_t i = 0; i < n_big; i++) {
-            const uint32_t b = hb[2 * i], n = hb[2 * i + 1];
-            if (n <= kBlockBucket) continue;
-            API_CK(W->tk0.ensure((size_t)n * 4));
-            API_CK(W->tv0.ensure((size_t)n * 4));
-            API_CK(W->tv1.ensure((size_t)n * 4));
-            const int which = radix_sort_u32(t->positions + b, W->tv0.as<uint32_t>(), W->tk0.as<uint32_t>(),
-                                             W->tv1.as<uint32_t>(), nullptr, n, n, passes, np, W->ps, st);
-            if (which)
-                API_CK(cudaMemcpyAsync(t->positions + b, W->tk0.p, (size_t)n * 4, cudaMemcpyDeviceToDevice, st));
-        }
-    }
-    API_CK(cudaStreamSynchronize(st));
-    API_CK(cudaGetLastError());
-    t->canonical = true;
-    return GXY_OK;
+gxy_status build_table(gxy_ctx* ctx, const gxy_dseq* seq, uint64_t lo, uint64_t hi, const Pattern& pat,
+                       uint32_t step, uint32_t mwc, gxy_table** out) {
+    return build_tables(ctx, seq, 1, &lo, &hi, pat, step, mwc, out);
 }
+
 
 gxy_status deliver(const gxy_hsp* v, uint64_t n, gxy_hsp_buf* out) {
     if (!out) return GXY_OK;
@@ -303,6 +272,7 @@ gxy_status gxy_ctx_create(int device, gxy_ctx** out) {
     API_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
     prims_init();
     filter_init();
+    table_init();
     gxy_ctx* c = new gxy_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
@@ -521,6 +491,39 @@ gxy_status gxy_table_build_view(gxy_ctx* ctx, const gxy_dseq* target, uint64_t l
     return build_table(ctx, target, lo, hi, pat, step, max_word_count, out);
 }
 
+gxy_status gxy_table_build_views(gxy_ctx* ctx, const gxy_dseq* target, uint32_t n, const uint64_t* lo,
+                                 const uint64_t* hi, const char* pattern01, uint32_t step, uint32_t max_word_count,
+                                 gxy_table** out) {
+    if (!ctx || !target || !out || (n && (!lo || !hi))) return GXY_EINVAL;
+    for (uint32_t v = 0; v < n; v++)
+        if (lo[v] > hi[v] || hi[v] > target->len) {
+            set_error("view outside the sequence");
+            return GXY_EINVAL;
+        }
+    if (step < 1) {
+        set_error("step must be >= 1 (src/pos_table.rs:36)");
+        return GXY_EINVAL;
+    }
+    if (n == 0) return GXY_OK;
+    Pattern pat;
+    API_TRY(parse_pattern(pattern01, pat));
+    API_TRY(set_device(ctx));
+    if (2 * (int)pat.weight + table_view_bits(n) <= 32)
+        return build_tables(ctx, target, n, lo, hi, pat, step, max_word_count, out);
+    // Too many views for one key: one sort per view.
+    for (uint32_t v = 0; v < n; v++) {
+        const gxy_status s = build_tables(ctx, target, 1, lo + v, hi + v, pat, step, max_word_count, out + v);
+        if (s != GXY_OK) {
+            for (uint32_t u = 0; u < v; u++) {
+                gxy_table_free(out[u]);
+                out[u] = nullptr;
+            }
+            return s;
+        }
+    }
+    return GXY_OK;
+}
+
 gxy_status gxy_table_prune_hot_words(gxy_table* t, uint32_t limit) {
     if (!t) return GXY_EINVAL;
     API_TRY(set_device(t->ctx));
@@ -542,13 +545,6 @@ gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_p
 gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions) {
     if (!t) return GXY_EINVAL;
     API_TRY(set_device(t->ctx));
-    if (positions && !t->canonical) {
-        // Bucket order is an internal detail until it is observed here; the
-        // table's contents (and every search on it) are the same either way.
-        WorkerLease L(t->ctx);
-        if (!L.w) return L.err;
-        API_TRY(canonicalize(const_cast<gxy_table*>(t), L.w));
-    }
     if (starts) API_CK(cudaMemcpy(starts, t->starts, (t->num_words + 1) * 4, cudaMemcpyDeviceToHost));
     if (positions && t->npos) API_CK(cudaMemcpy(positions, t->positions, t->npos * 4, cudaMemcpyDeviceToHost));
     return GXY_OK;
@@ -557,9 +553,11 @@ gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* po
 gxy_status gxy_table_free(gxy_table* t) {
     if (!t) return GXY_OK;
     cudaSetDevice(t->device);
-    dev_free(t->starts);
-    dev_free(t->positions);
-    dev_free(t->occ);
+    if (t->own_arrays) {
+        dev_free(t->starts);
+        dev_free(t->positions);
+    }
+    t->mem.reset();
     dseq_destroy(t->owned);
     delete t;
     return GXY_OK;

@@ -23,15 +23,6 @@ const char* last_error() { return g_err.c_str(); }
         if (s_ != GXY_OK) return s_;  \
     } while (0)
 
-#define GXY_CK(call)                                                                         \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess) {                                                             \
-            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
-            return e_ == cudaErrorMemoryAllocation ? GXY_ENOMEM : GXY_ECUDA;                 \
-        }                                                                                    \
-    } while (0)
-
 cudaError_t DevBuf::ensure(size_t need) {
     if (need <= bytes && p) return cudaSuccess;
     if (p) cudaFreeAsync(p, st);

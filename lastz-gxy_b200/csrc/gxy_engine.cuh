@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -118,20 +119,30 @@ struct gxy_dseq {
     cudaStream_t st = nullptr;   // stream the allocation is ordered on
 };
 
+// The device arrays of the tables built together by one sort (one table, or
+// every view of a multi-view build); freed when the last of them is freed.
+struct TableMem {
+    int device = 0;
+    uint32_t* starts = nullptr;      // tables x (num_words + 1)
+    uint32_t* positions = nullptr;   // the tables' positions, one after the other
+    uint32_t* occ = nullptr;         // tables x occupancy words
+    ~TableMem();
+};
+
 struct gxy_table {
     gxy_ctx* ctx = nullptr;
     int device = 0;   // as gxy_dseq::device
     gxy_dseq* owned = nullptr;
     const gxy_dseq* seq = nullptr;
     uint64_t lo = 0, hi = 0;
-    uint32_t* starts = nullptr;
-    uint32_t* positions = nullptr;
-    uint32_t* occ = nullptr;   // bit (w & 31) of occ[w >> 5]: bucket w is non-empty
+    std::shared_ptr<TableMem> mem;
+    uint32_t* starts = nullptr;      // in mem, or this table's own array after a prune
+    uint32_t* positions = nullptr;   // likewise
+    bool own_arrays = false;         // starts and positions are this table's own (after a prune)
+    uint32_t* occ = nullptr;   // bit (w & 31) of occ[w >> 5]: bucket w is non-empty (in mem)
     uint64_t num_words = 0;
     uint64_t npos = 0;
-    // Positions within a bucket are in ascending order (the reference's
-    // order) only once canonical; searches do not depend on that order.
-    bool canonical = true;
+    // Positions within a bucket are in ascending order, the reference's order.
     gxy::Pattern pat{};
     uint32_t step = 1;
     const void* hc = nullptr;
@@ -168,6 +179,36 @@ void dseq_destroy(gxy_dseq* s);
 void dseq_destroy_async(gxy_dseq* s, cudaStream_t st);
 gxy_status dseq_fill_host(gxy_dseq* d, const gxy_packed_seq* h, cudaStream_t st);
 SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi);
+
+// Returns from the calling function with a status when a CUDA call fails.
+#define GXY_CK(call)                                                                         \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+            return e_ == cudaErrorMemoryAllocation ? GXY_ENOMEM : GXY_ECUDA;                 \
+        }                                                                                    \
+    } while (0)
+
+// Windows of a sequence of len bases for a pattern of span L:
+// iter_with_stride (src/seeds.rs:151-161) visits 0, step, ... <= len - L.
+inline uint32_t n_windows(uint64_t len, uint32_t L, uint32_t step) {
+    if (len < L) return 0;
+    return (uint32_t)((len - L) / step + 1);
+}
+
+// PosTable::build (src/pos_table.rs:35-83) for n views [lo[v], hi[v]) of one
+// sequence as one stable radix sort of their seedable windows by (view, word)
+// (csrc/gxy_table.cu): fills starts (n x (nw + 1) entries), positions (view
+// after view) and the occupancy bitmaps (n x ceil(nw / 32) words), then
+// first_host[0 .. n] = where each view's positions begin (a host sync).
+gxy_status sort_build_views(const gxy_dseq* seq, uint32_t n_views, const uint64_t* lo, const uint64_t* hi,
+                            const Pattern& pat, uint32_t step, uint32_t* starts, uint32_t* positions, uint32_t* occ,
+                            uint32_t* first_host, Worker* W);
+// Bits of the view index in a multi-view build's sort key.
+int table_view_bits(uint32_t n_views);
+// Kernel attributes of the table build; once per device, before any capture.
+void table_init();
 
 // SeedPattern::parse (src/seeds.rs:38-51) with the engine's limits: at most
 // 32 positions (src/seeds.rs:28-32), weight at most kMaxWeight.

@@ -135,128 +135,6 @@ void launch_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, 
     k_seed_words<<<blocks, 256, 0, st>>>(view, pat, step, nwin, sentinel, keys, vals, counts);
 }
 
-// Both table passes give each thread four windows at a time (stride apart,
-// so a warp's loads stay coalesced): four independent word loads, atomics and
-// stores in flight instead of one dependent chain per window.
-__global__ void k_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* counts) {
-    const uint32_t S = gridDim.x * blockDim.x;
-    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nwin; k0 += 4 * S) {
-        uint32_t w[4];
-        bool ok[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const uint32_t k = k0 + u * S;
-            ok[u] = k < nwin && word_at(view, pat, k * step, w[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-            if (ok[u]) atomicAdd(&counts[w[u]], 1u);
-    }
-}
-
-void launch_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* counts,
-                        cudaStream_t st) {
-    if (!nwin) return;
-    const int blocks = (int)umin64((nwin + 255) / 256, 148 * 16);
-    count_launch();
-    k_count_words<<<blocks, 256, 0, st>>>(view, pat, step, nwin, counts);
-}
-
-__global__ void k_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* cursor,
-                               uint32_t* positions) {
-    const uint32_t S = gridDim.x * blockDim.x;
-    for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nwin; k0 += 4 * S) {
-        uint32_t w[4], slot[4];
-        bool ok[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const uint32_t k = k0 + u * S;
-            ok[u] = k < nwin && word_at(view, pat, k * step, w[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-            if (ok[u]) slot[u] = atomicAdd(&cursor[w[u]], 1u);
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-            if (ok[u]) positions[slot[u]] = (k0 + u * S) * step;
-    }
-}
-
-void launch_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* cursor,
-                         uint32_t* positions, cudaStream_t st) {
-    if (!nwin) return;
-    const int blocks = (int)umin64((nwin + 255) / 256, 148 * 16);
-    count_launch();
-    k_fill_buckets<<<blocks, 256, 0, st>>>(view, pat, step, nwin, cursor, positions);
-}
-
-__global__ void k_sort_small_buckets(const uint32_t* starts, uint64_t nw, uint32_t* pos, uint32_t* big,
-                                     uint32_t* n_big, uint32_t big_cap) {
-    for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = starts[w], n = starts[w + 1] - b;
-        if (n <= 1) continue;
-        if (n > 16) {
-            const uint32_t i = atomicAdd(n_big, 1u);
-            if (i < big_cap) {
-                big[2 * i] = b;
-                big[2 * i + 1] = n;
-            }
-            continue;
-        }
-        uint32_t v[16];
-        for (uint32_t i = 0; i < n; i++) v[i] = pos[b + i];
-        for (uint32_t i = 1; i < n; i++) {
-            const uint32_t x = v[i];
-            uint32_t j = i;
-            while (j > 0 && v[j - 1] > x) {
-                v[j] = v[j - 1];
-                j--;
-            }
-            v[j] = x;
-        }
-        for (uint32_t i = 0; i < n; i++) pos[b + i] = v[i];
-    }
-}
-
-void launch_sort_small_buckets(const uint32_t* starts, uint64_t num_words, uint32_t* positions, uint32_t* big,
-                               uint32_t* n_big, uint32_t big_cap, cudaStream_t st) {
-    count_launch();
-    k_sort_small_buckets<<<148 * 8, 256, 0, st>>>(starts, num_words, positions, big, n_big, big_cap);
-}
-
-// Bitonic sort of one bucket (<= kBlockBucket positions) in shared memory.
-__global__ __launch_bounds__(1024) void k_sort_block_buckets(const uint32_t* big, uint32_t* pos) {
-    __shared__ uint32_t s[kBlockBucket];
-    const uint32_t b = big[2 * blockIdx.x], n = big[2 * blockIdx.x + 1];
-    if (n > kBlockBucket) return;   // sorted by the caller's radix path
-    uint32_t m = 1;
-    while (m < n) m <<= 1;
-    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) s[i] = i < n ? pos[b + i] : 0xffffffffu;
-    __syncthreads();
-    for (uint32_t k = 2; k <= m; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const uint32_t x = s[i], y = s[l];
-                    const bool up = (i & k) == 0;
-                    if (up ? x > y : x < y) {
-                        s[i] = y;
-                        s[l] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) pos[b + i] = s[i];
-}
-
-void launch_sort_block_buckets(const uint32_t* big, uint32_t n_big, uint32_t* positions, cudaStream_t st) {
-    if (!n_big) return;
-    count_launch();
-    k_sort_block_buckets<<<n_big, 1024, 0, st>>>(big, positions);
-}
 
 __global__ void k_prune_counts(const uint32_t* starts, uint64_t nw, uint32_t limit, uint32_t* counts2) {
     for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nw; w += (uint64_t)gridDim.x * blockDim.x) {

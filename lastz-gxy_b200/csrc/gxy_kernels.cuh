@@ -49,23 +49,6 @@ void launch_reverse_complement(const uint64_t* icodes, const uint32_t* ivalid, c
 // window that is not seedable; val = view-local position.  counts[word]++.
 void launch_seed_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t num_words_sentinel,
                        uint32_t* keys, uint32_t* vals, uint32_t* counts, cudaStream_t st);
-// counts[word]++ for every seedable window k*step of the view.
-void launch_count_words(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* counts,
-                        cudaStream_t st);
-// Fills each bucket: positions[cursor[w]++] = p for every seedable window p
-// (cursor = a copy of starts, left at the bucket ends).  The order of
-// positions within a bucket is arbitrary; launch_sort_*_buckets puts it in
-// ascending order.
-void launch_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_t nwin, uint32_t* cursor,
-                         uint32_t* positions, cudaStream_t st);
-// Sorts every bucket of at most 16 positions in place (one thread each) and
-// lists the larger ones as (first, size) pairs in big[0 .. 2 * *n_big)
-// (entries past big_cap are dropped; *n_big still counts them).
-void launch_sort_small_buckets(const uint32_t* starts, uint64_t num_words, uint32_t* positions, uint32_t* big,
-                               uint32_t* n_big, uint32_t big_cap, cudaStream_t st);
-// Sorts the listed buckets of at most kBlockBucket positions, one block each.
-constexpr uint32_t kBlockBucket = 4096;
-void launch_sort_block_buckets(const uint32_t* big, uint32_t n_big, uint32_t* positions, cudaStream_t st);
 // prune_hot_words: counts2[w] = bucket size when <= limit, else 0.
 void launch_prune_counts(const uint32_t* starts, uint64_t num_words, uint32_t limit, uint32_t* counts2,
                          cudaStream_t st);

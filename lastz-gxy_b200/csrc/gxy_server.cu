@@ -44,11 +44,6 @@ struct Request {
     std::vector<gxy_hsp> plus, minus;
 };
 
-uint32_t windows_of(uint64_t len, uint32_t L, uint32_t step) {
-    if (len < L) return 0;
-    return (uint32_t)((len - L) / step + 1);
-}
-
 }  // namespace
 }  // namespace gxy
 
@@ -155,7 +150,7 @@ gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
             u.starts = t->starts;
             u.positions = t->positions;
             u.occ = t->occ;
-            u.nwin = windows_of(q->len, pat.len, s->params.step);
+            u.nwin = n_windows(q->len, pat.len, s->params.step);
             u.primary_lo = u.primary_hi = 0;
             u.avg_bucket = t->num_words ? (double)t->npos / (double)t->num_words : 0.0;
             plan.push_back(u);

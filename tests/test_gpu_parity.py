@@ -93,10 +93,10 @@ def test_table_bit_exact(gxy, ctx, pattern, step, mwc):
     assert np.array_equal(pos, ot.positions())
 
 
-# Table builds fill buckets through atomic cursors; the download puts every
-# bucket in ascending order by size class (<= 16 one thread, <= 4096 one
-# block, larger the radix sort).  All three against the oracle, after a
-# search on the same table (searches do not need the order).
+# The build is a stable radix sort of the windows by word, so every bucket
+# holds its positions in ascending order straight from the build -- small
+# buckets, buckets of thousands (a poly-A run, a tandem repeat) -- against the
+# oracle, after a search on the same table.
 @pytest.mark.parametrize("pattern,step", [("111", 1), ("11011", 1), (P12, 1), ("111", 2)])
 def test_table_bucket_orders(gxy, ctx, pattern, step):
     rng = np.random.default_rng(7 + step + len(pattern))
@@ -120,6 +120,55 @@ def test_table_bucket_orders(gxy, ctx, pattern, step):
     got2 = gxy.search(tab, T, gxy.PackedSeq.from_ascii(q2), gxy.ScoringMatrix.hoxd70(), sp)
     want2, _ = O.search(ot, O.pack_ascii(s), O.pack_ascii(q2), orc_params(gxy.ScoringMatrix.hoxd70(), sp))
     assert as_tuples(got2) == as_tuples(want2) and len(want2) > 0
+
+
+def test_table_full_size_bit_exact(gxy, ctx):
+    # A 10 Mbp chromosome-style target (repeat families, soft-masked runs,
+    # N blocks), 12of19 and step 1, and a 2 Mbp target at step 2: starts and
+    # positions equal the reference's stable scatter, bucket order included.
+    from lastz_gxy_b200 import synth
+    for n, step in ((10_000_000, 1), (2_000_000, 2)):
+        s = synth.chromosome(np.random.default_rng(n + step), n, families=n // 5000, nblocks=20).tobytes()
+        T = gxy.PackedSeq.from_ascii(s)
+        tab = gxy.PosTable.build(T, P12, step, ctx=ctx)
+        starts, pos = tab.arrays()
+        ot = O.Table(O.pack_ascii(s), P12, step)
+        assert np.array_equal(starts, ot.starts())
+        assert np.array_equal(pos, ot.positions())
+        assert int(np.diff(starts.astype(np.int64)).max()) > 5
+        tab.free()
+
+
+@pytest.mark.parametrize("mwc", [0, 3])
+def test_table_build_views(gxy, ctx, mwc):
+    # Overlapping chunk views of one device sequence (chunk_target's shape,
+    # src/driver.rs:156-194), an empty view and one shorter than the pattern,
+    # built by one sort: each equals its own build_view and the oracle's
+    # table of the sliced chunk; freeing them in any order leaves the rest
+    # intact.
+    from lastz_gxy_b200 import synth
+    s = synth.chromosome(np.random.default_rng(41), 3_000_000, families=600, nblocks=4).tobytes()
+    dT = gxy.PackedSeq.from_ascii(s).to_device(ctx)
+    ranges = [(lo, hi) for lo, hi, _, _ in gxy.chunk_target(len(s), 400_000, 20_000)]
+    ranges += [(1000, 1000), (5000, 5010), (0, len(s))]
+    tabs = gxy.PosTable.build_views(dT, ranges, P12, 1, mwc, ctx=ctx)
+    assert len(tabs) == len(ranges)
+    gone = (3, 0, len(ranges) - 1)
+    for i in gone:
+        tabs[i].free()
+    for i, ((lo, hi), t) in enumerate(zip(ranges, tabs)):
+        if i in gone:
+            continue
+        starts, pos = t.arrays()
+        one = gxy.PosTable.build_view(dT, lo, hi, P12, 1, mwc, ctx=ctx)
+        s1, p1 = one.arrays()
+        one.free()
+        assert np.array_equal(starts, s1) and np.array_equal(pos, p1), (lo, hi)
+        if i in (1, len(ranges) - 3, len(ranges) - 2):
+            ot = O.Table(O.pack_ascii(s[lo:hi]), P12, 1, mwc)
+            assert np.array_equal(starts, ot.starts()) and np.array_equal(pos, ot.positions()), (lo, hi)
+        t.free()
+    dT.free()
 
 
 def test_tiny_weight_tables(gxy, ctx):
