@@ -180,15 +180,15 @@ def table_bytes(npos: int, lt: int, weight: int = 12) -> float:
 
 
 def table_roofline(ms_list, npos, lt: int, peak: float, views: int = 1, workload: str = "") -> dict:
-    """PosTable::build on the device (a stable radix sort of the seedable
-    windows by word, then the bucket starts) against table_bytes; time = CUDA
-    events around the whole build call (allocation and the host sync
-    included).  For a multi-view build npos is a list of (positions, bp)."""
+    """PosTable::build on the device (counts, scan, fill through atomic
+    cursors, in-bucket sorts) against table_bytes; time = CUDA events around
+    the whole build call (allocation and the host sync included).  For a
+    multi-view build npos is a list of (positions, bp)."""
     ms = statistics.median(ms_list)
     b = sum(table_bytes(n, l) for n, l in npos) if views > 1 else table_bytes(npos if npos else lt, lt)
     ach = b / (ms / 1e3) / 1e9
-    out = {"bound": "hbm", "kernel": "table build (k_radix_hist/k_radix_scatter over the seed words, "
-                                     "k_tbl_first + k_tbl_starts + k_tbl_gaps)",
+    out = {"bound": "hbm", "kernel": "table build (k_count_words + scan + k_fill_buckets + "
+                                     "k_sort_small_buckets / k_sort_block_buckets)",
            "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
            "build_ms": round(ms, 3), "algorithmic_bytes": int(b)}
     if workload:
@@ -720,7 +720,7 @@ def run_chunked(args):
     dQ = g.PackedSeq.from_ascii(pr.query.tobytes()).to_device(ctx)
     chunks = g.chunk_target(len(pr.target), 10_000_000, 50_000)
     # One chunk's table alone (timed three times), then every chunk's table
-    # from one sort.
+    # from one build (one count, scan, fill and bucket sort over all chunks).
     mid = chunks[len(chunks) // 2]
     one_ms = []
     for _ in range(3):
@@ -739,7 +739,7 @@ def run_chunked(args):
                                             workload="chunk %d..%d (%d bp)" % (mid[0], mid[1], mid[1] - mid[0])),
                 "all_chunks": table_roofline([table_ms], [(t.total_positions(), hi - lo) for t, (lo, hi, _, _) in
                                                           zip(tabs, chunks)], 0, pk, views=len(chunks),
-                                             workload="%d chunk tables from one sort" % len(chunks))}
+                                             workload="%d chunk tables from one build" % len(chunks))}
     units = [(ci, 0, st, chunks[ci][2], chunks[ci][3]) for ci in range(len(chunks)) for st in (0, 1)]
     mbp2_total = sum(mbp2(c[3] - c[2], len(pr.query), 1) for c in chunks) * 2
     out = {"workload": "chunked: %d bp target x %d bp query, %d chunks x 2 strands" % (

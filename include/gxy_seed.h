@@ -389,9 +389,11 @@ typedef struct {
     uint64_t big_bases;
     uint32_t max_big_inflight;
     uint32_t reserved_;
-    /* When > 0, each dispatcher sizes its buffers at start for a query of
-     * this many bases against the largest resident table, so that requests up
-     * to that size never wait for a device allocation. */
+    /* When > 0, each dispatcher sizes every buffer a batch uses at start for
+     * a query of this many bases against the largest resident table, and a
+     * batch then takes at most this many query bases (per strand) besides its
+     * first request: no request that size or smaller waits for a device
+     * allocation (growing a buffer by gigabytes took up to 0.7 s on a B200). */
     uint64_t warm_bases;
 } gxy_server_opts;
 

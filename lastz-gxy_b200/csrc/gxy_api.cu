@@ -86,6 +86,7 @@ gxy_status prune_table(gxy_table* t, uint32_t limit, Worker* W) {
     }
     t->starts = new_starts;
     t->positions = newpos;
+    t->pos_base = 0;
     t->own_arrays = true;
     t->npos = total2;
     // Pruned buckets are empty now: their occupancy bits go.
@@ -119,23 +120,23 @@ gxy_status build_tables(gxy_ctx* ctx, const gxy_dseq* seq, uint32_t n, const uin
     Worker* W = L.w;
     cudaStream_t st = W->st;
     const uint64_t nw = 1ull << (2 * pat.weight);
-    const uint64_t occ_words = (nw + 31) / 32;
+    const uint64_t G = (uint64_t)n * nw;   // buckets of all views
     uint64_t total = 0;
     for (uint32_t v = 0; v < n; v++) total += n_windows(hi[v] - lo[v], pat.len, step);
     auto mem = std::make_shared<TableMem>();
     mem->device = ctx->device;
-    // A stable sort of the seedable windows by (view, word)
-    // (src/pos_table.rs:42-75), which also fills starts and the occupancy
-    // bitmaps the searches test before they read a bucket's bounds.
-    cudaError_t e = dev_alloc((void**)&mem->starts, (size_t)n * (nw + 1) * 4, st);
+    // Counts -> scan -> fill -> in-bucket sorts (src/pos_table.rs:42-75),
+    // with the occupancy bitmap the searches test before they read a
+    // bucket's bounds.
+    cudaError_t e = dev_alloc((void**)&mem->starts, (size_t)(G + 1) * 4, st);
     if (e == cudaSuccess) e = dev_alloc((void**)&mem->positions, (size_t)std::max<uint64_t>(total, 1) * 4, st);
-    if (e == cudaSuccess) e = dev_alloc((void**)&mem->occ, (size_t)n * occ_words * 4, st);
+    if (e == cudaSuccess) e = dev_alloc((void**)&mem->occ, (size_t)((G + 31) / 32) * 4, st);
     if (e != cudaSuccess) {
         set_error(std::string("table allocation: ") + cudaGetErrorString(e));
         return GXY_ENOMEM;
     }
     std::vector<uint32_t> first((size_t)n + 1);
-    API_TRY(sort_build_views(seq, n, lo, hi, pat, step, mem->starts, mem->positions, mem->occ, first.data(), W));
+    API_TRY(atomic_build_views(seq, n, lo, hi, pat, step, mem->starts, mem->positions, mem->occ, first.data(), W));
     std::vector<gxy_table*> made;
     auto fail = [&](gxy_status s) {
         for (gxy_table* t : made) {
@@ -159,9 +160,10 @@ gxy_status build_tables(gxy_ctx* ctx, const gxy_dseq* seq, uint32_t n, const uin
         t->pat = pat;
         t->step = step;
         t->mem = mem;
-        t->starts = mem->starts + (size_t)v * (nw + 1);
-        t->positions = mem->positions + first[v];
-        t->occ = mem->occ + (size_t)v * occ_words;
+        t->starts = mem->starts + (size_t)v * nw;
+        t->positions = mem->positions;
+        t->pos_base = first[v];
+        t->occ = mem->occ + (size_t)v * nw / 32;
         t->npos = first[v + 1] - first[v];
         if (mwc > 0) {
             const gxy_status ps = prune_table(t, mwc, W);
@@ -302,7 +304,7 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         dseq_destroy(w->qstage);
         dseq_destroy(w->tstage);
         for (gxy_dseq* d : w->rc_tmp) dseq_destroy(d);
-        DevBuf* tb[] = {&w->tk0, &w->tv0, &w->tk1, &w->tv1};
+        DevBuf* tb[] = {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->tocc};
         for (DevBuf* b : tb) b->release();
         for (int i = 0; i < 5; i++)
             if (w->ev[i]) cudaEventDestroy(w->ev[i]);
@@ -508,9 +510,10 @@ gxy_status gxy_table_build_views(gxy_ctx* ctx, const gxy_dseq* target, uint32_t 
     Pattern pat;
     API_TRY(parse_pattern(pattern01, pat));
     API_TRY(set_device(ctx));
-    if (2 * (int)pat.weight + table_view_bits(n) <= 32)
+    if (pat.weight >= 3 && (uint64_t)n << (2 * pat.weight) < (1ull << 32))
         return build_tables(ctx, target, n, lo, hi, pat, step, max_word_count, out);
-    // Too many views for one key: one sort per view.
+    // Views of under 32 buckets, or more buckets than 32-bit starts can
+    // index: one build per view.
     for (uint32_t v = 0; v < n; v++) {
         const gxy_status s = build_tables(ctx, target, 1, lo + v, hi + v, pat, step, max_word_count, out + v);
         if (s != GXY_OK) {
@@ -545,8 +548,14 @@ gxy_status gxy_table_info(const gxy_table* t, uint64_t* num_words, uint64_t* n_p
 gxy_status gxy_table_download(const gxy_table* t, uint32_t* starts, uint32_t* positions) {
     if (!t) return GXY_EINVAL;
     API_TRY(set_device(t->ctx));
-    if (starts) API_CK(cudaMemcpy(starts, t->starts, (t->num_words + 1) * 4, cudaMemcpyDeviceToHost));
-    if (positions && t->npos) API_CK(cudaMemcpy(positions, t->positions, t->npos * 4, cudaMemcpyDeviceToHost));
+    if (starts) {
+        API_CK(cudaMemcpy(starts, t->starts, (t->num_words + 1) * 4, cudaMemcpyDeviceToHost));
+        // The table's own indices: from its first position on.
+        if (t->pos_base)
+            for (uint64_t w = 0; w <= t->num_words; w++) starts[w] -= t->pos_base;
+    }
+    if (positions && t->npos)
+        API_CK(cudaMemcpy(positions, t->positions + t->pos_base, t->npos * 4, cudaMemcpyDeviceToHost));
     return GXY_OK;
 }
 

@@ -138,7 +138,7 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     for (DevBuf* b : {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->prim_sums, &w->prim_hist, &w->counters, &w->d_units,
                       &w->d_tsegs, &w->d_qsegs, &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags,
                       &w->offsets, &w->ohsp, &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2,
-                      &w->hits, &w->surv, &w->redo, &w->rk0, &w->rk1, &w->rv0, &w->rv1})
+                      &w->hits, &w->surv, &w->redo, &w->rk0, &w->rk1, &w->rv0, &w->rv1, &w->tocc})
         b->st = w->st;
     for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;
@@ -253,9 +253,21 @@ static void build_variants(const Pattern& pat, uint32_t transitions, uint32_t* v
             for (uint32_t j = i + 1; j < w; j++) vx[nv++] = (2u << shifts[i]) ^ (2u << shifts[j]);
 }
 
-gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t hits, uint64_t candidates) {
+gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t est_hits, uint64_t candidates, uint32_t max_units) {
     const uint64_t max_hits = std::max<uint32_t>(4096, ctx->tuning.max_hits_per_pass);
-    hits = std::min(hits, max_hits);
+    const uint64_t hits = std::min(est_hits, max_hits);
+    // The filter's survivors, sized as run_units sizes them.
+    const uint64_t want_s = std::min<uint64_t>(max_hits, (1 << 20) + (uint64_t)(est_hits / kRawPerSurvivorSlot));
+    if (want_s > W->surv_cap) {
+        W->surv.release();
+        W->surv_cap = want_s;
+    }
+    GXY_CK(W->surv.ensure((size_t)W->surv_cap * sizeof(Hit)));
+    GXY_CK(W->redo.ensure((size_t)2 * kRedoCap * 4));
+    const size_t mu = std::max<uint32_t>(max_units, 1);
+    GXY_CK(W->d_units.ensure(mu * sizeof(UnitDev)));
+    GXY_CK(W->d_tsegs.ensure(mu * sizeof(SeqView)));
+    GXY_CK(W->d_qsegs.ensure(mu * sizeof(SeqView)));
     candidates = std::min<uint64_t>(candidates, kMaxPresizedCandidates);
     if (hits > W->hit_cap) {
         W->hits.release();

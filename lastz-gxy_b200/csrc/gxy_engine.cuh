@@ -35,6 +35,7 @@ struct DevBuf {
 struct Worker {
     cudaStream_t st = nullptr;
     DevBuf tk0, tv0, tk1, tv1;    // table-build temporaries
+    DevBuf tocc;                  // table build: occupancy bitmap over all views' buckets and its word ranks
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // start, screen end, end, filter end, enumerate end
     PrimScratch ps{};
     DevBuf prim_sums, prim_hist;
@@ -123,9 +124,9 @@ struct gxy_dseq {
 // every view of a multi-view build); freed when the last of them is freed.
 struct TableMem {
     int device = 0;
-    uint32_t* starts = nullptr;      // tables x (num_words + 1)
+    uint32_t* starts = nullptr;      // tables x num_words + 1 global bucket starts
     uint32_t* positions = nullptr;   // the tables' positions, one after the other
-    uint32_t* occ = nullptr;         // tables x occupancy words
+    uint32_t* occ = nullptr;         // occupancy bits of all tables' buckets
     ~TableMem();
 };
 
@@ -140,6 +141,9 @@ struct gxy_table {
     uint32_t* positions = nullptr;   // likewise
     bool own_arrays = false;         // starts and positions are this table's own (after a prune)
     uint32_t* occ = nullptr;   // bit (w & 31) of occ[w >> 5]: bucket w is non-empty (in mem)
+    // starts[w] index the shared positions array (positions points at its
+    // start); this table's positions begin at pos_base (0 after a prune).
+    uint32_t pos_base = 0;
     uint64_t num_words = 0;
     uint64_t npos = 0;
     // Positions within a bucket are in ascending order, the reference's order.
@@ -198,15 +202,14 @@ inline uint32_t n_windows(uint64_t len, uint32_t L, uint32_t step) {
 }
 
 // PosTable::build (src/pos_table.rs:35-83) for n views [lo[v], hi[v]) of one
-// sequence as one stable radix sort of their seedable windows by (view, word)
-// (csrc/gxy_table.cu): fills starts (n x (nw + 1) entries), positions (view
-// after view) and the occupancy bitmaps (n x ceil(nw / 32) words), then
-// first_host[0 .. n] = where each view's positions begin (a host sync).
-gxy_status sort_build_views(const gxy_dseq* seq, uint32_t n_views, const uint64_t* lo, const uint64_t* hi,
-                            const Pattern& pat, uint32_t step, uint32_t* starts, uint32_t* positions, uint32_t* occ,
-                            uint32_t* first_host, Worker* W);
-// Bits of the view index in a multi-view build's sort key.
-int table_view_bits(uint32_t n_views);
+// sequence at once (csrc/gxy_table.cu), view v's word w being bucket
+// g = v * 4^w + w: fills starts (n * 4^w + 1 global bucket starts), positions
+// (all views' positions, each bucket ascending) and the occupancy bitmap
+// over all buckets, then first_host[0 .. n] = starts[v * 4^w] (a host sync).
+// More than one view needs at least 32 buckets per view.
+gxy_status atomic_build_views(const gxy_dseq* seq, uint32_t n_views, const uint64_t* lo, const uint64_t* hi,
+                              const Pattern& pat, uint32_t step, uint32_t* starts, uint32_t* positions,
+                              uint32_t* occ, uint32_t* first_host, Worker* W);
 // Kernel attributes of the table build; once per device, before any capture.
 void table_init();
 
@@ -219,10 +222,12 @@ gxy_status parse_pattern(const char* s, Pattern& pat);
 gxy_status check_params(const gxy_search_params* p, uint64_t max_cols);
 
 // Runs units through screen -> sort -> walk -> compaction on worker W.
-// Grows a worker's raw-hit and candidate buffers (and its pinned result
-// staging) to at least the given sizes now, so that no later call pays for
-// the allocation.
-gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t hits, uint64_t candidates);
+// Grows every buffer run_units sizes from a raw-hit estimate -- raw hits,
+// survivors, candidates, the redo lists, the plan arrays for max_units units
+// and the pinned result staging -- to what an estimate of est_hits raw hits
+// and `candidates` candidates needs, so that no later call of that size pays
+// for an allocation.
+gxy_status reserve_worker(gxy_ctx* ctx, Worker* W, uint64_t est_hits, uint64_t candidates, uint32_t max_units);
 gxy_status run_units(gxy_ctx* ctx, Worker* W, const std::vector<UnitPlan>& units, std::vector<SeqView>& tsegs,
                      std::vector<SeqView>& qsegs, const Pattern& pat, const gxy_search_params& p, bool use_graph,
                      RunResult& out);

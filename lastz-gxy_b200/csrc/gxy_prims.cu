@@ -243,7 +243,7 @@ int radix_impl(K* ka, uint32_t* va, K* kb, uint32_t* vb, const uint32_t* n_dev, 
         count_launch();
         k_radix_scatter<K><<<grid, kSortThreads, smem, st>>>(ArraySrc<K>{kin, vin}, kout, vout, n_dev, n_host,
                                                              n_cap, passes[p].shift, passes[p].bits, ps.hist,
-                                                             ps.block_sums, nullptr);
+                                                             ps.block_sums);
         K* tk = kin; kin = kout; kout = tk;
         uint32_t* tv = vin; vin = vout; vout = tv;
     }

@@ -1,7 +1,7 @@
 // gxy_radix.cuh -- the device side of the scan and the stable LSD radix sort
 // (gxy_prims.cuh has the host entry points).  The radix kernels read their
-// items through a source: ArraySrc reads key and value arrays; a source may
-// also compute its items (the table build's seed words) and leave some out.
+// items through a source type (ArraySrc: key and value arrays); a source
+// whose load returns false leaves that item out of the output.
 #pragma once
 
 #include <cstdint>
@@ -131,13 +131,13 @@ struct SortSmem {
 };
 
 // Items the source leaves out are dropped (the output holds the kept items
-// only, in stable order); n_out (optional) receives the number kept.
+// only, in stable order).
 template <typename K, typename Src>
 __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(Src src, K* __restrict__ kout,
                                                                  uint32_t* __restrict__ vout,
                                                                  const uint32_t* n_dev, uint64_t n_host, uint64_t n_cap,
                                                                  int shift, int bits, const uint32_t* hist,
-                                                                 const uint32_t* totals, uint32_t* n_out) {
+                                                                 const uint32_t* totals) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
     const uint64_t n = read_n(n_dev, n_host, n_cap);
@@ -155,7 +155,6 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(Src src, K* __re
         const uint32_t t = d < radix ? totals[d] : 0u;
         const uint32_t g = block_excl_scan<kSortThreads>(t, S.warp_tmp, &S.total);
         S.off[d] = d < radix ? g + hist[(uint64_t)d * gridDim.x + blockIdx.x] : 0u;
-        if (n_out && blockIdx.x == 0 && d == 0) *n_out = S.total;
     }
     for (uint64_t tb = beg; tb < end; tb += kSortTile) {
         for (int i = threadIdx.x; i < kSortWarps * kRadixMax; i += kSortThreads) (&S.wcnt[0][0])[i] = 0;

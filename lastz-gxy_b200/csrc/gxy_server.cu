@@ -202,7 +202,7 @@ void dispatcher(gxy_server* s) {
         for (const gxy_table* t : s->tables)
             if (t->num_words) avg = std::max(avg, (double)t->npos / (double)t->num_words);
         const double est = (double)(1 << 20) + 1.5 * (double)s->opts.warm_bases * n_var * avg * strands;
-        reserve_worker(s->ctx, W, (uint64_t)est, (uint64_t)(est / kHitsPerCandidate));
+        reserve_worker(s->ctx, W, (uint64_t)est, (uint64_t)(est / kHitsPerCandidate), s->opts.max_batch_units);
     }
     {
         std::lock_guard<std::mutex> g(s->mu);
@@ -392,6 +392,9 @@ gxy_status gxy_server_create(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* c
     if (!o.max_streams) o.max_streams = 2;
     if (!o.max_batch_units) o.max_batch_units = 1024;
     if (!o.max_batch_bases) o.max_batch_bases = 16ull << 20;
+    // Batches no larger than the warmed buffers: one that outgrew them would
+    // reallocate gigabytes while requests wait.
+    if (o.warm_bases) o.max_batch_bases = std::min<uint64_t>(o.max_batch_bases, o.warm_bases * (o.both_strands ? 2 : 1));
     if (!o.big_bases) o.big_bases = 1ull << 20;
     if (!o.max_big_inflight) o.max_big_inflight = 1;
     s->opts = o;
