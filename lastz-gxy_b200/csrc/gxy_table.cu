@@ -13,11 +13,11 @@
 //     leaves a copy in the counts array: the cursors;
 //  3. k_fill_buckets drops every window's position into its bucket through
 //     an atomic cursor -- in an arbitrary order inside the bucket;
-//  4. k_sort_small_buckets writes the occupancy bitmap and puts every bucket
-//     of up to 16 positions in ascending order in registers,
-//     k_sort_block_buckets those up to kBlockBucket in shared memory, and the
-//     radix sort the few larger ones, so every bucket holds the reference's
-//     order when the build returns.
+//  4. k_sort_small_buckets writes the occupancy bitmap and orders every
+//     bucket of 2 or 3 positions on the spot, k_sort_warp_buckets those up to
+//     32 a warp each, k_sort_block_buckets those up to kBlockBucket in shared
+//     memory, and the radix sort the few larger ones, so every bucket holds
+//     the reference's order when the build returns.
 //
 // View v's table is a window onto the shared arrays: its starts are the
 // global starts g = v * 4^w .. v * 4^w + 4^w (global indices into the shared
@@ -75,64 +75,116 @@ __global__ void k_fill_buckets(SeqView view, Pattern pat, uint32_t step, uint32_
     }
 }
 
-// Ascending bitonic network over 16 registers (unused slots hold ~0u).
-__device__ __forceinline__ void sort16(uint32_t (&v)[16]) {
+__device__ __forceinline__ void cswap(uint32_t& x, uint32_t& y) {
+    const uint32_t lo = min(x, y), hi = max(x, y);
+    x = lo;
+    y = hi;
+}
+
+// Files bucket g (first index b, n positions) for the sort that fits it.
+__device__ __forceinline__ void order_bucket(uint32_t* __restrict__ pos, uint32_t b, uint32_t n, uint2* mid,
+                                             uint32_t* n_mid, uint2* big, uint32_t* n_big, uint2* huge,
+                                             uint32_t* n_huge) {
+    if (n <= 1) return;
+    if (n > 3) {
+        if (n > kBlockBucket) huge[atomicAdd(n_huge, 1u)] = make_uint2(b, n);
+        else if (n > 32) big[atomicAdd(n_big, 1u)] = make_uint2(b, n);
+        else mid[atomicAdd(n_mid, 1u)] = make_uint2(b, n);
+        return;
+    }
+    uint32_t x = pos[b], y = pos[b + 1];
+    if (n == 2) {
+        if (x > y) {
+            pos[b] = y;
+            pos[b + 1] = x;
+        }
+        return;
+    }
+    uint32_t z = pos[b + 2];
+    cswap(x, y);
+    cswap(y, z);
+    cswap(x, y);
+    pos[b] = x;
+    pos[b + 1] = y;
+    pos[b + 2] = z;
+}
+
+// One pass over the bucket starts, four buckets a thread (one 16-byte load;
+// the fifth start comes from the next lane): each group of eight lanes
+// assembles one 32-bucket occupancy word; buckets of 2 or 3 positions --
+// nearly all the buckets that need it at chromosome scale -- are put in
+// order on the spot, larger ones listed for the warp sort (mid, <= 32), the
+// block sort (big, <= kBlockBucket) or the radix sort (huge), as (first
+// index, size) pairs.  The lists hold every such bucket: at most n / 4 + 1,
+// n / 33 + 1 and n / (kBlockBucket + 1) + 1 of them for n positions.
+__global__ void k_sort_small_buckets(const uint32_t* __restrict__ starts, uint64_t nb, uint32_t* __restrict__ pos,
+                                     uint32_t* __restrict__ occ, uint2* __restrict__ mid, uint32_t* n_mid,
+                                     uint2* __restrict__ big, uint32_t* n_big, uint2* __restrict__ huge,
+                                     uint32_t* n_huge) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nb128 = (nb + 127) & ~(uint64_t)127;   // whole warps: every lane reaches the shuffles
+    for (uint64_t g0 = 4 * (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x); g0 < nb128;
+         g0 += 4 * (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t s[4] = {0, 0, 0, 0};
+        if (g0 + 3 < nb) {
+            const uint4 v = *reinterpret_cast<const uint4*>(starts + g0);
+            s[0] = v.x;
+            s[1] = v.y;
+            s[2] = v.z;
+            s[3] = v.w;
+        } else {
+            // starts has nb + 1 entries: the next lane's first may be starts[nb].
 #pragma unroll
-    for (int k = 2; k <= 16; k <<= 1) {
+            for (int k = 0; k < 4; k++)
+                if (g0 + k <= nb) s[k] = starts[g0 + k];
+        }
+        uint32_t next = __shfl_down_sync(kFull, s[0], 1);
+        if (lane == 31 && g0 + 4 <= nb) next = starts[g0 + 4];
+        uint32_t n[4], nib = 0;
 #pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int k = 0; k < 4; k++) {
+            const uint32_t e = k < 3 ? s[k + 1] : next;
+            n[k] = g0 + k < nb ? e - s[k] : 0u;
+            nib |= (n[k] != 0 ? 1u : 0u) << k;
+        }
+        // Eight lanes cover 32 buckets: OR their nibbles into one word.
+        uint32_t word = nib << (4 * (lane & 7));
+        word |= __shfl_xor_sync(kFull, word, 1);
+        word |= __shfl_xor_sync(kFull, word, 2);
+        word |= __shfl_xor_sync(kFull, word, 4);
+        if ((lane & 7) == 0 && g0 < nb) occ[g0 >> 5] = word;
 #pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const uint32_t x = v[i], y = v[l];
-                    const bool up = (i & k) == 0;
-                    const bool sw = up ? x > y : x < y;
-                    v[i] = sw ? y : x;
-                    v[l] = sw ? x : y;
-                }
+        for (int k = 0; k < 4; k++) order_bucket(pos, s[k], n[k], mid, n_mid, big, n_big, huge, n_huge);
+    }
+}
+
+// Listed buckets of 4..32 positions, a warp each: a bitonic sort across the
+// lanes by shuffles.
+__global__ void k_sort_warp_buckets(const uint2* __restrict__ mid, const uint32_t* n_mid, uint32_t* __restrict__ pos) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nl = *n_mid;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); e < nl; e += warps) {
+        const uint32_t b = mid[e].x, n = mid[e].y;
+        uint32_t x = lane < n ? pos[b + lane] : 0xffffffffu;
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const uint32_t y = __shfl_xor_sync(kFull, x, j);
+                const bool up = (lane & k) == 0;
+                const bool low = (lane & j) == 0;
+                // the lower lane of a pair keeps the smaller in an ascending run
+                x = (low == up) ? min(x, y) : max(x, y);
             }
         }
+        if (lane < n) pos[b + lane] = x;
     }
 }
 
-// One pass over the bucket starts: each warp writes the occupancy word of
-// its 32 buckets; buckets of 2..16 positions are sorted in registers, larger
-// ones listed for the block sort (big) or, past kBlockBucket, for the radix
-// sort (huge), as (first index, size) pairs.  The lists hold every such
-// bucket: at most n / 17 + 1 and n / (kBlockBucket + 1) + 1 of them for n
-// positions.
-__global__ void k_sort_small_buckets(const uint32_t* __restrict__ starts, uint64_t nb, uint32_t* __restrict__ pos,
-                                     uint32_t* __restrict__ occ, uint2* __restrict__ big, uint32_t* n_big,
-                                     uint2* __restrict__ huge, uint32_t* n_huge) {
-    const uint64_t nb32 = (nb + 31) & ~(uint64_t)31;   // whole warps: every lane reaches the ballot
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < nb32; g += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t b = 0, n = 0;
-        if (g < nb) {
-            b = starts[g];
-            n = starts[g + 1] - b;
-        }
-        const uint32_t m = __ballot_sync(kFull, n != 0);
-        if ((threadIdx.x & 31) == 0) occ[g >> 5] = m;
-        if (n <= 1) continue;
-        if (n > 16) {
-            if (n > kBlockBucket) huge[atomicAdd(n_huge, 1u)] = make_uint2(b, n);
-            else big[atomicAdd(n_big, 1u)] = make_uint2(b, n);
-            continue;
-        }
-        uint32_t v[16];
-#pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = (uint32_t)i < n ? pos[b + i] : 0xffffffffu;
-        sort16(v);
-#pragma unroll
-        for (int i = 0; i < 16; i++)
-            if ((uint32_t)i < n) pos[b + i] = v[i];
-    }
-}
-
-// Bitonic sort of listed buckets (17 .. kBlockBucket positions) in shared
+// Bitonic sort of listed buckets (33 .. kBlockBucket positions) in shared
 // memory, a block each.
-__global__ __launch_bounds__(1024) void k_sort_block_buckets(const uint2* __restrict__ big, const uint32_t* n_big,
+__global__ __launch_bounds__(256) void k_sort_block_buckets(const uint2* __restrict__ big, const uint32_t* n_big,
                                                              uint32_t* __restrict__ pos) {
     __shared__ uint32_t s[kBlockBucket];
     const uint32_t nl = *n_big;
@@ -192,17 +244,19 @@ gxy_status atomic_build_views(const gxy_dseq* seq, uint32_t n_views, const uint6
         set_error("more than 2^32 windows in one table build");
         return GXY_EUNSUPPORTED;
     }
-    const uint64_t n_big_cap = total / 17 + 1, n_huge_cap = total / (kBlockBucket + 1) + 1;
+    const uint64_t n_mid_cap = total / 4 + 1, n_big_cap = total / 33 + 1,
+                   n_huge_cap = total / (kBlockBucket + 1) + 1;
     GXY_CK(W->tk0.ensure((G + 1) * 4));
-    GXY_CK(W->tv0.ensure((n_big_cap + n_huge_cap) * 8));
+    GXY_CK(W->tv0.ensure((n_mid_cap + n_big_cap + n_huge_cap) * 8));
     GXY_CK(W->tv1.ensure(64 + ((size_t)n_views + 1) * 4));
     uint32_t* counts = W->tk0.as<uint32_t>();
-    uint2* big = W->tv0.as<uint2>();
+    uint2* mid = W->tv0.as<uint2>();
+    uint2* big = mid + n_mid_cap;
     uint2* huge = big + n_big_cap;
-    uint32_t* ctr = W->tv1.as<uint32_t>();   // [0] big buckets, [1] huge buckets
+    uint32_t* ctr = W->tv1.as<uint32_t>();   // [0] big buckets, [1] huge buckets, [2] mid buckets
     uint32_t* first = ctr + 16;
     GXY_CK(cudaMemsetAsync(counts, 0, (G + 1) * 4, st));
-    GXY_CK(cudaMemsetAsync(ctr, 0, 8, st));
+    GXY_CK(cudaMemsetAsync(ctr, 0, 12, st));
     std::vector<SeqView> views(n_views);
     for (uint32_t v = 0; v < n_views; v++) views[v] = view_of(seq, lo[v], hi[v]);
     const int cblocks = 148 * 16;
@@ -220,9 +274,10 @@ gxy_status atomic_build_views(const gxy_dseq* seq, uint32_t n_views, const uint6
         k_fill_buckets<<<(int)std::min<uint64_t>((nwin[v] + 255) / 256, cblocks), 256, 0, st>>>(
             views[v], pat, step, nwin[v], counts + (uint64_t)v * nw, positions);
     }
-    count_launch(3);
-    k_sort_small_buckets<<<148 * 16, 256, 0, st>>>(starts, G, positions, occ, big, ctr, huge, ctr + 1);
-    k_sort_block_buckets<<<148 * 2, 1024, 0, st>>>(big, ctr, positions);
+    count_launch(4);
+    k_sort_small_buckets<<<148 * 16, 256, 0, st>>>(starts, G, positions, occ, mid, ctr + 2, big, ctr, huge, ctr + 1);
+    k_sort_warp_buckets<<<148 * 4, 256, 0, st>>>(mid, ctr + 2, positions);
+    k_sort_block_buckets<<<148 * 2, 256, 0, st>>>(big, ctr, positions);
     k_view_firsts<<<1, 256, 0, st>>>(starts, nw, n_views, first);
     GXY_CK(cudaGetLastError());
     std::vector<uint32_t> h(16 + (size_t)n_views + 1);

@@ -122,6 +122,35 @@ def test_table_bucket_orders(gxy, ctx, pattern, step):
     assert as_tuples(got2) == as_tuples(want2) and len(want2) > 0
 
 
+def test_table_bucket_size_classes(gxy, ctx):
+    # Random 40 bp units each repeated k times (k = 2 .. 5000) between random
+    # spacers: buckets of every size class the build orders differently
+    # (2-3 in place, 4-32 a warp, 33-4096 a block, larger the radix sort),
+    # one table and as views, against the oracle.
+    rng = np.random.default_rng(12)
+    parts = []
+    for k in (2, 3, 4, 5, 9, 16, 31, 32, 33, 40, 100, 1000, 4096, 4097, 5000):
+        unit = rand_ascii(rng, 40, b"ACGT", None)
+        parts.append(rand_ascii(rng, 300, b"ACGT", None) + unit * k)
+    s = b"".join(parts)
+    T = gxy.PackedSeq.from_ascii(s)
+    tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    starts, pos = tab.arrays()
+    ot = O.Table(O.pack_ascii(s), P12, 1)
+    assert np.array_equal(starts, ot.starts()) and np.array_equal(pos, ot.positions())
+    assert int(np.diff(starts.astype(np.int64)).max()) > 4096
+    tab.free()
+    dT = T.to_device(ctx)
+    half = len(s) // 2
+    views = gxy.PosTable.build_views(dT, [(0, half), (half - 1000, len(s))], P12, 1, ctx=ctx)
+    for (lo, hi), t in zip([(0, half), (half - 1000, len(s))], views):
+        st2, p2 = t.arrays()
+        o2 = O.Table(O.pack_ascii(s[lo:hi]), P12, 1)
+        assert np.array_equal(st2, o2.starts()) and np.array_equal(p2, o2.positions()), (lo, hi)
+        t.free()
+    dT.free()
+
+
 def test_table_full_size_bit_exact(gxy, ctx):
     # A 10 Mbp chromosome-style target (repeat families, soft-masked runs,
     # N blocks), 12of19 and step 1, and a 2 Mbp target at step 2: starts and
