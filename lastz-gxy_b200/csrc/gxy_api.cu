@@ -107,6 +107,7 @@ TableMem::~TableMem() {
     dev_free(starts);
     dev_free(positions);
     dev_free(occ);
+    dev_free(ilv);
 }
 
 namespace {
@@ -134,6 +135,25 @@ gxy_status build_tables(gxy_ctx* ctx, const gxy_dseq* seq, uint32_t n, const uin
     if (e != cudaSuccess) {
         set_error(std::string("table allocation: ") + cudaGetErrorString(e));
         return GXY_ENOMEM;
+    }
+    // The interleaved copy of the sequence words the views cover (with two
+    // words of margin each side: the filter's windows reach 32 positions
+    // left of a view and one word past its end).
+    {
+        uint64_t lo_min = UINT64_MAX, hi_max = 0;
+        for (uint32_t v = 0; v < n; v++) {
+            lo_min = std::min(lo_min, lo[v]);
+            hi_max = std::max(hi_max, hi[v]);
+        }
+        const uint64_t w0 = (kPad + lo_min) / 32, w1 = (kPad + hi_max) / 32;
+        mem->ilv_first = w0 >= 2 ? w0 - 2 : 0;
+        const uint64_t last = std::min<uint64_t>(seq->nwords - 1, w1 + 2);
+        e = dev_alloc((void**)&mem->ilv, (size_t)(last + 1 - mem->ilv_first) * 16, st);
+        if (e != cudaSuccess) {
+            set_error(std::string("table allocation: ") + cudaGetErrorString(e));
+            return GXY_ENOMEM;
+        }
+        launch_interleave(seq->codes, seq->valid, seq->mask, mem->ilv_first, last + 1 - mem->ilv_first, mem->ilv, st);
     }
     std::vector<uint32_t> first((size_t)n + 1);
     API_TRY(atomic_build_views(seq, n, lo, hi, pat, step, mem->starts, mem->positions, mem->occ, first.data(), W));
@@ -582,7 +602,7 @@ gxy_status gxy_search(gxy_ctx* ctx, const gxy_table* table, const gxy_packed_seq
     WorkerLease L(ctx);
     if (!L.w) return L.err;
     Worker* W = L.w;
-    SeqView T = view_of(table->seq, table->lo, table->hi);
+    SeqView T = table_view(table);
     if (!same_host_seq(table, target)) {
         if (target->len != table->hi - table->lo) {
             set_error("target length differs from the sequence the table was built on");
@@ -612,7 +632,7 @@ gxy_status gxy_search_dseq(gxy_ctx* ctx, const gxy_table* table, const gxy_dseq*
     API_TRY(set_device(ctx));
     WorkerLease L(ctx);
     if (!L.w) return L.err;
-    const SeqView T = view_of(table->seq, table->lo, table->hi);
+    const SeqView T = table_view(table);
     const SeqView Q = view_of(query, 0, query->len);
     return search_impl(ctx, L.w, table, T, Q, params, out, stats);
 }
@@ -661,7 +681,7 @@ static gxy_status batch_run(gxy_ctx* ctx, uint32_t n_tables, const gxy_table* co
         const gxy_table* t = tables[u.table];
         if (tseg_of[u.table] < 0) {
             tseg_of[u.table] = (int)tsegs.size();
-            tsegs.push_back(view_of(t->seq, t->lo, t->hi));
+            tsegs.push_back(table_view(t));
         }
         const size_t qi = 2 * (size_t)u.query + u.strand;
         if (qseg_of[qi] < 0) {

@@ -33,7 +33,30 @@ struct SeqView {
     uint64_t base;
     uint32_t len;
     uint32_t key_base;
+    // Optional interleaved copy (a table's target): the 32-position word i's
+    // codes, valid and mask bits as one 16-byte record ilv[i - ilv_first], so
+    // that a random 32-position window takes two loads instead of four.
+    const uint4* ilv = nullptr;
+    uint64_t ilv_first = 0;
 };
+
+// Codes and valid bits of the 32 positions from global position gp, from the
+// interleaved copy when the view has one.
+__device__ __forceinline__ void load_window32(const SeqView& S, uint64_t gp, uint64_t& codes, uint32_t& valid) {
+    const uint64_t i = gp >> 5;
+    const uint32_t s = (uint32_t)(gp & 31);
+    if (S.ilv) {
+        const uint4 a = __ldg(S.ilv + (i - S.ilv_first));
+        const uint4 b = __ldg(S.ilv + (i + 1 - S.ilv_first));
+        const uint64_t lo = ((uint64_t)a.y << 32) | a.x, hi = ((uint64_t)b.y << 32) | b.x;
+        codes = s ? ((lo >> (2 * s)) | (hi << (64 - 2 * s))) : lo;
+        valid = __funnelshift_r(a.z, b.z, s);
+    } else {
+        const uint64_t lo = __ldg(S.codes + i), hi = __ldg(S.codes + i + 1);
+        codes = s ? ((lo >> (2 * s)) | (hi << (64 - 2 * s))) : lo;
+        valid = __funnelshift_r(__ldg(S.valid + i), __ldg(S.valid + i + 1), s);
+    }
+}
 
 // One reference search() call: a (target segment, query segment) pair with
 // the target's position table (src/seed_search.rs:45-51).

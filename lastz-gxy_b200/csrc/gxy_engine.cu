@@ -119,6 +119,15 @@ SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi) {
     return v;
 }
 
+SeqView table_view(const gxy_table* t) {
+    SeqView v = view_of(t->seq, t->lo, t->hi);
+    if (t->mem && t->mem->ilv) {
+        v.ilv = t->mem->ilv;
+        v.ilv_first = t->mem->ilv_first;
+    }
+    return v;
+}
+
 Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
     {
         std::lock_guard<std::mutex> g(ctx->mu);

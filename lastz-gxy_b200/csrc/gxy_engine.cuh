@@ -127,6 +127,8 @@ struct TableMem {
     uint32_t* starts = nullptr;      // tables x num_words + 1 global bucket starts
     uint32_t* positions = nullptr;   // the tables' positions, one after the other
     uint32_t* occ = nullptr;         // occupancy bits of all tables' buckets
+    uint4* ilv = nullptr;            // interleaved copy of the sequence words the views cover
+    uint64_t ilv_first = 0;          // the first of those words
     ~TableMem();
 };
 
@@ -183,6 +185,8 @@ void dseq_destroy(gxy_dseq* s);
 void dseq_destroy_async(gxy_dseq* s, cudaStream_t st);
 gxy_status dseq_fill_host(gxy_dseq* d, const gxy_packed_seq* h, cudaStream_t st);
 SeqView view_of(const gxy_dseq* s, uint64_t lo, uint64_t hi);
+// A table's target view, with the table's interleaved copy of it.
+SeqView table_view(const gxy_table* t);
 
 // Returns from the calling function with a status when a CUDA call fails.
 #define GXY_CK(call)                                                                         \
@@ -210,6 +214,10 @@ inline uint32_t n_windows(uint64_t len, uint32_t L, uint32_t step) {
 gxy_status atomic_build_views(const gxy_dseq* seq, uint32_t n_views, const uint64_t* lo, const uint64_t* hi,
                               const Pattern& pat, uint32_t step, uint32_t* starts, uint32_t* positions,
                               uint32_t* occ, uint32_t* first_host, Worker* W);
+// ilv[j] = the 16-byte record (codes, valid, mask) of sequence word first + j,
+// for j < n (SeqView::ilv).
+void launch_interleave(const uint64_t* codes, const uint32_t* valid, const uint32_t* mask, uint64_t first, uint64_t n,
+                       uint4* ilv, cudaStream_t st);
 // Kernel attributes of the table build; once per device, before any capture.
 void table_init();
 

@@ -22,9 +22,13 @@
 //    permute, one shared-memory load and three integer operations per four
 //    columns, against five operations per column in the exact screen;
 //  - a hit survives when the bounded seed footprint + both sides' bests reach
-//    hspthresh, or when a side is still running after f_cap columns.
+//    hspthresh, or when a side is still running after f_cap columns;
+//  - target windows come from the table's interleaved copy of its target
+//    (two 16-byte loads per 32-position window): the lanes' target positions
+//    are random, and these gathers are what bounds the kernel, while a warp's
+//    query positions come from one tile of windows.
 //
-// Survivors (about 3 % of the raw hits on chromosome-scale inputs) go to a
+// Survivors (about 1 % of the raw hits on chromosome-scale inputs) go to a
 // second hit array, where the exact screen (k_screen) takes them.  The
 // dropped hits are exactly hits whose exact score is below hspthresh, so the
 // pipeline's output does not change.
@@ -97,8 +101,10 @@ __device__ __forceinline__ int32_t seed_bound(const SeqView& T, const SeqView& Q
                                               uint32_t L, uint64_t f_inv, int32_t ub0, uint32_t lane8,
                                               const unsigned char* lut) {
     const uint64_t tg = T.base + t, qg = Q.base + q;
-    const uint64_t x = fold_cols(load_codes32(T.codes, tg) ^ load_codes32(Q.codes, qg),
-                                 load_bits32(T.valid, tg) & load_bits32(Q.valid, qg), f_inv);
+    uint64_t tc;
+    uint32_t tv;
+    load_window32(T, tg, tc, tv);
+    const uint64_t x = fold_cols(tc ^ load_codes32(Q.codes, qg), tv & load_bits32(Q.valid, qg), f_inv);
     int32_t sd = 0;
 #pragma unroll
     for (int g = 0; g < 8; g++) {
@@ -200,13 +206,19 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
         uint32_t vr = kFull, vl = kFull;
         if (nr) {
             const uint64_t tg = T.base + ht + L + rext, qg = Q.base + hq + L + rext;
-            xr = load_codes32(T.codes, tg) ^ load_codes32(Q.codes, qg);
-            vr = load_bits32(T.valid, tg) & load_bits32(Q.valid, qg);
+            uint64_t tc;
+            uint32_t tv;
+            load_window32(T, tg, tc, tv);
+            xr = tc ^ load_codes32(Q.codes, qg);
+            vr = tv & load_bits32(Q.valid, qg);
         }
         if (nl) {
             const uint64_t tg = T.base + ht - lext - 32, qg = Q.base + hq - lext - 32;
-            xl = rev_pairs64(load_codes32(T.codes, tg) ^ load_codes32(Q.codes, qg));
-            vl = __brev(load_bits32(T.valid, tg) & load_bits32(Q.valid, qg));
+            uint64_t tc;
+            uint32_t tv;
+            load_window32(T, tg, tc, tv);
+            xl = rev_pairs64(tc ^ load_codes32(Q.codes, qg));
+            vl = __brev(tv & load_bits32(Q.valid, qg));
         }
         const bool slow = (nr && (nr < 32 || vr != kFull)) || (nl && (nl < 32 || vl != kFull));
         if (__any_sync(kFull, slow)) {

@@ -113,7 +113,7 @@ gxy_status run_batch(gxy_server* s, Worker* W, std::vector<Request*>& batch) {
         const gxy_table* t = s->tables[q->table];
         if (tseg_of[q->table] < 0) {
             tseg_of[q->table] = (int)tsegs.size();
-            tsegs.push_back(view_of(t->seq, t->lo, t->hi));
+            tsegs.push_back(table_view(t));
         }
         gxy_dseq* d = nullptr;
         gxy_status e = dseq_alloc(s->ctx, q->len, &d, stream);
