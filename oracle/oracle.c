@@ -751,3 +751,323 @@ uint64_t orc_best_chain(const orc_hsp* hsps, uint64_t n, orc_hsp* out) {
     free(parent);
     return len;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Gapped extension (src/gapped_extend.rs:78-460): the banded 3-state       */
+/* affine x-drop DP of extend_one_side (:178-412) run to the right of the   */
+/* anchor and, on reversed inputs, to its left; the traceback's edit script */
+/* (src/edit_script.rs:47-104: run-length runs, push merges equal ops).     */
+/* Rows are allocated as the DP reaches them instead of (n+1) rows up front */
+/* (:236-243); every row starts as NEG_INF / State::M like the reference's  */
+/* preallocated storage, so the values read are the same.                   */
+/* ------------------------------------------------------------------------ */
+#define G_NEG_INF (INT32_MIN / 4)   /* src/gapped_extend.rs:44 */
+enum { G_M = 0, G_X = 1, G_Y = 2 };  /* State (:46-51) */
+
+typedef struct {
+    uint32_t* runs;   /* count << 2 | op */
+    uint32_t n, cap;
+} g_script;
+
+/* EditScript::push (src/edit_script.rs:63-74). */
+static int g_push(g_script* s, uint32_t op, uint32_t cnt) {
+    if (cnt == 0) return 0;
+    if (s->n && (s->runs[s->n - 1] & 3u) == op) {
+        s->runs[s->n - 1] += cnt << 2;
+        return 0;
+    }
+    if (s->n == s->cap) {
+        uint32_t nc = s->cap ? s->cap * 2 : 16;
+        uint32_t* r = (uint32_t*)realloc(s->runs, (size_t)nc * 4);
+        if (!r) return -1;
+        s->runs = r;
+        s->cap = nc;
+    }
+    s->runs[s->n++] = (cnt << 2) | op;
+    return 0;
+}
+
+/* pair_score (:160-166) on (code, valid) of the sliced inputs. */
+static inline int32_t g_pair(const orc_seq* t, int64_t ti, const orc_seq* q, int64_t qi, const orc_params* p) {
+    if (s_valid(t, (uint64_t)ti) && s_valid(q, (uint64_t)qi))
+        return p->sub[s_code(t, (uint64_t)ti) * 4 + s_code(q, (uint64_t)qi)];
+    return p->ambig;
+}
+
+typedef struct {
+    int32_t score;
+    uint32_t t_span, q_span;
+    g_script script;   /* root-to-tip, as OneSide.script */
+} g_side;
+
+/* extend_one_side (:178-412).  The sliced input of the reference is target
+ * element i-1 = T[t0 + dir*i] and query element j-1 = Q[q0 + dir*j]
+ * (dir +1: the right slice from anchor+1; dir -1: the reversed left slice). */
+static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q, int64_t q0, int64_t m, int dir,
+                      const orc_params* p, const orc_gapped_params* gp, g_side* out) {
+    memset(out, 0, sizeof(*out));
+    if (n == 0 || m == 0) return 0;
+    const int32_t goe = gp->gap_open + gp->gap_extend, ge = gp->gap_extend, ydrop = gp->y_drop;
+    int64_t radius;
+    if (ge > 0) {
+        int32_t r = sat_sub(ydrop, goe) / ge;
+        radius = (r > 0 ? r : 0) + 2;
+    } else {
+        radius = m + 1;
+    }
+    int64_t bw = 4 * radius + 4;
+    if (bw > m + 1) bw = m + 1;
+    /* Rows grow on demand; row_lo, mm/xx/yy and the from-states per row. */
+    int64_t rows_cap = 0;
+    int64_t* row_lo = NULL;
+    int32_t *mm = NULL, *xx = NULL, *yy = NULL;
+    uint8_t *mf = NULL, *xf = NULL, *yf = NULL;
+    int rc = 0;
+#define G_GROW(i)                                                                                      \
+    if ((i) >= rows_cap) {                                                                             \
+        int64_t nc = rows_cap ? rows_cap * 2 : 64;                                                     \
+        if (nc > n + 1) nc = n + 1;                                                                    \
+        int64_t* a = (int64_t*)realloc(row_lo, (size_t)nc * 8);                                        \
+        if (a) row_lo = a;                                                                             \
+        int32_t* b1 = (int32_t*)realloc(mm, (size_t)(nc * bw) * 4);                                    \
+        if (b1) mm = b1;                                                                               \
+        int32_t* b2 = (int32_t*)realloc(xx, (size_t)(nc * bw) * 4);                                    \
+        if (b2) xx = b2;                                                                               \
+        int32_t* b3 = (int32_t*)realloc(yy, (size_t)(nc * bw) * 4);                                    \
+        if (b3) yy = b3;                                                                               \
+        uint8_t* c1 = (uint8_t*)realloc(mf, (size_t)(nc * bw));                                        \
+        if (c1) mf = c1;                                                                               \
+        uint8_t* c2 = (uint8_t*)realloc(xf, (size_t)(nc * bw));                                        \
+        if (c2) xf = c2;                                                                               \
+        uint8_t* c3 = (uint8_t*)realloc(yf, (size_t)(nc * bw));                                        \
+        if (c3) yf = c3;                                                                               \
+        if (!a || !b1 || !b2 || !b3 || !c1 || !c2 || !c3) {                                            \
+            rc = -1;                                                                                   \
+            goto done;                                                                                 \
+        }                                                                                              \
+        for (int64_t k = rows_cap * bw; k < nc * bw; k++) {                                           \
+            mm[k] = xx[k] = yy[k] = G_NEG_INF;                                                         \
+            mf[k] = xf[k] = yf[k] = G_M;                                                               \
+        }                                                                                              \
+        rows_cap = nc;                                                                                 \
+    }
+    G_GROW(0);
+    mm[0] = 0;
+    int32_t best_score = 0;
+    int64_t bi = 0, bj = 0;
+    int best_state = G_M;
+    int64_t lo = 0, hi = 0;
+    row_lo[0] = 0;
+    for (int64_t i = 0; i <= n; i++) {
+        G_GROW(i);
+        const int64_t j_lo = lo > radius ? lo - radius : 0;
+        int64_t j_hi = hi + radius;
+        if (j_hi > m) j_hi = m;
+        if (j_hi > j_lo + bw - 1) j_hi = j_lo + bw - 1;
+        row_lo[i] = j_lo;
+        const int64_t lo_this = j_lo;
+        const int64_t lo_prev = i >= 1 ? row_lo[i - 1] : 0;
+        const int64_t hi_prev_excl = lo_prev + bw;
+        const int64_t base_this = i * bw, base_prev = i >= 1 ? (i - 1) * bw : 0;
+        for (int64_t j = j_lo; j <= j_hi; j++) {
+            if (i == 0 && j == 0) continue;
+            int32_t best = G_NEG_INF;
+            const int64_t here = base_this + (j - lo_this);
+            if (i >= 1) {   /* X: gap in query (:282-302) */
+                int32_t pm = G_NEG_INF, px = G_NEG_INF;
+                if (j >= lo_prev && j < hi_prev_excl) {
+                    const int64_t off = base_prev + (j - lo_prev);
+                    pm = mm[off];
+                    px = xx[off];
+                }
+                const int32_t fm = pm - goe, fx = px - ge;
+                const int32_t v = fm >= fx ? fm : fx;
+                xx[here] = v;
+                xf[here] = fm >= fx ? G_M : G_X;
+                if (v > best) best = v;
+            }
+            if (j >= 1) {   /* Y: gap in target (:305-327) */
+                int32_t pm = G_NEG_INF, py = G_NEG_INF;
+                if (j - 1 >= lo_this) {
+                    const int64_t off = base_this + (j - 1 - lo_this);
+                    pm = mm[off];
+                    py = yy[off];
+                }
+                const int32_t fm = pm - goe, fy = py - ge;
+                const int32_t v = fm >= fy ? fm : fy;
+                yy[here] = v;
+                yf[here] = fm >= fy ? G_M : G_Y;
+                if (v > best) best = v;
+            }
+            if (i >= 1 && j >= 1) {   /* M (:330-350) */
+                const int32_t s = g_pair(T, t0 + dir * i, Q, q0 + dir * j, p);
+                int32_t fm = G_NEG_INF, fx = G_NEG_INF, fy = G_NEG_INF;
+                if (j - 1 >= lo_prev && j - 1 < hi_prev_excl) {
+                    const int64_t off = base_prev + (j - 1 - lo_prev);
+                    fm = mm[off];
+                    fx = xx[off];
+                    fy = yy[off];
+                }
+                int32_t prev;
+                uint8_t from;
+                if (fm >= fx && fm >= fy) {
+                    prev = fm;
+                    from = G_M;
+                } else if (fx >= fy) {
+                    prev = fx;
+                    from = G_X;
+                } else {
+                    prev = fy;
+                    from = G_Y;
+                }
+                const int32_t v = prev + s;
+                mm[here] = v;
+                mf[here] = from;
+                if (v > best) best = v;
+            }
+            if (best > best_score) {   /* :353-363 */
+                best_score = best;
+                best_state = mm[here] == best ? G_M : (xx[here] == best ? G_X : G_Y);
+                bi = i;
+                bj = j;
+            }
+        }
+        /* x-drop prune of the touched cells (:366-398). */
+        const int32_t threshold = sat_sub(best_score, ydrop);
+        int64_t new_lo = -1, new_hi = 0;
+        for (int64_t j = j_lo; j <= j_hi; j++) {
+            const int64_t here = i * bw + (j - row_lo[i]);
+            int32_t alive = mm[here] > xx[here] ? mm[here] : xx[here];
+            if (yy[here] > alive) alive = yy[here];
+            if (alive >= threshold) {
+                if (new_lo < 0) new_lo = j;
+                new_hi = j;
+            } else {
+                mm[here] = xx[here] = yy[here] = G_NEG_INF;
+            }
+        }
+        if (new_lo < 0) break;
+        lo = new_lo;
+        hi = new_hi;
+    }
+    /* Traceback from the best cell (:404-437), emitted tip to root, then
+     * reversed (:439). */
+    {
+        int64_t i = bi, j = bj;
+        int st = best_state;
+        g_script tip = {0};
+        while (i > 0 || j > 0) {
+            const int64_t h = i * bw + (j - row_lo[i]);
+            if (st == G_M) {
+                if (g_push(&tip, 0, 1)) { rc = -1; break; }
+                st = mf[h];
+                i--;
+                j--;
+            } else if (st == G_X) {
+                if (g_push(&tip, 2, 1)) { rc = -1; break; }
+                st = xf[h];
+                i--;
+            } else {
+                if (g_push(&tip, 1, 1)) { rc = -1; break; }
+                st = yf[h];
+                j--;
+            }
+        }
+        if (rc == 0) {
+            for (uint32_t k = tip.n; k-- > 0;) {
+                if (g_push(&out->script, tip.runs[k] & 3u, tip.runs[k] >> 2)) { rc = -1; break; }
+            }
+        }
+        free(tip.runs);
+    }
+    out->score = best_score;
+    out->t_span = (uint32_t)bi;
+    out->q_span = (uint32_t)bj;
+done:
+#undef G_GROW
+    free(row_lo);
+    free(mm);
+    free(xx);
+    free(yy);
+    free(mf);
+    free(xf);
+    free(yf);
+    return rc;
+}
+
+/* extend (src/gapped_extend.rs:78-132). */
+int orc_gapped_extend(const orc_seq* t, const orc_seq* q, const orc_params* p, const orc_gapped_params* gp,
+                      uint32_t t_pos, uint32_t q_pos, orc_gapped_aln* out) {
+    memset(out, 0, sizeof(*out));
+    if ((uint64_t)t_pos >= t->len || (uint64_t)q_pos >= q->len) return -2;
+    const int32_t col = g_pair(t, t_pos, q, q_pos, p);
+    g_side right, left;
+    if (g_one_side(t, t_pos, (int64_t)t->len - t_pos - 1, q, q_pos, (int64_t)q->len - q_pos - 1, 1, p, gp, &right))
+        return -1;
+    if (g_one_side(t, t_pos, t_pos, q, q_pos, q_pos, -1, p, gp, &left)) {
+        free(right.script.runs);
+        return -1;
+    }
+    const int32_t total = sat_add(sat_add(col, left.score), right.score);
+    int rc = 0;
+    if (total >= gp->gapped_threshold) {
+        g_script s = {0};
+        int bad = 0;
+        for (uint32_t k = left.script.n; k-- > 0 && !bad;)   /* left_raw.script.reversed() */
+            bad = g_push(&s, left.script.runs[k] & 3u, left.script.runs[k] >> 2);
+        if (!bad) bad = g_push(&s, 0, 1);   /* the anchor column */
+        for (uint32_t k = 0; k < right.script.n && !bad; k++)
+            bad = g_push(&s, right.script.runs[k] & 3u, right.script.runs[k] >> 2);
+        if (bad) {
+            free(s.runs);
+            rc = -1;
+        } else {
+            out->t_start = t_pos - left.t_span;
+            out->q_start = q_pos - left.q_span;
+            out->t_len = left.t_span + 1 + right.t_span;
+            out->q_len = left.q_span + 1 + right.q_span;
+            out->score = total;
+            out->n_runs = s.n;
+            out->runs = s.runs;
+            rc = 1;
+        }
+    }
+    out->left_score = left.score;
+    out->right_score = right.score;
+    free(right.script.runs);
+    free(left.script.runs);
+    return rc;
+}
+
+typedef struct {
+    const orc_seq *t, *q;
+    const orc_params* p;
+    const orc_gapped_params* gp;
+    const uint32_t *tp, *qp;
+    orc_gapped_aln* out;
+    int* rc;
+    uint64_t n;
+    int nth, me;
+} g_job;
+
+static void* g_worker(void* arg) {
+    g_job* J = (g_job*)arg;
+    for (uint64_t i = (uint64_t)J->me; i < J->n; i += (uint64_t)J->nth)
+        J->rc[i] = orc_gapped_extend(J->t, J->q, J->p, J->gp, J->tp[i], J->qp[i], &J->out[i]);
+    return NULL;
+}
+
+int orc_gapped_extend_many(const orc_seq* t, const orc_seq* q, const orc_params* p, const orc_gapped_params* gp,
+                           const uint32_t* t_pos, const uint32_t* q_pos, uint64_t n, int n_threads,
+                           orc_gapped_aln* out, int* rc) {
+    if (n_threads < 1) n_threads = 1;
+    pthread_t th[256];
+    g_job jobs[256];
+    if (n_threads > 256) n_threads = 256;
+    for (int k = 0; k < n_threads; k++) {
+        jobs[k] = (g_job){t, q, p, gp, t_pos, q_pos, out, rc, n, n_threads, k};
+        if (pthread_create(&th[k], NULL, g_worker, &jobs[k])) return -1;
+    }
+    for (int k = 0; k < n_threads; k++) pthread_join(th[k], NULL);
+    return 0;
+}

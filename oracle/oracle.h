@@ -132,6 +132,37 @@ void orc_diag_free(void* h);
  * into out (up to n HSPs) in t_start order; returns its length. */
 uint64_t orc_best_chain(const orc_hsp* hsps, uint64_t n, orc_hsp* out);
 
+/* ---- gapped extension (src/gapped_extend.rs:78-460) ---- */
+/* GappedParams (src/gapped_extend.rs:27-31) plus the ScoringMatrix gap
+ * fields (src/scoring.rs:35-36). */
+typedef struct {
+    int32_t gap_open;
+    int32_t gap_extend;
+    int32_t y_drop;
+    int32_t gapped_threshold;
+} orc_gapped_params;
+
+/* GappedAlignment (src/gapped_extend.rs:54-63); runs = the EditScript,
+ * count << 2 | op with op 0 = Match, 1 = InsertQuery, 2 = DeleteQuery
+ * (src/edit_script.rs:17-22).  left/right_score: the two sides' DP bests,
+ * set whether or not the total passes. */
+typedef struct {
+    uint32_t t_start, q_start, t_len, q_len;
+    int32_t score;
+    uint32_t n_runs;
+    uint32_t* runs;   /* malloc'd; free with orc_free */
+    int32_t left_score, right_score;
+} orc_gapped_aln;
+
+/* extend(): 1 = Some (out filled), 0 = None (total below gapped_threshold),
+ * -1 = out of memory, -2 = anchor outside a sequence. */
+int orc_gapped_extend(const orc_seq* t, const orc_seq* q, const orc_params* p, const orc_gapped_params* gp,
+                      uint32_t t_pos, uint32_t q_pos, orc_gapped_aln* out);
+/* n anchors over n_threads POSIX threads; rc[i] = orc_gapped_extend's return. */
+int orc_gapped_extend_many(const orc_seq* t, const orc_seq* q, const orc_params* p, const orc_gapped_params* gp,
+                           const uint32_t* t_pos, const uint32_t* q_pos, uint64_t n, int n_threads,
+                           orc_gapped_aln* out, int* rc);
+
 void orc_free(void* p);
 
 #ifdef __cplusplus

@@ -61,6 +61,17 @@ class OrcStats(C.Structure):
     _fields_ = [("windows", C.c_uint64), ("raw_hits", C.c_uint64), ("extended", C.c_uint64), ("hsps", C.c_uint64)]
 
 
+class OrcGappedParams(C.Structure):
+    _fields_ = [("gap_open", C.c_int32), ("gap_extend", C.c_int32), ("y_drop", C.c_int32),
+                ("gapped_threshold", C.c_int32)]
+
+
+class OrcGappedAln(C.Structure):
+    _fields_ = [("t_start", C.c_uint32), ("q_start", C.c_uint32), ("t_len", C.c_uint32), ("q_len", C.c_uint32),
+                ("score", C.c_int32), ("n_runs", C.c_uint32), ("runs", C.POINTER(C.c_uint32)),
+                ("left_score", C.c_int32), ("right_score", C.c_int32)]
+
+
 HSP_DTYPE = np.dtype([("t_start", "<u4"), ("q_start", "<u4"), ("length", "<u4"), ("score", "<i4")])
 
 _lib = None
@@ -99,6 +110,12 @@ def lib():
         L.orc_best_chain.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p]
         L.orc_best_chain.restype = C.c_uint64
         L.orc_free.argtypes = [C.c_void_p]
+        L.orc_gapped_extend.argtypes = [P(OrcSeq), P(OrcSeq), P(OrcParams), P(OrcGappedParams), C.c_uint32,
+                                        C.c_uint32, P(OrcGappedAln)]
+        L.orc_gapped_extend.restype = C.c_int
+        L.orc_gapped_extend_many.argtypes = [P(OrcSeq), P(OrcSeq), P(OrcParams), P(OrcGappedParams), C.c_void_p,
+                                             C.c_void_p, C.c_uint64, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_gapped_extend_many.restype = C.c_int
         L.orc_diag_new.restype = C.c_void_p
         L.orc_diag_admit.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
         L.orc_diag_admit.restype = C.c_int
@@ -386,6 +403,59 @@ def parse_2bit(data: bytes) -> list:
                     asc[i] = asc[i] | 0x20
         out.append((name, bytes(asc)))
     return out
+
+
+# ---- gapped extension (src/gapped_extend.rs:78-460) through liboracle -------
+OPS = "MID"   # EditOp Match / InsertQuery / DeleteQuery as CIGAR letters (src/edit_script.rs:17-33)
+
+
+def gapped_params(gap_open=400, gap_extend=30, y_drop=9400, gapped_threshold=3000) -> OrcGappedParams:
+    """GappedParams::default() (src/gapped_extend.rs:33-43) with HOXD70's gap
+    costs (src/scoring.rs:25-26)."""
+    return OrcGappedParams(gap_open, gap_extend, y_drop, gapped_threshold)
+
+
+def _aln_result(a: OrcGappedAln):
+    runs = [int(a.runs[k]) for k in range(a.n_runs)]
+    lib().orc_free(C.cast(a.runs, C.c_void_p))
+    return {"t_start": a.t_start, "q_start": a.q_start, "t_len": a.t_len, "q_len": a.q_len, "score": a.score,
+            "runs": runs}
+
+
+def gapped_extend(t: Seq, q: Seq, p: OrcParams, gp: OrcGappedParams, t_pos: int, q_pos: int):
+    """extend() (src/gapped_extend.rs:78-132): a dict (t_start, q_start,
+    t_len, q_len, score, runs) or None when the total is below the gapped
+    threshold.  runs: count << 2 | op, op 0 = M, 1 = I, 2 = D."""
+    a = OrcGappedAln()
+    rc = lib().orc_gapped_extend(C.byref(t.c()), C.byref(q.c()), C.byref(p), C.byref(gp), t_pos, q_pos, C.byref(a))
+    if rc < 0:
+        raise MemoryError("orc_gapped_extend") if rc == -1 else ValueError("anchor outside a sequence")
+    return _aln_result(a) if rc == 1 else None
+
+
+def gapped_extend_many(t: Seq, q: Seq, p: OrcParams, gp: OrcGappedParams, t_pos, q_pos, threads: int = 1):
+    """extend() for many anchors on `threads` host threads: a list of dicts or
+    None, as gapped_extend."""
+    tp = np.ascontiguousarray(t_pos, np.uint32)
+    qp = np.ascontiguousarray(q_pos, np.uint32)
+    n = len(tp)
+    if n == 0:
+        return []
+    outs = (OrcGappedAln * n)()
+    rc = np.zeros(n, np.int32)
+    lib().orc_gapped_extend_many(C.byref(t.c()), C.byref(q.c()), C.byref(p), C.byref(gp), tp.ctypes.data,
+                                 qp.ctypes.data, n, threads, C.addressof(outs), rc.ctypes.data)
+    res = []
+    for k in range(n):
+        if rc[k] < 0:
+            raise MemoryError("orc_gapped_extend") if rc[k] == -1 else ValueError("anchor outside a sequence")
+        res.append(_aln_result(outs[k]) if rc[k] == 1 else None)
+    return res
+
+
+def cigar(runs) -> str:
+    """EditScript::to_cigar (src/edit_script.rs:122-129): count + letter per run."""
+    return "".join(f"{r >> 2}{OPS[r & 3]}" for r in runs)
 
 
 # ---- HSP consumers: pure-Python restatements ---------------------------------

@@ -315,3 +315,209 @@ def test_driver_records_chunk_order_equals_one_sort_per_group():
                     recs.add((t + lo, q, ln, sc))
         want.extend((0, 0, strand, t, q, ln, sc) for t, q, ln, sc in sorted(recs))
     assert got == want
+
+
+# ---- src/gapped_extend.rs:462-602 (gapped extension) ---------------------------------
+def _gx(t: bytes, q: bytes, hsp_t: int, hsp_q: int, offset: int, y_drop: int, thr: int):
+    # anchor_from_hsp (:470-476): the anchor sits `offset` columns into the HSP.
+    T, Q = O.pack_ascii(t), O.pack_ascii(q)
+    return O.gapped_extend(T, Q, HOX(), O.gapped_params(y_drop=y_drop, gapped_threshold=thr),
+                           hsp_t + offset, hsp_q + offset)
+
+
+def _spans(runs):
+    tsp = sum(r >> 2 for r in runs if (r & 3) in (0, 2))
+    qsp = sum(r >> 2 for r in runs if (r & 3) in (0, 1))
+    return tsp, qsp
+
+
+def test_gapped_perfect_match_stays_ungapped():   # :478-490
+    s = b"ACGTACGTACGTACGT"
+    a = _gx(s, s, 0, 0, 8, 500, 100)
+    assert (a["t_start"], a["q_start"], a["t_len"], a["q_len"]) == (0, 0, 16, 16)
+    assert O.cigar(a["runs"]) == "16M"
+
+
+def test_gapped_single_insertion_is_recovered():   # :492-510
+    a = _gx(b"ACGTACGTACGT", b"ACGTACGGTACGT", 0, 0, 3, 1000, 100)
+    assert a["t_len"] == 12 and a["q_len"] == 13
+    assert "1I" in O.cigar(a["runs"])
+    assert _spans(a["runs"]) == (12, 13)
+
+
+def test_gapped_single_deletion_is_recovered():   # :512-525
+    a = _gx(b"ACGTACGGTACGT", b"ACGTACGTACGT", 0, 0, 3, 1000, 100)
+    assert a["t_len"] == 13 and a["q_len"] == 12
+    assert "1D" in O.cigar(a["runs"])
+
+
+def test_gapped_below_threshold_returns_none():   # :527-534
+    assert _gx(b"ACGT", b"ACGT", 0, 0, 1, 500, 100_000) is None
+
+
+def test_gapped_extension_stops_at_diverging_tail():   # :536-550
+    a = _gx(b"TTTTTTTTACGTACGTACGTACGTACGTACGTTTTTTTTT", b"AAAAAAAAACGTACGTACGTACGTACGTACGTAAAAAAAA",
+            8, 8, 12, 300, 500)
+    assert 24 <= a["t_len"] <= 32
+
+
+def test_gapped_banded_dp_accommodates_large_gap():   # :552-585
+    core = b"GATTACACATGGCATGTCGAATGCCTAGCATGTCA"
+    t = core + core
+    q = core + b"AGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAG" + core
+    a = _gx(t, q, 0, 0, 5, 9400, 500)
+    assert a["t_len"] >= 60 and a["q_len"] >= 110
+    assert "I" in O.cigar(a["runs"])
+
+
+def test_gapped_script_spans_equal_reported_lengths():   # :587-600
+    a = _gx(b"AAAGATTACACATGGCATGTCGATTTT", b"GATACACATGGCAGTCGA", 3, 0, 3, 5000, 100)
+    assert _spans(a["runs"]) == (a["t_len"], a["q_len"])
+
+
+def test_gapped_many_threads_equals_one():
+    # The threaded batch form is the same function per anchor.
+    rng = np.random.default_rng(5)
+    t = rand_ascii(rng, 3000, b"ACGT")
+    q = bytearray(t)
+    for i in rng.choice(len(q), 300, replace=False):
+        q[i] = b"ACGT"[rng.integers(4)]
+    q = bytes(q[:1500] + q[1510:])
+    T, Q = O.pack_ascii(t), O.pack_ascii(q)
+    tp = rng.integers(0, 1400, 40)
+    qp = tp + rng.integers(-3, 3, 40).clip(0)
+    gp = O.gapped_params(gapped_threshold=0)
+    many = O.gapped_extend_many(T, Q, HOX(), gp, tp, qp, threads=4)
+    one = [O.gapped_extend(T, Q, HOX(), gp, int(a), int(b)) for a, b in zip(tp, qp)]
+    assert many == one
+    assert any(a is not None for a in many)
+
+
+def _py_extend(t: bytes, q: bytes, tp: int, qp: int, go: int, ge: int, ydrop: int, thr: int):
+    """A second, direct restatement of extend() (src/gapped_extend.rs:78-132,
+    :178-460) with the reference's up-front (n+1) x band_width storage, for
+    small cases: checks the C oracle's on-demand rows and run merging."""
+    sub = [[91, -114, -31, -123], [-114, 100, -125, -31], [-31, -125, 100, -114], [-123, -31, -114, 91]]
+    enc = {ord(c): i for i, c in enumerate("ACGT")}
+    enc.update({ord(c): i for i, c in enumerate("acgt")})
+    NEG = -(2 ** 31) // 4
+
+    def pair(a, b):
+        return sub[enc[a]][enc[b]] if a in enc and b in enc else -100
+
+    def one_side(T, Q):
+        n, m = len(T), len(Q)
+        if n == 0 or m == 0:
+            return 0, 0, 0, []
+        goe = go + ge
+        radius = (max(int((ydrop - goe) / ge), 0) + 2) if ge > 0 else m + 1
+        bw = min(4 * radius + 4, m + 1)
+        row_lo = [0] * (n + 1)
+        size = (n + 1) * bw
+        mm, xx, yy = [NEG] * size, [NEG] * size, [NEG] * size
+        mf, xf, yf = [0] * size, [0] * size, [0] * size
+        mm[0] = 0
+        best_score, best_cell = 0, (0, 0, 0)
+        lo = hi = 0
+        for i in range(n + 1):
+            j_lo = max(lo - radius, 0)
+            j_hi = min(hi + radius, m, j_lo + bw - 1)
+            row_lo[i] = j_lo
+            lo_prev = row_lo[i - 1] if i >= 1 else 0
+            for j in range(j_lo, j_hi + 1):
+                if i == 0 and j == 0:
+                    continue
+                best = NEG
+                here = i * bw + (j - j_lo)
+                inb = lambda jj: lo_prev <= jj < lo_prev + bw
+                if i >= 1:
+                    pm, px = (mm[(i - 1) * bw + j - lo_prev], xx[(i - 1) * bw + j - lo_prev]) if inb(j) else (NEG, NEG)
+                    fm, fx = pm - goe, px - ge
+                    xx[here], xf[here] = (fm, 0) if fm >= fx else (fx, 1)
+                    best = max(best, xx[here])
+                if j >= 1:
+                    pm, py = (mm[here - 1], yy[here - 1]) if j - 1 >= j_lo else (NEG, NEG)
+                    fm, fy = pm - goe, py - ge
+                    yy[here], yf[here] = (fm, 0) if fm >= fy else (fy, 2)
+                    best = max(best, yy[here])
+                if i >= 1 and j >= 1:
+                    s = pair(T[i - 1], Q[j - 1])
+                    o = (i - 1) * bw + j - 1 - lo_prev
+                    fm, fx, fy = (mm[o], xx[o], yy[o]) if inb(j - 1) else (NEG, NEG, NEG)
+                    if fm >= fx and fm >= fy:
+                        prev, fr = fm, 0
+                    elif fx >= fy:
+                        prev, fr = fx, 1
+                    else:
+                        prev, fr = fy, 2
+                    mm[here], mf[here] = prev + s, fr
+                    best = max(best, mm[here])
+                if best > best_score:
+                    best_score = best
+                    st = 0 if mm[here] == best else (1 if xx[here] == best else 2)
+                    best_cell = (i, j, st)
+            thr_ = best_score - ydrop
+            new_lo, new_hi = None, 0
+            for j in range(j_lo, j_hi + 1):
+                h = i * bw + (j - j_lo)
+                if max(mm[h], xx[h], yy[h]) >= thr_:
+                    new_lo = j if new_lo is None else new_lo
+                    new_hi = j
+                else:
+                    mm[h] = xx[h] = yy[h] = NEG
+            if new_lo is None:
+                break
+            lo, hi = new_lo, new_hi
+        i, j, st = best_cell
+        ops = []
+        while i > 0 or j > 0:
+            h = i * bw + (j - row_lo[i])
+            if st == 0:
+                ops.append(0); st = mf[h]; i -= 1; j -= 1
+            elif st == 1:
+                ops.append(2); st = xf[h]; i -= 1
+            else:
+                ops.append(1); st = yf[h]; j -= 1
+        return best_score, best_cell[0], best_cell[1], ops[::-1]
+
+    R = one_side(t[tp + 1:], q[qp + 1:])
+    L = one_side(t[:tp][::-1], q[:qp][::-1])
+    total = pair(t[tp], q[qp]) + L[0] + R[0]
+    if total < thr:
+        return None
+    ops = L[3][::-1] + [0] + R[3]
+    runs = []
+    for op in ops:
+        if runs and (runs[-1] & 3) == op:
+            runs[-1] += 4
+        else:
+            runs.append(4 | op)
+    return {"t_start": tp - L[1], "q_start": qp - L[2], "t_len": L[1] + 1 + R[1], "q_len": L[2] + 1 + R[2],
+            "score": total, "runs": runs}
+
+
+@pytest.mark.parametrize("go,ge,ydrop", [(400, 30, 9400), (400, 30, 300), (400, 30, 1200), (0, 30, 700), (400, 0, 500),
+                                         (50, 5, 2000)])
+def test_gapped_c_oracle_equals_direct_restatement(go, ge, ydrop):
+    rng = np.random.default_rng(go + ge + ydrop)
+    for case in range(12):
+        n = int(rng.integers(1, 160))
+        t = bytearray(rand_ascii(rng, n, b"ACGTACGTacgtN"))
+        q = bytearray(t)
+        for _ in range(int(rng.integers(0, 6))):   # indels and substitutions
+            k = int(rng.integers(0, len(q)))
+            r = rng.integers(3)
+            if r == 0:
+                q[k:k] = rand_ascii(rng, int(rng.integers(1, 9)), b"ACGT")
+            elif r == 1:
+                del q[k:k + int(rng.integers(1, 9))]
+            else:
+                q[k] = b"ACGTN"[rng.integers(5)]
+        if not q:
+            q = bytearray(b"A")
+        t, q = bytes(t), bytes(q)
+        tp, qp = int(rng.integers(0, len(t))), int(rng.integers(0, len(q)))
+        want = _py_extend(t, q, tp, qp, go, ge, ydrop, -10 ** 6)
+        got = O.gapped_extend(O.pack_ascii(t), O.pack_ascii(q), HOX(),
+                              O.gapped_params(go, ge, ydrop, -10 ** 6), tp, qp)
+        assert got == want, (case, t, q, tp, qp)
