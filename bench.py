@@ -866,6 +866,81 @@ def run_input(args):
     return out
 
 
+def run_gapped(args):
+    """Gapped extension (src/gapped_extend.rs:78-460) of the plain workload's
+    top-scoring anchors: the plus-strand HSPs of the 10 Mbp pair, their
+    anchors (choose_anchor, window 31), the --anchors highest-scoring ones
+    extended in one gxy_gapped_extend call.  Rate = DP cells (each side's band
+    width summed over its rows) per second of the DP kernel, and anchors per
+    second of the whole call.  The oracle extends a sample of the same anchors
+    on the host cores (one thread, and every thread) and must agree with the
+    device on every one of them."""
+    import numpy as np
+    g = _pkg()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    tgt, qry = workload(0)
+    ctx = g.Context(0)
+    m = g.ScoringMatrix.hoxd70()
+    T, Q = g.PackedSeq.from_ascii(tgt), g.PackedSeq.from_ascii(qry)
+    dT, dQ = T.to_device(ctx), Q.to_device(ctx)
+    tab = g.PosTable.build(dT, P12, 1, ctx=ctx)
+    hsps = g.search_device(tab, dQ, m, g.SearchParams())
+    anchors = g.choose_anchors(dT, dQ, hsps, m, 31, ctx)
+    order = np.argsort(-hsps["score"], kind="stable")[:args.anchors]
+    A = np.ascontiguousarray(anchors[order])
+    gp = g.GappedParams()
+    for _ in range(max(1, args.warmup)):
+        g.gapped_extend(dT, dQ, A, m, gp, ctx=ctx)
+    runs = []
+    for _ in range(max(1, args.steps)):
+        st = {}
+        t0 = time.perf_counter()
+        res = g.gapped_extend(dT, dQ, A, m, gp, ctx=ctx, stats=st)
+        runs.append((time.perf_counter() - t0, st))
+    wall = statistics.median(r[0] for r in runs)
+    st = runs[len(runs) // 2][1]
+    dev_s = statistics.median(r[1]["device_ms"] for r in runs) / 1e3
+    cells = st["cells"]
+    # The oracle on a sample of the anchors, spread over the ranked list.
+    k = max(1, min(args.gapped_sample, len(A)))
+    samp = np.linspace(0, len(A) - 1, k).astype(int)
+    OT, OQ = O.pack_ascii(tgt), O.pack_ascii(qry)
+    og = O.gapped_params()
+    t0 = time.perf_counter()
+    want = O.gapped_extend_many(OT, OQ, O.params(), og, A[samp, 0], A[samp, 1], threads=host_threads())
+    t_all = time.perf_counter() - t0
+    one = samp[: max(1, k // 4)]
+    t0 = time.perf_counter()
+    O.gapped_extend_many(OT, OQ, O.params(), og, A[one, 0], A[one, 1], threads=1)
+    t_one = time.perf_counter() - t0
+    same = all((w is None and res[i] is None) or
+               (w is not None and res[i] is not None and
+                (res[i].t_start, res[i].q_start, res[i].t_len, res[i].q_len, res[i].score) ==
+                (w["t_start"], w["q_start"], w["t_len"], w["q_len"], w["score"]) and
+                [int(x) for x in res[i].script] == list(w["runs"]))
+               for i, w in zip(samp, want))
+    # Cells of the sampled anchors, for the host rates: the device's per-call
+    # count scaled by the sample's share of the aligned columns.
+    cols = lambda idx: sum((res[i].t_len + res[i].q_len) if res[i] is not None else 0 for i in idx)  # noqa: E731
+    tot_cols = max(1, cols(range(len(A))))
+    cells_all = cells * cols(samp) / tot_cols
+    cells_one = cells * cols(one) / tot_cols
+    return {
+        "workload": f"gapped extension of the {len(A)} highest-scoring plus-strand anchors of the plain 10 Mbp pair "
+                    f"(HOXD70, gap 400/30, y_drop 9400, gapped_threshold 3000)",
+        "anchors": len(A), "passed": sum(r is not None for r in res), "rows": st["rows"], "cells": cells,
+        "device_ms": round(dev_s * 1e3, 3), "call_ms": round(wall * 1e3, 3),
+        "cells_per_s": round(cells / dev_s, 1), "anchors_per_s": round(len(A) / wall, 1),
+        "band_cells_per_lane": st["band_cells_per_lane"], "reruns": st["reruns"],
+        "cpu_baseline": {"kind": "port", "all_cores": {"cores": host_threads(), "anchors": int(k), "s": round(t_all, 3),
+                                                       "cells_per_s": round(cells_all / t_all, 1)},
+                         "one_core": {"cores": 1, "anchors": int(len(one)), "s": round(t_one, 3),
+                                      "cells_per_s": round(cells_one / t_one, 1)}},
+        "same_as_oracle_on_sample": same,
+    }
+
+
 def run_case(args):
     """One plus-strand search on the chromosome-style workload of --length bp
     (target and query both that long): the small case the ncu captures use."""
@@ -893,7 +968,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--plain-only", action="store_true",
                     help="default workload: skip the batched and served legs of the line")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "chunked", "case", "input"])
+    ap.add_argument("--workload", default="plain",
+                    choices=["plain", "batched", "served", "chunked", "case", "input", "gapped"])
+    ap.add_argument("--anchors", type=int, default=1024, help="gapped workload: anchors extended per call")
+    ap.add_argument("--gapped-sample", type=int, default=32, help="gapped workload: anchors the oracle extends")
     ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
     ap.add_argument("--streams", type=int, default=2, help="served workload: dispatcher streams")
     ap.add_argument("--batch-units", type=int, default=64, help="served workload: units per batch at most")
@@ -925,6 +1003,9 @@ def main():
         return
     if args.workload == "input":
         print(json.dumps(run_input(args)), flush=True)
+        return
+    if args.workload == "gapped":
+        print(json.dumps(run_gapped(args)), flush=True)
         return
     if world > 1:
         import datetime

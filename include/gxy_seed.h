@@ -369,6 +369,70 @@ gxy_status gxy_best_chain(const gxy_hsp* hsps, uint64_t n, gxy_hsp* out, uint64_
 gxy_status gxy_best_chain_groups(gxy_ctx* ctx, const gxy_hsp* hsps, const uint64_t* group_offsets,
                                  uint32_t n_groups, gxy_hsp* out, uint64_t* chain_len);
 
+/* ---- gapped extension (src/gapped_extend.rs:78-460) ---------------------- */
+/* GappedParams (src/gapped_extend.rs:27-31) plus the ScoringMatrix's affine
+ * gap costs (src/scoring.rs:35-36): a gap of k columns costs
+ * gap_open + k * gap_extend. */
+typedef struct {
+    int32_t gap_open;
+    int32_t gap_extend;
+    int32_t y_drop;
+    int32_t gapped_threshold;
+} gxy_gapped_params;
+
+/* GappedAlignment (src/gapped_extend.rs:54-63) of one anchor.  passed = 1 when
+ * extend() returns Some (total >= gapped_threshold); then the coordinates are
+ * set (t_start in the target view's coordinates) and the edit script is
+ * runs[script_off .. script_off + script_len) of the result.  passed = 0 is
+ * None: score holds the total, everything else is 0. */
+typedef struct {
+    uint32_t t_start;
+    uint32_t q_start;
+    uint32_t t_len;
+    uint32_t q_len;
+    int32_t score;
+    uint32_t passed;
+    uint64_t script_off;
+    uint32_t script_len;
+    uint32_t pad_;
+} gxy_gapped_aln;
+
+/* One call's alignments (one per anchor, in anchor order) and their edit
+ * scripts (EditScript, src/edit_script.rs:47-74): a run is count << 2 | op,
+ * op 0 = Match, 1 = InsertQuery (gap in the target), 2 = DeleteQuery (gap in
+ * the query); adjacent runs never share an op.  Free with
+ * gxy_gapped_result_free. */
+typedef struct {
+    gxy_gapped_aln* alns;
+    uint32_t* runs;
+    uint64_t n_alns;
+    uint64_t n_runs;
+} gxy_gapped_result;
+
+typedef struct {
+    uint64_t rows;                 /* DP rows computed over all sides */
+    uint64_t cells;                /* DP cells computed (the band's width summed over the rows) */
+    double device_ms;              /* CUDA-event time of the DP kernel (last run) */
+    uint32_t reruns;               /* runs repeated after the traceback storage had to grow */
+    uint32_t band_cells_per_lane;  /* cells of a row one lane of the DP warp holds */
+} gxy_gapped_stats;
+
+/* extend (src/gapped_extend.rs:78-132) for n anchors (t_pos[i], q_pos[i]) on
+ * the device, all against target[t_lo, t_hi) (the driver's chunk,
+ * src/driver.rs:395-414; t_lo = t_hi = 0: the whole target) and the whole
+ * query.  Scores: params->sub / ambig.  Every anchor is extended on its own,
+ * as one extend() call; results are bit-exact to the reference's, script
+ * included.  Anchors outside a sequence: GXY_EINVAL.  Outside the exact
+ * envelope (|scores| > 2^16, gap_open > 2^20, gap_extend > 2^16,
+ * y_drop > 2^27, a band wider than 2048 cells, or the largest positive
+ * score x the shorter sequence >= 2^31 - 2^20): GXY_EUNSUPPORTED.  stats may
+ * be NULL. */
+gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo, uint64_t t_hi,
+                             const gxy_dseq* query, const gxy_search_params* params, const gxy_gapped_params* gp,
+                             const uint32_t* t_pos, const uint32_t* q_pos, uint64_t n, gxy_gapped_result* out,
+                             gxy_gapped_stats* stats);
+void gxy_gapped_result_free(gxy_gapped_result* r);
+
 /* ---- serving loop ---------------------------------------------------------- */
 /* Keeps the given tables resident, admits submitted queries while device
  * memory is below max_device_bytes and in-flight units below max_units, and

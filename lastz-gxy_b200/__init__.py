@@ -30,7 +30,7 @@ RECORD_DTYPE = np.dtype([("group", "<u4"), ("t_start", "<u4"), ("q_start", "<u4"
 __all__ = [
     "GxyError", "HSP_DTYPE", "Context", "parse_fasta", "parse_2bit", "choose_anchors", "best_chain", "best_chain_groups", "PackedSeq", "DeviceSeq", "SeedPattern", "ScoringMatrix", "HspParams",
     "SearchParams", "PosTable", "search", "search_device", "batch_search", "batch_records", "RECORD_DTYPE",
-    "chunk_target", "extend_hits",
+    "chunk_target", "extend_hits", "GappedParams", "GappedAlignment", "gapped_extend", "cigar",
     "Server", "build", "canonical_sort",
 ]
 
@@ -626,6 +626,72 @@ def best_chain_groups(groups, ctx: Optional[Context] = None) -> list:
     check(lib().gxy_best_chain_groups(ctx.h, h.ctypes.data if len(h) else None, off.ctypes.data, len(arrs),
                                       out.ctypes.data if len(h) else None, ln.ctypes.data))
     return [out[int(off[g]):int(off[g]) + int(ln[g])].copy() for g in range(len(arrs))]
+
+
+@dataclass
+class GappedParams:
+    """GappedParams (src/gapped_extend.rs:27-43): upstream lastz's HOXD70 defaults."""
+    y_drop: int = 9400
+    gapped_threshold: int = 3000
+
+
+@dataclass
+class GappedAlignment:
+    """GappedAlignment (src/gapped_extend.rs:54-63); script = EditScript runs
+    (count << 2 | op, op 0 = Match, 1 = InsertQuery, 2 = DeleteQuery)."""
+    t_start: int
+    q_start: int
+    t_len: int
+    q_len: int
+    score: int
+    script: np.ndarray
+
+    def t_end(self) -> int:
+        return self.t_start + self.t_len
+
+    def q_end(self) -> int:
+        return self.q_start + self.q_len
+
+
+def cigar(script) -> str:
+    """EditScript::to_cigar (src/edit_script.rs:122-129)."""
+    return "".join(f"{int(r) >> 2}{'MID'[int(r) & 3]}" for r in script)
+
+
+def gapped_extend(target: DeviceSeq, query: DeviceSeq, anchors, matrix: ScoringMatrix, params: GappedParams,
+                  t_view: Optional[tuple] = None, ctx: Optional[Context] = None, stats: Optional[dict] = None) -> list:
+    """extend (src/gapped_extend.rs:78-132) for every anchor (t_pos, q_pos) of
+    an (n, 2) array, on the device: a list of GappedAlignment, or None where
+    the reference returns None.  t_view = (lo, hi) extends within that slice
+    of the target (the driver's chunk), anchors in its coordinates."""
+    ctx = ctx or target.ctx
+    a = np.ascontiguousarray(np.asarray(anchors, np.uint32).reshape(-1, 2))
+    tp, qp = np.ascontiguousarray(a[:, 0]), np.ascontiguousarray(a[:, 1])
+    n = len(a)
+    lo, hi = t_view if t_view is not None else (0, 0)
+    sp = _params_c(matrix, SearchParams())
+    gp = _lib.GappedParamsC(matrix.gap_open, matrix.gap_extend, params.y_drop, params.gapped_threshold)
+    res = _lib.GappedResultC()
+    st = _lib.GappedStatsC()
+    check(lib().gxy_gapped_extend(ctx.h, target.h, lo, hi, query.h, C.byref(sp), C.byref(gp),
+                                  tp.ctypes.data if n else None, qp.ctypes.data if n else None, n, C.byref(res),
+                                  C.byref(st)))
+    try:
+        runs = (np.ctypeslib.as_array(res.runs, (res.n_runs,)).copy() if res.n_runs else np.empty(0, np.uint32))
+        out = []
+        for k in range(n):
+            g = res.alns[k]
+            if not g.passed:
+                out.append(None)
+                continue
+            out.append(GappedAlignment(g.t_start, g.q_start, g.t_len, g.q_len, g.score,
+                                       runs[g.script_off:g.script_off + g.script_len].copy()))
+    finally:
+        lib().gxy_gapped_result_free(C.byref(res))
+    if stats is not None:
+        stats.update(rows=st.rows, cells=st.cells, device_ms=st.device_ms, reruns=st.reruns,
+                     band_cells_per_lane=st.band_cells_per_lane)
+    return out
 
 
 def chunk_target(target_len: int, primary_bp: int, halo_bp: int) -> list:

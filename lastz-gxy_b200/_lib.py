@@ -106,6 +106,27 @@ class ServerStatsC(C.Structure):
                 ("isolated", C.c_uint64), ("mem_refreshes", C.c_uint64)]
 
 
+class GappedParamsC(C.Structure):
+    _fields_ = [("gap_open", C.c_int32), ("gap_extend", C.c_int32), ("y_drop", C.c_int32),
+                ("gapped_threshold", C.c_int32)]
+
+
+class GappedAlnC(C.Structure):
+    _fields_ = [("t_start", C.c_uint32), ("q_start", C.c_uint32), ("t_len", C.c_uint32), ("q_len", C.c_uint32),
+                ("score", C.c_int32), ("passed", C.c_uint32), ("script_off", C.c_uint64),
+                ("script_len", C.c_uint32), ("pad_", C.c_uint32)]
+
+
+class GappedResultC(C.Structure):
+    _fields_ = [("alns", C.POINTER(GappedAlnC)), ("runs", C.POINTER(C.c_uint32)), ("n_alns", C.c_uint64),
+                ("n_runs", C.c_uint64)]
+
+
+class GappedStatsC(C.Structure):
+    _fields_ = [("rows", C.c_uint64), ("cells", C.c_uint64), ("device_ms", C.c_double), ("reruns", C.c_uint32),
+                ("band_cells_per_lane", C.c_uint32)]
+
+
 V = C.c_void_p
 P = C.POINTER
 U32, U64, I32, U8 = C.c_uint32, C.c_uint64, C.c_int32, C.c_uint8
@@ -157,6 +178,9 @@ SIGNATURES = {
     "gxy_choose_anchors": (C.c_int, [V, V, V, P(SearchParamsC), V, U64, U32, V, V]),
     "gxy_best_chain": (C.c_int, [V, U64, V, P(C.c_uint64)]),
     "gxy_best_chain_groups": (C.c_int, [V, V, V, U32, V, V]),
+    "gxy_gapped_extend": (C.c_int, [V, V, U64, U64, V, P(SearchParamsC), P(GappedParamsC), V, V, U64,
+                                    P(GappedResultC), P(GappedStatsC)]),
+    "gxy_gapped_result_free": (None, [P(GappedResultC)]),
     "gxy_parse_fasta": (C.c_int, [V, V, U64, P(SeqSetC)]),
     "gxy_parse_2bit": (C.c_int, [V, V, U64, P(SeqSetC)]),
     "gxy_seq_set_free": (None, [P(SeqSetC)]),

@@ -51,6 +51,7 @@ struct Worker {
     DevBuf surv;                  // hits of one pass that pass the upper-bound filter
     uint64_t surv_cap = 0;
     DevBuf redo;                  // the two lists of tiles a pass hands to the next one
+    DevBuf gpool, gruns, gaux;    // gapped extension: traceback row blocks, side runs, per-anchor arrays
     cudaGraphExec_t gexec = nullptr;   // the last batched launch's graph, updated in place when it fits
     uint64_t graph_updates = 0;
     uint32_t cand_cap = 0;

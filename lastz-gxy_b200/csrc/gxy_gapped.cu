@@ -1,0 +1,819 @@
+// gxy_gapped.cu -- gapped extension (src/gapped_extend.rs:78-460) on the device.
+//
+// extend() runs a banded 3-state affine x-drop DP (Gotoh M/X/Y) to the right
+// of an anchor and, on reversed inputs, to its left, then traces the best
+// cell back into a run-length edit script.  The DP is row by row: row i's
+// band is [lo - R, hi + R] around the previous row's surviving cells, capped
+// at band_width = min(4R + 4, m + 1) cells; after a row, the cells whose best
+// state is more than y_drop below the best score so far are killed.  These
+// rules (the band, the row-major first maximum, the kill) decide the result,
+// so the device keeps the row order.  One warp runs one side of one anchor:
+//
+//  - Lane k owns S consecutive cells of the row (S = band_width / 32 rounded
+//    up to 8; 40 for HOXD70's defaults).  X and M of a cell need the previous
+//    row only, so a lane forms them for its cells first (phase A).
+//  - Y is a max-plus recurrence along the row, Y[j] = max(M[j-1] - (O+E),
+//    Y[j-1] - E).  Each lane reduces its cells to one affine-max function
+//    x -> max(a, x - S*E); a warp shuffle scan composes them, giving every
+//    lane the exact Y entering its cells (phase B then runs the recurrence
+//    from there).  The arithmetic is the reference's i32 arithmetic: max-plus
+//    composition is exact.
+//  - The row lives in shared memory (best state H = max(M, X, Y) with its
+//    argmax, and the next row's X = max(M - (O+E), X - E) with its source),
+//    stored transposed (cell p at (p mod S) * 32 + p / S), so both the
+//    current row's writes and the next row's reads, at any shift of the
+//    band, hit 32 distinct banks.  A cell killed by the x-drop rule is not
+//    rewritten: the next row compares its H with the row's threshold and
+//    reads NEG_INF in its place, as the reference's cleared cell reads.
+//  - The three back-pointers of a cell (4 bits) go to global memory, rows in
+//    blocks of kRows kept by the warp across its tasks (a chain it grows from
+//    a shared pool as its longest side needs).  After the last row, lane 0
+//    walks from the best cell to (0, 0) and writes the runs.
+//
+// A last kernel joins the two sides per anchor: total = anchor column + left
+// best + right best (saturating), the left runs in walk order, the anchor's
+// Match merged with its neighbours, the right runs reversed
+// (src/gapped_extend.rs:99-131, src/edit_script.rs:63-92).
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gxy_engine.cuh"
+
+using namespace gxy;
+
+namespace {
+
+constexpr int32_t kNegInf = INT32_MIN / 4;   // NEG_INF (src/gapped_extend.rs:44)
+constexpr int32_t kLow = INT32_MIN / 2;      // "no contribution" in the row scan: below every DP value
+constexpr int kGapWarps = 4;                  // warps per block
+constexpr int kRows = 32;                     // DP rows per traceback block
+constexpr int kHdr = 4;                       // block header words: previous block, next block, first row, -
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kMaxS = 64;                     // cells per lane; band_width <= 32 * kMaxS
+
+// Side flags.
+constexpr uint32_t kFlagPool = 1;    // the traceback pool ran out: rerun with a larger one
+constexpr uint32_t kFlagRuns = 2;    // the run buffer ran out: rerun with a larger one
+constexpr uint32_t kFlagState = 4;   // inconsistent back-pointers (a bug; reported as an error)
+
+// Counters (u64): task cursor, pool blocks claimed, run words reserved, rows, cells, flags.
+enum { kCtrTask = 0, kCtrBlocks, kCtrRuns, kCtrRows, kCtrCells, kCtrFlags, kCtrWords = 8 };
+
+struct GapSide {
+    int32_t score;
+    uint32_t t_span;
+    uint32_t q_span;
+    uint32_t n_runs;
+    uint64_t run_off;
+    uint32_t flags;
+    uint32_t pad_;
+};
+
+struct GapArgs {
+    SeqView T, Q;
+    const uint32_t* t_pos;
+    const uint32_t* q_pos;
+    uint32_t n_anchors;
+    int32_t sub[16];
+    int32_t ambig;
+    int32_t goe;      // gap_open + gap_extend
+    int32_t ge;       // gap_extend
+    int32_t ydrop;
+    int64_t radius;   // band radius; < 0: m + 1 (gap_extend <= 0)
+    uint32_t* pool;
+    uint64_t pool_blocks;
+    uint32_t block_words;
+    uint32_t* runs;
+    uint64_t runs_cap;
+    unsigned long long* ctr;
+    GapSide* sides;   // [2a] left, [2a + 1] right
+};
+
+__device__ __forceinline__ int32_t sat_sub32(int32_t a, int32_t b) {
+    const int64_t r = (int64_t)a - b;
+    return r > INT32_MAX ? INT32_MAX : (r < INT32_MIN ? INT32_MIN : (int32_t)r);
+}
+__device__ __forceinline__ int32_t sat_add32(int32_t a, int32_t b) {
+    const int64_t r = (int64_t)a + b;
+    return r > INT32_MAX ? INT32_MAX : (r < INT32_MIN ? INT32_MIN : (int32_t)r);
+}
+
+// Swaps the two bits of every 2-bit field (undoes __brevll's swap inside a code).
+__device__ __forceinline__ uint64_t swap_pairs(uint64_t x) {
+    return ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
+}
+
+// Codes (2 bits each, two words) and valid bits of the 64 positions from
+// global position gp.
+__device__ __forceinline__ void load_window64(const SeqView& S, uint64_t gp, uint64_t& c_lo, uint64_t& c_hi,
+                                              uint64_t& v) {
+    const uint64_t w = gp >> 5;
+    const uint32_t s = (uint32_t)(gp & 31);
+    const uint64_t a = __ldg(S.codes + w), b = __ldg(S.codes + w + 1), c = __ldg(S.codes + w + 2);
+    c_lo = s ? ((a >> (2 * s)) | (b << (64 - 2 * s))) : a;
+    c_hi = s ? ((b >> (2 * s)) | (c << (64 - 2 * s))) : b;
+    const uint32_t va = __ldg(S.valid + w), vb = __ldg(S.valid + w + 1), vc = __ldg(S.valid + w + 2);
+    v = (uint64_t)__funnelshift_r(va, vb, s) | ((uint64_t)__funnelshift_r(vb, vc, s) << 32);
+}
+
+__device__ __forceinline__ uint32_t code_at(const SeqView& S, uint64_t gp) {
+    return (uint32_t)(__ldg(S.codes + (gp >> 5)) >> (2 * (gp & 31))) & 3u;
+}
+__device__ __forceinline__ uint32_t valid_at(const SeqView& S, uint64_t gp) {
+    return (__ldg(S.valid + (gp >> 5)) >> (gp & 31)) & 1u;
+}
+
+// (value, cell, state) with the larger value first, the smaller cell on ties:
+// the reference's strict `>` over a row-major scan keeps the first maximum.
+__device__ __forceinline__ void best_reduce(int32_t& v, int32_t& pc, uint32_t& st) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int32_t v2 = __shfl_xor_sync(kFull, v, o);
+        const int32_t p2 = __shfl_xor_sync(kFull, pc, o);
+        const uint32_t s2 = __shfl_xor_sync(kFull, st, o);
+        if (v2 > v || (v2 == v && p2 < pc)) {
+            v = v2;
+            pc = p2;
+            st = s2;
+        }
+    }
+}
+
+// One side of one anchor per warp, tasks claimed from a cursor.  S = cells per lane.
+template <int S>
+__global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
+    static_assert(S % 8 == 0 && S >= 8 && S <= kMaxS, "cells per lane");
+    extern __shared__ int32_t g_sm[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t* sH = g_sm + wid * (S * 32 * 2);
+    int32_t* sNX = sH + S * 32;
+    uint8_t* sST = reinterpret_cast<uint8_t*>(g_sm + kGapWarps * S * 32 * 2) + wid * S * 32;
+    const int32_t goe = a.goe, ge = a.ge;
+    // X of a cell whose upper neighbour is dead or outside the band.
+    const int32_t nx_dead = max(kNegInf - goe, kNegInf - ge);
+    const uint32_t nx_dead_from = (kNegInf - goe >= kNegInf - ge) ? 0u : 1u;
+    const uint64_t ntasks = 2ull * a.n_anchors;
+    const int32_t lane_shift = S * ge;   // Y decays by this over one lane's cells
+    constexpr int kWordsPerLane = S / 8;
+    constexpr int kRowWords = 32 * kWordsPerLane;
+    // This warp's chain of traceback blocks (kept across tasks).
+    uint32_t chain_head = kNone, chain_len = 0;
+    for (;;) {
+        unsigned long long task = 0;
+        if (lane == 0) task = atomicAdd(a.ctr + kCtrTask, 1ull);
+        task = __shfl_sync(kFull, task, 0);
+        if (task >= ntasks) break;
+        const uint32_t an = (uint32_t)(task >> 1);
+        const bool right = task & 1;
+        const int64_t dir = right ? 1 : -1;
+        const uint32_t t0 = a.t_pos[an], q0 = a.q_pos[an];
+        const int64_t n = right ? (int64_t)a.T.len - t0 - 1 : (int64_t)t0;
+        const int64_t m = right ? (int64_t)a.Q.len - q0 - 1 : (int64_t)q0;
+        GapSide res{};
+        if (n == 0 || m == 0) {
+            if (lane == 0) a.sides[task] = res;
+            continue;
+        }
+        const int64_t R = a.radius >= 0 ? a.radius : m + 1;
+        const int64_t bw = min(4 * R + 4, m + 1);
+        int64_t lo = 0, hi = 0;        // surviving cells of the previous row
+        int64_t pjl = 0;               // previous row's band start
+        int32_t pw = 0;                // previous row's band width
+        int32_t thr_prev = 0;          // previous row's kill threshold
+        int32_t best = 0;
+        int64_t bi = 0, bj = 0;
+        uint32_t bst = 0;
+        uint32_t flags = 0;
+        // Walk of the chain while filling: the block holding the current row.
+        uint32_t cur_blk = kNone;
+        uint32_t blk_index = 0;        // its position in the chain
+        bool store = true;
+        uint64_t rows = 0, cells = 0;
+        int64_t i = 0;
+        for (; i <= n; i++) {
+            const int64_t jl = lo > R ? lo - R : 0;
+            int64_t jh = min(hi + R, m);
+            jh = min(jh, jl + bw - 1);
+            const int32_t width = (int32_t)(jh - jl + 1);
+            if (width > 32 * S) {   // cannot happen: the host sizes S from band_width
+                flags |= kFlagState;
+                break;
+            }
+            rows++;
+            cells += (uint64_t)width;
+            // Scores of the row's target base against query codes 0..3.
+            int32_t s0 = a.ambig, s1 = a.ambig, s2 = a.ambig, s3 = a.ambig;
+            if (i >= 1) {
+                const uint64_t tg = a.T.base + (uint64_t)((int64_t)t0 + dir * i);
+                if (valid_at(a.T, tg)) {
+                    const uint32_t tc = code_at(a.T, tg);
+                    s0 = a.sub[tc * 4 + 0];
+                    s1 = a.sub[tc * 4 + 1];
+                    s2 = a.sub[tc * 4 + 2];
+                    s3 = a.sub[tc * 4 + 3];
+                }
+            }
+            const int32_t cbase = lane * S;
+            const int32_t con = min(max(width - cbase, 0), S);
+            // The lane's query bases, cell c at offset c.
+            uint64_t qlo = 0, qhi = 0, qv = 0;
+            if (con > 0 && i >= 1) {
+                if (right) {
+                    load_window64(a.Q, a.Q.base + (uint64_t)((int64_t)q0 + jl + cbase), qlo, qhi, qv);
+                } else {
+                    uint64_t l0, h0, v0;
+                    load_window64(a.Q, (uint64_t)((int64_t)a.Q.base + (int64_t)q0 - jl - cbase - 63), l0, h0, v0);
+                    qlo = swap_pairs(__brevll(h0));
+                    qhi = swap_pairs(__brevll(l0));
+                    qv = __brevll(v0);
+                }
+            }
+            // ---- phase A: X and M of the lane's cells from the previous row.
+            int32_t Mr[S], Xr[S];
+            uint32_t tb[kWordsPerLane];
+#pragma unroll
+            for (int k = 0; k < kWordsPerLane; k++) tb[k] = 0;
+            int32_t hm1 = kNegInf;   // H of the previous row's cell left of the current one (killed: NEG_INF)
+            uint32_t sm1 = 0;
+            {
+                const int32_t p = (int32_t)(jl + cbase - pjl) - 1;
+                if (i >= 1 && p >= 0 && p < pw) {
+                    const int ad = (p % S) * 32 + p / S;
+                    const int32_t h = sH[ad];
+                    if (h >= thr_prev) {
+                        hm1 = h;
+                        sm1 = sST[ad] & 3u;
+                    }
+                }
+            }
+            int32_t yl = kLow;   // Y of the lane's cells without what enters from the left
+#pragma unroll
+            for (int c = 0; c < S; c++) {
+                const int64_t j = jl + cbase + c;
+                const bool on = c < con;
+                const int32_t p = (int32_t)(j - pjl);
+                int32_t hp = kNegInf, nxp = nx_dead;
+                uint32_t stp = 0, nxf = nx_dead_from;
+                if (i >= 1 && on && p >= 0 && p < pw) {
+                    const int ad = (p % S) * 32 + p / S;
+                    const int32_t h = sH[ad];
+                    if (h >= thr_prev) {
+                        const uint32_t st = sST[ad];
+                        hp = h;
+                        nxp = sNX[ad];
+                        stp = st & 3u;
+                        nxf = (st >> 2) & 1u;
+                    }
+                }
+                int32_t M, X;
+                uint32_t mf = 0, xf = 0;
+                if (i == 0) {
+                    X = kNegInf;
+                    M = j == 0 ? 0 : kNegInf;
+                } else {
+                    X = nxp;
+                    xf = nxf;
+                    if (j == 0) {
+                        M = kNegInf;
+                    } else {
+                        const uint32_t qc =
+                            (uint32_t)((c < 32 ? (qlo >> (2 * c)) : (qhi >> (2 * (c & 31)))) & 3u);
+                        const bool qvb = (qv >> c) & 1u;
+                        const int32_t s =
+                            qvb ? ((qc & 2) ? ((qc & 1) ? s3 : s2) : ((qc & 1) ? s1 : s0)) : a.ambig;
+                        M = hm1 + s;
+                        mf = sm1;
+                    }
+                }
+                if (!on) {
+                    M = kNegInf;
+                    X = kNegInf;
+                }
+                Mr[c] = M;
+                Xr[c] = X;
+                tb[c >> 3] |= (mf | (xf << 2)) << (4 * (c & 7));
+                hm1 = hp;
+                sm1 = stp;
+                if (c + 1 < S) yl = max(max(M - goe, yl - ge), kLow);
+            }
+            // What the lane passes on: Y entering the cell after its last.
+            int32_t A = max(max(Mr[S - 1] - goe, yl - ge), kLow);
+            const int32_t yl_last = yl;
+            __syncwarp();
+            // ---- the row scan: compose x -> max(a_k, x - S*E) over the lanes.
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t Ap = __shfl_up_sync(kFull, A, o);
+                if (lane >= o) A = max(A, max(Ap - o * lane_shift, kLow));
+            }
+            // Y of the row's first cell: NEG_INF when it is column 0 (no Y
+            // there), else what NEG_INF neighbours give.
+            const int32_t T0 = jl == 0 ? kNegInf : max(kNegInf - goe, kNegInf - ge);
+            const int32_t tout = max(A, max(T0 - (lane + 1) * lane_shift, kLow));
+            int32_t tin = __shfl_up_sync(kFull, tout, 1);
+            if (lane == 0) tin = T0;
+            const int32_t ylast = max(yl_last, max(tin - (S - 1) * ge, kLow));
+            int32_t mleft = __shfl_up_sync(kFull, Mr[S - 1], 1);
+            int32_t yleft = __shfl_up_sync(kFull, ylast, 1);
+            if (lane == 0) {
+                mleft = kNegInf;
+                yleft = kNegInf;
+            }
+            // ---- phase B: Y, the cell's best state, the next row's X, the best.
+            int32_t lbest = INT32_MIN, lpc = INT32_MAX;
+            uint32_t lst = 0;
+#pragma unroll
+            for (int c = 0; c < S; c++) {
+                const int64_t j = jl + cbase + c;
+                const bool on = c < con;
+                int32_t Y;
+                uint32_t yf = 0;
+                if (j == 0) {
+                    Y = kNegInf;
+                } else {
+                    const int32_t fm = mleft - goe, fy = yleft - ge;
+                    Y = fm >= fy ? fm : fy;
+                    yf = fm >= fy ? 0u : 1u;
+                }
+                const int32_t M = Mr[c], X = Xr[c];
+                mleft = M;
+                yleft = Y;
+                const uint32_t hs = (M >= X && M >= Y) ? 0u : (X >= Y ? 1u : 2u);
+                const int32_t H = hs == 0 ? M : (hs == 1 ? X : Y);
+                const int32_t fm = M - goe, fx = X - ge;
+                const int32_t NX = fm >= fx ? fm : fx;
+                const uint32_t nxf = fm >= fx ? 0u : 1u;
+                if (on) {
+                    const int ad = c * 32 + lane;
+                    sH[ad] = H;
+                    sNX[ad] = NX;
+                    sST[ad] = (uint8_t)(hs | (nxf << 2));
+                    if (H > lbest) {
+                        lbest = H;
+                        lpc = cbase + c;
+                        lst = hs;
+                    }
+                }
+                tb[c >> 3] |= (yf << 3) << (4 * (c & 7));
+                Xr[c] = on ? H : kLow;   // H from here on
+            }
+            // ---- back-pointers of the row.
+            if (store && (i % kRows) == 0) {
+                // Next block of the chain, claimed from the pool when the chain ends here.
+                uint32_t nb = kNone;
+                if (lane == 0) {
+                    if (blk_index < chain_len) {
+                        nb = cur_blk == kNone ? chain_head : a.pool[(uint64_t)cur_blk * a.block_words + 1];
+                    } else {
+                        const unsigned long long b = atomicAdd(a.ctr + kCtrBlocks, 1ull);
+                        if (b < a.pool_blocks) {
+                            nb = (uint32_t)b;
+                            uint32_t* hdr = a.pool + (uint64_t)nb * a.block_words;
+                            hdr[0] = cur_blk;   // previous block in the chain
+                            hdr[1] = kNone;     // next
+                            if (cur_blk == kNone) {
+                                chain_head = nb;
+                            } else {
+                                a.pool[(uint64_t)cur_blk * a.block_words + 1] = nb;
+                            }
+                            chain_len++;
+                        }
+                    }
+                    if (nb != kNone) a.pool[(uint64_t)nb * a.block_words + 2] = (uint32_t)i;
+                }
+                nb = __shfl_sync(kFull, nb, 0);
+                chain_head = __shfl_sync(kFull, chain_head, 0);
+                chain_len = __shfl_sync(kFull, chain_len, 0);
+                if (nb == kNone) {
+                    store = false;
+                    flags |= kFlagPool;
+                } else {
+                    cur_blk = nb;
+                    blk_index++;
+                }
+            }
+            if (store) {
+                uint32_t* blk = a.pool + (uint64_t)cur_blk * a.block_words;
+                const int r = (int)(i % kRows);
+                if (lane == 0) blk[kHdr + r] = (uint32_t)jl;
+                uint32_t* row = blk + kHdr + kRows + (uint64_t)r * kRowWords + lane * kWordsPerLane;
+#pragma unroll
+                for (int k = 0; k < kWordsPerLane; k++)
+                    if (k * 8 < con) row[k] = tb[k];
+            }
+            // ---- the row's best, the threshold and the surviving cells.
+            best_reduce(lbest, lpc, lst);
+            if (lbest > best) {
+                best = lbest;
+                bi = i;
+                bj = jl + lpc;
+                bst = lst;
+            }
+            const int32_t thr = sat_sub32(best, a.ydrop);
+            int32_t first = INT32_MAX, last = -1;
+#pragma unroll
+            for (int c = 0; c < S; c++) {
+                if (Xr[c] >= thr) {
+                    first = min(first, cbase + c);
+                    last = cbase + c;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                first = min(first, __shfl_xor_sync(kFull, first, o));
+                last = max(last, __shfl_xor_sync(kFull, last, o));
+            }
+            __syncwarp();
+            if (last < 0) break;   // the whole row is dead
+            lo = jl + first;
+            hi = jl + last;
+            pjl = jl;
+            pw = width;
+            thr_prev = thr;
+        }
+        res.score = best;
+        res.t_span = (uint32_t)bi;
+        res.q_span = (uint32_t)bj;
+        if (!store) flags |= kFlagPool;
+        // ---- traceback from the best cell (src/gapped_extend.rs:404-437),
+        // runs written in walk order (tip to root).
+        if (lane == 0 && !(flags & (kFlagPool | kFlagState))) {
+            const uint64_t cap = (uint64_t)(bi + bj);
+            uint64_t off = 0;
+            if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
+            if (off + cap > a.runs_cap) {
+                flags |= kFlagRuns;
+            } else {
+                // The block of row bi: the chain's blocks hold rows in order.
+                uint32_t blk = chain_head;
+                for (int64_t k = 0; k < bi / kRows; k++) blk = a.pool[(uint64_t)blk * a.block_words + 1];
+                int64_t ti = bi, tj = bj;
+                uint32_t st = bst;
+                uint32_t op = 3, cnt = 0, nr = 0;
+                for (uint64_t step = 0; ti > 0 || tj > 0; step++) {
+                    if (step >= cap) {   // every step lowers ti + tj
+                        flags |= kFlagState;
+                        break;
+                    }
+                    const uint32_t* bp = a.pool + (uint64_t)blk * a.block_words;
+                    while (ti < (int64_t)bp[2] && bp[0] != kNone) {   // rows before this block: step back
+                        blk = bp[0];
+                        bp = a.pool + (uint64_t)blk * a.block_words;
+                    }
+                    if (ti < (int64_t)bp[2]) {
+                        flags |= kFlagState;
+                        break;
+                    }
+                    const int r = (int)(ti - (int64_t)bp[2]);
+                    const int64_t p = tj - (int64_t)bp[kHdr + r];
+                    if (p < 0 || p >= 32 * S) {
+                        flags |= kFlagState;
+                        break;
+                    }
+                    const uint32_t nib =
+                        (bp[kHdr + kRows + (uint64_t)r * kRowWords + (p >> 3)] >> (4 * (p & 7))) & 15u;
+                    uint32_t eop;
+                    if (st == 0) {   // M: both advance
+                        if (ti == 0 || tj == 0) {
+                            flags |= kFlagState;
+                            break;
+                        }
+                        eop = 0;
+                        st = nib & 3u;
+                        ti--;
+                        tj--;
+                    } else if (st == 1) {   // X: gap in the query (DeleteQuery)
+                        if (ti == 0) {
+                            flags |= kFlagState;
+                            break;
+                        }
+                        eop = 2;
+                        st = ((nib >> 2) & 1u) ? 1u : 0u;
+                        ti--;
+                    } else {   // Y: gap in the target (InsertQuery)
+                        if (tj == 0) {
+                            flags |= kFlagState;
+                            break;
+                        }
+                        eop = 1;
+                        st = ((nib >> 3) & 1u) ? 2u : 0u;
+                        tj--;
+                    }
+                    if (eop == op) {
+                        cnt++;
+                    } else {
+                        if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                        op = eop;
+                        cnt = 1;
+                    }
+                }
+                if (!(flags & kFlagState)) {
+                    if (ti > 0 || tj > 0) flags |= kFlagState;
+                    if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                }
+                res.run_off = off;
+                res.n_runs = nr;
+            }
+        }
+        flags = __shfl_sync(kFull, flags, 0);
+        res.run_off = __shfl_sync(kFull, res.run_off, 0);
+        res.n_runs = __shfl_sync(kFull, res.n_runs, 0);
+        res.flags = flags;
+        if (lane == 0) {
+            a.sides[task] = res;
+            atomicAdd(a.ctr + kCtrRows, (unsigned long long)rows);
+            atomicAdd(a.ctr + kCtrCells, (unsigned long long)cells);
+            if (flags) atomicOr(a.ctr + kCtrFlags, (unsigned long long)flags);
+        }
+        __syncwarp();
+    }
+}
+
+// Per anchor: the total, the verdict, the joined run count.
+__global__ void k_gapped_join(GapArgs a, int32_t threshold, gxy_gapped_aln* out, uint32_t* counts) {
+    const uint32_t an = blockIdx.x * blockDim.x + threadIdx.x;
+    if (an >= a.n_anchors) return;
+    const GapSide L = a.sides[2 * an], R = a.sides[2 * an + 1];
+    const uint32_t t0 = a.t_pos[an], q0 = a.q_pos[an];
+    const uint64_t tg = a.T.base + t0, qg = a.Q.base + q0;
+    const int32_t col = (valid_at(a.T, tg) && valid_at(a.Q, qg)) ? a.sub[code_at(a.T, tg) * 4 + code_at(a.Q, qg)]
+                                                                  : a.ambig;
+    const int32_t total = sat_add32(sat_add32(col, L.score), R.score);
+    gxy_gapped_aln o{};
+    o.score = total;
+    uint32_t cnt = 0;
+    if (total >= threshold) {
+        o.passed = 1;
+        o.t_start = t0 - L.t_span;
+        o.q_start = q0 - L.q_span;
+        o.t_len = L.t_span + 1 + R.t_span;
+        o.q_len = L.q_span + 1 + R.q_span;
+        const uint32_t lm = L.n_runs && (a.runs[L.run_off + L.n_runs - 1] & 3u) == 0;
+        const uint32_t rm = R.n_runs && (a.runs[R.run_off + R.n_runs - 1] & 3u) == 0;
+        cnt = L.n_runs + R.n_runs + 1 - lm - rm;
+    }
+    o.script_len = cnt;
+    out[an] = o;
+    counts[an] = cnt;
+}
+
+// Per anchor (one warp): the joined runs at offs[an].
+__global__ void k_gapped_emit(GapArgs a, const gxy_gapped_aln* alns, const uint32_t* offs, uint32_t* out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nw = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t an = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); an < a.n_anchors; an += nw) {
+        if (!alns[an].passed) continue;
+        const GapSide L = a.sides[2 * an], R = a.sides[2 * an + 1];
+        const uint32_t* lr = a.runs + L.run_off;
+        const uint32_t* rr = a.runs + R.run_off;
+        const uint32_t lm = L.n_runs && (lr[L.n_runs - 1] & 3u) == 0;
+        const uint32_t rm = R.n_runs && (rr[R.n_runs - 1] & 3u) == 0;
+        const uint32_t nl = L.n_runs - lm, nr = R.n_runs - rm;
+        uint32_t* o = out + offs[an];
+        for (uint32_t k = lane; k < nl; k += 32) o[k] = lr[k];
+        if (lane == 0) {
+            const uint32_t mid = 1 + (lm ? lr[L.n_runs - 1] >> 2 : 0) + (rm ? rr[R.n_runs - 1] >> 2 : 0);
+            o[nl] = mid << 2;
+        }
+        for (uint32_t k = lane; k < nr; k += 32) o[nl + 1 + k] = rr[nr - 1 - k];
+    }
+}
+
+template <int S>
+cudaError_t launch_sides(const GapArgs& a, int sm_count, cudaStream_t st) {
+    const size_t smem = (size_t)kGapWarps * S * 32 * 9;
+    cudaError_t e = cudaFuncSetAttribute(k_gapped_sides<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gapped_sides<S>, kGapWarps * 32, smem);
+    if (e != cudaSuccess) return e;
+    const int blocks = sm_count * std::max(per_sm, 1);
+    count_launch();
+    k_gapped_sides<S><<<blocks, kGapWarps * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sides_for(int S, const GapArgs& a, int sm_count, cudaStream_t st) {
+    switch (S) {
+        case 8: return launch_sides<8>(a, sm_count, st);
+        case 16: return launch_sides<16>(a, sm_count, st);
+        case 24: return launch_sides<24>(a, sm_count, st);
+        case 32: return launch_sides<32>(a, sm_count, st);
+        case 40: return launch_sides<40>(a, sm_count, st);
+        case 48: return launch_sides<48>(a, sm_count, st);
+        case 56: return launch_sides<56>(a, sm_count, st);
+        default: return launch_sides<64>(a, sm_count, st);
+    }
+}
+
+// Warps the persistent launch runs at most (the pool is sized per warp).
+int max_warps(int S, int sm_count) {
+    const size_t smem = (size_t)kGapWarps * S * 32 * 9;
+    int per_sm = (int)std::max<size_t>(1, (size_t)(227 * 1024) / smem);
+    per_sm = std::min(per_sm, 16);
+    return sm_count * per_sm * kGapWarps;
+}
+
+struct WorkerLease {
+    gxy_ctx* ctx;
+    Worker* w;
+    gxy_status err;
+    explicit WorkerLease(gxy_ctx* c) : ctx(c), w(nullptr), err(GXY_OK) { w = checkout(c, &err); }
+    ~WorkerLease() {
+        if (w) checkin(ctx, w);
+    }
+};
+
+gxy_status fail(gxy_status s, const std::string& m) {
+    set_error(m);
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo, uint64_t t_hi,
+                             const gxy_dseq* query, const gxy_search_params* params, const gxy_gapped_params* gp,
+                             const uint32_t* t_pos, const uint32_t* q_pos, uint64_t n, gxy_gapped_result* out,
+                             gxy_gapped_stats* stats) {
+    if (!ctx || !target || !query || !params || !gp || !out || (n && (!t_pos || !q_pos)))
+        return fail(GXY_EINVAL, "null argument");
+    memset(out, 0, sizeof(*out));
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (t_lo == 0 && t_hi == 0) t_hi = target->len;
+    if (t_lo > t_hi || t_hi > target->len) return fail(GXY_EINVAL, "target view outside the target");
+    const uint64_t lt = t_hi - t_lo, lq = query->len;
+    if (lt >= (1ull << 32) || lq >= (1ull << 32)) return fail(GXY_EUNSUPPORTED, "sequences of 2^32 bases or more");
+    if (n >= (1ull << 31)) return fail(GXY_EUNSUPPORTED, "2^31 anchors or more");
+    for (uint64_t k = 0; k < n; k++)
+        if (t_pos[k] >= lt || q_pos[k] >= lq) return fail(GXY_EINVAL, "anchor outside its sequence");
+    // The exact envelope: every DP value formed stays far from i32 limits, and
+    // values formed from NEG_INF stay below every threshold.
+    int64_t smax = std::abs((int64_t)params->ambig);
+    for (int k = 0; k < 16; k++) smax = std::max<int64_t>(smax, std::abs((int64_t)params->sub[k]));
+    if (smax > (1 << 16)) return fail(GXY_EUNSUPPORTED, "substitution scores beyond +-65536");
+    if (gp->gap_open < 0 || gp->gap_open > (1 << 20) || gp->gap_extend < 0 || gp->gap_extend > (1 << 16))
+        return fail(GXY_EUNSUPPORTED, "gap costs outside [0, 2^20] (open) / [0, 2^16] (extend)");
+    if (gp->y_drop < 0 || gp->y_drop > (1 << 27)) return fail(GXY_EUNSUPPORTED, "y_drop outside [0, 2^27]");
+    // A cell's score is at most the largest positive column score times the
+    // columns of the shorter sequence.
+    int64_t spos = std::max<int64_t>(0, params->ambig);
+    for (int k = 0; k < 16; k++) spos = std::max<int64_t>(spos, params->sub[k]);
+    if ((double)spos * (double)(std::min(lt, lq) + 2) >= 2147483648.0 - 1048576.0)
+        return fail(GXY_EUNSUPPORTED, "scores could exceed 2^31 - 2^20 on sequences this long");
+    const int32_t goe = gp->gap_open + gp->gap_extend, ge = gp->gap_extend;
+    int64_t radius = -1;
+    if (ge > 0) {
+        const int64_t r = ((int64_t)gp->y_drop - goe) / ge;   // truncates toward zero, as Rust's i32 `/`
+        radius = std::max<int64_t>(r, 0) + 2;
+    }
+    // Band width bound over all sides: min(4R + 4, m + 1) with m < lq.
+    const int64_t bw_max = radius >= 0 ? std::min<int64_t>(4 * radius + 4, (int64_t)lq) : (int64_t)lq;
+    int S = (int)((bw_max + 31) / 32);
+    S = std::max(8, (S + 7) / 8 * 8);
+    if (S > kMaxS)
+        return fail(GXY_EUNSUPPORTED, "band wider than 2048 cells (y_drop / gap_extend too large for the device DP)");
+    out->n_alns = n;
+    out->alns = n ? (gxy_gapped_aln*)calloc(n, sizeof(gxy_gapped_aln)) : nullptr;
+    if (n && !out->alns) return fail(GXY_ENOMEM, "host allocation");
+    if (n == 0) return GXY_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(GXY_ECUDA, "cudaSetDevice");
+    WorkerLease Lw(ctx);
+    if (!Lw.w) {
+        gxy_gapped_result_free(out);
+        return Lw.err;
+    }
+    Worker* W = Lw.w;
+    cudaStream_t st = W->st;
+    // Per-anchor arrays: anchors (2 x u32), sides (2 x 32 B), joined records,
+    // run counts and offsets (+1), counters.
+    const size_t off_t = 0, off_q = off_t + n * 4, off_side = (off_q + n * 4 + 255) & ~(size_t)255,
+                 off_aln = off_side + 2 * n * sizeof(GapSide), off_cnt = off_aln + n * sizeof(gxy_gapped_aln),
+                 off_offs = off_cnt + n * 4, off_ctr = (off_offs + (n + 1) * 4 + 255) & ~(size_t)255,
+                 aux_bytes = off_ctr + kCtrWords * 8;
+    cudaError_t e = W->gaux.ensure(aux_bytes);
+    if (e != cudaSuccess) {
+        gxy_gapped_result_free(out);
+        return fail(GXY_ENOMEM, std::string("gapped buffers: ") + cudaGetErrorString(e));
+    }
+    unsigned char* aux = W->gaux.as<unsigned char>();
+    GapArgs A{};
+    A.T = view_of(target, t_lo, t_hi);
+    A.Q = view_of(query, 0, lq);
+    A.t_pos = reinterpret_cast<uint32_t*>(aux + off_t);
+    A.q_pos = reinterpret_cast<uint32_t*>(aux + off_q);
+    A.n_anchors = (uint32_t)n;
+    memcpy(A.sub, params->sub, sizeof(A.sub));
+    A.ambig = params->ambig;
+    A.goe = goe;
+    A.ge = ge;
+    A.ydrop = gp->y_drop;
+    A.radius = radius;
+    A.ctr = reinterpret_cast<unsigned long long*>(aux + off_ctr);
+    A.sides = reinterpret_cast<GapSide*>(aux + off_side);
+    gxy_gapped_aln* d_aln = reinterpret_cast<gxy_gapped_aln*>(aux + off_aln);
+    uint32_t* d_cnt = reinterpret_cast<uint32_t*>(aux + off_cnt);
+    uint32_t* d_offs = reinterpret_cast<uint32_t*>(aux + off_offs);
+    e = cudaMemcpyAsync(aux + off_t, t_pos, n * 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(aux + off_q, q_pos, n * 4, cudaMemcpyHostToDevice, st);
+    // The traceback pool: a chain of blocks per warp, kept across its tasks.
+    A.block_words = (uint32_t)(kHdr + kRows + kRows * 32 * (S / 8));
+    const int warps = max_warps(S, ctx->sm_count);
+    uint64_t want_blocks = std::max<uint64_t>((uint64_t)warps * 4, W->gpool.bytes / ((uint64_t)A.block_words * 4));
+    uint64_t want_runs = std::max<uint64_t>(n * 256, W->gruns.bytes / 4);
+    cudaEvent_t e0 = W->ev[0], e1 = W->ev[2];
+    unsigned long long ctr[kCtrWords] = {};
+    uint32_t reruns = 0;
+    for (int attempt = 0; e == cudaSuccess; attempt++) {
+        e = W->gpool.ensure(want_blocks * A.block_words * 4);
+        if (e == cudaSuccess) e = W->gruns.ensure(want_runs * 4);
+        if (e != cudaSuccess) break;
+        A.pool = W->gpool.as<uint32_t>();
+        A.pool_blocks = W->gpool.bytes / ((uint64_t)A.block_words * 4);
+        A.runs = W->gruns.as<uint32_t>();
+        A.runs_cap = W->gruns.bytes / 4;
+        e = cudaMemsetAsync(A.ctr, 0, kCtrWords * 8, st);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+        if (e == cudaSuccess) e = launch_sides_for(S, A, ctx->sm_count, st);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ctr, A.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) break;
+        if (ctr[kCtrFlags] & kFlagState) {
+            gxy_gapped_result_free(out);
+            return fail(GXY_ECUDA, "gapped extension: inconsistent traceback state");
+        }
+        if (!(ctr[kCtrFlags] & (kFlagPool | kFlagRuns))) break;
+        if (attempt >= 3) {
+            gxy_gapped_result_free(out);
+            return fail(GXY_ENOMEM, "gapped extension: traceback storage still short after growing it");
+        }
+        // Grow what ran out to what was asked for, with a margin, and run again.
+        if (ctr[kCtrFlags] & kFlagPool) want_blocks = std::max<uint64_t>(want_blocks * 2, ctr[kCtrBlocks] * 5 / 4 + 64);
+        if (ctr[kCtrFlags] & kFlagRuns) want_runs = std::max<uint64_t>(want_runs * 2, ctr[kCtrRuns] * 5 / 4 + 1024);
+        reruns++;
+    }
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    uint32_t total_runs = 0;
+    if (e == cudaSuccess) {
+        count_launch();
+        k_gapped_join<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A, gp->gapped_threshold, d_aln, d_cnt);
+        scan_u32(d_cnt, d_offs, nullptr, n, n, true, nullptr, W->ps, st);
+        e = cudaMemcpyAsync(&total_runs, d_offs + n, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out->alns, d_aln, n * sizeof(gxy_gapped_aln), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    uint32_t* d_final = nullptr;
+    if (e == cudaSuccess && total_runs) {
+        out->runs = (uint32_t*)malloc((size_t)total_runs * 4);
+        if (!out->runs) {
+            gxy_gapped_result_free(out);
+            return fail(GXY_ENOMEM, "host allocation");
+        }
+        e = cudaMallocAsync((void**)&d_final, (size_t)total_runs * 4, st);
+        if (e == cudaSuccess) {
+            const uint64_t blocks = std::min<uint64_t>((n + 7) / 8, (uint64_t)ctx->sm_count * 16);
+            count_launch();
+            k_gapped_emit<<<(unsigned)blocks, 256, 0, st>>>(A, d_aln, d_offs, d_final);
+            e = cudaMemcpyAsync(out->runs, d_final, (size_t)total_runs * 4, cudaMemcpyDeviceToHost, st);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (d_final) cudaFreeAsync(d_final, st);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        gxy_gapped_result_free(out);
+        return fail(e == cudaErrorMemoryAllocation ? GXY_ENOMEM : GXY_ECUDA,
+                    std::string("gapped extension: ") + cudaGetErrorString(e));
+    }
+    out->n_runs = total_runs;
+    // Offsets of the passing anchors' scripts: the scan's output, on the host.
+    uint64_t acc = 0;
+    for (uint64_t k = 0; k < n; k++) {
+        out->alns[k].script_off = acc;
+        acc += out->alns[k].script_len;
+    }
+    if (stats) {
+        stats->rows = ctr[kCtrRows];
+        stats->cells = ctr[kCtrCells];
+        stats->device_ms = ms;
+        stats->reruns = reruns;
+        stats->band_cells_per_lane = (uint32_t)S;
+    }
+    return GXY_OK;
+}
+
+void gxy_gapped_result_free(gxy_gapped_result* r) {
+    if (!r) return;
+    free(r->alns);
+    free(r->runs);
+    r->alns = nullptr;
+    r->runs = nullptr;
+    r->n_alns = r->n_runs = 0;
+}
+
+}  // extern "C"

@@ -758,8 +758,10 @@ uint64_t orc_best_chain(const orc_hsp* hsps, uint64_t n, orc_hsp* out) {
 /* anchor and, on reversed inputs, to its left; the traceback's edit script */
 /* (src/edit_script.rs:47-104: run-length runs, push merges equal ops).     */
 /* Rows are allocated as the DP reaches them instead of (n+1) rows up front */
-/* (:236-243); every row starts as NEG_INF / State::M like the reference's  */
-/* preallocated storage, so the values read are the same.                   */
+/* (:236-243), and the scores of only the previous and the current row are */
+/* kept (the recurrences and the prune read no others); every row starts as */
+/* NEG_INF / State::M like the reference's preallocated storage, so the    */
+/* values read are the same.  The back-pointers are kept for every row.    */
 /* ------------------------------------------------------------------------ */
 #define G_NEG_INF (INT32_MIN / 4)   /* src/gapped_extend.rs:44 */
 enum { G_M = 0, G_X = 1, G_Y = 2 };  /* State (:46-51) */
@@ -817,40 +819,38 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
     }
     int64_t bw = 4 * radius + 4;
     if (bw > m + 1) bw = m + 1;
-    /* Rows grow on demand; row_lo, mm/xx/yy and the from-states per row. */
+    /* Back-pointer rows grow on demand; scores: rows i & 1 (two rows). */
     int64_t rows_cap = 0;
     int64_t* row_lo = NULL;
-    int32_t *mm = NULL, *xx = NULL, *yy = NULL;
+    int32_t* mm = (int32_t*)malloc((size_t)(2 * bw) * 4);
+    int32_t* xx = (int32_t*)malloc((size_t)(2 * bw) * 4);
+    int32_t* yy = (int32_t*)malloc((size_t)(2 * bw) * 4);
     uint8_t *mf = NULL, *xf = NULL, *yf = NULL;
     int rc = 0;
+    if (!mm || !xx || !yy) {
+        rc = -1;
+        goto done;
+    }
 #define G_GROW(i)                                                                                      \
     if ((i) >= rows_cap) {                                                                             \
         int64_t nc = rows_cap ? rows_cap * 2 : 64;                                                     \
         if (nc > n + 1) nc = n + 1;                                                                    \
         int64_t* a = (int64_t*)realloc(row_lo, (size_t)nc * 8);                                        \
         if (a) row_lo = a;                                                                             \
-        int32_t* b1 = (int32_t*)realloc(mm, (size_t)(nc * bw) * 4);                                    \
-        if (b1) mm = b1;                                                                               \
-        int32_t* b2 = (int32_t*)realloc(xx, (size_t)(nc * bw) * 4);                                    \
-        if (b2) xx = b2;                                                                               \
-        int32_t* b3 = (int32_t*)realloc(yy, (size_t)(nc * bw) * 4);                                    \
-        if (b3) yy = b3;                                                                               \
         uint8_t* c1 = (uint8_t*)realloc(mf, (size_t)(nc * bw));                                        \
         if (c1) mf = c1;                                                                               \
         uint8_t* c2 = (uint8_t*)realloc(xf, (size_t)(nc * bw));                                        \
         if (c2) xf = c2;                                                                               \
         uint8_t* c3 = (uint8_t*)realloc(yf, (size_t)(nc * bw));                                        \
         if (c3) yf = c3;                                                                               \
-        if (!a || !b1 || !b2 || !b3 || !c1 || !c2 || !c3) {                                            \
+        if (!a || !c1 || !c2 || !c3) {                                                                 \
             rc = -1;                                                                                   \
             goto done;                                                                                 \
         }                                                                                              \
-        for (int64_t k = rows_cap * bw; k < nc * bw; k++) {                                           \
-            mm[k] = xx[k] = yy[k] = G_NEG_INF;                                                         \
-            mf[k] = xf[k] = yf[k] = G_M;                                                               \
-        }                                                                                              \
+        for (int64_t k = rows_cap * bw; k < nc * bw; k++) mf[k] = xf[k] = yf[k] = G_M;                 \
         rows_cap = nc;                                                                                 \
     }
+    for (int64_t k = 0; k < 2 * bw; k++) mm[k] = xx[k] = yy[k] = G_NEG_INF;
     G_GROW(0);
     mm[0] = 0;
     int32_t best_score = 0;
@@ -860,6 +860,8 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
     row_lo[0] = 0;
     for (int64_t i = 0; i <= n; i++) {
         G_GROW(i);
+        if (i >= 2)   /* row i's score storage was row i-2's: back to NEG_INF, as a fresh row */
+            for (int64_t k = (i & 1) * bw; k < (i & 1) * bw + bw; k++) mm[k] = xx[k] = yy[k] = G_NEG_INF;
         const int64_t j_lo = lo > radius ? lo - radius : 0;
         int64_t j_hi = hi + radius;
         if (j_hi > m) j_hi = m;
@@ -868,7 +870,8 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
         const int64_t lo_this = j_lo;
         const int64_t lo_prev = i >= 1 ? row_lo[i - 1] : 0;
         const int64_t hi_prev_excl = lo_prev + bw;
-        const int64_t base_this = i * bw, base_prev = i >= 1 ? (i - 1) * bw : 0;
+        const int64_t base_this = (i & 1) * bw, base_prev = i >= 1 ? ((i - 1) & 1) * bw : 0;
+        const int64_t tb_this = i * bw;   /* back-pointers of row i */
         for (int64_t j = j_lo; j <= j_hi; j++) {
             if (i == 0 && j == 0) continue;
             int32_t best = G_NEG_INF;
@@ -883,7 +886,7 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
                 const int32_t fm = pm - goe, fx = px - ge;
                 const int32_t v = fm >= fx ? fm : fx;
                 xx[here] = v;
-                xf[here] = fm >= fx ? G_M : G_X;
+                xf[tb_this + (j - lo_this)] = fm >= fx ? G_M : G_X;
                 if (v > best) best = v;
             }
             if (j >= 1) {   /* Y: gap in target (:305-327) */
@@ -896,7 +899,7 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
                 const int32_t fm = pm - goe, fy = py - ge;
                 const int32_t v = fm >= fy ? fm : fy;
                 yy[here] = v;
-                yf[here] = fm >= fy ? G_M : G_Y;
+                yf[tb_this + (j - lo_this)] = fm >= fy ? G_M : G_Y;
                 if (v > best) best = v;
             }
             if (i >= 1 && j >= 1) {   /* M (:330-350) */
@@ -922,7 +925,7 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
                 }
                 const int32_t v = prev + s;
                 mm[here] = v;
-                mf[here] = from;
+                mf[tb_this + (j - lo_this)] = from;
                 if (v > best) best = v;
             }
             if (best > best_score) {   /* :353-363 */
@@ -936,7 +939,7 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
         const int32_t threshold = sat_sub(best_score, ydrop);
         int64_t new_lo = -1, new_hi = 0;
         for (int64_t j = j_lo; j <= j_hi; j++) {
-            const int64_t here = i * bw + (j - row_lo[i]);
+            const int64_t here = base_this + (j - row_lo[i]);
             int32_t alive = mm[here] > xx[here] ? mm[here] : xx[here];
             if (yy[here] > alive) alive = yy[here];
             if (alive >= threshold) {

@@ -1,0 +1,182 @@
+"""Gapped extension on the device (src/gapped_extend.rs:78-460) against the
+oracle: the reference's own cases, random small cases over the band and gap
+parameters (N's, anchors at the sequence ends, one-sided extensions), and
+every anchor of real searches over planted homologous segments with indels,
+in a whole target and in a chunk of it.  Equality is exact: score,
+coordinates and every run of the edit script."""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import rand_ascii
+
+pytestmark = pytest.mark.gpu
+P12 = "1110100110010101111"
+
+
+def orc_result(a):
+    if a is None:
+        return None
+    return (a["t_start"], a["q_start"], a["t_len"], a["q_len"], a["score"], list(a["runs"]))
+
+
+def gpu_result(a):
+    if a is None:
+        return None
+    return (a.t_start, a.q_start, a.t_len, a.q_len, a.score, [int(r) for r in a.script])
+
+
+def both(gxy, ctx, t: bytes, q: bytes, anchors, go=400, ge=30, ydrop=9400, thr=3000, view=None, threads=8):
+    m = gxy.ScoringMatrix.hoxd70()
+    m.gap_open, m.gap_extend = go, ge
+    dT = gxy.PackedSeq.from_ascii(t).to_device(ctx)
+    dQ = gxy.PackedSeq.from_ascii(q).to_device(ctx)
+    st = {}
+    got = gxy.gapped_extend(dT, dQ, anchors, m, gxy.GappedParams(ydrop, thr), t_view=view, ctx=ctx, stats=st)
+    tt = t if view is None else t[view[0]:view[1]]
+    OT, OQ = O.pack_ascii(tt), O.pack_ascii(q)
+    a = np.asarray(anchors, np.int64).reshape(-1, 2)
+    want = O.gapped_extend_many(OT, OQ, O.params(), O.gapped_params(go, ge, ydrop, thr), a[:, 0], a[:, 1],
+                                threads=threads)
+    return [gpu_result(x) for x in got], [orc_result(x) for x in want], st
+
+
+def test_gapped_known_answers(gxy, ctx):
+    # src/gapped_extend.rs:478-600, anchors = HSP start + offset.
+    cases = [
+        (b"ACGTACGTACGTACGT", b"ACGTACGTACGTACGT", 8, 8, 500, 100),
+        (b"ACGTACGTACGT", b"ACGTACGGTACGT", 3, 3, 1000, 100),
+        (b"ACGTACGGTACGT", b"ACGTACGTACGT", 3, 3, 1000, 100),
+        (b"ACGT", b"ACGT", 1, 1, 500, 100000),
+        (b"TTTTTTTTACGTACGTACGTACGTACGTACGTTTTTTTTT", b"AAAAAAAAACGTACGTACGTACGTACGTACGTAAAAAAAA", 20, 20, 300, 500),
+        (b"AAAGATTACACATGGCATGTCGATTTT", b"GATACACATGGCAGTCGA", 6, 3, 5000, 100),
+    ]
+    core = b"GATTACACATGGCATGTCGAATGCCTAGCATGTCA"
+    cases.append((core + core, core + b"AGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAG" + core, 5, 5, 9400, 500))
+    for t, q, tp, qp, yd, thr in cases:
+        g, w, _ = both(gxy, ctx, t, q, [(tp, qp)], ydrop=yd, thr=thr)
+        assert g == w, (t, q)
+    g, _, _ = both(gxy, ctx, b"ACGTACGTACGTACGT", b"ACGTACGTACGTACGT", [(8, 8)], ydrop=500, thr=100)
+    assert gxy.cigar(g[0][5]) == "16M"
+    g, _, _ = both(gxy, ctx, core + core, core + b"AGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAGCTAG" + core, [(5, 5)],
+                   ydrop=9400, thr=500)
+    assert g[0][2] >= 60 and g[0][3] >= 110 and "I" in gxy.cigar(g[0][5])
+
+
+def _mutate(rng, s: bytes, nedits: int) -> bytes:
+    q = bytearray(s)
+    for _ in range(nedits):
+        if not q:
+            break
+        k = int(rng.integers(0, len(q)))
+        r = rng.integers(3)
+        if r == 0:
+            q[k:k] = rand_ascii(rng, int(rng.integers(1, 12)), b"ACGT")
+        elif r == 1:
+            del q[k:k + int(rng.integers(1, 12))]
+        else:
+            q[k] = b"ACGTN"[rng.integers(5)]
+    return bytes(q) or b"A"
+
+
+@pytest.mark.parametrize("go,ge,ydrop", [(400, 30, 9400), (400, 30, 300), (400, 30, 1500), (0, 30, 700),
+                                         (400, 0, 500), (50, 5, 2000), (400, 30, 0)])
+def test_gapped_random_small(gxy, ctx, go, ge, ydrop):
+    # Short sequences (bands as wide as the query, m + 1 cells), anchors
+    # anywhere including both ends, N's and soft-masked bases.
+    rng = np.random.default_rng(1000 + go + ge + ydrop)
+    for case in range(8):
+        n = int(rng.integers(1, 400))
+        t = rand_ascii(rng, n, b"ACGTACGTacgtN")
+        q = _mutate(rng, t, int(rng.integers(0, 12)))
+        anchors = [(int(rng.integers(0, len(t))), int(rng.integers(0, len(q)))) for _ in range(24)]
+        anchors += [(0, 0), (len(t) - 1, len(q) - 1), (0, len(q) - 1), (len(t) - 1, 0)]
+        g, w, _ = both(gxy, ctx, t, q, anchors, go, ge, ydrop, thr=-10 ** 6)
+        assert g == w, case
+
+
+def planted(rng, n: int, segs: int, seg_len=(300, 3000), identity=(0.78, 0.95)):
+    """A random target and query sharing `segs` diverged segments (substitutions
+    and indels, half of them reverse-complemented), elsewhere unrelated."""
+    from lastz_gxy_b200 import synth
+    t = np.frombuffer(rand_ascii(rng, n, b"ACGT"), np.uint8).copy()
+    q = np.frombuffer(rand_ascii(rng, n, b"ACGT"), np.uint8).copy()
+    for _ in range(segs):
+        ln = int(rng.integers(*seg_len))
+        a = int(rng.integers(0, n - ln))
+        b = int(rng.integers(0, n - ln))
+        ev = synth.evolve(rng, t[a:a + ln].copy(), float(rng.uniform(*identity)), 0.01)[:ln]
+        if rng.random() < 0.5:   # half of them on the minus strand
+            ev = np.frombuffer(ev.tobytes().translate(bytes.maketrans(b"ACGT", b"TGCA"))[::-1], np.uint8)
+        q[b:b + len(ev)] = ev
+    low = rng.random(n) < 0.05
+    t[low] = np.where((t[low] >= 65) & (t[low] <= 90), t[low] + 32, t[low])
+    q[rng.random(n) < 0.002] = ord("N")
+    return t.tobytes(), q.tobytes()
+
+
+def search_anchors(gxy, ctx, t: bytes, q: bytes, view=None):
+    tt = t if view is None else t[view[0]:view[1]]
+    T, Q = gxy.PackedSeq.from_ascii(tt), gxy.PackedSeq.from_ascii(q)
+    m = gxy.ScoringMatrix.hoxd70()
+    tab = gxy.PosTable.build(T, P12, 1, ctx=ctx)
+    hsps = gxy.search(tab, T, Q, m, gxy.SearchParams(1, gxy.HspParams(910, 2000), 1))
+    dT, dQ = T.to_device(ctx), Q.to_device(ctx)
+    return gxy.choose_anchors(dT, dQ, hsps, m, 31, ctx), hsps
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_gapped_on_search_anchors(gxy, ctx, seed):
+    # The driver's step: HSPs -> choose_anchor -> extend, every anchor
+    # (src/driver.rs:395-414), both strands of the query.
+    rng = np.random.default_rng(70 + seed)
+    t, q = planted(rng, 60000, 14)
+    rc = q.translate(bytes.maketrans(b"ACGTacgtN", b"TGCAtgcaN"))[::-1]
+    for qq in (q, rc):
+        anchors, hsps = search_anchors(gxy, ctx, t, qq)
+        assert len(anchors) > 10
+        g, w, st = both(gxy, ctx, t, qq, anchors)
+        assert g == w
+        assert sum(x is not None for x in g) > 5
+        assert st["rows"] > 0 and st["cells"] >= st["rows"]
+
+
+def test_gapped_in_a_chunk_view(gxy, ctx):
+    # Extension bounded by a chunk of the target (the driver extends against
+    # chunk.seq, src/driver.rs:299-310): anchors in chunk coordinates.
+    rng = np.random.default_rng(91)
+    t, q = planted(rng, 80000, 16)
+    view = (17000, 61000)
+    anchors, _ = search_anchors(gxy, ctx, t, q, view)
+    assert len(anchors) > 5
+    g, w, _ = both(gxy, ctx, t, q, anchors, view=view)
+    assert g == w
+
+
+def test_gapped_long_alignment(gxy, ctx):
+    # One 40 kbp homologous stretch: a side of thousands of rows (a deep chain
+    # of traceback blocks) and a long edit script.
+    from lastz_gxy_b200 import synth
+    rng = np.random.default_rng(5)
+    t = np.frombuffer(rand_ascii(rng, 40000, b"ACGT"), np.uint8).copy()
+    q = synth.evolve(rng, t.copy(), 0.9, 0.005)
+    t, q = t.tobytes(), q.tobytes()
+    anchors, hsps = search_anchors(gxy, ctx, t, q)
+    top = np.argsort(-hsps["score"], kind="stable")[:3]
+    g, w, st = both(gxy, ctx, t, q, anchors[top], thr=0)
+    assert g == w
+    assert max(x[2] for x in g if x) > 20000
+
+
+def test_gapped_rejects(gxy, ctx):
+    dT = gxy.PackedSeq.from_ascii(b"ACGTACGTAC").to_device(ctx)
+    m = gxy.ScoringMatrix.hoxd70()
+    with pytest.raises(gxy.GxyError):   # anchor outside the target
+        gxy.gapped_extend(dT, dT, [(10, 0)], m, gxy.GappedParams(), ctx=ctx)
+    big = gxy.PackedSeq.from_ascii(b"ACGT" * 2000).to_device(ctx)
+    m2 = gxy.ScoringMatrix.hoxd70()
+    m2.gap_extend = 1   # band of 4 * 9000 cells: wider than the device DP holds
+    with pytest.raises(gxy.GxyError) as e:
+        gxy.gapped_extend(big, big, [(10, 10)], m2, gxy.GappedParams(), ctx=ctx)
+    assert e.value.status == 3
+    assert gxy.gapped_extend(dT, dT, np.zeros((0, 2), np.uint32), m, gxy.GappedParams(), ctx=ctx) == []
