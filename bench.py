@@ -933,12 +933,42 @@ def run_gapped(args):
         "device_ms": round(dev_s * 1e3, 3), "call_ms": round(wall * 1e3, 3),
         "cells_per_s": round(cells / dev_s, 1), "anchors_per_s": round(len(A) / wall, 1),
         "band_cells_per_lane": st["band_cells_per_lane"], "reruns": st["reruns"],
+        "max_side_rows": st["max_side_rows"], "second_pass_sides": st["second_pass_sides"],
+        "us_per_row_of_longest_side": round(dev_s * 1e6 / max(1, st["max_side_rows"]), 3),
         "cpu_baseline": {"kind": "port", "all_cores": {"cores": host_threads(), "anchors": int(k), "s": round(t_all, 3),
                                                        "cells_per_s": round(cells_all / t_all, 1)},
                          "one_core": {"cores": 1, "anchors": int(len(one)), "s": round(t_one, 3),
                                       "cells_per_s": round(cells_one / t_one, 1)}},
         "same_as_oracle_on_sample": same,
     }
+
+
+def run_gapped_case(args):
+    """One long gapped extension, the small case the ncu captures use: a
+    --length bp iid target and its 90%-identity copy (0.5% indels); the
+    anchors of the three highest-scoring plus-strand HSPs."""
+    import numpy as np
+    g = _pkg()
+    from lastz_gxy_b200 import synth
+    rng = np.random.default_rng(5)
+    t = synth.iid(rng, args.length, 0.41)
+    q = synth.evolve(rng, t.copy(), 0.9, 0.005)
+    ctx = g.Context(0)
+    m = g.ScoringMatrix.hoxd70()
+    dT = g.PackedSeq.from_ascii(t.tobytes()).to_device(ctx)
+    dQ = g.PackedSeq.from_ascii(q.tobytes()).to_device(ctx)
+    tab = g.PosTable.build(dT, P12, 1, ctx=ctx)
+    hsps = g.search_device(tab, dQ, m, g.SearchParams())
+    anchors = g.choose_anchors(dT, dQ, hsps, m, 31, ctx)
+    A = np.ascontiguousarray(anchors[np.argsort(-hsps["score"], kind="stable")[:3]])
+    out = []
+    for _ in range(max(1, args.steps)):
+        st = {}
+        res = g.gapped_extend(dT, dQ, A, m, g.GappedParams(), ctx=ctx, stats=st)
+        out.append({"device_ms": round(st["device_ms"], 3), "rows": st["rows"], "max_side_rows": st["max_side_rows"],
+                    "us_per_row_of_longest_side": round(st["device_ms"] * 1e3 / max(1, st["max_side_rows"]), 3),
+                    "passed": sum(r is not None for r in res)})
+    return {"workload": f"gapped case {args.length} bp", "runs": out}
 
 
 def run_case(args):
@@ -969,7 +999,7 @@ def main():
     ap.add_argument("--plain-only", action="store_true",
                     help="default workload: skip the batched and served legs of the line")
     ap.add_argument("--workload", default="plain",
-                    choices=["plain", "batched", "served", "chunked", "case", "input", "gapped"])
+                    choices=["plain", "batched", "served", "chunked", "case", "input", "gapped", "gapped_case"])
     ap.add_argument("--anchors", type=int, default=1024, help="gapped workload: anchors extended per call")
     ap.add_argument("--gapped-sample", type=int, default=32, help="gapped workload: anchors the oracle extends")
     ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
@@ -1006,6 +1036,9 @@ def main():
         return
     if args.workload == "gapped":
         print(json.dumps(run_gapped(args)), flush=True)
+        return
+    if args.workload == "gapped_case":
+        print(json.dumps(run_gapped_case(args)), flush=True)
         return
     if world > 1:
         import datetime

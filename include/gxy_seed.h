@@ -141,6 +141,9 @@ typedef struct {
                                      passed on unexamined (a multiple of 32, 32..256) */
     uint32_t filter_claim;        /* upper-bound filter: raw hits a warp claims at a time (32..4096;
                                      1 = sized from each launch's hit count, the default) */
+    uint32_t gapped_pool_blocks;  /* gapped extension: traceback blocks the first pass may use at most
+                                     (0 = no limit: sized by the library); sides that do not fit run
+                                     again in an exactly sized second pass */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
@@ -413,8 +416,10 @@ typedef struct {
     uint64_t rows;                 /* DP rows computed over all sides */
     uint64_t cells;                /* DP cells computed (the band's width summed over the rows) */
     double device_ms;              /* CUDA-event time of the DP kernel (last run) */
-    uint32_t reruns;               /* runs repeated after the traceback storage had to grow */
+    uint32_t reruns;               /* first passes repeated after the run buffer had to grow */
     uint32_t band_cells_per_lane;  /* cells of a row one lane of the DP warp holds */
+    uint64_t max_side_rows;        /* rows of the longest side (sides run in parallel; rows are sequential) */
+    uint64_t second_pass_sides;    /* sides run again with exactly sized traceback storage */
 } gxy_gapped_stats;
 
 /* extend (src/gapped_extend.rs:78-132) for n anchors (t_pos[i], q_pos[i]) on

@@ -61,9 +61,11 @@ class Context:
         return cls._default[device]
 
     def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0,
-                   max_hits_per_pass=0, initial_candidates=0, filter_cap=0, filter_claim=0) -> None:
+                   max_hits_per_pass=0, initial_candidates=0, filter_cap=0, filter_claim=0,
+                   gapped_pool_blocks=0) -> None:
+        """Zero leaves a field unchanged; gapped_pool_blocks 0xffffffff lifts its limit."""
         t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass,
-                         initial_candidates, filter_cap, filter_claim)
+                         initial_candidates, filter_cap, filter_claim, gapped_pool_blocks)
         check(lib().gxy_ctx_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -72,7 +74,8 @@ class Context:
         return {"screen_warps": t.screen_warps, "screen_cap": t.screen_cap,
                 "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps,
                 "max_hits_per_pass": t.max_hits_per_pass, "initial_candidates": t.initial_candidates,
-                "filter_cap": t.filter_cap, "filter_claim": t.filter_claim}
+                "filter_cap": t.filter_cap, "filter_claim": t.filter_claim,
+                "gapped_pool_blocks": t.gapped_pool_blocks}
 
     def mark(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's primary stream."""
@@ -690,7 +693,8 @@ def gapped_extend(target: DeviceSeq, query: DeviceSeq, anchors, matrix: ScoringM
         lib().gxy_gapped_result_free(C.byref(res))
     if stats is not None:
         stats.update(rows=st.rows, cells=st.cells, device_ms=st.device_ms, reruns=st.reruns,
-                     band_cells_per_lane=st.band_cells_per_lane)
+                     band_cells_per_lane=st.band_cells_per_lane, max_side_rows=st.max_side_rows,
+                     second_pass_sides=st.second_pass_sides)
     return out
 
 

@@ -374,6 +374,7 @@ gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
     if (t->filter_cap) ctx->tuning.filter_cap = std::min<uint32_t>(256, std::max<uint32_t>(32, t->filter_cap & ~31u));
     if (t->filter_claim)
         ctx->tuning.filter_claim = t->filter_claim == 1 ? 1u : std::min<uint32_t>(4096, std::max<uint32_t>(32, t->filter_claim));
+    if (t->gapped_pool_blocks) ctx->tuning.gapped_pool_blocks = t->gapped_pool_blocks == 0xffffffffu ? 0u : t->gapped_pool_blocks;
     return GXY_OK;
 }
 

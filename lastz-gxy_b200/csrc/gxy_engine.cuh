@@ -52,6 +52,7 @@ struct Worker {
     uint64_t surv_cap = 0;
     DevBuf redo;                  // the two lists of tiles a pass hands to the next one
     DevBuf gpool, gruns, gaux;    // gapped extension: traceback row blocks, side runs, per-anchor arrays
+    uint64_t gpool_want = 0;      // gapped extension: the traceback pool an earlier call would have needed
     cudaGraphExec_t gexec = nullptr;   // the last batched launch's graph, updated in place when it fits
     uint64_t graph_updates = 0;
     uint32_t cand_cap = 0;
@@ -167,7 +168,7 @@ struct gxy_ctx {
     // Screen column cap 192 (the packed screen's limit): on the 10 Mbp plain
     // launch, longer screening leaves fewer candidates for the walk to
     // re-extend (two searches 4.27 ms, against 4.31 ms at 128 and 4.51 at 64).
-    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 1};
+    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 1, 0};
     cudaEvent_t marks[16] = {};
 };
 

@@ -57,9 +57,11 @@ constexpr int kMaxS = 64;                     // cells per lane; band_width <= 3
 constexpr uint32_t kFlagPool = 1;    // the traceback pool ran out: rerun with a larger one
 constexpr uint32_t kFlagRuns = 2;    // the run buffer ran out: rerun with a larger one
 constexpr uint32_t kFlagState = 4;   // inconsistent back-pointers (a bug; reported as an error)
+constexpr uint32_t kSideRuns2 = 1u << 8;   // the side's runs are in the second run buffer
 
-// Counters (u64): task cursor, pool blocks claimed, run words reserved, rows, cells, flags.
-enum { kCtrTask = 0, kCtrBlocks, kCtrRuns, kCtrRows, kCtrCells, kCtrFlags, kCtrWords = 8 };
+// Counters (u64): task cursor, pool blocks claimed, run words reserved, rows,
+// cells, flags, the most rows of one side.
+enum { kCtrTask = 0, kCtrBlocks, kCtrRuns, kCtrRows, kCtrCells, kCtrFlags, kCtrMaxRows, kCtrWords = 8 };
 
 struct GapSide {
     int32_t score;
@@ -67,8 +69,8 @@ struct GapSide {
     uint32_t q_span;
     uint32_t n_runs;
     uint64_t run_off;
-    uint32_t flags;
-    uint32_t pad_;
+    uint32_t flags;   // kFlag* | kSideRuns2
+    uint32_t rows;    // DP rows computed
 };
 
 struct GapArgs {
@@ -85,10 +87,17 @@ struct GapArgs {
     uint32_t* pool;
     uint64_t pool_blocks;
     uint32_t block_words;
-    uint32_t* runs;
+    uint32_t* runs;       // where this pass's tracebacks write
     uint64_t runs_cap;
+    const uint32_t* runs2;   // the second pass's runs (for the join)
     unsigned long long* ctr;
     GapSide* sides;   // [2a] left, [2a + 1] right
+    // Second pass: only the listed sides, side list[k] with its rows in the
+    // pool blocks base[k], base[k] + 1, ... (no chains); runs go to the second
+    // run buffer.  list == nullptr: every side, blocks in per-warp chains.
+    const uint32_t* list;
+    const uint64_t* base;
+    uint64_t n_list;
 };
 
 __device__ __forceinline__ int32_t sat_sub32(int32_t a, int32_t b) {
@@ -154,7 +163,7 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
     // X of a cell whose upper neighbour is dead or outside the band.
     const int32_t nx_dead = max(kNegInf - goe, kNegInf - ge);
     const uint32_t nx_dead_from = (kNegInf - goe >= kNegInf - ge) ? 0u : 1u;
-    const uint64_t ntasks = 2ull * a.n_anchors;
+    const uint64_t ntasks = a.list ? a.n_list : 2ull * a.n_anchors;
     const int32_t lane_shift = S * ge;   // Y decays by this over one lane's cells
     constexpr int kWordsPerLane = S / 8;
     constexpr int kRowWords = 32 * kWordsPerLane;
@@ -165,6 +174,8 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
         if (lane == 0) task = atomicAdd(a.ctr + kCtrTask, 1ull);
         task = __shfl_sync(kFull, task, 0);
         if (task >= ntasks) break;
+        const uint64_t fixed_base = a.list ? a.base[task] : 0;
+        if (a.list) task = a.list[task];
         const uint32_t an = (uint32_t)(task >> 1);
         const bool right = task & 1;
         const int64_t dir = right ? 1 : -1;
@@ -189,6 +200,7 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
         // Walk of the chain while filling: the block holding the current row.
         uint32_t cur_blk = kNone;
         uint32_t blk_index = 0;        // its position in the chain
+        if (a.list) chain_len = 0;
         bool store = true;
         uint64_t rows = 0, cells = 0;
         int64_t i = 0;
@@ -363,7 +375,15 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
             if (store && (i % kRows) == 0) {
                 // Next block of the chain, claimed from the pool when the chain ends here.
                 uint32_t nb = kNone;
-                if (lane == 0) {
+                if (lane == 0 && a.list) {
+                    // Second pass: this side's blocks are consecutive.
+                    nb = (uint32_t)(fixed_base + (uint64_t)(i / kRows));
+                    uint32_t* hdr = a.pool + (uint64_t)nb * a.block_words;
+                    hdr[0] = i == 0 ? kNone : nb - 1;
+                    hdr[1] = nb + 1;
+                    hdr[2] = (uint32_t)i;
+                    if (i == 0) chain_head = nb;
+                } else if (lane == 0) {
                     if (blk_index < chain_len) {
                         nb = cur_blk == kNone ? chain_head : a.pool[(uint64_t)cur_blk * a.block_words + 1];
                     } else {
@@ -388,7 +408,7 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                 chain_len = __shfl_sync(kFull, chain_len, 0);
                 if (nb == kNone) {
                     store = false;
-                    flags |= kFlagPool;
+                    flags |= kFlagPool;   // the DP goes on: score, best cell and rows stay exact
                 } else {
                     cur_blk = nb;
                     blk_index++;
@@ -443,6 +463,7 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
             const uint64_t cap = (uint64_t)(bi + bj);
             uint64_t off = 0;
             if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
+            if (a.list) flags |= kSideRuns2;
             if (off + cap > a.runs_cap) {
                 flags |= kFlagRuns;
             } else {
@@ -521,14 +542,20 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
         res.run_off = __shfl_sync(kFull, res.run_off, 0);
         res.n_runs = __shfl_sync(kFull, res.n_runs, 0);
         res.flags = flags;
+        res.rows = (uint32_t)rows;
         if (lane == 0) {
             a.sides[task] = res;
             atomicAdd(a.ctr + kCtrRows, (unsigned long long)rows);
             atomicAdd(a.ctr + kCtrCells, (unsigned long long)cells);
+            atomicMax(a.ctr + kCtrMaxRows, (unsigned long long)rows);
             if (flags) atomicOr(a.ctr + kCtrFlags, (unsigned long long)flags);
         }
         __syncwarp();
     }
+}
+
+__device__ __forceinline__ const uint32_t* side_runs(const GapArgs& a, const GapSide& s) {
+    return ((s.flags & kSideRuns2) ? a.runs2 : a.runs) + s.run_off;
 }
 
 // Per anchor: the total, the verdict, the joined run count.
@@ -550,8 +577,9 @@ __global__ void k_gapped_join(GapArgs a, int32_t threshold, gxy_gapped_aln* out,
         o.q_start = q0 - L.q_span;
         o.t_len = L.t_span + 1 + R.t_span;
         o.q_len = L.q_span + 1 + R.q_span;
-        const uint32_t lm = L.n_runs && (a.runs[L.run_off + L.n_runs - 1] & 3u) == 0;
-        const uint32_t rm = R.n_runs && (a.runs[R.run_off + R.n_runs - 1] & 3u) == 0;
+        const uint32_t* lr = side_runs(a, L), * rr = side_runs(a, R);
+        const uint32_t lm = L.n_runs && (lr[L.n_runs - 1] & 3u) == 0;
+        const uint32_t rm = R.n_runs && (rr[R.n_runs - 1] & 3u) == 0;
         cnt = L.n_runs + R.n_runs + 1 - lm - rm;
     }
     o.script_len = cnt;
@@ -566,8 +594,8 @@ __global__ void k_gapped_emit(GapArgs a, const gxy_gapped_aln* alns, const uint3
     for (uint64_t an = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); an < a.n_anchors; an += nw) {
         if (!alns[an].passed) continue;
         const GapSide L = a.sides[2 * an], R = a.sides[2 * an + 1];
-        const uint32_t* lr = a.runs + L.run_off;
-        const uint32_t* rr = a.runs + R.run_off;
+        const uint32_t* lr = side_runs(a, L);
+        const uint32_t* rr = side_runs(a, R);
         const uint32_t lm = L.n_runs && (lr[L.n_runs - 1] & 3u) == 0;
         const uint32_t rm = R.n_runs && (rr[R.n_runs - 1] & 3u) == 0;
         const uint32_t nl = L.n_runs - lm, nr = R.n_runs - rm;
@@ -719,20 +747,43 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     uint32_t* d_offs = reinterpret_cast<uint32_t*>(aux + off_offs);
     e = cudaMemcpyAsync(aux + off_t, t_pos, n * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(aux + off_q, q_pos, n * 4, cudaMemcpyHostToDevice, st);
-    // The traceback pool: a chain of blocks per warp, kept across its tasks.
+    // Pass 1: every side, back-pointers in per-warp chains of pool blocks.
+    // The pool is sized for 64 blocks per warp and grows toward what earlier
+    // calls needed, within a quarter of the free device memory.
     A.block_words = (uint32_t)(kHdr + kRows + kRows * 32 * (S / 8));
+    const uint64_t block_bytes = (uint64_t)A.block_words * 4;
     const int warps = max_warps(S, ctx->sm_count);
-    uint64_t want_blocks = std::max<uint64_t>((uint64_t)warps * 4, W->gpool.bytes / ((uint64_t)A.block_words * 4));
-    uint64_t want_runs = std::max<uint64_t>(n * 256, W->gruns.bytes / 4);
+    size_t free_b = 0, total_b = 0;
+    uint32_t pool_limit = 0;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        pool_limit = ctx->tuning.gapped_pool_blocks;
+    }
+    uint64_t want_pool = std::max<uint64_t>((uint64_t)warps * 64 * block_bytes, W->gpool_want);
+    if (want_pool > W->gpool.bytes) {   // growing: at most a quarter of the free memory
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+        const uint64_t pool_cap = std::max<uint64_t>((uint64_t)warps * 4 * block_bytes, free_b / 4);
+        want_pool = std::max<uint64_t>(std::min(want_pool, pool_cap), W->gpool.bytes);
+    } else {
+        want_pool = W->gpool.bytes;
+    }
+    // Runs: a side reserves best_i + best_j words (its longest possible
+    // script); the sides that stored their rows have at most the pool's rows.
+    uint64_t want_runs = std::max<uint64_t>({n * 512, W->gruns.bytes / 4, want_pool / block_bytes * kRows * 2});
     cudaEvent_t e0 = W->ev[0], e1 = W->ev[2];
     unsigned long long ctr[kCtrWords] = {};
     uint32_t reruns = 0;
+    A.list = nullptr;
+    A.base = nullptr;
+    A.n_list = 0;
+    A.runs2 = nullptr;
     for (int attempt = 0; e == cudaSuccess; attempt++) {
-        e = W->gpool.ensure(want_blocks * A.block_words * 4);
+        e = W->gpool.ensure(want_pool);
         if (e == cudaSuccess) e = W->gruns.ensure(want_runs * 4);
         if (e != cudaSuccess) break;
         A.pool = W->gpool.as<uint32_t>();
-        A.pool_blocks = W->gpool.bytes / ((uint64_t)A.block_words * 4);
+        A.pool_blocks = W->gpool.bytes / block_bytes;
+        if (pool_limit) A.pool_blocks = std::min<uint64_t>(A.pool_blocks, pool_limit);
         A.runs = W->gruns.as<uint32_t>();
         A.runs_cap = W->gruns.bytes / 4;
         e = cudaMemsetAsync(A.ctr, 0, kCtrWords * 8, st);
@@ -742,22 +793,103 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         if (e == cudaSuccess) e = cudaMemcpyAsync(ctr, A.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) break;
-        if (ctr[kCtrFlags] & kFlagState) {
-            gxy_gapped_result_free(out);
-            return fail(GXY_ECUDA, "gapped extension: inconsistent traceback state");
-        }
-        if (!(ctr[kCtrFlags] & (kFlagPool | kFlagRuns))) break;
-        if (attempt >= 3) {
-            gxy_gapped_result_free(out);
-            return fail(GXY_ENOMEM, "gapped extension: traceback storage still short after growing it");
-        }
-        // Grow what ran out to what was asked for, with a margin, and run again.
-        if (ctr[kCtrFlags] & kFlagPool) want_blocks = std::max<uint64_t>(want_blocks * 2, ctr[kCtrBlocks] * 5 / 4 + 64);
-        if (ctr[kCtrFlags] & kFlagRuns) want_runs = std::max<uint64_t>(want_runs * 2, ctr[kCtrRuns] * 5 / 4 + 1024);
+        // Only a short run buffer reruns the whole pass (the pool's shortfall
+        // goes to pass 2): grow it to what the sides reserved.
+        if (!(ctr[kCtrFlags] & kFlagRuns) || attempt >= 2) break;
+        want_runs = std::max<uint64_t>(want_runs * 2, ctr[kCtrRuns] * 5 / 4 + 1024);
         reruns++;
     }
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess && (ctr[kCtrFlags] & kFlagState)) {
+        gxy_gapped_result_free(out);
+        return fail(GXY_ECUDA, "gapped extension: inconsistent traceback state");
+    }
+    // Pass 2: the sides pass 1 could not store, each with exactly the blocks
+    // its rows need (pass 1 counted them), in groups that fit half the free
+    // memory; their runs go to a second buffer of exactly their reservations.
+    uint32_t* d_pool2 = nullptr;
+    uint32_t* d_runs2 = nullptr;
+    void* d_list = nullptr;
+    uint64_t pass2_sides = 0;
+    if (e == cudaSuccess && (ctr[kCtrFlags] & (kFlagPool | kFlagRuns))) {
+        std::vector<GapSide> sides(2 * n);
+        e = cudaMemcpyAsync(sides.data(), A.sides, 2 * n * sizeof(GapSide), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        std::vector<uint32_t> list;
+        std::vector<uint64_t> need;
+        uint64_t runs2 = 0, max_need = 0, tot_need = 0;
+        for (uint64_t k = 0; e == cudaSuccess && k < 2 * n; k++) {
+            if (!(sides[k].flags & (kFlagPool | kFlagRuns))) continue;
+            list.push_back((uint32_t)k);
+            const uint64_t nb = ((uint64_t)sides[k].rows + kRows - 1) / kRows;
+            need.push_back(nb);
+            max_need = std::max(max_need, nb);
+            tot_need += nb;
+            runs2 += (uint64_t)sides[k].t_span + sides[k].q_span;
+        }
+        pass2_sides = list.size();
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+        const uint64_t budget = std::max<uint64_t>(max_need, free_b / 2 / block_bytes);
+        const uint64_t group_blocks = std::min<uint64_t>(budget, tot_need);
+        if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_runs2, std::max<uint64_t>(runs2, 1) * 4, st);
+        if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_pool2, group_blocks * block_bytes, st);
+        if (e == cudaSuccess) e = cudaMallocAsync(&d_list, list.size() * 16, st);
+        // Later calls start with a pass-1 pool closer to this need.
+        W->gpool_want = (A.pool_blocks + tot_need) * block_bytes;
+        GapArgs B = A;
+        B.pool = d_pool2;
+        B.runs = d_runs2;
+        B.runs_cap = std::max<uint64_t>(runs2, 1);
+        uint32_t* dl = reinterpret_cast<uint32_t*>(d_list);
+        uint64_t* dbase = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(d_list) + list.size() * 8);
+        std::vector<uint64_t> base(list.size());
+        std::vector<uint32_t> lst(list.begin(), list.end());
+        uint64_t k0 = 0;
+        unsigned long long c2[kCtrWords] = {};
+        bool first_group = true;
+        while (e == cudaSuccess && k0 < list.size()) {
+            uint64_t k1 = k0, used = 0;
+            while (k1 < list.size() && used + need[k1] <= group_blocks) {
+                base[k1] = used;
+                used += need[k1];
+                k1++;
+            }
+            B.list = dl + k0;
+            B.base = dbase + k0;
+            B.n_list = k1 - k0;
+            B.pool_blocks = group_blocks;
+            e = cudaMemcpyAsync(dl + k0, lst.data() + k0, (k1 - k0) * 4, cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(dbase + k0, base.data() + k0, (k1 - k0) * 8, cudaMemcpyHostToDevice, st);
+            // The task cursor restarts; the run counter keeps counting across groups.
+            if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrTask, 0, 8, st);
+            if (e == cudaSuccess && first_group) e = cudaMemsetAsync(B.ctr + kCtrRuns, 0, 8, st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrFlags, 0, 8, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+            if (e == cudaSuccess) e = launch_sides_for(S, B, ctx->sm_count, st);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(c2, B.ctr, sizeof(c2), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess && (c2[kCtrFlags] & (kFlagPool | kFlagRuns | kFlagState))) {
+                cudaFreeAsync(d_pool2, st);
+                cudaFreeAsync(d_runs2, st);
+                cudaFreeAsync(d_list, st);
+                cudaStreamSynchronize(st);
+                gxy_gapped_result_free(out);
+                return fail(GXY_ECUDA, "gapped extension: the exactly sized second pass fell short");
+            }
+            float gms = 0.f;
+            if (e == cudaSuccess) cudaEventElapsedTime(&gms, e0, e1);
+            ms += gms;
+            ctr[kCtrRows] += c2[kCtrRows];
+            ctr[kCtrCells] += c2[kCtrCells];
+            ctr[kCtrMaxRows] = std::max(ctr[kCtrMaxRows], c2[kCtrMaxRows]);
+            first_group = false;
+            k0 = k1;
+        }
+        A.runs2 = d_runs2;
+    }
     uint32_t total_runs = 0;
     if (e == cudaSuccess) {
         count_launch();
@@ -784,6 +916,10 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (d_final) cudaFreeAsync(d_final, st);
     }
+    if (d_pool2) cudaFreeAsync(d_pool2, st);
+    if (d_runs2) cudaFreeAsync(d_runs2, st);
+    if (d_list) cudaFreeAsync(d_list, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) {
         gxy_gapped_result_free(out);
@@ -802,7 +938,9 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         stats->cells = ctr[kCtrCells];
         stats->device_ms = ms;
         stats->reruns = reruns;
+        stats->second_pass_sides = pass2_sides;
         stats->band_cells_per_lane = (uint32_t)S;
+        stats->max_side_rows = ctr[kCtrMaxRows];
     }
     return GXY_OK;
 }

@@ -168,6 +168,23 @@ def test_gapped_long_alignment(gxy, ctx):
     assert max(x[2] for x in g if x) > 20000
 
 
+def test_gapped_second_pass(gxy):
+    # A first pass with room for only a few traceback blocks: the sides that
+    # ran out are extended again with exactly sized storage, and every result
+    # still equals the oracle's.
+    c = gxy.Context(0)
+    c.set_tuning(gapped_pool_blocks=40)
+    rng = np.random.default_rng(17)
+    t, q = planted(rng, 60000, 14)
+    anchors, _ = search_anchors(gxy, c, t, q)
+    g, w, st = both(gxy, c, t, q, anchors)
+    assert g == w
+    assert st["second_pass_sides"] > 0
+    c.set_tuning(gapped_pool_blocks=0xffffffff)
+    g2, _, st2 = both(gxy, c, t, q, anchors)
+    assert g2 == w and st2["second_pass_sides"] == 0
+
+
 def test_gapped_rejects(gxy, ctx):
     dT = gxy.PackedSeq.from_ascii(b"ACGTACGTAC").to_device(ctx)
     m = gxy.ScoringMatrix.hoxd70()
