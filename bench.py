@@ -932,7 +932,7 @@ def run_gapped(args):
         "anchors": len(A), "passed": sum(r is not None for r in res), "rows": st["rows"], "cells": cells,
         "device_ms": round(dev_s * 1e3, 3), "call_ms": round(wall * 1e3, 3),
         "cells_per_s": round(cells / dev_s, 1), "anchors_per_s": round(len(A) / wall, 1),
-        "band_cells_per_lane": st["band_cells_per_lane"], "reruns": st["reruns"],
+        "warps_per_side": st["warps_per_side"], "reruns": st["reruns"],
         "max_side_rows": st["max_side_rows"], "second_pass_sides": st["second_pass_sides"],
         "us_per_row_of_longest_side": round(dev_s * 1e6 / max(1, st["max_side_rows"]), 3),
         "cpu_baseline": {"kind": "port", "all_cores": {"cores": host_threads(), "anchors": int(k), "s": round(t_all, 3),

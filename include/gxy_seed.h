@@ -417,7 +417,7 @@ typedef struct {
     uint64_t cells;                /* DP cells computed (the band's width summed over the rows) */
     double device_ms;              /* CUDA-event time of the DP kernel (last run) */
     uint32_t reruns;               /* first passes repeated after the run buffer had to grow */
-    uint32_t band_cells_per_lane;  /* cells of a row one lane of the DP warp holds */
+    uint32_t warps_per_side;       /* warps of the block that runs one side (8 cells of a row a thread) */
     uint64_t max_side_rows;        /* rows of the longest side (sides run in parallel; rows are sequential) */
     uint64_t second_pass_sides;    /* sides run again with exactly sized traceback storage */
 } gxy_gapped_stats;

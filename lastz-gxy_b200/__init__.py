@@ -693,7 +693,7 @@ def gapped_extend(target: DeviceSeq, query: DeviceSeq, anchors, matrix: ScoringM
         lib().gxy_gapped_result_free(C.byref(res))
     if stats is not None:
         stats.update(rows=st.rows, cells=st.cells, device_ms=st.device_ms, reruns=st.reruns,
-                     band_cells_per_lane=st.band_cells_per_lane, max_side_rows=st.max_side_rows,
+                     warps_per_side=st.warps_per_side, max_side_rows=st.max_side_rows,
                      second_pass_sides=st.second_pass_sides)
     return out
 

@@ -124,7 +124,7 @@ class GappedResultC(C.Structure):
 
 class GappedStatsC(C.Structure):
     _fields_ = [("rows", C.c_uint64), ("cells", C.c_uint64), ("device_ms", C.c_double), ("reruns", C.c_uint32),
-                ("band_cells_per_lane", C.c_uint32), ("max_side_rows", C.c_uint64),
+                ("warps_per_side", C.c_uint32), ("max_side_rows", C.c_uint64),
                 ("second_pass_sides", C.c_uint64)]
 
 

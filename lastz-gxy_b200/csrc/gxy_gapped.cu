@@ -7,28 +7,33 @@
 // at band_width = min(4R + 4, m + 1) cells; after a row, the cells whose best
 // state is more than y_drop below the best score so far are killed.  These
 // rules (the band, the row-major first maximum, the kill) decide the result,
-// so the device keeps the row order.  One warp runs one side of one anchor:
+// so the device keeps the row order.  One block of W warps runs one side of
+// one anchor (W = band_width / 256 rounded up: 5 for HOXD70's defaults), so
+// a row costs each thread only 8 cells:
 //
-//  - Lane k owns S consecutive cells of the row (S = band_width / 32 rounded
-//    up to 8; 40 for HOXD70's defaults).  X and M of a cell need the previous
-//    row only, so a lane forms them for its cells first (phase A).
+//  - Thread k owns cells [8k, 8k + 8) of the row.  X and M of a cell need the
+//    previous row only, so a thread forms them for its cells first (phase A).
 //  - Y is a max-plus recurrence along the row, Y[j] = max(M[j-1] - (O+E),
-//    Y[j-1] - E).  Each lane reduces its cells to one affine-max function
-//    x -> max(a, x - S*E); a warp shuffle scan composes them, giving every
-//    lane the exact Y entering its cells (phase B then runs the recurrence
-//    from there).  The arithmetic is the reference's i32 arithmetic: max-plus
-//    composition is exact.
+//    Y[j-1] - E).  Each thread reduces its cells to one affine-max function
+//    x -> max(a, x - 8E); a warp shuffle scan composes them, and each warp
+//    folds in the warps before it through shared memory, giving every thread
+//    the exact Y entering its cells (phase B then runs the recurrence from
+//    there; the entering Y's source is M exactly when the M term reaches it).
+//    The arithmetic is the reference's i32 arithmetic: max-plus composition
+//    is exact.
 //  - The row lives in shared memory (best state H = max(M, X, Y) with its
 //    argmax, and the next row's X = max(M - (O+E), X - E) with its source),
-//    stored transposed (cell p at (p mod S) * 32 + p / S), so both the
+//    stored transposed (cell p at (p mod 8) * threads + p / 8), so both the
 //    current row's writes and the next row's reads, at any shift of the
-//    band, hit 32 distinct banks.  A cell killed by the x-drop rule is not
+//    band, hit distinct banks.  A cell killed by the x-drop rule is not
 //    rewritten: the next row compares its H with the row's threshold and
 //    reads NEG_INF in its place, as the reference's cleared cell reads.
-//  - The three back-pointers of a cell (4 bits) go to global memory, rows in
-//    blocks of kRows kept by the warp across its tasks (a chain it grows from
-//    a shared pool as its longest side needs).  After the last row, lane 0
-//    walks from the best cell to (0, 0) and writes the runs.
+//  - The three back-pointers of a cell (4 bits; one word per thread and row)
+//    go to global memory, rows in pool blocks of kRows kept by the CUDA block
+//    across its tasks (a chain it grows from a shared pool as its longest side
+//    needs).  After the last row, thread 0 walks from the best cell to (0, 0)
+//    and writes the runs.  Sides whose rows did not fit the pool run again
+//    with exactly sized storage.
 //
 // A last kernel joins the two sides per anchor: total = anchor column + left
 // best + right best (saturating), the left runs in walk order, the anchor's
@@ -47,11 +52,11 @@ namespace {
 
 constexpr int32_t kNegInf = INT32_MIN / 4;   // NEG_INF (src/gapped_extend.rs:44)
 constexpr int32_t kLow = INT32_MIN / 2;      // "no contribution" in the row scan: below every DP value
-constexpr int kGapWarps = 4;                  // warps per block
+constexpr int kCells = 8;                     // cells of a row per thread
+constexpr int kMaxW = 8;                      // warps per side; band_width <= 256 * kMaxW
 constexpr int kRows = 32;                     // DP rows per traceback block
 constexpr int kHdr = 4;                       // block header words: previous block, next block, first row, -
 constexpr uint32_t kNone = 0xffffffffu;
-constexpr int kMaxS = 64;                     // cells per lane; band_width <= 32 * kMaxS
 
 // Side flags.
 constexpr uint32_t kFlagPool = 1;    // the traceback pool ran out: rerun with a larger one
@@ -114,19 +119,6 @@ __device__ __forceinline__ uint64_t swap_pairs(uint64_t x) {
     return ((x >> 1) & 0x5555555555555555ull) | ((x & 0x5555555555555555ull) << 1);
 }
 
-// Codes (2 bits each, two words) and valid bits of the 64 positions from
-// global position gp.
-__device__ __forceinline__ void load_window64(const SeqView& S, uint64_t gp, uint64_t& c_lo, uint64_t& c_hi,
-                                              uint64_t& v) {
-    const uint64_t w = gp >> 5;
-    const uint32_t s = (uint32_t)(gp & 31);
-    const uint64_t a = __ldg(S.codes + w), b = __ldg(S.codes + w + 1), c = __ldg(S.codes + w + 2);
-    c_lo = s ? ((a >> (2 * s)) | (b << (64 - 2 * s))) : a;
-    c_hi = s ? ((b >> (2 * s)) | (c << (64 - 2 * s))) : b;
-    const uint32_t va = __ldg(S.valid + w), vb = __ldg(S.valid + w + 1), vc = __ldg(S.valid + w + 2);
-    v = (uint64_t)__funnelshift_r(va, vb, s) | ((uint64_t)__funnelshift_r(vb, vc, s) << 32);
-}
-
 __device__ __forceinline__ uint32_t code_at(const SeqView& S, uint64_t gp) {
     return (uint32_t)(__ldg(S.codes + (gp >> 5)) >> (2 * (gp & 31))) & 3u;
 }
@@ -150,29 +142,37 @@ __device__ __forceinline__ void best_reduce(int32_t& v, int32_t& pc, uint32_t& s
     }
 }
 
-// One side of one anchor per warp, tasks claimed from a cursor.  S = cells per lane.
-template <int S>
-__global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
-    static_assert(S % 8 == 0 && S >= 8 && S <= kMaxS, "cells per lane");
+// One side of one anchor per block of W warps, tasks claimed from a cursor.
+// Thread k of the block owns cells [8k, 8k + 8) of the row (band_width <= 256 W).
+template <int W>
+__global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
+    constexpr int S = kCells;
+    constexpr int NT = W * 32;        // threads (and lanes of the row) per block
+    constexpr int kRowWords = NT;     // one back-pointer word (8 cells) per thread and row
     extern __shared__ int32_t g_sm[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int32_t* sH = g_sm + wid * (S * 32 * 2);
-    int32_t* sNX = sH + S * 32;
-    uint8_t* sST = reinterpret_cast<uint8_t*>(g_sm + kGapWarps * S * 32 * 2) + wid * S * 32;
+    int32_t* sH = g_sm;                       // the row: best state H
+    int32_t* sNX = sH + NT * S;               // the next row's X
+    uint8_t* sST = reinterpret_cast<uint8_t*>(sNX + NT * S);   // H's state | next X's source << 2
+    __shared__ int32_t s_wA[W];               // each warp's composed row function
+    __shared__ int32_t s_wM[W];               // M of each warp's last cell
+    __shared__ int32_t s_bv[W], s_bp[W], s_first[W], s_last[W];
+    __shared__ uint32_t s_bs[W];
+    __shared__ unsigned long long s_task;
+    __shared__ uint32_t s_blk, s_head;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int32_t goe = a.goe, ge = a.ge;
     // X of a cell whose upper neighbour is dead or outside the band.
     const int32_t nx_dead = max(kNegInf - goe, kNegInf - ge);
     const uint32_t nx_dead_from = (kNegInf - goe >= kNegInf - ge) ? 0u : 1u;
     const uint64_t ntasks = a.list ? a.n_list : 2ull * a.n_anchors;
-    const int32_t lane_shift = S * ge;   // Y decays by this over one lane's cells
-    constexpr int kWordsPerLane = S / 8;
-    constexpr int kRowWords = 32 * kWordsPerLane;
-    // This warp's chain of traceback blocks (kept across tasks).
+    const int32_t lane_shift = S * ge;        // Y decays by this over one thread's cells
+    // This block's chain of traceback blocks (kept across tasks; thread 0's).
     uint32_t chain_head = kNone, chain_len = 0;
     for (;;) {
-        unsigned long long task = 0;
-        if (lane == 0) task = atomicAdd(a.ctr + kCtrTask, 1ull);
-        task = __shfl_sync(kFull, task, 0);
+        if (tid == 0) s_task = atomicAdd(a.ctr + kCtrTask, 1ull);
+        __syncthreads();
+        unsigned long long task = s_task;
+        __syncthreads();
         if (task >= ntasks) break;
         const uint64_t fixed_base = a.list ? a.base[task] : 0;
         if (a.list) task = a.list[task];
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
         const int64_t m = right ? (int64_t)a.Q.len - q0 - 1 : (int64_t)q0;
         GapSide res{};
         if (n == 0 || m == 0) {
-            if (lane == 0) a.sides[task] = res;
+            if (tid == 0) a.sides[task] = res;
             continue;
         }
         const int64_t R = a.radius >= 0 ? a.radius : m + 1;
@@ -197,24 +197,56 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
         int64_t bi = 0, bj = 0;
         uint32_t bst = 0;
         uint32_t flags = 0;
-        // Walk of the chain while filling: the block holding the current row.
-        uint32_t cur_blk = kNone;
-        uint32_t blk_index = 0;        // its position in the chain
+        uint32_t cur_blk = kNone;      // thread 0: the chain block holding the current row
+        uint32_t blk_index = 0;
         if (a.list) chain_len = 0;
         bool store = true;
         uint64_t rows = 0, cells = 0;
-        int64_t i = 0;
-        for (; i <= n; i++) {
+        const int cbase = tid * S;
+        for (int64_t i = 0; i <= n; i++) {
             const int64_t jl = lo > R ? lo - R : 0;
             int64_t jh = min(hi + R, m);
             jh = min(jh, jl + bw - 1);
             const int32_t width = (int32_t)(jh - jl + 1);
-            if (width > 32 * S) {   // cannot happen: the host sizes S from band_width
+            if (width > NT * S) {   // cannot happen: the host sizes W from band_width
                 flags |= kFlagState;
                 break;
             }
             rows++;
             cells += (uint64_t)width;
+            // Thread 0 takes the traceback block of this row (every kRows rows).
+            if (tid == 0 && store && (i % kRows) == 0) {
+                uint32_t nb = kNone;
+                if (a.list) {   // second pass: this side's blocks are consecutive
+                    nb = (uint32_t)(fixed_base + (uint64_t)(i / kRows));
+                    uint32_t* hdr = a.pool + (uint64_t)nb * a.block_words;
+                    hdr[0] = i == 0 ? kNone : nb - 1;
+                    hdr[1] = nb + 1;
+                    if (i == 0) chain_head = nb;
+                } else if (blk_index < chain_len) {
+                    nb = cur_blk == kNone ? chain_head : a.pool[(uint64_t)cur_blk * a.block_words + 1];
+                } else {
+                    const unsigned long long b = atomicAdd(a.ctr + kCtrBlocks, 1ull);
+                    if (b < a.pool_blocks) {
+                        nb = (uint32_t)b;
+                        uint32_t* hdr = a.pool + (uint64_t)nb * a.block_words;
+                        hdr[0] = cur_blk;   // previous block in the chain
+                        hdr[1] = kNone;     // next
+                        if (cur_blk == kNone) {
+                            chain_head = nb;
+                        } else {
+                            a.pool[(uint64_t)cur_blk * a.block_words + 1] = nb;
+                        }
+                        chain_len++;
+                    }
+                }
+                if (nb != kNone) {
+                    a.pool[(uint64_t)nb * a.block_words + 2] = (uint32_t)i;
+                    cur_blk = nb;
+                    blk_index++;
+                }
+                s_blk = nb;
+            }
             // Scores of the row's target base against query codes 0..3.
             int32_t s0 = a.ambig, s1 = a.ambig, s2 = a.ambig, s3 = a.ambig;
             if (i >= 1) {
@@ -227,32 +259,32 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                     s3 = a.sub[tc * 4 + 3];
                 }
             }
-            const int32_t cbase = lane * S;
             const int32_t con = min(max(width - cbase, 0), S);
-            // The lane's query bases, cell c at offset c.
-            uint64_t qlo = 0, qhi = 0, qv = 0;
+            // The thread's query bases, cell c at offset c (2 bits each) and its valid bit.
+            uint64_t qc64 = 0;
+            uint32_t qv = 0;
             if (con > 0 && i >= 1) {
                 if (right) {
-                    load_window64(a.Q, a.Q.base + (uint64_t)((int64_t)q0 + jl + cbase), qlo, qhi, qv);
+                    load_window32(a.Q, a.Q.base + (uint64_t)((int64_t)q0 + jl + cbase), qc64, qv);
                 } else {
-                    uint64_t l0, h0, v0;
-                    load_window64(a.Q, (uint64_t)((int64_t)a.Q.base + (int64_t)q0 - jl - cbase - 63), l0, h0, v0);
-                    qlo = swap_pairs(__brevll(h0));
-                    qhi = swap_pairs(__brevll(l0));
-                    qv = __brevll(v0);
+                    uint64_t c0;
+                    uint32_t v0;
+                    load_window32(a.Q, (uint64_t)((int64_t)a.Q.base + (int64_t)q0 - jl - cbase - 31), c0, v0);
+                    qc64 = swap_pairs(__brevll(c0));
+                    qv = __brev(v0);
                 }
             }
-            // ---- phase A: X and M of the lane's cells from the previous row.
+            const bool col0 = (jl == 0) && tid == 0;   // this thread's cell 0 is column 0
+            const int32_t d = (int32_t)(jl - pjl);      // previous-frame index of this row's cell 0
+            // ---- phase A: X and M of the thread's cells from the previous row.
             int32_t Mr[S], Xr[S];
-            uint32_t tb[kWordsPerLane];
-#pragma unroll
-            for (int k = 0; k < kWordsPerLane; k++) tb[k] = 0;
+            uint32_t tb = 0;
             int32_t hm1 = kNegInf;   // H of the previous row's cell left of the current one (killed: NEG_INF)
             uint32_t sm1 = 0;
-            {
-                const int32_t p = (int32_t)(jl + cbase - pjl) - 1;
-                if (i >= 1 && p >= 0 && p < pw) {
-                    const int ad = (p % S) * 32 + p / S;
+            if (i >= 1) {
+                const int32_t p = d + cbase - 1;
+                if (p >= 0 && p < pw) {
+                    const int ad = (p & (S - 1)) * NT + (p >> 3);
                     const int32_t h = sH[ad];
                     if (h >= thr_prev) {
                         hm1 = h;
@@ -260,16 +292,15 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                     }
                 }
             }
-            int32_t yl = kLow;   // Y of the lane's cells without what enters from the left
+            int32_t yl = kLow;   // Y of the thread's cells without what enters from the left
 #pragma unroll
             for (int c = 0; c < S; c++) {
-                const int64_t j = jl + cbase + c;
                 const bool on = c < con;
-                const int32_t p = (int32_t)(j - pjl);
+                const int32_t p = d + cbase + c;
                 int32_t hp = kNegInf, nxp = nx_dead;
                 uint32_t stp = 0, nxf = nx_dead_from;
                 if (i >= 1 && on && p >= 0 && p < pw) {
-                    const int ad = (p % S) * 32 + p / S;
+                    const int ad = (p & (S - 1)) * NT + (p >> 3);
                     const int32_t h = sH[ad];
                     if (h >= thr_prev) {
                         const uint32_t st = sST[ad];
@@ -283,15 +314,14 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                 uint32_t mf = 0, xf = 0;
                 if (i == 0) {
                     X = kNegInf;
-                    M = j == 0 ? 0 : kNegInf;
+                    M = (c == 0 && col0) ? 0 : kNegInf;
                 } else {
                     X = nxp;
                     xf = nxf;
-                    if (j == 0) {
+                    if (c == 0 && col0) {
                         M = kNegInf;
                     } else {
-                        const uint32_t qc =
-                            (uint32_t)((c < 32 ? (qlo >> (2 * c)) : (qhi >> (2 * (c & 31)))) & 3u);
+                        const uint32_t qc = (uint32_t)(qc64 >> (2 * c)) & 3u;
                         const bool qvb = (qv >> c) & 1u;
                         const int32_t s =
                             qvb ? ((qc & 2) ? ((qc & 1) ? s3 : s2) : ((qc & 1) ? s1 : s0)) : a.ambig;
@@ -305,45 +335,53 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                 }
                 Mr[c] = M;
                 Xr[c] = X;
-                tb[c >> 3] |= (mf | (xf << 2)) << (4 * (c & 7));
+                tb |= (mf | (xf << 2)) << (4 * c);
                 hm1 = hp;
                 sm1 = stp;
                 if (c + 1 < S) yl = max(max(M - goe, yl - ge), kLow);
             }
-            // What the lane passes on: Y entering the cell after its last.
+            // What the thread passes on: Y entering the cell after its last.
             int32_t A = max(max(Mr[S - 1] - goe, yl - ge), kLow);
-            const int32_t yl_last = yl;
-            __syncwarp();
-            // ---- the row scan: compose x -> max(a_k, x - S*E) over the lanes.
+            // ---- the row scan: compose x -> max(a_k, x - S*E) over the threads.
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int32_t Ap = __shfl_up_sync(kFull, A, o);
                 if (lane >= o) A = max(A, max(Ap - o * lane_shift, kLow));
             }
-            // Y of the row's first cell: NEG_INF when it is column 0 (no Y
-            // there), else what NEG_INF neighbours give.
-            const int32_t T0 = jl == 0 ? kNegInf : max(kNegInf - goe, kNegInf - ge);
-            const int32_t tout = max(A, max(T0 - (lane + 1) * lane_shift, kLow));
-            int32_t tin = __shfl_up_sync(kFull, tout, 1);
-            if (lane == 0) tin = T0;
-            const int32_t ylast = max(yl_last, max(tin - (S - 1) * ge, kLow));
-            int32_t mleft = __shfl_up_sync(kFull, Mr[S - 1], 1);
-            int32_t yleft = __shfl_up_sync(kFull, ylast, 1);
-            if (lane == 0) {
-                mleft = kNegInf;
-                yleft = kNegInf;
+            if (lane == 31) {
+                s_wA[wid] = A;
+                s_wM[wid] = Mr[S - 1];
             }
+            __syncthreads();   // every thread's reads of the previous row are done
+            // Y of the row's first cell: NEG_INF when it is column 0 (no Y
+            // there), else what NEG_INF neighbours give; then across the
+            // warps before this one.
+            int32_t Tw = jl == 0 ? kNegInf : max(kNegInf - goe, kNegInf - ge);
+            for (int v = 0; v < wid; v++) Tw = max(s_wA[v], max(Tw - 32 * lane_shift, kLow));
+            const int32_t tout = max(A, max(Tw - (lane + 1) * lane_shift, kLow));
+            int32_t tin = __shfl_up_sync(kFull, tout, 1);
+            int32_t mleft = __shfl_up_sync(kFull, Mr[S - 1], 1);
+            if (lane == 0) {
+                tin = Tw;
+                mleft = wid == 0 ? kNegInf : s_wM[wid - 1];
+            }
+            const uint32_t blk = store ? s_blk : kNone;
             // ---- phase B: Y, the cell's best state, the next row's X, the best.
             int32_t lbest = INT32_MIN, lpc = INT32_MAX;
             uint32_t lst = 0;
+            int32_t yleft = 0;
 #pragma unroll
             for (int c = 0; c < S; c++) {
-                const int64_t j = jl + cbase + c;
                 const bool on = c < con;
                 int32_t Y;
                 uint32_t yf = 0;
-                if (j == 0) {
+                if (c == 0 && col0) {
                     Y = kNegInf;
+                } else if (c == 0) {
+                    // Y = max(M_left - (O+E), Y_left - E), formed by the scan;
+                    // its source is M exactly when the M term reaches it.
+                    Y = tin;
+                    yf = (tin == mleft - goe) ? 0u : 1u;
                 } else {
                     const int32_t fm = mleft - goe, fy = yleft - ge;
                     Y = fm >= fy ? fm : fy;
@@ -358,7 +396,7 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                 const int32_t NX = fm >= fx ? fm : fx;
                 const uint32_t nxf = fm >= fx ? 0u : 1u;
                 if (on) {
-                    const int ad = c * 32 + lane;
+                    const int ad = c * NT + tid;
                     sH[ad] = H;
                     sNX[ad] = NX;
                     sST[ad] = (uint8_t)(hs | (nxf << 2));
@@ -368,68 +406,43 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                         lst = hs;
                     }
                 }
-                tb[c >> 3] |= (yf << 3) << (4 * (c & 7));
+                tb |= (yf << 3) << (4 * c);
                 Xr[c] = on ? H : kLow;   // H from here on
             }
-            // ---- back-pointers of the row.
-            if (store && (i % kRows) == 0) {
-                // Next block of the chain, claimed from the pool when the chain ends here.
-                uint32_t nb = kNone;
-                if (lane == 0 && a.list) {
-                    // Second pass: this side's blocks are consecutive.
-                    nb = (uint32_t)(fixed_base + (uint64_t)(i / kRows));
-                    uint32_t* hdr = a.pool + (uint64_t)nb * a.block_words;
-                    hdr[0] = i == 0 ? kNone : nb - 1;
-                    hdr[1] = nb + 1;
-                    hdr[2] = (uint32_t)i;
-                    if (i == 0) chain_head = nb;
-                } else if (lane == 0) {
-                    if (blk_index < chain_len) {
-                        nb = cur_blk == kNone ? chain_head : a.pool[(uint64_t)cur_blk * a.block_words + 1];
-                    } else {
-                        const unsigned long long b = atomicAdd(a.ctr + kCtrBlocks, 1ull);
-                        if (b < a.pool_blocks) {
-                            nb = (uint32_t)b;
-                            uint32_t* hdr = a.pool + (uint64_t)nb * a.block_words;
-                            hdr[0] = cur_blk;   // previous block in the chain
-                            hdr[1] = kNone;     // next
-                            if (cur_blk == kNone) {
-                                chain_head = nb;
-                            } else {
-                                a.pool[(uint64_t)cur_blk * a.block_words + 1] = nb;
-                            }
-                            chain_len++;
-                        }
-                    }
-                    if (nb != kNone) a.pool[(uint64_t)nb * a.block_words + 2] = (uint32_t)i;
-                }
-                nb = __shfl_sync(kFull, nb, 0);
-                chain_head = __shfl_sync(kFull, chain_head, 0);
-                chain_len = __shfl_sync(kFull, chain_len, 0);
-                if (nb == kNone) {
-                    store = false;
-                    flags |= kFlagPool;   // the DP goes on: score, best cell and rows stay exact
-                } else {
-                    cur_blk = nb;
-                    blk_index++;
-                }
-            }
-            if (store) {
-                uint32_t* blk = a.pool + (uint64_t)cur_blk * a.block_words;
+            // ---- back-pointers of the row: one word (8 cells) per thread.
+            if (blk != kNone) {
+                uint32_t* bp = a.pool + (uint64_t)blk * a.block_words;
                 const int r = (int)(i % kRows);
-                if (lane == 0) blk[kHdr + r] = (uint32_t)jl;
-                uint32_t* row = blk + kHdr + kRows + (uint64_t)r * kRowWords + lane * kWordsPerLane;
-#pragma unroll
-                for (int k = 0; k < kWordsPerLane; k++)
-                    if (k * 8 < con) row[k] = tb[k];
+                if (tid == 0) bp[kHdr + r] = (uint32_t)jl;
+                if (con > 0) bp[kHdr + kRows + (uint64_t)r * kRowWords + tid] = tb;
+            } else if (store) {
+                store = false;
+                flags |= kFlagPool;   // the DP goes on: score, best cell and rows stay exact
             }
             // ---- the row's best, the threshold and the surviving cells.
             best_reduce(lbest, lpc, lst);
-            if (lbest > best) {
-                best = lbest;
+            if (lane == 0) {
+                s_bv[wid] = lbest;
+                s_bp[wid] = lpc;
+                s_bs[wid] = lst;
+            }
+            // The threshold needs the row's best: the surviving cells are
+            // found against the best of the rows so far and this row's best.
+            __syncthreads();
+            int32_t rv = s_bv[0], rp = s_bp[0];
+            uint32_t rs = s_bs[0];
+            for (int v = 1; v < W; v++) {
+                if (s_bv[v] > rv) {   // warps in cell order: the first maximum stays on ties
+                    rv = s_bv[v];
+                    rp = s_bp[v];
+                    rs = s_bs[v];
+                }
+            }
+            if (rv > best) {
+                best = rv;
                 bi = i;
-                bj = jl + lpc;
-                bst = lst;
+                bj = jl + rp;
+                bst = rs;
             }
             const int32_t thr = sat_sub32(best, a.ydrop);
             int32_t first = INT32_MAX, last = -1;
@@ -445,7 +458,17 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
                 first = min(first, __shfl_xor_sync(kFull, first, o));
                 last = max(last, __shfl_xor_sync(kFull, last, o));
             }
-            __syncwarp();
+            if (lane == 0) {
+                s_first[wid] = first;
+                s_last[wid] = last;
+            }
+            __syncthreads();
+            first = s_first[0];
+            last = s_last[0];
+            for (int v = 1; v < W; v++) {
+                first = min(first, s_first[v]);
+                last = max(last, s_last[v]);
+            }
             if (last < 0) break;   // the whole row is dead
             lo = jl + first;
             hi = jl + last;
@@ -457,100 +480,99 @@ __global__ void __launch_bounds__(kGapWarps * 32) k_gapped_sides(GapArgs a) {
         res.t_span = (uint32_t)bi;
         res.q_span = (uint32_t)bj;
         if (!store) flags |= kFlagPool;
+        if (tid == 0) s_head = chain_head;
+        __syncthreads();   // back-pointer rows written by every thread are visible to thread 0
         // ---- traceback from the best cell (src/gapped_extend.rs:404-437),
-        // runs written in walk order (tip to root).
-        if (lane == 0 && !(flags & (kFlagPool | kFlagState))) {
-            const uint64_t cap = (uint64_t)(bi + bj);
-            uint64_t off = 0;
-            if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
-            if (a.list) flags |= kSideRuns2;
-            if (off + cap > a.runs_cap) {
-                flags |= kFlagRuns;
-            } else {
-                // The block of row bi: the chain's blocks hold rows in order.
-                uint32_t blk = chain_head;
-                for (int64_t k = 0; k < bi / kRows; k++) blk = a.pool[(uint64_t)blk * a.block_words + 1];
-                int64_t ti = bi, tj = bj;
-                uint32_t st = bst;
-                uint32_t op = 3, cnt = 0, nr = 0;
-                for (uint64_t step = 0; ti > 0 || tj > 0; step++) {
-                    if (step >= cap) {   // every step lowers ti + tj
-                        flags |= kFlagState;
-                        break;
-                    }
-                    const uint32_t* bp = a.pool + (uint64_t)blk * a.block_words;
-                    while (ti < (int64_t)bp[2] && bp[0] != kNone) {   // rows before this block: step back
-                        blk = bp[0];
-                        bp = a.pool + (uint64_t)blk * a.block_words;
-                    }
-                    if (ti < (int64_t)bp[2]) {
-                        flags |= kFlagState;
-                        break;
-                    }
-                    const int r = (int)(ti - (int64_t)bp[2]);
-                    const int64_t p = tj - (int64_t)bp[kHdr + r];
-                    if (p < 0 || p >= 32 * S) {
-                        flags |= kFlagState;
-                        break;
-                    }
-                    const uint32_t nib =
-                        (bp[kHdr + kRows + (uint64_t)r * kRowWords + (p >> 3)] >> (4 * (p & 7))) & 15u;
-                    uint32_t eop;
-                    if (st == 0) {   // M: both advance
-                        if (ti == 0 || tj == 0) {
+        // runs written in walk order (tip to root), by thread 0.
+        if (tid == 0) {
+            if (!(flags & (kFlagPool | kFlagState))) {
+                const uint64_t cap = (uint64_t)(bi + bj);
+                uint64_t off = 0;
+                if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
+                if (a.list) flags |= kSideRuns2;
+                if (off + cap > a.runs_cap) {
+                    flags |= kFlagRuns;
+                } else {
+                    // The block of row bi: the chain's blocks hold rows in order.
+                    uint32_t blk = s_head;
+                    for (int64_t k = 0; k < bi / kRows; k++) blk = a.pool[(uint64_t)blk * a.block_words + 1];
+                    int64_t ti = bi, tj = bj;
+                    uint32_t st = bst;
+                    uint32_t op = 3, cnt = 0, nr = 0;
+                    for (uint64_t step = 0; ti > 0 || tj > 0; step++) {
+                        if (step >= cap) {   // every step lowers ti + tj
                             flags |= kFlagState;
                             break;
                         }
-                        eop = 0;
-                        st = nib & 3u;
-                        ti--;
-                        tj--;
-                    } else if (st == 1) {   // X: gap in the query (DeleteQuery)
-                        if (ti == 0) {
+                        const uint32_t* bp = a.pool + (uint64_t)blk * a.block_words;
+                        while (ti < (int64_t)bp[2] && bp[0] != kNone) {   // rows before this block: step back
+                            blk = bp[0];
+                            bp = a.pool + (uint64_t)blk * a.block_words;
+                        }
+                        if (ti < (int64_t)bp[2]) {
                             flags |= kFlagState;
                             break;
                         }
-                        eop = 2;
-                        st = ((nib >> 2) & 1u) ? 1u : 0u;
-                        ti--;
-                    } else {   // Y: gap in the target (InsertQuery)
-                        if (tj == 0) {
+                        const int r = (int)(ti - (int64_t)bp[2]);
+                        const int64_t p = tj - (int64_t)bp[kHdr + r];
+                        if (p < 0 || p >= NT * S) {
                             flags |= kFlagState;
                             break;
                         }
-                        eop = 1;
-                        st = ((nib >> 3) & 1u) ? 2u : 0u;
-                        tj--;
+                        const uint32_t nib =
+                            (bp[kHdr + kRows + (uint64_t)r * kRowWords + (p >> 3)] >> (4 * (p & 7))) & 15u;
+                        uint32_t eop;
+                        if (st == 0) {   // M: both advance
+                            if (ti == 0 || tj == 0) {
+                                flags |= kFlagState;
+                                break;
+                            }
+                            eop = 0;
+                            st = nib & 3u;
+                            ti--;
+                            tj--;
+                        } else if (st == 1) {   // X: gap in the query (DeleteQuery)
+                            if (ti == 0) {
+                                flags |= kFlagState;
+                                break;
+                            }
+                            eop = 2;
+                            st = ((nib >> 2) & 1u) ? 1u : 0u;
+                            ti--;
+                        } else {   // Y: gap in the target (InsertQuery)
+                            if (tj == 0) {
+                                flags |= kFlagState;
+                                break;
+                            }
+                            eop = 1;
+                            st = ((nib >> 3) & 1u) ? 2u : 0u;
+                            tj--;
+                        }
+                        if (eop == op) {
+                            cnt++;
+                        } else {
+                            if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                            op = eop;
+                            cnt = 1;
+                        }
                     }
-                    if (eop == op) {
-                        cnt++;
-                    } else {
+                    if (!(flags & kFlagState)) {
+                        if (ti > 0 || tj > 0) flags |= kFlagState;
                         if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
-                        op = eop;
-                        cnt = 1;
                     }
+                    res.run_off = off;
+                    res.n_runs = nr;
                 }
-                if (!(flags & kFlagState)) {
-                    if (ti > 0 || tj > 0) flags |= kFlagState;
-                    if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
-                }
-                res.run_off = off;
-                res.n_runs = nr;
             }
-        }
-        flags = __shfl_sync(kFull, flags, 0);
-        res.run_off = __shfl_sync(kFull, res.run_off, 0);
-        res.n_runs = __shfl_sync(kFull, res.n_runs, 0);
-        res.flags = flags;
-        res.rows = (uint32_t)rows;
-        if (lane == 0) {
+            res.flags = flags;
+            res.rows = (uint32_t)rows;
             a.sides[task] = res;
             atomicAdd(a.ctr + kCtrRows, (unsigned long long)rows);
             atomicAdd(a.ctr + kCtrCells, (unsigned long long)cells);
             atomicMax(a.ctr + kCtrMaxRows, (unsigned long long)rows);
             if (flags) atomicOr(a.ctr + kCtrFlags, (unsigned long long)flags);
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
@@ -609,39 +631,41 @@ __global__ void k_gapped_emit(GapArgs a, const gxy_gapped_aln* alns, const uint3
     }
 }
 
-template <int S>
+template <int W>
+size_t sides_smem() {
+    return (size_t)W * 32 * kCells * 9;
+}
+
+template <int W>
 cudaError_t launch_sides(const GapArgs& a, int sm_count, cudaStream_t st) {
-    const size_t smem = (size_t)kGapWarps * S * 32 * 9;
-    cudaError_t e = cudaFuncSetAttribute(k_gapped_sides<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+    const size_t smem = sides_smem<W>();
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gapped_sides<S>, kGapWarps * 32, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gapped_sides<W>, W * 32, smem);
     if (e != cudaSuccess) return e;
     const int blocks = sm_count * std::max(per_sm, 1);
     count_launch();
-    k_gapped_sides<S><<<blocks, kGapWarps * 32, smem, st>>>(a);
+    k_gapped_sides<W><<<blocks, W * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sides_for(int S, const GapArgs& a, int sm_count, cudaStream_t st) {
-    switch (S) {
-        case 8: return launch_sides<8>(a, sm_count, st);
-        case 16: return launch_sides<16>(a, sm_count, st);
-        case 24: return launch_sides<24>(a, sm_count, st);
-        case 32: return launch_sides<32>(a, sm_count, st);
-        case 40: return launch_sides<40>(a, sm_count, st);
-        case 48: return launch_sides<48>(a, sm_count, st);
-        case 56: return launch_sides<56>(a, sm_count, st);
-        default: return launch_sides<64>(a, sm_count, st);
+cudaError_t launch_sides_for(int W, const GapArgs& a, int sm_count, cudaStream_t st) {
+    switch (W) {
+        case 1: return launch_sides<1>(a, sm_count, st);
+        case 2: return launch_sides<2>(a, sm_count, st);
+        case 3: return launch_sides<3>(a, sm_count, st);
+        case 4: return launch_sides<4>(a, sm_count, st);
+        case 5: return launch_sides<5>(a, sm_count, st);
+        case 6: return launch_sides<6>(a, sm_count, st);
+        case 7: return launch_sides<7>(a, sm_count, st);
+        default: return launch_sides<8>(a, sm_count, st);
     }
 }
 
-// Warps the persistent launch runs at most (the pool is sized per warp).
-int max_warps(int S, int sm_count) {
-    const size_t smem = (size_t)kGapWarps * S * 32 * 9;
-    int per_sm = (int)std::max<size_t>(1, (size_t)(227 * 1024) / smem);
-    per_sm = std::min(per_sm, 16);
-    return sm_count * per_sm * kGapWarps;
+// Blocks the persistent launch runs at most (the first pass's pool is sized per block).
+int max_blocks(int W, int sm_count) {
+    const size_t smem = (size_t)W * 32 * kCells * 9;
+    int per_sm = (int)std::min<size_t>((size_t)(228 * 1024) / (smem + 1024), (size_t)(64 / W));
+    return sm_count * std::max(per_sm, 1);
 }
 
 struct WorkerLease {
@@ -700,9 +724,8 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     }
     // Band width bound over all sides: min(4R + 4, m + 1) with m < lq.
     const int64_t bw_max = radius >= 0 ? std::min<int64_t>(4 * radius + 4, (int64_t)lq) : (int64_t)lq;
-    int S = (int)((bw_max + 31) / 32);
-    S = std::max(8, (S + 7) / 8 * 8);
-    if (S > kMaxS)
+    const int Wd = (int)std::max<int64_t>(1, (bw_max + 32 * kCells - 1) / (32 * kCells));
+    if (Wd > kMaxW)
         return fail(GXY_EUNSUPPORTED, "band wider than 2048 cells (y_drop / gap_extend too large for the device DP)");
     out->n_alns = n;
     out->alns = n ? (gxy_gapped_aln*)calloc(n, sizeof(gxy_gapped_aln)) : nullptr;
@@ -747,22 +770,22 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     uint32_t* d_offs = reinterpret_cast<uint32_t*>(aux + off_offs);
     e = cudaMemcpyAsync(aux + off_t, t_pos, n * 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(aux + off_q, q_pos, n * 4, cudaMemcpyHostToDevice, st);
-    // Pass 1: every side, back-pointers in per-warp chains of pool blocks.
-    // The pool is sized for 64 blocks per warp and grows toward what earlier
+    // Pass 1: every side, back-pointers in per-block chains of pool blocks.
+    // The pool is sized for 64 pool blocks per CUDA block and grows toward what earlier
     // calls needed, within a quarter of the free device memory.
-    A.block_words = (uint32_t)(kHdr + kRows + kRows * 32 * (S / 8));
+    A.block_words = (uint32_t)(kHdr + kRows + kRows * 32 * Wd);
     const uint64_t block_bytes = (uint64_t)A.block_words * 4;
-    const int warps = max_warps(S, ctx->sm_count);
+    const int blocks_max = max_blocks(Wd, ctx->sm_count);
     size_t free_b = 0, total_b = 0;
     uint32_t pool_limit = 0;
     {
         std::lock_guard<std::mutex> g(ctx->mu);
         pool_limit = ctx->tuning.gapped_pool_blocks;
     }
-    uint64_t want_pool = std::max<uint64_t>((uint64_t)warps * 64 * block_bytes, W->gpool_want);
+    uint64_t want_pool = std::max<uint64_t>((uint64_t)blocks_max * 64 * block_bytes, W->gpool_want);
     if (want_pool > W->gpool.bytes) {   // growing: at most a quarter of the free memory
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
-        const uint64_t pool_cap = std::max<uint64_t>((uint64_t)warps * 4 * block_bytes, free_b / 4);
+        const uint64_t pool_cap = std::max<uint64_t>((uint64_t)blocks_max * 4 * block_bytes, free_b / 4);
         want_pool = std::max<uint64_t>(std::min(want_pool, pool_cap), W->gpool.bytes);
     } else {
         want_pool = W->gpool.bytes;
@@ -788,7 +811,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         A.runs_cap = W->gruns.bytes / 4;
         e = cudaMemsetAsync(A.ctr, 0, kCtrWords * 8, st);
         if (e == cudaSuccess) e = cudaEventRecord(e0, st);
-        if (e == cudaSuccess) e = launch_sides_for(S, A, ctx->sm_count, st);
+        if (e == cudaSuccess) e = launch_sides_for(Wd, A, ctx->sm_count, st);
         if (e == cudaSuccess) e = cudaEventRecord(e1, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(ctr, A.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -867,7 +890,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
             if (e == cudaSuccess && first_group) e = cudaMemsetAsync(B.ctr + kCtrRuns, 0, 8, st);
             if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrFlags, 0, 8, st);
             if (e == cudaSuccess) e = cudaEventRecord(e0, st);
-            if (e == cudaSuccess) e = launch_sides_for(S, B, ctx->sm_count, st);
+            if (e == cudaSuccess) e = launch_sides_for(Wd, B, ctx->sm_count, st);
             if (e == cudaSuccess) e = cudaEventRecord(e1, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(c2, B.ctr, sizeof(c2), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -939,7 +962,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         stats->device_ms = ms;
         stats->reruns = reruns;
         stats->second_pass_sides = pass2_sides;
-        stats->band_cells_per_lane = (uint32_t)S;
+        stats->warps_per_side = (uint32_t)Wd;
         stats->max_side_rows = ctr[kCtrMaxRows];
     }
     return GXY_OK;
