@@ -866,7 +866,7 @@ def run_input(args):
     return out
 
 
-def run_gapped(args):
+def run_gapped(args, steps=None, warmup=None):
     """Gapped extension (src/gapped_extend.rs:78-460) of the plain workload's
     top-scoring anchors: the plus-strand HSPs of the 10 Mbp pair, their
     anchors (choose_anchor, window 31), the --anchors highest-scoring ones
@@ -890,10 +890,12 @@ def run_gapped(args):
     order = np.argsort(-hsps["score"], kind="stable")[:args.anchors]
     A = np.ascontiguousarray(anchors[order])
     gp = g.GappedParams()
-    for _ in range(max(1, args.warmup)):
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    for _ in range(max(1, warmup)):
         g.gapped_extend(dT, dQ, A, m, gp, ctx=ctx)
     runs = []
-    for _ in range(max(1, args.steps)):
+    for _ in range(max(1, steps)):
         st = {}
         t0 = time.perf_counter()
         res = g.gapped_extend(dT, dQ, A, m, gp, ctx=ctx, stats=st)
@@ -1052,6 +1054,9 @@ def main():
         # serving trace (served vs serial plain launches, latency quantiles).
         out["batched"] = batched_summary(run_batched(args))
         out["served"] = served_summary(run_served(args))
+        # Gapped extension (src/gapped_extend.rs:78-460) of the workload's top
+        # anchors, checked against the oracle on a sample in the same run.
+        out["gapped"] = run_gapped(args, steps=3, warmup=1)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
