@@ -1002,8 +1002,8 @@ def main():
                     help="default workload: skip the batched and served legs of the line")
     ap.add_argument("--workload", default="plain",
                     choices=["plain", "batched", "served", "chunked", "case", "input", "gapped", "gapped_case"])
-    ap.add_argument("--anchors", type=int, default=1024, help="gapped workload: anchors extended per call")
-    ap.add_argument("--gapped-sample", type=int, default=32, help="gapped workload: anchors the oracle extends")
+    ap.add_argument("--anchors", type=int, default=512, help="gapped workload: anchors extended per call")
+    ap.add_argument("--gapped-sample", type=int, default=16, help="gapped workload: anchors the oracle extends")
     ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
     ap.add_argument("--streams", type=int, default=2, help="served workload: dispatcher streams")
     ap.add_argument("--batch-units", type=int, default=64, help="served workload: units per batch at most")
