@@ -881,6 +881,8 @@ def run_gapped(args, steps=None, warmup=None):
     import oracle as O
     tgt, qry = workload(0)
     ctx = g.Context(0)
+    if args.gapped_cells:
+        ctx.set_tuning(gapped_cells=args.gapped_cells)
     m = g.ScoringMatrix.hoxd70()
     T, Q = g.PackedSeq.from_ascii(tgt), g.PackedSeq.from_ascii(qry)
     dT, dQ = T.to_device(ctx), Q.to_device(ctx)
@@ -936,6 +938,7 @@ def run_gapped(args, steps=None, warmup=None):
         "cells_per_s": round(cells / dev_s, 1), "anchors_per_s": round(len(A) / wall, 1),
         "warps_per_side": st["warps_per_side"], "reruns": st["reruns"],
         "max_side_rows": st["max_side_rows"], "second_pass_sides": st["second_pass_sides"],
+        "cells_per_thread": st["cells_per_thread"],
         "us_per_row_of_longest_side": round(dev_s * 1e6 / max(1, st["max_side_rows"]), 3),
         "cpu_baseline": {"kind": "port", "all_cores": {"cores": host_threads(), "anchors": int(k), "s": round(t_all, 3),
                                                        "cells_per_s": round(cells_all / t_all, 1)},
@@ -956,6 +959,8 @@ def run_gapped_case(args):
     t = synth.iid(rng, args.length, 0.41)
     q = synth.evolve(rng, t.copy(), 0.9, 0.005)
     ctx = g.Context(0)
+    if args.gapped_cells:
+        ctx.set_tuning(gapped_cells=args.gapped_cells)
     m = g.ScoringMatrix.hoxd70()
     dT = g.PackedSeq.from_ascii(t.tobytes()).to_device(ctx)
     dQ = g.PackedSeq.from_ascii(q.tobytes()).to_device(ctx)
@@ -968,6 +973,7 @@ def run_gapped_case(args):
         st = {}
         res = g.gapped_extend(dT, dQ, A, m, g.GappedParams(), ctx=ctx, stats=st)
         out.append({"device_ms": round(st["device_ms"], 3), "rows": st["rows"], "max_side_rows": st["max_side_rows"],
+                    "cells_per_thread": st["cells_per_thread"], "warps_per_side": st["warps_per_side"],
                     "us_per_row_of_longest_side": round(st["device_ms"] * 1e3 / max(1, st["max_side_rows"]), 3),
                     "passed": sum(r is not None for r in res)})
     return {"workload": f"gapped case {args.length} bp", "runs": out}
@@ -1004,6 +1010,7 @@ def main():
                     choices=["plain", "batched", "served", "chunked", "case", "input", "gapped", "gapped_case"])
     ap.add_argument("--anchors", type=int, default=512, help="gapped workload: anchors extended per call")
     ap.add_argument("--gapped-sample", type=int, default=16, help="gapped workload: anchors the oracle extends")
+    ap.add_argument("--gapped-cells", type=int, default=0, help="gapped workloads: DP cells per thread (4 or 8)")
     ap.add_argument("--requests", type=int, default=200, help="served workload: requests in the trace")
     ap.add_argument("--streams", type=int, default=2, help="served workload: dispatcher streams")
     ap.add_argument("--batch-units", type=int, default=64, help="served workload: units per batch at most")

@@ -144,6 +144,7 @@ typedef struct {
     uint32_t gapped_pool_blocks;  /* gapped extension: traceback blocks the first pass may use at most
                                      (0 = no limit: sized by the library); sides that do not fit run
                                      again in an exactly sized second pass */
+    uint32_t gapped_cells;        /* gapped extension: cells of a DP row per thread, 4 or 8 (0 = 8) */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);
@@ -420,6 +421,8 @@ typedef struct {
     uint32_t warps_per_side;       /* warps of the block that runs one side (8 cells of a row a thread) */
     uint64_t max_side_rows;        /* rows of the longest side (sides run in parallel; rows are sequential) */
     uint64_t second_pass_sides;    /* sides run again with exactly sized traceback storage */
+    uint32_t cells_per_thread;     /* cells of a DP row one thread holds (4 or 8) */
+    uint32_t pad_;
 } gxy_gapped_stats;
 
 /* extend (src/gapped_extend.rs:78-132) for n anchors (t_pos[i], q_pos[i]) on

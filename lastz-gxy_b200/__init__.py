@@ -62,10 +62,10 @@ class Context:
 
     def set_tuning(self, screen_warps=0, screen_cap=0, screen_blocks_per_sm=0, walk_warps=0,
                    max_hits_per_pass=0, initial_candidates=0, filter_cap=0, filter_claim=0,
-                   gapped_pool_blocks=0) -> None:
+                   gapped_pool_blocks=0, gapped_cells=0) -> None:
         """Zero leaves a field unchanged; gapped_pool_blocks 0xffffffff lifts its limit."""
         t = _lib.TuningC(screen_warps, screen_cap, screen_blocks_per_sm, walk_warps, max_hits_per_pass,
-                         initial_candidates, filter_cap, filter_claim, gapped_pool_blocks)
+                         initial_candidates, filter_cap, filter_claim, gapped_pool_blocks, gapped_cells)
         check(lib().gxy_ctx_set_tuning(self.h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -75,7 +75,7 @@ class Context:
                 "screen_blocks_per_sm": t.screen_blocks_per_sm, "walk_warps": t.walk_warps,
                 "max_hits_per_pass": t.max_hits_per_pass, "initial_candidates": t.initial_candidates,
                 "filter_cap": t.filter_cap, "filter_claim": t.filter_claim,
-                "gapped_pool_blocks": t.gapped_pool_blocks}
+                "gapped_pool_blocks": t.gapped_pool_blocks, "gapped_cells": t.gapped_cells}
 
     def mark(self, slot: int) -> None:
         """Records CUDA event `slot` on the context's primary stream."""
@@ -694,7 +694,7 @@ def gapped_extend(target: DeviceSeq, query: DeviceSeq, anchors, matrix: ScoringM
     if stats is not None:
         stats.update(rows=st.rows, cells=st.cells, device_ms=st.device_ms, reruns=st.reruns,
                      warps_per_side=st.warps_per_side, max_side_rows=st.max_side_rows,
-                     second_pass_sides=st.second_pass_sides)
+                     second_pass_sides=st.second_pass_sides, cells_per_thread=st.cells_per_thread)
     return out
 
 

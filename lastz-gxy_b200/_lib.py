@@ -66,7 +66,8 @@ class SeqSetC(C.Structure):
 class TuningC(C.Structure):
     _fields_ = [("screen_warps", C.c_uint32), ("screen_cap", C.c_uint32), ("screen_blocks_per_sm", C.c_uint32),
                 ("walk_warps", C.c_uint32), ("max_hits_per_pass", C.c_uint32), ("initial_candidates", C.c_uint32),
-                ("filter_cap", C.c_uint32), ("filter_claim", C.c_uint32), ("gapped_pool_blocks", C.c_uint32)]
+                ("filter_cap", C.c_uint32), ("filter_claim", C.c_uint32), ("gapped_pool_blocks", C.c_uint32),
+                ("gapped_cells", C.c_uint32)]
 
 
 class UnitC(C.Structure):
@@ -125,7 +126,7 @@ class GappedResultC(C.Structure):
 class GappedStatsC(C.Structure):
     _fields_ = [("rows", C.c_uint64), ("cells", C.c_uint64), ("device_ms", C.c_double), ("reruns", C.c_uint32),
                 ("warps_per_side", C.c_uint32), ("max_side_rows", C.c_uint64),
-                ("second_pass_sides", C.c_uint64)]
+                ("second_pass_sides", C.c_uint64), ("cells_per_thread", C.c_uint32), ("pad_", C.c_uint32)]
 
 
 V = C.c_void_p

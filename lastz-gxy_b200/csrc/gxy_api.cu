@@ -375,6 +375,13 @@ gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t) {
     if (t->filter_claim)
         ctx->tuning.filter_claim = t->filter_claim == 1 ? 1u : std::min<uint32_t>(4096, std::max<uint32_t>(32, t->filter_claim));
     if (t->gapped_pool_blocks) ctx->tuning.gapped_pool_blocks = t->gapped_pool_blocks == 0xffffffffu ? 0u : t->gapped_pool_blocks;
+    if (t->gapped_cells) {
+        if (t->gapped_cells != 4 && t->gapped_cells != 8) {
+            set_error("gapped_cells must be 4 or 8");
+            return GXY_EINVAL;
+        }
+        ctx->tuning.gapped_cells = t->gapped_cells;
+    }
     return GXY_OK;
 }
 

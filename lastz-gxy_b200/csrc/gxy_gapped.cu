@@ -52,8 +52,7 @@ namespace {
 
 constexpr int32_t kNegInf = INT32_MIN / 4;   // NEG_INF (src/gapped_extend.rs:44)
 constexpr int32_t kLow = INT32_MIN / 2;      // "no contribution" in the row scan: below every DP value
-constexpr int kCells = 8;                     // cells of a row per thread
-constexpr int kMaxW = 8;                      // warps per side; band_width <= 256 * kMaxW
+constexpr int kMaxCells = 2048;               // band_width at most (cells of a row per block)
 constexpr int kRows = 32;                     // DP rows per traceback block
 constexpr int kHdr = 4;                       // block header words: previous block, next block, first row, -
 constexpr uint32_t kNone = 0xffffffffu;
@@ -143,16 +142,18 @@ __device__ __forceinline__ void best_reduce(int32_t& v, int32_t& pc, uint32_t& s
 }
 
 // One side of one anchor per block of W warps, tasks claimed from a cursor.
-// Thread k of the block owns cells [8k, 8k + 8) of the row (band_width <= 256 W).
-template <int W>
+// Thread k of the block owns cells [S k, S k + S) of the row (band_width <= 32 W S).
+template <int W, int S>
 __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
-    constexpr int S = kCells;
-    constexpr int NT = W * 32;        // threads (and lanes of the row) per block
-    constexpr int kRowWords = NT;     // one back-pointer word (8 cells) per thread and row
+    static_assert(S == 4 || S == 8, "cells per thread");
+    constexpr int NT = W * 32;             // threads per block
+    constexpr int kRowWords = NT * S / 8;  // back-pointer words of a row (4 bits a cell)
     extern __shared__ int32_t g_sm[];
     int32_t* sH = g_sm;                       // the row: best state H
     int32_t* sNX = sH + NT * S;               // the next row's X
     uint8_t* sST = reinterpret_cast<uint8_t*>(sNX + NT * S);   // H's state | next X's source << 2
+    // One pool block staged for the traceback (after the row buffer).
+    uint32_t* sBlk = reinterpret_cast<uint32_t*>(sST + ((NT * S + 15) & ~15));
     __shared__ int32_t s_wA[W];               // each warp's composed row function
     __shared__ int32_t s_wM[W];               // M of each warp's last cell
     __shared__ int32_t s_bv[W], s_bp[W], s_first[W], s_last[W];
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
             if (i >= 1) {
                 const int32_t p = d + cbase - 1;
                 if (p >= 0 && p < pw) {
-                    const int ad = (p & (S - 1)) * NT + (p >> 3);
+                    const int ad = (p & (S - 1)) * NT + p / S;
                     const int32_t h = sH[ad];
                     if (h >= thr_prev) {
                         hm1 = h;
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
                 int32_t hp = kNegInf, nxp = nx_dead;
                 uint32_t stp = 0, nxf = nx_dead_from;
                 if (i >= 1 && on && p >= 0 && p < pw) {
-                    const int ad = (p & (S - 1)) * NT + (p >> 3);
+                    const int ad = (p & (S - 1)) * NT + p / S;
                     const int32_t h = sH[ad];
                     if (h >= thr_prev) {
                         const uint32_t st = sST[ad];
@@ -414,7 +415,13 @@ __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
                 uint32_t* bp = a.pool + (uint64_t)blk * a.block_words;
                 const int r = (int)(i % kRows);
                 if (tid == 0) bp[kHdr + r] = (uint32_t)jl;
-                if (con > 0) bp[kHdr + kRows + (uint64_t)r * kRowWords + tid] = tb;
+                if (con > 0) {
+                    if (S == 8) {
+                        bp[kHdr + kRows + (uint64_t)r * kRowWords + tid] = tb;
+                    } else {
+                        reinterpret_cast<uint16_t*>(bp + kHdr + kRows + (uint64_t)r * kRowWords)[tid] = (uint16_t)tb;
+                    }
+                }
             } else if (store) {
                 store = false;
                 flags |= kFlagPool;   // the DP goes on: score, best cell and rows stay exact
@@ -481,88 +488,104 @@ __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
         res.q_span = (uint32_t)bj;
         if (!store) flags |= kFlagPool;
         if (tid == 0) s_head = chain_head;
-        __syncthreads();   // back-pointer rows written by every thread are visible to thread 0
+        __syncthreads();   // back-pointer rows written by every thread are visible to every thread
         // ---- traceback from the best cell (src/gapped_extend.rs:404-437),
-        // runs written in walk order (tip to root), by thread 0.
+        // runs written in walk order (tip to root).  The block stages one pool
+        // block (32 rows) at a time in shared memory; thread 0 walks it.
+        int64_t ti = bi, tj = bj;
+        uint32_t st = bst, op = 3, cnt = 0, nr = 0;
+        uint64_t off = 0, cap = 0, step = 0;
+        bool walk = false;
         if (tid == 0) {
             if (!(flags & (kFlagPool | kFlagState))) {
-                const uint64_t cap = (uint64_t)(bi + bj);
-                uint64_t off = 0;
+                cap = (uint64_t)(bi + bj);
                 if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
                 if (a.list) flags |= kSideRuns2;
                 if (off + cap > a.runs_cap) {
                     flags |= kFlagRuns;
                 } else {
-                    // The block of row bi: the chain's blocks hold rows in order.
-                    uint32_t blk = s_head;
-                    for (int64_t k = 0; k < bi / kRows; k++) blk = a.pool[(uint64_t)blk * a.block_words + 1];
-                    int64_t ti = bi, tj = bj;
-                    uint32_t st = bst;
-                    uint32_t op = 3, cnt = 0, nr = 0;
-                    for (uint64_t step = 0; ti > 0 || tj > 0; step++) {
-                        if (step >= cap) {   // every step lowers ti + tj
-                            flags |= kFlagState;
-                            break;
-                        }
-                        const uint32_t* bp = a.pool + (uint64_t)blk * a.block_words;
-                        while (ti < (int64_t)bp[2] && bp[0] != kNone) {   // rows before this block: step back
-                            blk = bp[0];
-                            bp = a.pool + (uint64_t)blk * a.block_words;
-                        }
-                        if (ti < (int64_t)bp[2]) {
-                            flags |= kFlagState;
-                            break;
-                        }
-                        const int r = (int)(ti - (int64_t)bp[2]);
-                        const int64_t p = tj - (int64_t)bp[kHdr + r];
-                        if (p < 0 || p >= NT * S) {
-                            flags |= kFlagState;
-                            break;
-                        }
-                        const uint32_t nib =
-                            (bp[kHdr + kRows + (uint64_t)r * kRowWords + (p >> 3)] >> (4 * (p & 7))) & 15u;
-                        uint32_t eop;
-                        if (st == 0) {   // M: both advance
-                            if (ti == 0 || tj == 0) {
-                                flags |= kFlagState;
-                                break;
-                            }
-                            eop = 0;
-                            st = nib & 3u;
-                            ti--;
-                            tj--;
-                        } else if (st == 1) {   // X: gap in the query (DeleteQuery)
-                            if (ti == 0) {
-                                flags |= kFlagState;
-                                break;
-                            }
-                            eop = 2;
-                            st = ((nib >> 2) & 1u) ? 1u : 0u;
-                            ti--;
-                        } else {   // Y: gap in the target (InsertQuery)
-                            if (tj == 0) {
-                                flags |= kFlagState;
-                                break;
-                            }
-                            eop = 1;
-                            st = ((nib >> 3) & 1u) ? 2u : 0u;
-                            tj--;
-                        }
-                        if (eop == op) {
-                            cnt++;
-                        } else {
-                            if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
-                            op = eop;
-                            cnt = 1;
-                        }
-                    }
-                    if (!(flags & kFlagState)) {
-                        if (ti > 0 || tj > 0) flags |= kFlagState;
-                        if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
-                    }
+                    walk = true;
                     res.run_off = off;
-                    res.n_runs = nr;
                 }
+            }
+            // The block of row bi: the chain's blocks hold rows in order.
+            uint32_t blk = s_head;
+            if (walk)
+                for (int64_t k = 0; k < bi / kRows; k++) blk = a.pool[(uint64_t)blk * a.block_words + 1];
+            s_blk = walk && (ti > 0 || tj > 0) ? blk : kNone;
+        }
+        __syncthreads();
+        for (;;) {
+            const uint32_t blk = s_blk;
+            if (blk == kNone) break;
+            const uint32_t* src = a.pool + (uint64_t)blk * a.block_words;
+            for (uint32_t k = tid; k < a.block_words; k += NT) sBlk[k] = src[k];
+            __syncthreads();
+            if (tid == 0) {
+                const int64_t first_row = sBlk[2];
+                uint32_t next = kNone;
+                while (ti > 0 || tj > 0) {
+                    if (step++ >= cap) {   // every step lowers ti + tj
+                        flags |= kFlagState;
+                        break;
+                    }
+                    if (ti < first_row) {   // rows before this block: stage the previous one
+                        step--;
+                        next = sBlk[0];
+                        if (next == kNone) flags |= kFlagState;
+                        break;
+                    }
+                    const int r = (int)(ti - first_row);
+                    const int64_t p = tj - (int64_t)sBlk[kHdr + r];
+                    if (p < 0 || p >= NT * S) {
+                        flags |= kFlagState;
+                        break;
+                    }
+                    const uint32_t nib = (sBlk[kHdr + kRows + r * kRowWords + (int)(p >> 3)] >> (4 * (p & 7))) & 15u;
+                    uint32_t eop;
+                    if (st == 0) {   // M: both advance
+                        if (ti == 0 || tj == 0) {
+                            flags |= kFlagState;
+                            break;
+                        }
+                        eop = 0;
+                        st = nib & 3u;
+                        ti--;
+                        tj--;
+                    } else if (st == 1) {   // X: gap in the query (DeleteQuery)
+                        if (ti == 0) {
+                            flags |= kFlagState;
+                            break;
+                        }
+                        eop = 2;
+                        st = ((nib >> 2) & 1u) ? 1u : 0u;
+                        ti--;
+                    } else {   // Y: gap in the target (InsertQuery)
+                        if (tj == 0) {
+                            flags |= kFlagState;
+                            break;
+                        }
+                        eop = 1;
+                        st = ((nib >> 3) & 1u) ? 2u : 0u;
+                        tj--;
+                    }
+                    if (eop == op) {
+                        cnt++;
+                    } else {
+                        if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                        op = eop;
+                        cnt = 1;
+                    }
+                }
+                s_blk = (flags & kFlagState) ? kNone : next;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            if (walk && !(flags & kFlagState)) {
+                if (ti > 0 || tj > 0) flags |= kFlagState;
+                if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                res.n_runs = nr;
             }
             res.flags = flags;
             res.rows = (uint32_t)rows;
@@ -631,39 +654,63 @@ __global__ void k_gapped_emit(GapArgs a, const gxy_gapped_aln* alns, const uint3
     }
 }
 
-template <int W>
-size_t sides_smem() {
-    return (size_t)W * 32 * kCells * 9;
+// Dynamic shared memory of k_gapped_sides<W, S>: the row (9 bytes a cell)
+// and one staged pool block.
+size_t sides_smem(int W, int S, uint32_t block_words) {
+    const size_t cells = (size_t)W * 32 * S;
+    return cells * 8 + ((cells + 15) & ~(size_t)15) + (size_t)block_words * 4;
 }
 
-template <int W>
+template <int W, int S>
 cudaError_t launch_sides(const GapArgs& a, int sm_count, cudaStream_t st) {
-    const size_t smem = sides_smem<W>();
+    const size_t smem = sides_smem(W, S, a.block_words);
+    cudaError_t e = cudaFuncSetAttribute(k_gapped_sides<W, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gapped_sides<W>, W * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gapped_sides<W, S>, W * 32, smem);
     if (e != cudaSuccess) return e;
     const int blocks = sm_count * std::max(per_sm, 1);
     count_launch();
-    k_gapped_sides<W><<<blocks, W * 32, smem, st>>>(a);
+    k_gapped_sides<W, S><<<blocks, W * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sides_for(int W, const GapArgs& a, int sm_count, cudaStream_t st) {
+cudaError_t launch_sides_for(int W, int S, const GapArgs& a, int sm_count, cudaStream_t st) {
+    if (S == 8) {
+        switch (W) {
+            case 1: return launch_sides<1, 8>(a, sm_count, st);
+            case 2: return launch_sides<2, 8>(a, sm_count, st);
+            case 3: return launch_sides<3, 8>(a, sm_count, st);
+            case 4: return launch_sides<4, 8>(a, sm_count, st);
+            case 5: return launch_sides<5, 8>(a, sm_count, st);
+            case 6: return launch_sides<6, 8>(a, sm_count, st);
+            case 7: return launch_sides<7, 8>(a, sm_count, st);
+            default: return launch_sides<8, 8>(a, sm_count, st);
+        }
+    }
     switch (W) {
-        case 1: return launch_sides<1>(a, sm_count, st);
-        case 2: return launch_sides<2>(a, sm_count, st);
-        case 3: return launch_sides<3>(a, sm_count, st);
-        case 4: return launch_sides<4>(a, sm_count, st);
-        case 5: return launch_sides<5>(a, sm_count, st);
-        case 6: return launch_sides<6>(a, sm_count, st);
-        case 7: return launch_sides<7>(a, sm_count, st);
-        default: return launch_sides<8>(a, sm_count, st);
+        case 1: return launch_sides<1, 4>(a, sm_count, st);
+        case 2: return launch_sides<2, 4>(a, sm_count, st);
+        case 3: return launch_sides<3, 4>(a, sm_count, st);
+        case 4: return launch_sides<4, 4>(a, sm_count, st);
+        case 5: return launch_sides<5, 4>(a, sm_count, st);
+        case 6: return launch_sides<6, 4>(a, sm_count, st);
+        case 7: return launch_sides<7, 4>(a, sm_count, st);
+        case 8: return launch_sides<8, 4>(a, sm_count, st);
+        case 9: return launch_sides<9, 4>(a, sm_count, st);
+        case 10: return launch_sides<10, 4>(a, sm_count, st);
+        case 11: return launch_sides<11, 4>(a, sm_count, st);
+        case 12: return launch_sides<12, 4>(a, sm_count, st);
+        case 13: return launch_sides<13, 4>(a, sm_count, st);
+        case 14: return launch_sides<14, 4>(a, sm_count, st);
+        case 15: return launch_sides<15, 4>(a, sm_count, st);
+        default: return launch_sides<16, 4>(a, sm_count, st);
     }
 }
 
 // Blocks the persistent launch runs at most (the first pass's pool is sized per block).
-int max_blocks(int W, int sm_count) {
-    const size_t smem = (size_t)W * 32 * kCells * 9;
+int max_blocks(int W, int S, uint32_t block_words, int sm_count) {
+    const size_t smem = sides_smem(W, S, block_words);
     int per_sm = (int)std::min<size_t>((size_t)(228 * 1024) / (smem + 1024), (size_t)(64 / W));
     return sm_count * std::max(per_sm, 1);
 }
@@ -724,8 +771,13 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     }
     // Band width bound over all sides: min(4R + 4, m + 1) with m < lq.
     const int64_t bw_max = radius >= 0 ? std::min<int64_t>(4 * radius + 4, (int64_t)lq) : (int64_t)lq;
-    const int Wd = (int)std::max<int64_t>(1, (bw_max + 32 * kCells - 1) / (32 * kCells));
-    if (Wd > kMaxW)
+    int Sc = 8;
+    {
+        std::lock_guard<std::mutex> g(ctx->mu);
+        if (ctx->tuning.gapped_cells == 4) Sc = 4;
+    }
+    const int Wd = (int)std::max<int64_t>(1, (bw_max + 32 * Sc - 1) / (32 * Sc));
+    if (bw_max > kMaxCells)
         return fail(GXY_EUNSUPPORTED, "band wider than 2048 cells (y_drop / gap_extend too large for the device DP)");
     out->n_alns = n;
     out->alns = n ? (gxy_gapped_aln*)calloc(n, sizeof(gxy_gapped_aln)) : nullptr;
@@ -773,9 +825,9 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     // Pass 1: every side, back-pointers in per-block chains of pool blocks.
     // The pool is sized for 64 pool blocks per CUDA block and grows toward what earlier
     // calls needed, within a quarter of the free device memory.
-    A.block_words = (uint32_t)(kHdr + kRows + kRows * 32 * Wd);
+    A.block_words = (uint32_t)(kHdr + kRows + kRows * 32 * Wd * Sc / 8);
     const uint64_t block_bytes = (uint64_t)A.block_words * 4;
-    const int blocks_max = max_blocks(Wd, ctx->sm_count);
+    const int blocks_max = max_blocks(Wd, Sc, A.block_words, ctx->sm_count);
     size_t free_b = 0, total_b = 0;
     uint32_t pool_limit = 0;
     {
@@ -811,7 +863,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         A.runs_cap = W->gruns.bytes / 4;
         e = cudaMemsetAsync(A.ctr, 0, kCtrWords * 8, st);
         if (e == cudaSuccess) e = cudaEventRecord(e0, st);
-        if (e == cudaSuccess) e = launch_sides_for(Wd, A, ctx->sm_count, st);
+        if (e == cudaSuccess) e = launch_sides_for(Wd, Sc, A, ctx->sm_count, st);
         if (e == cudaSuccess) e = cudaEventRecord(e1, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(ctr, A.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -890,7 +942,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
             if (e == cudaSuccess && first_group) e = cudaMemsetAsync(B.ctr + kCtrRuns, 0, 8, st);
             if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrFlags, 0, 8, st);
             if (e == cudaSuccess) e = cudaEventRecord(e0, st);
-            if (e == cudaSuccess) e = launch_sides_for(Wd, B, ctx->sm_count, st);
+            if (e == cudaSuccess) e = launch_sides_for(Wd, Sc, B, ctx->sm_count, st);
             if (e == cudaSuccess) e = cudaEventRecord(e1, st);
             if (e == cudaSuccess) e = cudaMemcpyAsync(c2, B.ctr, sizeof(c2), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -963,6 +1015,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         stats->reruns = reruns;
         stats->second_pass_sides = pass2_sides;
         stats->warps_per_side = (uint32_t)Wd;
+        stats->cells_per_thread = (uint32_t)Sc;
         stats->max_side_rows = ctr[kCtrMaxRows];
     }
     return GXY_OK;

@@ -168,6 +168,24 @@ def test_gapped_long_alignment(gxy, ctx):
     assert max(x[2] for x in g if x) > 20000
 
 
+def test_gapped_four_cells_per_thread(gxy):
+    # The layout with 4 cells of a row per thread (twice the warps per side):
+    # the same results as the oracle on search anchors and on short pairs.
+    c = gxy.Context(0)
+    c.set_tuning(gapped_cells=4)
+    rng = np.random.default_rng(23)
+    t, q = planted(rng, 60000, 14)
+    anchors, _ = search_anchors(gxy, c, t, q)
+    g, w, st = both(gxy, c, t, q, anchors)
+    assert g == w and st["cells_per_thread"] == 4
+    for case in range(6):
+        tt = rand_ascii(rng, int(rng.integers(1, 500)), b"ACGTACGTacgtN")
+        qq = _mutate(rng, tt, int(rng.integers(0, 12)))
+        anchors = [(int(rng.integers(0, len(tt))), int(rng.integers(0, len(qq)))) for _ in range(16)]
+        g, w, _ = both(gxy, c, tt, qq, anchors, thr=-10 ** 6)
+        assert g == w, case
+
+
 def test_gapped_second_pass(gxy):
     # A first pass with room for only a few traceback blocks: the sides that
     # ran out are extended again with exactly sized storage, and every result
