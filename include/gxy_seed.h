@@ -144,7 +144,7 @@ typedef struct {
     uint32_t gapped_pool_blocks;  /* gapped extension: traceback blocks the first pass may use at most
                                      (0 = no limit: sized by the library); sides that do not fit run
                                      again in an exactly sized second pass */
-    uint32_t gapped_cells;        /* gapped extension: cells of a DP row per thread, 4 or 8 (0 = 8) */
+    uint32_t gapped_cells;        /* gapped extension: cells of a DP row per thread, 4 (the default) or 8 */
 } gxy_tuning;
 gxy_status gxy_ctx_set_tuning(gxy_ctx* ctx, const gxy_tuning* t);
 gxy_status gxy_ctx_get_tuning(gxy_ctx* ctx, gxy_tuning* t);

@@ -168,7 +168,7 @@ struct gxy_ctx {
     // Screen column cap 192 (the packed screen's limit): on the 10 Mbp plain
     // launch, longer screening leaves fewer candidates for the walk to
     // re-extend (two searches 4.27 ms, against 4.31 ms at 128 and 4.51 at 64).
-    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 1, 0, 8};
+    gxy_tuning tuning{8, 192, 4, 8, 256u << 20, 0, 96, 1, 0, 4};
     cudaEvent_t marks[16] = {};
 };
 

@@ -8,14 +8,14 @@
 // state is more than y_drop below the best score so far are killed.  These
 // rules (the band, the row-major first maximum, the kill) decide the result,
 // so the device keeps the row order.  One block of W warps runs one side of
-// one anchor (W = band_width / 256 rounded up: 5 for HOXD70's defaults), so
-// a row costs each thread only 8 cells:
+// one anchor, S = 4 (or 8) cells of a row a thread, W = band_width / (32 S)
+// rounded up (10 for HOXD70's defaults at S = 4):
 //
-//  - Thread k owns cells [8k, 8k + 8) of the row.  X and M of a cell need the
+//  - Thread k owns cells [S k, S k + S) of the row.  X and M of a cell need the
 //    previous row only, so a thread forms them for its cells first (phase A).
 //  - Y is a max-plus recurrence along the row, Y[j] = max(M[j-1] - (O+E),
 //    Y[j-1] - E).  Each thread reduces its cells to one affine-max function
-//    x -> max(a, x - 8E); a warp shuffle scan composes them, and each warp
+//    x -> max(a, x - S E); a warp shuffle scan composes them, and each warp
 //    folds in the warps before it through shared memory, giving every thread
 //    the exact Y entering its cells (phase B then runs the recurrence from
 //    there; the entering Y's source is M exactly when the M term reaches it).
@@ -23,16 +23,17 @@
 //    is exact.
 //  - The row lives in shared memory (best state H = max(M, X, Y) with its
 //    argmax, and the next row's X = max(M - (O+E), X - E) with its source),
-//    stored transposed (cell p at (p mod 8) * threads + p / 8), so both the
+//    stored transposed (cell p at (p mod S) * threads + p / S), so both the
 //    current row's writes and the next row's reads, at any shift of the
 //    band, hit distinct banks.  A cell killed by the x-drop rule is not
 //    rewritten: the next row compares its H with the row's threshold and
 //    reads NEG_INF in its place, as the reference's cleared cell reads.
-//  - The three back-pointers of a cell (4 bits; one word per thread and row)
+//  - The three back-pointers of a cell (4 bits; S / 8 words per thread and row)
 //    go to global memory, rows in pool blocks of kRows kept by the CUDA block
 //    across its tasks (a chain it grows from a shared pool as its longest side
-//    needs).  After the last row, thread 0 walks from the best cell to (0, 0)
-//    and writes the runs.  Sides whose rows did not fit the pool run again
+//    needs).  After the last row, the block stages one pool block at a time
+//    in shared memory and thread 0 walks it from the best cell to (0, 0),
+//    writing the runs.  Sides whose rows did not fit the pool run again
 //    with exactly sized storage.
 //
 // A last kernel joins the two sides per anchor: total = anchor column + left
@@ -771,10 +772,10 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     }
     // Band width bound over all sides: min(4R + 4, m + 1) with m < lq.
     const int64_t bw_max = radius >= 0 ? std::min<int64_t>(4 * radius + 4, (int64_t)lq) : (int64_t)lq;
-    int Sc = 8;
+    int Sc = 4;   // 4 cells a thread: 3.1-3.4 us a row at W = 10 against 3.85 us with 8 at W = 5
     {
         std::lock_guard<std::mutex> g(ctx->mu);
-        if (ctx->tuning.gapped_cells == 4) Sc = 4;
+        if (ctx->tuning.gapped_cells == 8) Sc = 8;
     }
     const int Wd = (int)std::max<int64_t>(1, (bw_max + 32 * Sc - 1) / (32 * Sc));
     if (bw_max > kMaxCells)
