@@ -168,16 +168,17 @@ def test_gapped_long_alignment(gxy, ctx):
     assert max(x[2] for x in g if x) > 20000
 
 
-def test_gapped_four_cells_per_thread(gxy):
-    # The layout with 4 cells of a row per thread (twice the warps per side):
-    # the same results as the oracle on search anchors and on short pairs.
+def test_gapped_eight_cells_per_thread(gxy):
+    # The layout with 8 cells of a row per thread (half the warps per side of
+    # the default 4): the same results as the oracle on search anchors and on
+    # short pairs.
     c = gxy.Context(0)
-    c.set_tuning(gapped_cells=4)
+    c.set_tuning(gapped_cells=8)
     rng = np.random.default_rng(23)
     t, q = planted(rng, 60000, 14)
     anchors, _ = search_anchors(gxy, c, t, q)
     g, w, st = both(gxy, c, t, q, anchors)
-    assert g == w and st["cells_per_thread"] == 4
+    assert g == w and st["cells_per_thread"] == 8
     for case in range(6):
         tt = rand_ascii(rng, int(rng.integers(1, 500)), b"ACGTACGTacgtN")
         qq = _mutate(rng, tt, int(rng.integers(0, 12)))
@@ -215,3 +216,30 @@ def test_gapped_rejects(gxy, ctx):
         gxy.gapped_extend(big, big, [(10, 10)], m2, gxy.GappedParams(), ctx=ctx)
     assert e.value.status == 3
     assert gxy.gapped_extend(dT, dT, np.zeros((0, 2), np.uint32), m, gxy.GappedParams(), ctx=ctx) == []
+
+
+def test_gapped_plain_workload_full_size(gxy, ctx):
+    # The 10 Mbp plain workload, plus strand: the 24 highest-scoring anchors
+    # (sides of up to ~280 k rows, long chains of pool blocks) and 24 more
+    # spread over the ranked list, extended in one call and compared with the
+    # oracle run on the host threads.
+    import os
+    from lastz_gxy_b200 import synth
+    pr = synth.c2()
+    t, q = pr.target.tobytes(), pr.query.tobytes()
+    m = gxy.ScoringMatrix.hoxd70()
+    T, Q = gxy.PackedSeq.from_ascii(t), gxy.PackedSeq.from_ascii(q)
+    dT, dQ = T.to_device(ctx), Q.to_device(ctx)
+    tab = gxy.PosTable.build(dT, P12, 1, ctx=ctx)
+    hsps = gxy.search_device(tab, dQ, m, gxy.SearchParams())
+    anchors = gxy.choose_anchors(dT, dQ, hsps, m, 31, ctx)
+    order = np.argsort(-hsps["score"], kind="stable")
+    pick = np.concatenate([order[:24], order[np.linspace(24, len(order) - 1, 24).astype(int)]])
+    A = np.ascontiguousarray(anchors[pick])
+    st = {}
+    got = gxy.gapped_extend(dT, dQ, A, m, gxy.GappedParams(), ctx=ctx, stats=st)
+    OT, OQ = O.pack_ascii(t), O.pack_ascii(q)
+    want = O.gapped_extend_many(OT, OQ, O.params(), O.gapped_params(), A[:, 0], A[:, 1],
+                                threads=max(1, min(16, os.cpu_count() or 1)))
+    assert [gpu_result(x) for x in got] == [orc_result(x) for x in want]
+    assert st["max_side_rows"] > 50_000
