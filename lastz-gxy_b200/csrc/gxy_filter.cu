@@ -49,55 +49,6 @@ __device__ __forceinline__ uint64_t fold_cols(uint64_t x, uint32_t keep, uint64_
     return (x & m) | (pat & ~m);
 }
 
-// The 32-bit word (codes, valid) of target word index i: from the table's
-// interleaved copy when the view has one.
-__device__ __forceinline__ void t_word(const SeqView& T, uint64_t i, uint64_t& c, uint32_t& v) {
-    if (T.ilv) {
-        const uint4 r = __ldg(T.ilv + (i - T.ilv_first));
-        c = ((uint64_t)r.y << 32) | r.x;
-        v = r.z;
-    } else {
-        c = __ldg(T.codes + i);
-        v = __ldg(T.valid + i);
-    }
-}
-
-// The 32 target positions from gp, where (kc, kv) is the word a previous
-// window of the same side already loaded when `have`: the word after gp's
-// first (right side, `next_is_hi`) or gp's first word itself (left side).
-// Returns the window and leaves in (kc, kv) the word the side's next window
-// shares with this one.
-__device__ __forceinline__ void t_window_carry(const SeqView& T, uint64_t gp, bool right, bool have, uint64_t& kc,
-                                               uint32_t& kv, uint64_t& codes, uint32_t& valid) {
-    const uint64_t i = gp >> 5;
-    const uint32_t s = (uint32_t)(gp & 31);
-    uint64_t lo, hi;
-    uint32_t lv, hv;
-    if (right) {   // windows advance by 32: this window's first word is the last window's second
-        if (have) {
-            lo = kc;
-            lv = kv;
-        } else {
-            t_word(T, i, lo, lv);
-        }
-        t_word(T, i + 1, hi, hv);
-        kc = hi;
-        kv = hv;
-    } else {       // windows step back by 32: this window's second word is the last window's first
-        if (have) {
-            hi = kc;
-            hv = kv;
-        } else {
-            t_word(T, i + 1, hi, hv);
-        }
-        t_word(T, i, lo, lv);
-        kc = lo;
-        kv = lv;
-    }
-    codes = s ? ((lo >> (2 * s)) | (hi << (64 - 2 * s))) : lo;
-    valid = __funnelshift_r(lv, hv, s);
-}
-
 struct FSide {
     int32_t run;
     int32_t best;
@@ -198,9 +149,6 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
     uint32_t ht = 0, hq = 0, hu = 0xffffffffu, cur_unit = 0xffffffffu;
     uint32_t rext = 0, lext = 0, rrem = 0, lrem = 0;
     int32_t rrun = 0, rbest = 0, lrun = 0, lbest = 0;
-    // Each side's last target word that its next window shares (valid after a full step).
-    uint64_t rkc = 0, lkc = 0;
-    uint32_t rkv = 0, lkv = 0;
     SeqView T{}, Q{};
     for (;;) {
         const uint32_t im = __ballot_sync(kFull, !busy);
@@ -256,14 +204,11 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
         const uint32_t nr = ralive ? min(32u, rrem) : 0u, nl = lalive ? min(32u, lrem) : 0u;
         uint64_t xr = 0, xl = 0;
         uint32_t vr = kFull, vl = kFull;
-        // A side's windows move by exactly 32 positions while it runs (a
-        // shorter step is its last), so from its second step on, one of the
-        // two target words is the previous window's.
         if (nr) {
             const uint64_t tg = T.base + ht + L + rext, qg = Q.base + hq + L + rext;
             uint64_t tc;
             uint32_t tv;
-            t_window_carry(T, tg, true, rext != 0, rkc, rkv, tc, tv);
+            load_window32(T, tg, tc, tv);
             xr = tc ^ load_codes32(Q.codes, qg);
             vr = tv & load_bits32(Q.valid, qg);
         }
@@ -271,7 +216,7 @@ __global__ __launch_bounds__(NW * 32, 2) void k_filter_hits(const __grid_constan
             const uint64_t tg = T.base + ht - lext - 32, qg = Q.base + hq - lext - 32;
             uint64_t tc;
             uint32_t tv;
-            t_window_carry(T, tg, false, lext != 0, lkc, lkv, tc, tv);
+            load_window32(T, tg, tc, tv);
             xl = rev_pairs64(tc ^ load_codes32(Q.codes, qg));
             vl = __brev(tv & load_bits32(Q.valid, qg));
         }
