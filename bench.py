@@ -74,17 +74,29 @@ def profiled_traffic():
         return None
 
 
-def measured_traffic(tr, kernel: str, raw_hits: float):
-    """(bytes, source) of `kernel` for a launch with raw_hits raw hits: the
-    measured bytes when the capture is of this workload (same raw hits), else
-    the measurement scaled by raw hits and labelled an estimate."""
+def measured_traffic(tr, kernel: str, raw_by_strand):
+    """(bytes, source) of `kernel` per launch, averaged over the strands'
+    launches like the achieved rate: a strand whose launch is the one ncu
+    captured (same raw hits: the plus strand of this workload) takes the
+    measured bytes; any other takes them scaled by its raw hits."""
     if not tr or kernel not in tr.get("kernels", {}):
         return None, None
     k = tr["kernels"][kernel]
     b = k["dram_read_bytes"] + k["dram_write_bytes"]
-    if tr.get("raw_hits") == int(round(raw_hits)):
-        return int(b), f"measured: ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch ({tr['workload']})"
-    return int(b * raw_hits / tr["raw_hits"]), "ESTIMATE: the ncu capture in profiles/kernel_traffic.json scaled by raw hits"
+    vals, exact = [], 0
+    for raw in raw_by_strand:
+        if tr.get("raw_hits") == int(round(raw)):
+            vals.append(b)
+            exact += 1
+        else:
+            vals.append(b * raw / tr["raw_hits"])
+    src = "ncu dram__bytes_read.sum + dram__bytes_write.sum (profiles/kernel_traffic.json)"
+    if exact == len(vals):
+        return int(sum(vals) / len(vals)), f"measured: {src} of this launch ({tr['workload']})"
+    if exact:
+        return int(sum(vals) / len(vals)), (f"mean over the strands' launches: measured for the plus strand ({src}, "
+                                            f"{tr['workload']}), the minus strand's scaled by its raw hits")
+    return int(sum(vals) / len(vals)), f"ESTIMATE: {src} scaled by raw hits"
 
 
 class ClockSampler:
@@ -338,7 +350,8 @@ def run_ours(args, rank: int, world: int, device: int):
         if ms <= 0 or ms_alone <= 0:
             continue   # not timed (a multi-pass launch)
         byt = statistics.mean(fb(s) for s in stats)
-        traffic, tsrc = measured_traffic(tr, name, raw)
+        traffic, tsrc = measured_traffic(tr, name, [statistics.mean(x["raw_hits"] for x in stats[0::2]),
+                                                    statistics.mean(x["raw_hits"] for x in stats[1::2])])
         kern[name] = {"bound": "hbm", "kernel": name, "achieved": round(byt / (ms / 1e3) / 1e9, 1),
                       "peak": peak, "unit": "GB/s", "frac": round(byt / (ms / 1e3) / 1e9 / peak, 4),
                       "traffic": traffic, "traffic_source": tsrc,
