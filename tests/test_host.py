@@ -129,7 +129,9 @@ def test_ctypes_layouts_match_the_header(gxy, tmp_path):
              "gxy_tuning": _lib.TuningC, "gxy_unit": _lib.UnitC, "gxy_batch_result": _lib.BatchResultC,
              "gxy_unit_place": _lib.PlaceC, "gxy_record_result": _lib.RecordResultC,
              "gxy_batch_opts": _lib.BatchOptsC, "gxy_server_opts": _lib.ServerOptsC,
-             "gxy_server_stats": _lib.ServerStatsC}
+             "gxy_server_stats": _lib.ServerStatsC, "gxy_gapped_params": _lib.GappedParamsC,
+             "gxy_gapped_aln": _lib.GappedAlnC, "gxy_gapped_result": _lib.GappedResultC,
+             "gxy_gapped_stats": _lib.GappedStatsC}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gxy_seed.h"', 'int main(void) {']
     for cname, py in pairs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
