@@ -604,7 +604,7 @@ __device__ __forceinline__ const uint32_t* side_runs(const GapArgs& a, const Gap
     return ((s.flags & kSideRuns2) ? a.runs2 : a.runs) + s.run_off;
 }
 
-// Per anchor: the total, the verdict, the joined run count.
+// Per anchor: the total, pass or fail, the joined run count.
 __global__ void k_gapped_join(GapArgs a, int32_t threshold, gxy_gapped_aln* out, uint32_t* counts) {
     const uint32_t an = blockIdx.x * blockDim.x + threadIdx.x;
     if (an >= a.n_anchors) return;
