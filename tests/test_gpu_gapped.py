@@ -168,6 +168,36 @@ def test_gapped_long_alignment(gxy, ctx):
     assert max(x[2] for x in g if x) > 20000
 
 
+@pytest.mark.parametrize("name", ["scaled", "asymmetric"])
+def test_gapped_other_matrices(gxy, ctx, name):
+    # Substitution scores other than HOXD70 (a uniform match/mismatch matrix
+    # and an asymmetric one, each with its own ambiguous score): the column
+    # scores enter M through the same per-row lookup as the defaults.
+    if name == "scaled":
+        sub = [[150 if r == c else -120 for c in range(4)] for r in range(4)]
+        ambig = -80
+    else:
+        sub = [[91, -114, -31, -123], [-100, 100, -125, -31], [-40, -110, 100, -114], [-123, -20, -114, 80]]
+        ambig = -150
+    rng = np.random.default_rng(7 if name == "scaled" else 8)
+    m = gxy.ScoringMatrix.hoxd70()
+    m.sub = [row[:] for row in sub]
+    m.ambig_score = ambig
+    gp = O.gapped_params(400, 30, 3000, -10 ** 6)
+    flat = [x for row in sub for x in row]
+    for case in range(6):
+        t = rand_ascii(rng, int(rng.integers(50, 2000)), b"ACGTACGTacgtN")
+        q = _mutate(rng, t, int(rng.integers(0, 20)))
+        anchors = [(int(rng.integers(0, len(t))), int(rng.integers(0, len(q)))) for _ in range(12)]
+        dT = gxy.PackedSeq.from_ascii(t).to_device(ctx)
+        dQ = gxy.PackedSeq.from_ascii(q).to_device(ctx)
+        got = gxy.gapped_extend(dT, dQ, anchors, m, gxy.GappedParams(3000, -10 ** 6), ctx=ctx)
+        a = np.asarray(anchors, np.int64)
+        want = O.gapped_extend_many(O.pack_ascii(t), O.pack_ascii(q), O.params(sub=flat, ambig=ambig), gp,
+                                    a[:, 0], a[:, 1], threads=4)
+        assert [gpu_result(x) for x in got] == [orc_result(x) for x in want], case
+
+
 def test_gapped_eight_cells_per_thread(gxy):
     # The layout with 8 cells of a row per thread (half the warps per side of
     # the default 4): the same results as the oracle on search anchors and on

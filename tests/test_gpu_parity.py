@@ -339,6 +339,35 @@ def test_entropy_gate(gxy, ctx):
     assert g == o
 
 
+@pytest.mark.parametrize("thr", [500, 1500, 2200, 2600, 3200, 5000])
+def test_entropy_gate_thresholds(gxy, ctx, thr):
+    # The gate (src/entropy.rs:27-67, applied at src/seed_search.rs:102-112)
+    # decides which passing HSPs set the diagonal's cover, so it changes which
+    # later hits are admitted: sequences mixing random stretches with di- and
+    # tri-nucleotide repeats and homopolymer runs (entropies from 0 to 2 bits)
+    # at a sweep of thresholds, in f64 on both sides.
+    rng = np.random.default_rng(40 + thr)
+    parts_t, parts_q = [], []
+    for k in range(24):
+        kind = k % 4
+        if kind == 0:
+            t, q = homologous_pair(rng, 1500, 0.9)
+        else:
+            unit = [b"AT", b"CAG", b"A", b"GC"][int(rng.integers(4))] if kind != 3 else b"ACGTTGCA"
+            t = (unit * (900 // len(unit) + 1))[:900]
+            q = bytearray(t)
+            for i in rng.choice(len(q), 30, replace=False):
+                q[i] = b"ACGT"[rng.integers(4)]
+            q = bytes(q)
+        parts_t.append(t)
+        parts_q.append(q)
+    t, q = b"".join(parts_t), b"".join(parts_q)
+    sp = gxy.SearchParams(1, gxy.HspParams(910, 1500), 1, entropy_threshold=thr)
+    g, o = both(gxy, ctx, t, q, P12, sp)
+    assert g == o
+    assert len(o) > 0
+
+
 def test_max_word_count(gxy, ctx):
     rng = np.random.default_rng(12)
     t, q = homologous_pair(rng, 30000, 0.85)
