@@ -339,7 +339,7 @@ def test_entropy_gate(gxy, ctx):
     assert g == o
 
 
-@pytest.mark.parametrize("thr", [500, 1500, 2200, 2600, 3200, 5000])
+@pytest.mark.parametrize("thr", [500, 2200, 5000])
 def test_entropy_gate_thresholds(gxy, ctx, thr):
     # The gate (src/entropy.rs:27-67, applied at src/seed_search.rs:102-112)
     # decides which passing HSPs set the diagonal's cover, so it changes which
