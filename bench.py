@@ -951,7 +951,7 @@ def run_gapped(args, steps=None, warmup=None):
         "cells_per_s": round(cells / dev_s, 1), "anchors_per_s": round(len(A) / wall, 1),
         "warps_per_side": st["warps_per_side"], "reruns": st["reruns"],
         "max_side_rows": st["max_side_rows"], "second_pass_sides": st["second_pass_sides"],
-        "cells_per_thread": st["cells_per_thread"],
+        "cells_per_thread": st["cells_per_thread"], "second_pass_cells": st["second_pass_cells"],
         "us_per_row_of_longest_side": round(dev_s * 1e6 / max(1, st["max_side_rows"]), 3),
         "cpu_baseline": {"kind": "port", "all_cores": {"cores": host_threads(), "anchors": int(k), "s": round(t_all, 3),
                                                        "cells_per_s": round(cells_all / t_all, 1)},

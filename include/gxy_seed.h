@@ -414,8 +414,8 @@ typedef struct {
 } gxy_gapped_result;
 
 typedef struct {
-    uint64_t rows;                 /* DP rows computed over all sides */
-    uint64_t cells;                /* DP cells computed (the band's width summed over the rows) */
+    uint64_t rows;                 /* DP rows of all sides (each side's DP once) */
+    uint64_t cells;                /* DP cells of all sides (the band's width summed over the rows) */
     double device_ms;              /* CUDA-event time of the DP kernel (last run) */
     uint32_t reruns;               /* first passes repeated after the run buffer had to grow */
     uint32_t warps_per_side;       /* warps of the block that runs one side (8 cells of a row a thread) */
@@ -423,6 +423,7 @@ typedef struct {
     uint64_t second_pass_sides;    /* sides run again with exactly sized traceback storage */
     uint32_t cells_per_thread;     /* cells of a DP row one thread holds (4 or 8) */
     uint32_t pad_;
+    uint64_t second_pass_cells;    /* DP cells computed again by the second pass (not in cells) */
 } gxy_gapped_stats;
 
 /* extend (src/gapped_extend.rs:78-132) for n anchors (t_pos[i], q_pos[i]) on

@@ -694,7 +694,8 @@ def gapped_extend(target: DeviceSeq, query: DeviceSeq, anchors, matrix: ScoringM
     if stats is not None:
         stats.update(rows=st.rows, cells=st.cells, device_ms=st.device_ms, reruns=st.reruns,
                      warps_per_side=st.warps_per_side, max_side_rows=st.max_side_rows,
-                     second_pass_sides=st.second_pass_sides, cells_per_thread=st.cells_per_thread)
+                     second_pass_sides=st.second_pass_sides, cells_per_thread=st.cells_per_thread,
+                     second_pass_cells=st.second_pass_cells)
     return out
 
 

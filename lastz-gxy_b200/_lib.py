@@ -126,7 +126,8 @@ class GappedResultC(C.Structure):
 class GappedStatsC(C.Structure):
     _fields_ = [("rows", C.c_uint64), ("cells", C.c_uint64), ("device_ms", C.c_double), ("reruns", C.c_uint32),
                 ("warps_per_side", C.c_uint32), ("max_side_rows", C.c_uint64),
-                ("second_pass_sides", C.c_uint64), ("cells_per_thread", C.c_uint32), ("pad_", C.c_uint32)]
+                ("second_pass_sides", C.c_uint64), ("cells_per_thread", C.c_uint32), ("pad_", C.c_uint32),
+                ("second_pass_cells", C.c_uint64)]
 
 
 V = C.c_void_p

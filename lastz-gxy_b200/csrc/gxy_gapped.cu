@@ -887,7 +887,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     uint32_t* d_pool2 = nullptr;
     uint32_t* d_runs2 = nullptr;
     void* d_list = nullptr;
-    uint64_t pass2_sides = 0;
+    uint64_t pass2_sides = 0, pass2_cells = 0;
     if (e == cudaSuccess && (ctr[kCtrFlags] & (kFlagPool | kFlagRuns))) {
         std::vector<GapSide> sides(2 * n);
         e = cudaMemcpyAsync(sides.data(), A.sides, 2 * n * sizeof(GapSide), cudaMemcpyDeviceToHost, st);
@@ -958,9 +958,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
             float gms = 0.f;
             if (e == cudaSuccess) cudaEventElapsedTime(&gms, e0, e1);
             ms += gms;
-            ctr[kCtrRows] += c2[kCtrRows];
-            ctr[kCtrCells] += c2[kCtrCells];
-            ctr[kCtrMaxRows] = std::max(ctr[kCtrMaxRows], c2[kCtrMaxRows]);
+            pass2_cells += c2[kCtrCells];
             first_group = false;
             k0 = k1;
         }
@@ -1015,6 +1013,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         stats->device_ms = ms;
         stats->reruns = reruns;
         stats->second_pass_sides = pass2_sides;
+        stats->second_pass_cells = pass2_cells;
         stats->warps_per_side = (uint32_t)Wd;
         stats->cells_per_thread = (uint32_t)Sc;
         stats->max_side_rows = ctr[kCtrMaxRows];
