@@ -941,6 +941,8 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
             // The task cursor restarts; the run counter keeps counting across groups.
             if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrTask, 0, 8, st);
             if (e == cudaSuccess && first_group) e = cudaMemsetAsync(B.ctr + kCtrRuns, 0, 8, st);
+            // Rows and cells count this group's sides only.
+            if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrRows, 0, 16, st);
             if (e == cudaSuccess) e = cudaMemsetAsync(B.ctr + kCtrFlags, 0, 8, st);
             if (e == cudaSuccess) e = cudaEventRecord(e0, st);
             if (e == cudaSuccess) e = launch_sides_for(Wd, Sc, B, ctx->sm_count, st);
