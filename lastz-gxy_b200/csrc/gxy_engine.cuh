@@ -53,7 +53,6 @@ struct Worker {
     DevBuf redo;                  // the two lists of tiles a pass hands to the next one
     DevBuf gpool, gruns, gaux;    // gapped extension: traceback row blocks, side runs, per-anchor arrays
     uint64_t gpool_want = 0;      // gapped extension: the traceback pool an earlier call would have needed
-    uint64_t gruns_want = 0;      // gapped extension: the run words an earlier call's first pass asked for
     cudaGraphExec_t gexec = nullptr;   // the last batched launch's graph, updated in place when it fits
     uint64_t graph_updates = 0;
     uint32_t cand_cap = 0;

@@ -844,9 +844,10 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         want_pool = W->gpool.bytes;
     }
     // Runs: a side reserves best_i + best_j words (its longest possible
-    // script).  A side that finds the run buffer short goes to the second
-    // pass with the pool's, and later calls start from what this one asked for.
-    uint64_t want_runs = std::max<uint64_t>({n * 512, W->gruns.bytes / 4, W->gruns_want});
+    // script); the sides that stored their rows have at most the pool's rows,
+    // and best_j stays within a band of best_i.  A side that finds the run
+    // buffer short goes to the second pass with the pool's.
+    uint64_t want_runs = std::max<uint64_t>({n * 512, W->gruns.bytes / 4, want_pool / block_bytes * kRows * 4});
     cudaEvent_t e0 = W->ev[0], e1 = W->ev[2];
     unsigned long long ctr[kCtrWords] = {};
     uint32_t reruns = 0;
@@ -869,7 +870,6 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         if (e == cudaSuccess) e = cudaMemcpyAsync(ctr, A.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
-    if (e == cudaSuccess && (ctr[kCtrFlags] & kFlagRuns)) W->gruns_want = ctr[kCtrRuns] + ctr[kCtrRuns] / 4;
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
     if (e == cudaSuccess && (ctr[kCtrFlags] & kFlagState)) {
