@@ -417,7 +417,7 @@ typedef struct {
     uint64_t rows;                 /* DP rows of all sides (each side's DP once) */
     uint64_t cells;                /* DP cells of all sides (the band's width summed over the rows) */
     double device_ms;              /* CUDA-event time of the DP kernel (last run) */
-    uint32_t reruns;               /* second-pass launches (groups of sides that fit the memory) */
+    uint32_t reruns;               /* first passes repeated after the run buffer had to grow */
     uint32_t warps_per_side;       /* warps of the block that runs one side (8 cells of a row a thread) */
     uint64_t max_side_rows;        /* rows of the longest side (sides run in parallel; rows are sequential) */
     uint64_t second_pass_sides;    /* sides run again with exactly sized traceback storage */

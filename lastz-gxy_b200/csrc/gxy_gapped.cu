@@ -844,10 +844,8 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         want_pool = W->gpool.bytes;
     }
     // Runs: a side reserves best_i + best_j words (its longest possible
-    // script); the sides that stored their rows have at most the pool's rows,
-    // and best_j stays within a band of best_i.  A side that finds the run
-    // buffer short goes to the second pass with the pool's.
-    uint64_t want_runs = std::max<uint64_t>({n * 512, W->gruns.bytes / 4, want_pool / block_bytes * kRows * 4});
+    // script); the sides that stored their rows have at most the pool's rows.
+    uint64_t want_runs = std::max<uint64_t>({n * 512, W->gruns.bytes / 4, want_pool / block_bytes * kRows * 2});
     cudaEvent_t e0 = W->ev[0], e1 = W->ev[2];
     unsigned long long ctr[kCtrWords] = {};
     uint32_t reruns = 0;
@@ -855,20 +853,27 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     A.base = nullptr;
     A.n_list = 0;
     A.runs2 = nullptr;
-    if (e == cudaSuccess) {
+    for (int attempt = 0; e == cudaSuccess; attempt++) {
         e = W->gpool.ensure(want_pool);
         if (e == cudaSuccess) e = W->gruns.ensure(want_runs * 4);
+        if (e != cudaSuccess) break;
         A.pool = W->gpool.as<uint32_t>();
         A.pool_blocks = W->gpool.bytes / block_bytes;
         if (pool_limit) A.pool_blocks = std::min<uint64_t>(A.pool_blocks, pool_limit);
         A.runs = W->gruns.as<uint32_t>();
         A.runs_cap = W->gruns.bytes / 4;
-        if (e == cudaSuccess) e = cudaMemsetAsync(A.ctr, 0, kCtrWords * 8, st);
+        e = cudaMemsetAsync(A.ctr, 0, kCtrWords * 8, st);
         if (e == cudaSuccess) e = cudaEventRecord(e0, st);
         if (e == cudaSuccess) e = launch_sides_for(Wd, Sc, A, ctx->sm_count, st);
         if (e == cudaSuccess) e = cudaEventRecord(e1, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(ctr, A.ctr, sizeof(ctr), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) break;
+        // Only a short run buffer reruns the whole pass (the pool's shortfall
+        // goes to pass 2): grow it to what the sides reserved.
+        if (!(ctr[kCtrFlags] & kFlagRuns) || attempt >= 2) break;
+        want_runs = std::max<uint64_t>(want_runs * 2, ctr[kCtrRuns] * 5 / 4 + 1024);
+        reruns++;
     }
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
@@ -957,7 +962,6 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
             ms += gms;
             pass2_cells += c2[kCtrCells];
             first_group = false;
-            reruns++;
             k0 = k1;
         }
         A.runs2 = d_runs2;
