@@ -324,7 +324,7 @@ gxy_status gxy_ctx_destroy(gxy_ctx* ctx) {
         dseq_destroy(w->qstage);
         dseq_destroy(w->tstage);
         for (gxy_dseq* d : w->rc_tmp) dseq_destroy(d);
-        DevBuf* tb[] = {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->tocc, &w->gpool, &w->gruns, &w->gaux};
+        DevBuf* tb[] = {&w->tk0, &w->tv0, &w->tk1, &w->tv1, &w->tocc, &w->gpool, &w->gruns, &w->gaux, &w->gscr};
         for (DevBuf* b : tb) b->release();
         for (int i = 0; i < 5; i++)
             if (w->ev[i]) cudaEventDestroy(w->ev[i]);

@@ -148,7 +148,7 @@ Worker* checkout(gxy_ctx* ctx, gxy_status* err) {
                       &w->d_tsegs, &w->d_qsegs, &w->ck0, &w->ck1, &w->cv0, &w->cv1, &w->cands, &w->flags,
                       &w->offsets, &w->ohsp, &w->rhsp, &w->runit, &w->rhsp2, &w->runit2, &w->perm, &w->perm2,
                       &w->hits, &w->surv, &w->redo, &w->rk0, &w->rk1, &w->rv0, &w->rv1, &w->tocc,
-                      &w->gpool, &w->gruns, &w->gaux})
+                      &w->gpool, &w->gruns, &w->gaux, &w->gscr})
         b->st = w->st;
     for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&w->ev[i]);
     w->ps.grid = ctx->sm_count * 2;

@@ -52,6 +52,7 @@ struct Worker {
     uint64_t surv_cap = 0;
     DevBuf redo;                  // the two lists of tiles a pass hands to the next one
     DevBuf gpool, gruns, gaux;    // gapped extension: traceback row blocks, side runs, per-anchor arrays
+    DevBuf gscr;                  // gapped extension: one run scratch per CUDA block of the first pass
     uint64_t gpool_want = 0;      // gapped extension: the traceback pool an earlier call would have needed
     cudaGraphExec_t gexec = nullptr;   // the last batched launch's graph, updated in place when it fits
     uint64_t graph_updates = 0;

@@ -60,8 +60,10 @@ constexpr uint32_t kNone = 0xffffffffu;
 
 // Side flags.
 constexpr uint32_t kFlagPool = 1;    // the traceback pool ran out: rerun with a larger one
-constexpr uint32_t kFlagRuns = 2;    // the run buffer ran out: rerun with a larger one
+constexpr uint32_t kFlagRuns = 2;    // the run buffer ran out: the first pass reruns with a larger one
 constexpr uint32_t kFlagState = 4;   // inconsistent back-pointers (a bug; reported as an error)
+constexpr uint32_t kFlagScratch = 8; // more runs than the block's scratch holds: the second pass
+constexpr uint32_t kScratchWords = 16384;   // first pass: run scratch per CUDA block (64 KB)
 constexpr uint32_t kSideRuns2 = 1u << 8;   // the side's runs are in the second run buffer
 
 // Counters (u64): task cursor, pool blocks claimed, run words reserved, rows,
@@ -103,6 +105,12 @@ struct GapArgs {
     const uint32_t* list;
     const uint64_t* base;
     uint64_t n_list;
+    // First pass: each CUDA block walks its sides' tracebacks into its own
+    // scratch of scratch_words words, then copies the runs out to a range of
+    // exactly their number.  The grid has at most scratch_blocks blocks.
+    uint32_t* scratch;
+    uint32_t scratch_words;
+    uint32_t scratch_blocks;
 };
 
 __device__ __forceinline__ int32_t sat_sub32(int32_t a, int32_t b) {
@@ -493,20 +501,33 @@ __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
         // ---- traceback from the best cell (src/gapped_extend.rs:404-437),
         // runs written in walk order (tip to root).  The block stages one pool
         // block (32 rows) at a time in shared memory; thread 0 walks it.
+        // The first pass walks into the block's scratch and reserves exactly
+        // the runs written; the second pass reserves best_i + best_j words (the
+        // longest possible script) and writes in place.
         int64_t ti = bi, tj = bj;
         uint32_t st = bst, op = 3, cnt = 0, nr = 0;
         uint64_t off = 0, cap = 0, step = 0;
         bool walk = false;
+        uint32_t* wr = nullptr;   // where the walk writes its runs
+        uint64_t wcap = 0;        // and how many it may write there
         if (tid == 0) {
             if (!(flags & (kFlagPool | kFlagState))) {
                 cap = (uint64_t)(bi + bj);
-                if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
-                if (a.list) flags |= kSideRuns2;
-                if (off + cap > a.runs_cap) {
-                    flags |= kFlagRuns;
+                if (a.list) {
+                    if (cap) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)cap);
+                    flags |= kSideRuns2;
+                    if (off + cap > a.runs_cap) {
+                        flags |= kFlagRuns;
+                    } else {
+                        walk = true;
+                        wr = a.runs + off;
+                        wcap = cap;
+                        res.run_off = off;
+                    }
                 } else {
                     walk = true;
-                    res.run_off = off;
+                    wr = a.scratch + (uint64_t)blockIdx.x * a.scratch_words;
+                    wcap = a.scratch_words;
                 }
             }
             // The block of row bi: the chain's blocks hold rows in order.
@@ -573,21 +594,53 @@ __global__ void __launch_bounds__(W * 32) k_gapped_sides(GapArgs a) {
                     if (eop == op) {
                         cnt++;
                     } else {
-                        if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                        if (cnt) {
+                            if (nr >= wcap) {   // more runs than the scratch holds: the second pass
+                                flags |= kFlagScratch;
+                                break;
+                            }
+                            wr[nr++] = (cnt << 2) | op;
+                        }
                         op = eop;
                         cnt = 1;
                     }
                 }
-                s_blk = (flags & kFlagState) ? kNone : next;
+                s_blk = (flags & (kFlagState | kFlagScratch)) ? kNone : next;
             }
             __syncthreads();
         }
         if (tid == 0) {
-            if (walk && !(flags & kFlagState)) {
+            if (walk && !(flags & (kFlagState | kFlagScratch))) {
                 if (ti > 0 || tj > 0) flags |= kFlagState;
-                if (cnt) a.runs[off + nr++] = (cnt << 2) | op;
+                if (cnt) {
+                    if (nr >= wcap) flags |= kFlagScratch;
+                    else wr[nr++] = (cnt << 2) | op;
+                }
                 res.n_runs = nr;
             }
+            // First pass: the runs' range in the run buffer, exactly nr words.
+            s_task = ~0ull;   // no copy
+            if (!a.list && walk && !(flags & (kFlagState | kFlagScratch))) {
+                if (nr) off = atomicAdd(a.ctr + kCtrRuns, (unsigned long long)nr);
+                if (off + nr > a.runs_cap) {
+                    flags |= kFlagRuns;
+                } else {
+                    res.run_off = off;
+                    s_task = ((unsigned long long)nr << 40) | off;
+                }
+            }
+        }
+        __syncthreads();
+        {
+            const unsigned long long cp = s_task;
+            if (cp != ~0ull) {
+                const uint32_t n_cp = (uint32_t)(cp >> 40);
+                const uint64_t o_cp = cp & ((1ull << 40) - 1);
+                const uint32_t* sc = a.scratch + (uint64_t)blockIdx.x * a.scratch_words;
+                for (uint32_t k = tid; k < n_cp; k += NT) a.runs[o_cp + k] = sc[k];
+            }
+        }
+        if (tid == 0) {
             res.flags = flags;
             res.rows = (uint32_t)rows;
             a.sides[task] = res;
@@ -670,7 +723,8 @@ cudaError_t launch_sides(const GapArgs& a, int sm_count, cudaStream_t st) {
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gapped_sides<W, S>, W * 32, smem);
     if (e != cudaSuccess) return e;
-    const int blocks = sm_count * std::max(per_sm, 1);
+    int blocks = sm_count * std::max(per_sm, 1);
+    if (!a.list) blocks = std::min<int>(blocks, (int)a.scratch_blocks);   // one run scratch a block
     count_launch();
     k_gapped_sides<W, S><<<blocks, W * 32, smem, st>>>(a);
     return cudaGetLastError();
@@ -843,9 +897,9 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     } else {
         want_pool = W->gpool.bytes;
     }
-    // Runs: a side reserves best_i + best_j words (its longest possible
-    // script); the sides that stored their rows have at most the pool's rows.
-    uint64_t want_runs = std::max<uint64_t>({n * 512, W->gruns.bytes / 4, want_pool / block_bytes * kRows * 2});
+    // Runs: a first-pass side reserves exactly the runs it wrote (the second
+    // pass reserves best_i + best_j words in a buffer of its own).
+    uint64_t want_runs = std::max<uint64_t>(n * 1024, W->gruns.bytes / 4);
     cudaEvent_t e0 = W->ev[0], e1 = W->ev[2];
     unsigned long long ctr[kCtrWords] = {};
     uint32_t reruns = 0;
@@ -853,6 +907,11 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     A.base = nullptr;
     A.n_list = 0;
     A.runs2 = nullptr;
+    // First pass: a run scratch per resident CUDA block.
+    A.scratch_words = kScratchWords;
+    A.scratch_blocks = (uint32_t)blocks_max;
+    if (e == cudaSuccess) e = W->gscr.ensure((size_t)blocks_max * kScratchWords * 4);
+    A.scratch = W->gscr.as<uint32_t>();
     for (int attempt = 0; e == cudaSuccess; attempt++) {
         e = W->gpool.ensure(want_pool);
         if (e == cudaSuccess) e = W->gruns.ensure(want_runs * 4);
@@ -888,7 +947,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     uint32_t* d_runs2 = nullptr;
     void* d_list = nullptr;
     uint64_t pass2_sides = 0, pass2_cells = 0;
-    if (e == cudaSuccess && (ctr[kCtrFlags] & (kFlagPool | kFlagRuns))) {
+    if (e == cudaSuccess && (ctr[kCtrFlags] & (kFlagPool | kFlagRuns | kFlagScratch))) {
         std::vector<GapSide> sides(2 * n);
         e = cudaMemcpyAsync(sides.data(), A.sides, 2 * n * sizeof(GapSide), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -896,7 +955,7 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
         std::vector<uint64_t> need;
         uint64_t runs2 = 0, max_need = 0, tot_need = 0;
         for (uint64_t k = 0; e == cudaSuccess && k < 2 * n; k++) {
-            if (!(sides[k].flags & (kFlagPool | kFlagRuns))) continue;
+            if (!(sides[k].flags & (kFlagPool | kFlagRuns | kFlagScratch))) continue;
             list.push_back((uint32_t)k);
             const uint64_t nb = ((uint64_t)sides[k].rows + kRows - 1) / kRows;
             need.push_back(nb);
