@@ -800,6 +800,7 @@ typedef struct {
     int32_t score;
     uint32_t t_span, q_span;
     g_script script;   /* root-to-tip, as OneSide.script */
+    uint64_t cells;    /* DP cells computed: the band's width summed over the rows */
 } g_side;
 
 /* extend_one_side (:178-412).  The sliced input of the reference is target
@@ -867,6 +868,7 @@ static int g_one_side(const orc_seq* T, int64_t t0, int64_t n, const orc_seq* Q,
         if (j_hi > m) j_hi = m;
         if (j_hi > j_lo + bw - 1) j_hi = j_lo + bw - 1;
         row_lo[i] = j_lo;
+        out->cells += (uint64_t)(j_hi - j_lo + 1);
         const int64_t lo_this = j_lo;
         const int64_t lo_prev = i >= 1 ? row_lo[i - 1] : 0;
         const int64_t hi_prev_excl = lo_prev + bw;
@@ -1036,6 +1038,7 @@ int orc_gapped_extend(const orc_seq* t, const orc_seq* q, const orc_params* p, c
         }
     }
     out->left_score = left.score;
+    out->cells = left.cells + right.cells;
     out->right_score = right.score;
     free(right.script.runs);
     free(left.script.runs);

@@ -152,6 +152,7 @@ typedef struct {
     uint32_t n_runs;
     uint32_t* runs;   /* malloc'd; free with orc_free */
     int32_t left_score, right_score;
+    uint64_t cells;   /* DP cells of both sides (the bands' widths summed over the rows) */
 } orc_gapped_aln;
 
 /* extend(): 1 = Some (out filled), 0 = None (total below gapped_threshold),

@@ -69,7 +69,7 @@ class OrcGappedParams(C.Structure):
 class OrcGappedAln(C.Structure):
     _fields_ = [("t_start", C.c_uint32), ("q_start", C.c_uint32), ("t_len", C.c_uint32), ("q_len", C.c_uint32),
                 ("score", C.c_int32), ("n_runs", C.c_uint32), ("runs", C.POINTER(C.c_uint32)),
-                ("left_score", C.c_int32), ("right_score", C.c_int32)]
+                ("left_score", C.c_int32), ("right_score", C.c_int32), ("cells", C.c_uint64)]
 
 
 HSP_DTYPE = np.dtype([("t_start", "<u4"), ("q_start", "<u4"), ("length", "<u4"), ("score", "<i4")])
@@ -433,9 +433,11 @@ def gapped_extend(t: Seq, q: Seq, p: OrcParams, gp: OrcGappedParams, t_pos: int,
     return _aln_result(a) if rc == 1 else None
 
 
-def gapped_extend_many(t: Seq, q: Seq, p: OrcParams, gp: OrcGappedParams, t_pos, q_pos, threads: int = 1):
+def gapped_extend_many(t: Seq, q: Seq, p: OrcParams, gp: OrcGappedParams, t_pos, q_pos, threads: int = 1,
+                       cells: list | None = None):
     """extend() for many anchors on `threads` host threads: a list of dicts or
-    None, as gapped_extend."""
+    None, as gapped_extend.  `cells`, when given, receives each anchor's DP
+    cell count (both sides)."""
     tp = np.ascontiguousarray(t_pos, np.uint32)
     qp = np.ascontiguousarray(q_pos, np.uint32)
     n = len(tp)
@@ -446,6 +448,8 @@ def gapped_extend_many(t: Seq, q: Seq, p: OrcParams, gp: OrcGappedParams, t_pos,
     lib().orc_gapped_extend_many(C.byref(t.c()), C.byref(q.c()), C.byref(p), C.byref(gp), tp.ctypes.data,
                                  qp.ctypes.data, n, threads, C.addressof(outs), rc.ctypes.data)
     res = []
+    if cells is not None:
+        cells.extend(int(outs[k].cells) for k in range(n))
     for k in range(n):
         if rc[k] < 0:
             raise MemoryError("orc_gapped_extend") if rc[k] == -1 else ValueError("anchor outside a sequence")

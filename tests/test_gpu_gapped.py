@@ -36,8 +36,10 @@ def both(gxy, ctx, t: bytes, q: bytes, anchors, go=400, ge=30, ydrop=9400, thr=3
     tt = t if view is None else t[view[0]:view[1]]
     OT, OQ = O.pack_ascii(tt), O.pack_ascii(q)
     a = np.asarray(anchors, np.int64).reshape(-1, 2)
+    cells = []
     want = O.gapped_extend_many(OT, OQ, O.params(), O.gapped_params(go, ge, ydrop, thr), a[:, 0], a[:, 1],
-                                threads=threads)
+                                threads=threads, cells=cells)
+    st["oracle_cells"] = sum(cells)
     return [gpu_result(x) for x in got], [orc_result(x) for x in want], st
 
 
@@ -139,6 +141,7 @@ def test_gapped_on_search_anchors(gxy, ctx, seed):
         assert g == w
         assert sum(x is not None for x in g) > 5
         assert st["rows"] > 0 and st["cells"] >= st["rows"]
+        assert st["cells"] == st["oracle_cells"]   # the same bands, row by row
 
 
 def test_gapped_in_a_chunk_view(gxy, ctx):
