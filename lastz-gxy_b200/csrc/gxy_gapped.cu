@@ -899,7 +899,8 @@ gxy_status gxy_gapped_extend(gxy_ctx* ctx, const gxy_dseq* target, uint64_t t_lo
     }
     // Runs: a first-pass side reserves exactly the runs it wrote (the second
     // pass reserves best_i + best_j words in a buffer of its own).
-    uint64_t want_runs = std::max<uint64_t>(n * 1024, W->gruns.bytes / 4);
+    uint64_t want_runs = std::max<uint64_t>(std::max<uint64_t>(n * 512, std::min<uint64_t>(n * 4096, 1ull << 28)),
+                                            W->gruns.bytes / 4);
     cudaEvent_t e0 = W->ev[0], e1 = W->ev[2];
     unsigned long long ctr[kCtrWords] = {};
     uint32_t reruns = 0;
