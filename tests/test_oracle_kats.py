@@ -393,7 +393,7 @@ def test_gapped_many_threads_equals_one():
     assert any(a is not None for a in many)
 
 
-def _py_extend(t: bytes, q: bytes, tp: int, qp: int, go: int, ge: int, ydrop: int, thr: int):
+def _py_extend(t: bytes, q: bytes, tp: int, qp: int, go: int, ge: int, ydrop: int, thr: int, cells_out=None):
     """A second, direct restatement of extend() (src/gapped_extend.rs:78-132,
     :178-460) with the reference's up-front (n+1) x band_width storage, for
     small cases: checks the C oracle's on-demand rows and run merging."""
@@ -404,6 +404,8 @@ def _py_extend(t: bytes, q: bytes, tp: int, qp: int, go: int, ge: int, ydrop: in
 
     def pair(a, b):
         return sub[enc[a]][enc[b]] if a in enc and b in enc else -100
+
+    ncells = [0]
 
     def one_side(T, Q):
         n, m = len(T), len(Q)
@@ -423,6 +425,7 @@ def _py_extend(t: bytes, q: bytes, tp: int, qp: int, go: int, ge: int, ydrop: in
             j_lo = max(lo - radius, 0)
             j_hi = min(hi + radius, m, j_lo + bw - 1)
             row_lo[i] = j_lo
+            ncells[0] += j_hi - j_lo + 1
             lo_prev = row_lo[i - 1] if i >= 1 else 0
             for j in range(j_lo, j_hi + 1):
                 if i == 0 and j == 0:
@@ -483,6 +486,8 @@ def _py_extend(t: bytes, q: bytes, tp: int, qp: int, go: int, ge: int, ydrop: in
     R = one_side(t[tp + 1:], q[qp + 1:])
     L = one_side(t[:tp][::-1], q[:qp][::-1])
     total = pair(t[tp], q[qp]) + L[0] + R[0]
+    if cells_out is not None:
+        cells_out.append(ncells[0])
     if total < thr:
         return None
     ops = L[3][::-1] + [0] + R[3]
@@ -517,7 +522,12 @@ def test_gapped_c_oracle_equals_direct_restatement(go, ge, ydrop):
             q = bytearray(b"A")
         t, q = bytes(t), bytes(q)
         tp, qp = int(rng.integers(0, len(t))), int(rng.integers(0, len(q)))
-        want = _py_extend(t, q, tp, qp, go, ge, ydrop, -10 ** 6)
+        pc = []
+        want = _py_extend(t, q, tp, qp, go, ge, ydrop, -10 ** 6, pc)
         got = O.gapped_extend(O.pack_ascii(t), O.pack_ascii(q), HOX(),
                               O.gapped_params(go, ge, ydrop, -10 ** 6), tp, qp)
         assert got == want, (case, t, q, tp, qp)
+        cc = []
+        O.gapped_extend_many(O.pack_ascii(t), O.pack_ascii(q), HOX(), O.gapped_params(go, ge, ydrop, -10 ** 6),
+                             [tp], [qp], cells=cc)
+        assert cc == pc   # the DP cells: the band widths summed over the rows of both sides
