@@ -10,6 +10,10 @@ pinned by the reference's known-answer tests (tests/test_oracle_kats.py).
 golden_c1.npz   the 30 kbp workload: both strands' full HSP sets + input hashes
 golden_c2.json  the 10 Mbp workload: per strand, HSP count and sha256 of the
                 canonical HSP array (16 bytes per HSP) + input hashes
+golden_gapped.npz  the 30 kbp workload's gapped extension (`python
+                tests/golden/make_golden.py gapped`): the anchor of every
+                plus-strand HSP (choose_anchor, window 31) and the oracle's
+                extend() of each -- coordinates, score and edit-script runs
 golden_scale.json  sampled units of the three large workloads at their full
                 size (`python tests/golden/make_golden.py scale`, ~15 min on 8
                 cores): the uneven batch (the longest contig and 15 more,
@@ -177,8 +181,38 @@ def main():
     print("c2", out["plus"]["n"], out["minus"]["n"], round(time.time() - t0, 2), "s")
 
 
+def gapped(threads=None):
+    """The 30 kbp workload's gapped extension (src/gapped_extend.rs:78-132):
+    every plus-strand HSP's anchor, extended by the oracle with HOXD70's gap
+    costs and GappedParams::default()."""
+    import numpy as np
+    import oracle as O
+    synth = _synth()
+    threads = threads or os.cpu_count() or 4
+    t0 = time.time()
+    pr = synth.c1()
+    t, q = pr.target.tobytes(), pr.query.tobytes()
+    T, Q = O.pack_ascii(t), O.pack_ascii(q)
+    hsps, _ = O.search(O.Table(T, P12, 1), T, Q, O.params())
+    hox = [O.HOXD70[4 * r:4 * r + 4] for r in range(4)]
+    anchors = np.array([O.choose_anchor(h, T, Q, hox, -100, 31) for h in hsps], np.uint32).reshape(-1, 2)
+    res = O.gapped_extend_many(T, Q, O.params(), O.gapped_params(), anchors[:, 0], anchors[:, 1], threads=threads)
+    alns = np.zeros((len(res), 6), np.int64)   # t_start, q_start, t_len, q_len, score, passed
+    runs, offs = [], [0]
+    for k, a in enumerate(res):
+        if a is not None:
+            alns[k] = (a["t_start"], a["q_start"], a["t_len"], a["q_len"], a["score"], 1)
+            runs += a["runs"]
+        offs.append(len(runs))
+    np.savez_compressed(os.path.join(HERE, "golden_gapped.npz"), target_sha=sha(t), query_sha=sha(q),
+                        anchors=anchors, alns=alns, runs=np.array(runs, np.uint32), offsets=np.array(offs, np.int64))
+    print("gapped", len(res), "anchors", sum(a is not None for a in res), "passed", round(time.time() - t0, 1), "s")
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "scale":
         scale()
+    elif len(sys.argv) > 1 and sys.argv[1] == "gapped":
+        gapped()
     else:
         main()

@@ -41,3 +41,22 @@ def test_c2_full_size_golden_hash(gxy, ctx):
     assert hashlib.sha256(minus.tobytes()).hexdigest() == g["minus"]["sha256"]
     assert sp["raw_hits"] == g["plus"]["raw_hits"] and sm["raw_hits"] == g["minus"]["raw_hits"]
     assert sp["windows"] == g["plus"]["windows"]
+
+
+def test_gapped_golden(gxy, ctx):
+    # Every anchor of golden_gapped.npz (the 30 kbp workload's plus-strand
+    # HSPs, choose_anchor window 31) extended on the device in one call.
+    from lastz_gxy_b200 import synth
+    g = np.load(os.path.join(HERE, "golden", "golden_gapped.npz"))
+    pr = synth.c1()
+    dT = gxy.PackedSeq.from_ascii(pr.target.tobytes()).to_device(ctx)
+    dQ = gxy.PackedSeq.from_ascii(pr.query.tobytes()).to_device(ctx)
+    got = gxy.gapped_extend(dT, dQ, g["anchors"], gxy.ScoringMatrix.hoxd70(), gxy.GappedParams(), ctx=ctx)
+    assert len(got) == len(g["anchors"])
+    for k, a in enumerate(got):
+        row = g["alns"][k]
+        if row[5] == 0:
+            assert a is None
+            continue
+        assert (a.t_start, a.q_start, a.t_len, a.q_len, a.score) == tuple(int(x) for x in row[:5])
+        assert [int(x) for x in a.script] == [int(x) for x in g["runs"][g["offsets"][k]:g["offsets"][k + 1]]]
